@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the PowerLLEL_Channel DNS time step on B200.
+
+Metric: grid-points x steps per second of the full time step (RK2 stencils,
+FFT + tridiagonal Poisson projection, bulk forcing, boundary updates and the
+NaN/CFL/divergence checks every nt_check steps) on the Re_tau ~ 550 channel
+768 x 384 x 256 (domain 2pi x pi x 2, tanh stretching 1.8, Re_b = 20000,
+CFL-controlled dt with CFL 0.5), FP64, seeded laminar + noise initial field
+generated on the device.  Every field (613 MB) is larger than the 126 MB L2,
+so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); each GPU runs an independent
+replica of the channel (the single-channel path does not shard), so the
+scaling is weak and no collective touches the data path: the ranks only meet
+in a barrier and in the max-over-ranks reduction of the timed region.
+
+``--impl reference`` times the reference algorithm's CPU path -- the FP64
+oracle restatement in ``oracle/`` (the SYCL/oneMKL reference cannot be built
+on this image) -- on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # Re_tau ~ 550 channel (the headline throughput configuration)
+    "re550": dict(nx=768, ny=384, nz=256, lx=2 * math.pi, ly=math.pi, lz=2.0, stretch_ratio=1.8,
+                  re=10000.0, dt=1e-3, cfl_target=0.5),
+    # Re_tau ~ 180 channel, 128 x 64 x 64 (the reference's CPU-runnable case)
+    "re180": dict(nx=128, ny=64, nz=64, lx=4 * math.pi, ly=2 * math.pi, lz=2.0, stretch_ratio=1.5,
+                  re=2800.0, dt=2e-3, cfl_target=0.0),
+}
+
+# Algorithmic HBM bytes per grid point of each kernel of the fused FP64 step:
+# every distinct array a kernel must read counted once, every array it writes
+# counted once (halos and 1-D coefficients excluded).
+KERNEL_BYTES_PER_POINT = {
+    "rk1+bound(u1)": 48,          # read u,v,w; write u1,v1,w1
+    "rk2+bound(u)": 72,           # read u1,v1,w1,u,v,w; write u,v,w
+    "calcRHS+fft_x_fwd": 32,      # read u,v,w; write spectral array
+    "fft_y_fwd": 16,              # spectral array in place
+    "trid_z": 16,                 # spectral array in place (pivot table excluded)
+    "fft_y_bwd": 16,
+    "fft_x_bwd+bound(p)": 16,     # read spectral array; write p
+    "correct+mean": 56,           # read p,u,v,w; write u,v,w
+    "force+bound(u)": 16,         # read u; write u
+}
+STEP_BYTES_PER_POINT = sum(KERNEL_BYTES_PER_POINT.values())  # 288
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload):
+    """dram read+write bytes per launch of each kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload, {})
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def channel_params(wl, nt_check):
+    from powerllel_channel_sycl_b200 import make_params
+    return make_params(
+        nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], lx=wl["lx"], ly=wl["ly"], lz=wl["lz"],
+        mesh_type=1, stretch_func=0, stretch_ratio=wl["stretch_ratio"], re=wl["re"], u_ref=1.0,
+        l_ref=1.0, dt=wl["dt"], nt_check=nt_check, cfl_limit=1.0, div_limit=1e-9,
+        initial_field="poi", init_with_noise=1, noise_intensity=0.1, is_forced=[1, 0, 0],
+        vel_force=[1.0, 0.0, 0.0], cfl_target=wl["cfl_target"])
+
+
+def cpu_oracle_rate(wl, budget_s: float, max_steps: int, warmup: int):
+    """Oracle (FP64 C++ restatement, OpenMP) on the host cores: pts*steps/s."""
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    case = oracle.Case(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], ly=wl["ly"], lz=wl["lz"],
+                       dt=wl["dt"], re=wl["re"], stretch_ratio=wl["stretch_ratio"])
+    u, v, w = case.init_flow("poi", noise_intensity=0.1)
+    u1, v1, w1, p = case.zeros(), case.zeros(), case.zeros(), case.zeros()
+    _ = case.ps
+    npts = wl["nx"] * wl["ny"] * wl["nz"]
+    t_first = None
+    for _ in range(max(0, warmup)):
+        t0 = time.perf_counter()
+        case.step(u, v, w, u1, v1, w1, p, 1)
+        t_first = time.perf_counter() - t0
+    if t_first is None:
+        t0 = time.perf_counter()
+        case.step(u, v, w, u1, v1, w1, p, 1)
+        t_first = time.perf_counter() - t0
+    nsteps = int(max(1, min(max_steps, budget_s // max(t_first, 1e-9))))
+    t0 = time.perf_counter()
+    case.step(u, v, w, u1, v1, w1, p, nsteps)
+    dt = time.perf_counter() - t0
+    return npts * nsteps / dt, nsteps, threads
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if _cuda_ok() else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def _cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def max_over_ranks(value: float, pg, local: int) -> float:
+    if pg is None:
+        return value
+    import torch
+    dev = torch.device("cuda", local) if _cuda_ok() else torch.device("cpu")
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        if _cuda_ok():
+            pg.barrier(device_ids=[local])
+        else:
+            pg.barrier()
+
+
+def run_reference(args, wl, rank, world, pg):
+    if rank != 0:
+        return None
+    rate, nsteps, threads = cpu_oracle_rate(wl, budget_s=args.ref_budget, max_steps=args.steps,
+                                            warmup=min(args.warmup, 1))
+    npts = wl["nx"] * wl["ny"] * wl["nz"]
+    sample = (f"{nsteps} full FP64 steps (of {args.steps} requested) of the {wl['nx']}x{wl['ny']}x"
+              f"{wl['nz']} channel after {min(args.warmup, 1)} warm-up step(s), oracle restatement "
+              f"of the reference path (the SYCL/oneMKL reference cannot be built here), "
+              f"{threads} OpenMP threads")
+    line = {
+        "impl": "reference",
+        "metric": "grid-pts*steps/s", "value": rate, "unit": "grid-pt*step/s",
+        "n_gpus": world, "steps": nsteps, "warmup": min(args.warmup, 1),
+        "ms_per_step": 1e3 * npts / rate, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, wl),
+        "cpu_baseline": {"value": rate, "unit": "grid-pt*step/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": "grid-pt*step/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    return line
+
+
+def workload_config(args, wl):
+    return {"workload": (f"channel DNS step {wl['nx']}x{wl['ny']}x{wl['nz']}, "
+                         f"Re_b={2 * wl['re']:.0f}, FP64 plain form"
+                         + (f", CFL-controlled dt (CFL {wl['cfl_target']})" if wl["cfl_target"] else
+                            f", dt={wl['dt']}")),
+            "nx": wl["nx"], "ny": wl["ny"], "nz": wl["nz"], "precision": "fp64",
+            "nt_check": args.nt_check, "parallelism": f"replicas x{args.gpus}",
+            "l2": "fields (613 MB each) larger than L2; no flush"
+            if wl["nx"] * wl["ny"] * wl["nz"] > 20_000_000 else "working set partly L2-resident"}
+
+
+def run_ours(args, wl, rank, world, local, pg):
+    import torch  # noqa: F401  (device init; the library owns its stream)
+    from powerllel_channel_sycl_b200 import Channel
+    from powerllel_channel_sycl_b200._lib import lib
+    import ctypes as C
+
+    npts = wl["nx"] * wl["ny"] * wl["nz"]
+    ch = Channel(channel_params(wl, args.nt_check), device=local)
+    ch.initFlow()
+    ch.step(args.warmup)
+    ch.sync()
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    torch.cuda.synchronize(local)
+    with ClockSampler(local) as clk:
+        ms = ch.step_timed(args.steps)
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    ms_max = max_over_ranks(ms, pg, local)
+    value = world * npts * args.steps / (ms_max / 1e3)
+    ok, cfl, div = ch.last_check()
+
+    # per-kernel device times of the same fused kernels (plain launches with
+    # CUDA events between them on the library's stream)
+    prof_steps = max(2, min(5, args.steps))
+    prof = ch.profile_step(prof_steps)
+    total = sum(prof.values())
+    dom = max(prof, key=prof.get)
+    dom_ms = prof[dom] / prof_steps
+    peak, peak_kind = load_peaks()
+    achieved = KERNEL_BYTES_PER_POINT[dom] * npts / (dom_ms / 1e3) / 1e9
+    traffic = load_traffic(args.workload).get(dom)
+    kernels = {k: {"ms": v / prof_steps, "share": v / total,
+                   "gbs": KERNEL_BYTES_PER_POINT[k] * npts / (v / prof_steps / 1e3) / 1e9}
+               for k, v in prof.items()}
+
+    # end to end through the C ABI with host buffers: upload the state from
+    # pinned host memory, K steps each followed by a device->host read of the
+    # step's check values, download the final u, v, w, p
+    nfield = (wl["nx"] + 2) * (wl["ny"] + 2) * (wl["nz"] + 2)
+    L = lib()
+    hbuf = {}
+    for name in ("u", "v", "w", "p"):
+        ptr = C.c_void_p()
+        rc = L.plc_host_alloc(nfield * 8, C.byref(ptr))
+        if rc != 0:
+            raise RuntimeError("plc_host_alloc failed")
+        hbuf[name] = ptr
+    fid = {"u": 0, "v": 1, "w": 2, "p": 6}
+    for name in ("u", "v", "w"):
+        L.plc_download(ch._ctx, fid[name], hbuf[name])
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    for name in ("u", "v", "w"):
+        rc = L.plc_upload(ch._ctx, fid[name], hbuf[name])
+        assert rc == 0
+    for _ in range(args.steps):
+        ch.step(1)
+        ch.check()  # device->host read of the step's NaN/CFL/divergence values
+    for name in ("u", "v", "w", "p"):
+        rc = L.plc_download(ch._ctx, fid[name], hbuf[name])
+        assert rc == 0
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, pg, local)
+    for name in hbuf:
+        L.plc_host_free(hbuf[name])
+    e2e_value = world * npts * args.steps / e2e_s
+    h2d = 3 * nfield * 8 / args.steps
+    d2h = (4 * nfield * 8 + args.steps * 40) / args.steps
+
+    line = {
+        "metric": "grid-pts*steps/s", "value": value, "unit": "grid-pt*step/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, wl),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic,
+                     "bytes_per_point": KERNEL_BYTES_PER_POINT[dom]},
+        "step_roofline": {"bytes_per_point_step": STEP_BYTES_PER_POINT,
+                          "achieved_gbs": STEP_BYTES_PER_POINT * value / world / 1e9,
+                          "frac": STEP_BYTES_PER_POINT * value / world / 1e9 / peak},
+        "kernels": kernels,
+        "e2e": {"value": e2e_value, "unit": "grid-pt*step/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps * ch.kernels_per_step + (args.steps // args.nt_check
+                                                            if args.nt_check else 0),
+        "clocks": clk.summary(),
+        "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0], "dt": ch.dt},
+    }
+    ch.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, nsteps, threads = cpu_oracle_rate(wl, budget_s=args.cpu_budget, max_steps=1,
+                                                warmup=0)
+        line["cpu_baseline"] = {
+            "value": rate, "unit": "grid-pt*step/s", "cores": threads, "kind": "port",
+            "sample": (f"{nsteps} full FP64 step(s) of the same {wl['nx']}x{wl['ny']}x{wl['nz']} "
+                       f"case by the oracle restatement (OpenMP, {threads} threads)")}
+    return line if rank == 0 else None
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawTextHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="re550")
+    ap.add_argument("--nt-check", type=int, default=10)
+    ap.add_argument("--cpu-budget", type=float, default=60.0)
+    ap.add_argument("--ref-budget", type=float, default=120.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    wl = WORKLOADS[args.workload]
+    rank, world, local, pg = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, wl, rank, world, pg)
+        else:
+            line = run_ours(args, wl, rank, world, local, pg)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

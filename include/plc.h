@@ -1,0 +1,279 @@
+/*
+ * plc.h -- C ABI of the B200 (sm_100a) PowerLLEL_Channel DNS time step.
+ *
+ * This is the drop-in boundary for the hot path of xiejb6/PowerLLEL_Channel_SYCL
+ * at p_row = p_col = 1: one entry point per module function of the reference
+ * (src/mod_calcVel.hh, mod_calcRHS.hh, mod_updateBound.hh,
+ * mod_poisson_solver.hh, mod_fft.hh, mod_utils.hh) plus a fused, CUDA-graph
+ * captured time step.  Every function returns PLC_OK (0) or a negative status;
+ * plc_last_error(ctx) gives the message (plc_last_error(NULL) for failures of
+ * plc_create and of the context-free helpers).
+ *
+ * Field layout (same as the reference's _Array3D with one halo cell per side,
+ * src/mod_type.hh:81-306): interior nx*ny*nz, stored as (nx+2)*(ny+2)*(nz+2)
+ * doubles, x fastest; the reference index (i,j,k), 0 <= i <= nx+1, maps to
+ * i + (nx+2)*(j + (ny+2)*k).  The spectral work array of the Poisson solver
+ * (var_xpen of src/mod_poisson_solver.cc:196-198) is nx*ny*nz doubles, x
+ * fastest, no halos, in the reference's packed real-spectrum order.
+ *
+ * Pointers named d_* are DEVICE pointers on the context's GPU; h_* are host
+ * pointers.  Calls are ordered on the context's CUDA stream; functions that
+ * return host values (plc_mean, plc_check, downloads) synchronise it.
+ * A context is not safe for concurrent use by several host threads.
+ */
+#ifndef PLC_H
+#define PLC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PLC_OK 0
+#define PLC_ERR_ARG (-1)        /* bad argument or unsupported configuration */
+#define PLC_ERR_SIZE (-2)       /* grid size unsupported (odd, or FFT length not 2^a*3^b) */
+#define PLC_ERR_DECOMP (-3)     /* p_row*p_col != 1 */
+#define PLC_ERR_CUDA (-4)       /* CUDA runtime error */
+#define PLC_ERR_CHECK (-5)      /* NaN / CFL / divergence check failed */
+#define PLC_ERR_IO (-6)         /* file could not be read or parsed */
+#define PLC_ERR_NOMEM (-7)      /* device allocation failed */
+#define PLC_ERR_STATE (-8)      /* call not valid in the context's state */
+
+/* ---- field identifiers (mod_variables.hh:7-9) ---- */
+#define PLC_U 0
+#define PLC_V 1
+#define PLC_W 2
+#define PLC_U1 3
+#define PLC_V1 4
+#define PLC_W1 5
+#define PLC_P 6
+#define PLC_SPEC 7 /* nx*ny*nz spectral work array (var_xpen) */
+
+/* ---- precision forms ---- */
+#define PLC_FP64 0  /* plain FP64, parity with the reference */
+#define PLC_MIXED 1 /* FP32 stencils/FFTs, FP64 scalars and low modes */
+
+/* ---- initial fields (mod_initFlow.cc:47-102) ---- */
+#define PLC_INIT_UNI 0
+#define PLC_INIT_POI 1
+#define PLC_INIT_LOG 2
+#define PLC_INIT_MPI 3
+
+/*
+ * Every key of the reference's param.json (src/mod_parameters.hh:15-88,
+ * read by src/mod_parameters.cc:48-168), with the reference's defaults.
+ */
+typedef struct plc_params {
+  /* PARA */
+  int p_row, p_col;
+  /* MESH */
+  int read_mesh, mesh_type, stretch_func;
+  double stretch_ratio;
+  int nx, ny, nz;
+  double lx, ly, lz;
+  /* TIME */
+  int nt_end, nt_check;
+  double dt, cfl_limit, div_limit;
+  /* RESTART */
+  int is_restart;
+  char fn_prefix_input_inst[128];
+  char fn_prefix_input_stat[128];
+  /* PHYSICAL */
+  double re, u_ref, l_ref;
+  int initial_field; /* PLC_INIT_* */
+  double u0;
+  int init_with_noise;
+  double noise_intensity;
+  int smooth_wall_visc;
+  double u_crf;
+  /* FORCE */
+  int is_forced[3];
+  double vel_force[3];
+  /* STATISTICS */
+  int nt_init_stat, sample_interval;
+  int stat_which_var[11];
+  /* OUTPUT */
+  int nt_out_scrn, nt_out_inst, nt_out_stat, nt_out_save;
+  int overwrite_save, auto_cleanup, num_retained, nt_out_moni;
+  /* MONITOR */
+  int out_forcing, out_probe_point;
+  int probe_ijk[3];
+  int out_skf_z[2];
+  int out_region, nt_out_region;
+  int region_ijk[6];
+  /* B200 build options (not in the reference's param.json) */
+  int precision; /* PLC_FP64 (default) or PLC_MIXED */
+  double cfl_target; /* > 0: dt = cfl_target / max CFL rate, evaluated every nt_check steps */
+} plc_params;
+
+typedef struct plc_value_index {
+  /* mod_utils::value_index_pair_t (src/mod_utils.hh:7-12), global 1-based */
+  double value;
+  int ig, jg, kg;
+} plc_value_index;
+
+typedef struct plc_ctx plc_ctx;
+
+/* ---- configuration: replaces readInputParam (src/mod_parameters.cc:220-260) ---- */
+/* Fills the reference defaults (keys missing from param.json keep them). */
+int plc_params_default(plc_params *prm);
+/* Parses a param.json file; sections missing -> PLC_ERR_IO, like the reference's throw. */
+int plc_params_read_json(const char *path, plc_params *prm);
+/* checkMeshAndPara (src/mod_parameters.cc:170-211) plus the B200 limits. */
+int plc_params_check(const plc_params *prm);
+
+/* ---- context: owns the mesh, fields, Poisson state and CUDA stream ---- */
+/* initMesh (src/mod_mesh.cc:13-76) + allocVariables (mod_variables.cc:4-12)
+ * + init_poisson_solver (mod_poisson_solver.cc:180-315).  dzf_global (nz+2
+ * entries, k = 0..nz+1) may be NULL, in which case the mesh is generated
+ * from mesh_type/stretch_func/stretch_ratio (read_mesh = 1 requires it). */
+int plc_create(const plc_params *prm, const double *h_dzf_global, int device,
+               plc_ctx **out);
+int plc_destroy(plc_ctx *ctx);
+const char *plc_last_error(const plc_ctx *ctx);
+int plc_sync(plc_ctx *ctx);
+
+/* Mesh arrays as the reference holds them (nz+2 entries each, k = 0..nz+1):
+ * which = 0 dzf_global, 1 dzf, 2 dzf_inv, 3 dzc, 4 dzc_inv, 5 dzflzi,
+ * 6 zc_global. */
+int plc_get_mesh(const plc_ctx *ctx, int which, double *h_out);
+/* Device pointer and element count of a context-owned array (PLC_U..PLC_SPEC). */
+int plc_field_ptr(plc_ctx *ctx, int field, double **d_ptr, size_t *count);
+/* Copy a whole halo'd field (or the spectral array) between host and device. */
+int plc_upload(plc_ctx *ctx, int field, const double *h_src);
+int plc_download(plc_ctx *ctx, int field, double *h_dst);
+/* Current time step (device-resident; changes under CFL control). */
+int plc_get_dt(plc_ctx *ctx, double *dt);
+int plc_set_dt(plc_ctx *ctx, double dt);
+
+/* ---- mod_calcVel (src/mod_calcVel.hh:6-14) ---- */
+/* transform2CRF (mod_calcVel.cc:13-25); vel_force is updated in place on the host. */
+int plc_transform2crf(plc_ctx *ctx, double vel_crf, double *d_vel, double *vel_force);
+/* timeIntVelRK1 (mod_calcVel.cc:27-138): u1 = u + dt*(visc - conv), interior only. */
+int plc_time_int_vel_rk1(plc_ctx *ctx, double u_crf, const double *d_u,
+                         const double *d_v, const double *d_w, double *d_u1,
+                         double *d_v1, double *d_w1);
+/* timeIntVelRK2 (mod_calcVel.cc:140-251): u = (u1 + dt*(visc - conv)(u1) + u)/2. */
+int plc_time_int_vel_rk2(plc_ctx *ctx, double u_crf, double *d_u, double *d_v,
+                         double *d_w, const double *d_u1, const double *d_v1,
+                         const double *d_w1);
+/* correctVel (mod_calcVel.cc:253-278): u -= dt*grad(p), interior only. */
+int plc_correct_vel(plc_ctx *ctx, const double *d_p, double *d_u, double *d_v,
+                    double *d_w);
+/* forceVel (mod_calcVel.cc:280-320): bulk mean per forced component, then a
+ * uniform shift of the interior.  force_out (3 doubles, host, may be NULL)
+ * receives vel_force - mean. */
+int plc_force_vel(plc_ctx *ctx, double *d_u, double *d_v, double *d_w,
+                  double *force_out);
+
+/* ---- mod_calcRHS (src/mod_calcRHS.hh:6-7) ---- */
+/* calcRHS (mod_calcRHS.cc:7-33): rhs = div(u)/dt on the interior. */
+int plc_calc_rhs(plc_ctx *ctx, const double *d_u, const double *d_v,
+                 const double *d_w, double *d_rhs);
+
+/* ---- mod_updateBound (src/mod_updateBound.hh:6-8) ---- */
+/* updateBoundVel (mod_updateBound.cc:263-285): periodic x/y halos, no-slip z walls. */
+int plc_update_bound_vel(plc_ctx *ctx, double u_crf, double *d_u, double *d_v,
+                         double *d_w);
+/* imposeBCVel (mod_updateBound.cc:217-261); at p_row = p_col = 1 it is the
+ * same as plc_update_bound_vel because the y halo is a self-exchange. */
+int plc_impose_bc_vel(plc_ctx *ctx, double *d_u, double *d_v, double *d_w,
+                      double u_crf);
+/* updateBoundP (mod_updateBound.cc:287-330): periodic x/y, zero gradient in z. */
+int plc_update_bound_p(plc_ctx *ctx, double *d_p);
+
+/* ---- mod_poisson_solver (src/mod_poisson_solver.hh:5-10) ---- */
+/* init_poisson_solver (mod_poisson_solver.cc:180-315).  Called by plc_create
+ * with ("PP","PP","NN"); calling it again rebuilds the solver for a new
+ * dzf_global.  Only "PP","PP","NN" is supported, as in the reference. */
+int plc_init_poisson_solver(plc_ctx *ctx, const double *h_dzf_global,
+                            const char *bctype_x, const char *bctype_y,
+                            const char *bctype_z);
+/* execute_poisson_solver (mod_poisson_solver.cc:454-510): in place, rhs -> phi. */
+int plc_execute_poisson_solver(plc_ctx *ctx, double *d_p);
+/* free_poisson_solver (mod_poisson_solver.cc:512-537). */
+int plc_free_poisson_solver(plc_ctx *ctx);
+/* ssolve_trid (mod_poisson_solver.cc:317-357) on the spectral array. */
+int plc_solve_trid(plc_ctx *ctx, double *d_var);
+
+/* ---- mod_fft (src/mod_fft.hh:4-11) ---- */
+/* execute_fft_fwd_xpen (mod_fft.cc:60-88): p interior -> packed x spectrum. */
+int plc_fft_fwd_xpen(plc_ctx *ctx, const double *d_p, double *d_var);
+/* execute_fft_bwd_xpen (mod_fft.cc:90-120): packed x spectrum -> p interior, scaled by 1/(nx*ny). */
+int plc_fft_bwd_xpen(plc_ctx *ctx, const double *d_var, double *d_p);
+/* execute_fft_fwd_ypen / bwd_ypen (mod_fft.cc:122-187): in place along y. */
+int plc_fft_fwd_ypen(plc_ctx *ctx, double *d_var);
+int plc_fft_bwd_ypen(plc_ctx *ctx, double *d_var);
+/* get_eigen_values (mod_fft.cc:196-222), host only, "PP". */
+int plc_get_eigen_values(int ist, int isz, int isz_global, const char *bctype,
+                         double *h_lambda);
+
+/* ---- mod_utils (src/mod_utils.hh:14-27) ---- */
+/* Mean (mod_utils.cc:30-51): sum(var*dzflzi)/nx_global/ny_global over the interior. */
+int plc_mean(plc_ctx *ctx, int nx_global, int ny_global, const double *d_var,
+             double *mean);
+/* checkNaN (mod_utils.cc:77-106): *passed = 1 if no NaN (halos included). */
+int plc_check_nan(plc_ctx *ctx, const double *d_var, int *passed);
+/* calcMaxCFL (mod_utils.cc:108-150) and calcMaxDiv (:164-205). */
+int plc_calc_max_cfl(plc_ctx *ctx, const double *d_u, const double *d_v,
+                     const double *d_w, plc_value_index *cfl_max);
+int plc_calc_max_div(plc_ctx *ctx, const double *d_u, const double *d_v,
+                     const double *d_w, plc_value_index *div_max);
+
+/* ---- initial field (mod_initFlow.cc:47-102) on the context's u, v, w ---- */
+/* Followed by transform2CRF and the boundary update, as main.cc:73-82. */
+int plc_init_flow(plc_ctx *ctx);
+
+/* ---- fused time step: main.cc:116-154 on the context's fields ---- */
+/* Runs nsteps steps of the plain sequence RK1, RK2, RHS, Poisson, correction,
+ * forcing and boundary updates with fused kernels replayed from one captured
+ * CUDA graph.  Every nt_check steps (counted from the context's step counter)
+ * the NaN/CFL/divergence checks of main.cc:156-178 run on the device; a
+ * failure returns PLC_ERR_CHECK with the values in plc_last_error and in
+ * plc_last_check. */
+int plc_step(plc_ctx *ctx, int nsteps);
+/* Values of the last NaN/CFL/divergence check run by plc_step or plc_check. */
+int plc_last_check(plc_ctx *ctx, int *nan_passed, plc_value_index *cfl_max,
+                   plc_value_index *div_max);
+/* The checks of main.cc:156-178 on the context's u, v, w right now. */
+int plc_check(plc_ctx *ctx, int *nan_passed, plc_value_index *cfl_max,
+              plc_value_index *div_max);
+/* Number of steps taken by plc_step so far. */
+int plc_step_count(plc_ctx *ctx, long long *count);
+/* Number of kernel launches one plc_step step issues (graph nodes). */
+int plc_kernels_per_step(plc_ctx *ctx, int *count);
+/* plc_step(ctx, nsteps) bracketed by CUDA events on the context's stream;
+ * *ms receives the device time between the events (checks included). */
+int plc_step_timed(plc_ctx *ctx, int nsteps, double *ms);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after the library's. */
+int plc_get_stream(plc_ctx *ctx, void **stream);
+/* Runs nsteps plain steps launching the kernels of the fused step one by one
+ * with CUDA events between them and adds each kernel's device time (ms) to
+ * ms_per_kernel[0..count-1]; *count receives the number of kernels per step
+ * (at most 16).  Used for per-kernel roofline figures; advances the state. */
+int plc_profile_step(plc_ctx *ctx, int nsteps, float *ms_per_kernel, int *count);
+/* Name of kernel i of the fused step (static string). */
+const char *plc_step_kernel_name(int i);
+
+/* ---- host-only helpers (no GPU needed) ---- */
+/* initMeshByFunc (src/mod_mesh.cc:95-125): dzf_global[0..nz+1]. */
+int plc_mesh_by_func(int mesh_type, int stretch_func, double stretch_ratio, int nz,
+                     double lz, double *h_dzf_global);
+/* The Poisson solver's tridiagonal tables (mod_poisson_solver.cc:35-98,
+ * 231-282): reciprocal pre-factored pivots 1/b, laid out (nz, ny/2+1,
+ * nx/2+1) over the distinct wavenumber pairs, 0 where the last pivot is 0;
+ * h_a and h_c receive a[nz] and c[nz]. */
+int plc_trid_tables(int nx, int ny, int nz, double lx, double ly,
+                    const double *h_dzf_global, double *h_rpiv, double *h_a,
+                    double *h_c);
+/* Pinned host memory for fast uploads/downloads. */
+int plc_host_alloc(size_t bytes, void **ptr);
+int plc_host_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLC_H */

@@ -1,0 +1,921 @@
+// C ABI of libplc.so: context management, the module entry points of the
+// reference (mod_calcVel, mod_calcRHS, mod_updateBound, mod_poisson_solver,
+// mod_fft, mod_utils, mod_initFlow) and the fused, graph-captured time step.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "plc_internal.h"
+
+namespace {
+thread_local std::string g_err;  // errors without a context
+}
+
+plc::Geo plc_ctx::geo() const {
+  plc::Geo g;
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.X = nx + 2;
+  g.Y = ny + 2;
+  g.XY = (long long)g.X * g.Y;
+  g.dx_inv = dx_inv;
+  g.dy_inv = dy_inv;
+  g.re_inv = re_inv;
+  const size_t m = (size_t)nz + 2;
+  g.dzf = d_mesh;
+  g.dzf_inv = d_mesh + m;
+  g.dzc_inv = d_mesh + 2 * m;
+  g.dzflzi = d_mesh + 3 * m;
+  return g;
+}
+
+namespace plc {
+
+int set_error(plc_ctx *ctx, int code, const std::string &msg) {
+  if (ctx)
+    ctx->err = msg;
+  else
+    g_err = msg;
+  return code;
+}
+
+int cuda_status(plc_ctx *ctx, cudaError_t e, const char *what) {
+  return set_error(ctx, PLC_ERR_CUDA,
+                   std::string("CUDA error '") + cudaGetErrorString(e) + "' in " + what);
+}
+
+namespace {
+
+bool fft_length_ok(int n) {
+  int r[16], np;
+  return n >= 2 && (n % 2 == 0) && host_fft_factor(n, r, &np);
+}
+
+// Largest number of line pairs per block that divides `pairs` and keeps the
+// two shared-memory buffers under `cap` bytes.
+int choose_lines(int n, int pairs, size_t cap) {
+  int best = 1;
+  for (int d = 1; d <= pairs; ++d)
+    if (pairs % d == 0 && fft_smem_bytes(n, d) <= cap) best = d;
+  return best;
+}
+
+int upload_step_consts(plc_ctx *c, double dt) {
+  StepConst sc;
+  memset(&sc, 0, sizeof sc);
+  // the same host arithmetic as the reference: mod_calcVel.cc:36,256-258,
+  // mod_calcRHS.cc:11-13
+  sc.dt = dt;
+  sc.dti = 1.0 / dt;
+  sc.dtidxi = sc.dti * c->dx_inv;
+  sc.dtidyi = sc.dti * c->dy_inv;
+  sc.dtdxi = dt * c->dx_inv;
+  sc.dtdyi = dt * c->dy_inv;
+  // keep force/mean/cfl fields as they are on the device
+  PLC_CUDA(c, cudaMemcpyAsync(c->d_sc, &sc, 6 * sizeof(double), cudaMemcpyHostToDevice,
+                              c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->dt_host = dt;
+  return PLC_OK;
+}
+
+void free_poisson(plc_ctx *c) {
+  cudaFree(c->d_rpiv);
+  cudaFree(c->d_ac);
+  cudaFree(c->plan_x.tw);
+  cudaFree(c->plan_y.tw);
+  c->d_rpiv = nullptr;
+  c->d_ac = nullptr;
+  c->plan_x.tw = nullptr;
+  c->plan_y.tw = nullptr;
+  c->poisson_ready = false;
+}
+
+int init_poisson(plc_ctx *c, const double *dzf_global) {
+  free_poisson(c);
+  std::vector<double> rpiv, a, cc;
+  host_trid_tables(c->nx, c->ny, c->nz, c->dx, c->dy, dzf_global, rpiv, a, cc);
+  PLC_CUDA(c, cudaMalloc(&c->d_rpiv, rpiv.size() * sizeof(double)));
+  PLC_CUDA(c, cudaMemcpy(c->d_rpiv, rpiv.data(), rpiv.size() * sizeof(double),
+                         cudaMemcpyHostToDevice));
+  std::vector<double> ac(a);
+  ac.insert(ac.end(), cc.begin(), cc.end());
+  PLC_CUDA(c, cudaMalloc(&c->d_ac, ac.size() * sizeof(double)));
+  PLC_CUDA(c, cudaMemcpy(c->d_ac, ac.data(), ac.size() * sizeof(double), cudaMemcpyHostToDevice));
+  FftPlan *plans[2] = {&c->plan_x, &c->plan_y};
+  const int ns[2] = {c->nx, c->ny};
+  for (int d = 0; d < 2; ++d) {
+    FftPlan &p = *plans[d];
+    p.n = ns[d];
+    if (!host_fft_factor(p.n, p.radix, &p.npass))
+      return set_error(c, PLC_ERR_SIZE, "FFT length is not 2^a*3^b");
+    std::vector<double> tw;
+    host_twiddles(p.n, tw);
+    PLC_CUDA(c, cudaMalloc(&p.tw, tw.size() * sizeof(double)));
+    PLC_CUDA(c, cudaMemcpy(p.tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const size_t cap = 64 * 1024;
+  c->fft_lines_x = choose_lines(c->nx, c->ny / 2, cap);
+  c->fft_lines_y = choose_lines(c->ny, c->nx / 2, cap);
+  size_t need = fft_smem_bytes(c->nx, c->fft_lines_x);
+  const size_t need_y = fft_smem_bytes(c->ny, c->fft_lines_y);
+  if (need_y > need) need = need_y;
+  int dev_max = 0;
+  PLC_CUDA(c, cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  if (need > (size_t)dev_max)
+    return set_error(c, PLC_ERR_SIZE, "FFT line too long for shared memory");
+  PLC_CUDA(c, fft_configure(need > 48 * 1024 ? need : 48 * 1024));
+  c->poisson_ready = true;
+  return PLC_OK;
+}
+
+int check_ptr(plc_ctx *c, const void *p, const char *name) {
+  if (!p) return set_error(c, PLC_ERR_ARG, std::string("null pointer: ") + name);
+  return PLC_OK;
+}
+
+#define PLC_CHECK_CTX(c) \
+  if (!(c)) return plc::set_error(nullptr, PLC_ERR_ARG, "null context")
+#define PLC_REQ(c, p) \
+  if (int _r = check_ptr(c, p, #p)) return _r
+
+void to_ijk(const plc_ctx *c, long long idx, plc_value_index *out, double value) {
+  const long long X = c->nx + 2, XY = X * (c->ny + 2);
+  out->value = value;
+  out->kg = (int)(idx / XY);
+  out->jg = (int)((idx % XY) / X);
+  out->ig = (int)(idx % X);
+}
+
+int run_check(plc_ctx *c, int what, const double *u, const double *v, const double *w) {
+  PLC_CUDA(c, launch_check(c, u, v, w, what, c->stream));
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_check, c->d_check, sizeof(CheckResult), cudaMemcpyDeviceToHost,
+                              c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
+const char *const kStepKernelNames[] = {
+    "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
+    "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+mean", "force+bound(u)"};
+constexpr int kStepKernels = 9;
+
+// Launches of one fused step (main.cc:116-154) on the context's fields.  With
+// ev != nullptr, ev[0] is recorded before the first kernel and ev[q+1] after
+// kernel q (per-kernel timing; not used inside graph capture).
+int enqueue_step(plc_ctx *c, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+  double *u = c->d_field[PLC_U], *v = c->d_field[PLC_V], *w = c->d_field[PLC_W];
+  double *u1 = c->d_field[PLC_U1], *v1 = c->d_field[PLC_V1], *w1 = c->d_field[PLC_W1];
+  double *p = c->d_field[PLC_P], *spec = c->d_field[PLC_SPEC];
+  const double u_crf = c->prm.u_crf;
+  int q = 0;
+  auto mark = [&]() -> cudaError_t {
+    return ev ? cudaEventRecord(ev[q++], s) : cudaSuccess;
+  };
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_rk(c, 1, true, u_crf, u, v, w, u1, v1, w1, s));     // RK1 + bound(u1)
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_rk(c, 2, true, u_crf, u1, v1, w1, u, v, w, s));     // RK2 + bound(u)
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_fft_x_fwd(c, nullptr, u, v, w, spec, s));           // calcRHS + x-FFT
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_fft_y(c, spec, false, s));                          // y-FFT
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_trid(c, spec, s));                                  // z solve
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_fft_y(c, spec, true, s));                           // y-iFFT
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_fft_x_bwd(c, spec, p, true, s));                    // x-iFFT + bound(p)
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_correct(c, true, p, u, v, w, s));                   // correct + mean
+  PLC_CUDA(c, mark());
+  PLC_CUDA(c, launch_force_apply(c, true, u, v, w, s));                  // force + bound(u)
+  PLC_CUDA(c, mark());
+  return PLC_OK;
+}
+
+int build_graph(plc_ctx *c) {
+  if (c->graph) return PLC_OK;
+  cudaGraph_t g = nullptr;
+  PLC_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(c, c->stream);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc != PLC_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_status(c, e, "cudaStreamEndCapture");
+  size_t nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nodes);
+  e = cudaGraphInstantiate(&c->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_status(c, e, "cudaGraphInstantiate");
+  c->graph_kernels = (int)nodes;
+  return PLC_OK;
+}
+
+}  // namespace
+}  // namespace plc
+
+using namespace plc;
+
+extern "C" {
+
+int plc_params_default(plc_params *prm) {
+  if (!prm) return set_error(nullptr, PLC_ERR_ARG, "null params");
+  memset(prm, 0, sizeof *prm);
+  // mod_parameters.hh:15-88: globals are zero unless given a default there
+  prm->p_row = 1;
+  prm->p_col = 1;
+  snprintf(prm->fn_prefix_input_inst, sizeof prm->fn_prefix_input_inst, "save");
+  snprintf(prm->fn_prefix_input_stat, sizeof prm->fn_prefix_input_stat, "save_stat");
+  prm->u0 = 0.0;
+  prm->init_with_noise = 0;
+  prm->noise_intensity = 0.0;
+  prm->smooth_wall_visc = 0;
+  prm->u_crf = 0.0;
+  prm->sample_interval = 0;
+  prm->overwrite_save = 1;
+  prm->auto_cleanup = 1;
+  prm->num_retained = 0;
+  prm->nt_out_moni = 0;
+  prm->precision = PLC_FP64;
+  prm->cfl_target = 0.0;
+  return PLC_OK;
+}
+
+int plc_params_read_json(const char *path, plc_params *prm) {
+  if (!path || !prm) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  std::string err;
+  int rc = host_parse_param_json(path, prm, err);
+  if (rc != PLC_OK) return set_error(nullptr, rc, err);
+  return PLC_OK;
+}
+
+int plc_params_check(const plc_params *prm) {
+  if (!prm) return set_error(nullptr, PLC_ERR_ARG, "null params");
+  if (prm->p_row * prm->p_col != 1)
+    return set_error(nullptr, PLC_ERR_DECOMP,
+                     "PowerLLEL.ERROR: only p_row = p_col = 1 (one GPU) is supported");
+  // checkMeshAndPara, mod_parameters.cc:174-177
+  if (prm->nx <= 0 || prm->ny <= 0 || prm->nz <= 0 || prm->nx % 2 || prm->ny % 2 || prm->nz % 2)
+    return set_error(nullptr, PLC_ERR_SIZE,
+                     "PowerLLEL.ERROR.checkInputParam: <nx>, <ny>, <nz> should be even integers!");
+  if (!fft_length_ok(prm->nx) || !fft_length_ok(prm->ny))
+    return set_error(nullptr, PLC_ERR_SIZE, "nx and ny must be of the form 2^a*3^b");
+  if (!(prm->dt > 0.0) || !(prm->re > 0.0) || !(prm->lx > 0.0) || !(prm->ly > 0.0) ||
+      !(prm->lz > 0.0) || !(prm->u_ref > 0.0) || !(prm->l_ref > 0.0))
+    return set_error(nullptr, PLC_ERR_ARG, "dt, re, lx, ly, lz, u_ref and l_ref must be positive");
+  if (prm->precision != PLC_FP64 && prm->precision != PLC_MIXED)
+    return set_error(nullptr, PLC_ERR_ARG, "unknown precision form");
+  if (prm->precision == PLC_MIXED)
+    return set_error(nullptr, PLC_ERR_ARG, "the mixed-precision form is not built into this library");
+  return PLC_OK;
+}
+
+int plc_create(const plc_params *prm, const double *h_dzf_global, int device, plc_ctx **out) {
+  if (!prm || !out) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (int rc = plc_params_check(prm)) return rc;
+  if (prm->read_mesh && !h_dzf_global)
+    return set_error(nullptr, PLC_ERR_ARG, "read_mesh = 1 needs dzf_global (mesh.in)");
+  plc_ctx *c = new (std::nothrow) plc_ctx;
+  if (!c) return set_error(nullptr, PLC_ERR_NOMEM, "host allocation failed");
+  c->prm = *prm;
+  c->device = device;
+  c->nx = prm->nx;
+  c->ny = prm->ny;
+  c->nz = prm->nz;
+  // mod_mesh.cc:26-29 and mod_parameters.cc:259
+  c->dx = prm->lx / prm->nx;
+  c->dy = prm->ly / prm->ny;
+  c->dx_inv = 1.0 / c->dx;
+  c->dy_inv = 1.0 / c->dy;
+  c->re_inv = prm->u_ref * prm->l_ref / prm->re;
+  c->nfield = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  c->nspec = (size_t)c->nx * c->ny * c->nz;
+  auto fail = [&](int rc) {
+    std::string msg = c->err;
+    plc_destroy(c);
+    return set_error(nullptr, rc, msg);
+  };
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaSetDevice"));
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaStreamCreate"));
+  // mesh
+  const int nz = c->nz;
+  const size_t m = (size_t)nz + 2;
+  c->h_dzf_global.assign(m, 0.0);
+  if (h_dzf_global)
+    memcpy(c->h_dzf_global.data(), h_dzf_global, m * sizeof(double));
+  else
+    host_mesh_by_func(prm->mesh_type, prm->stretch_func, prm->stretch_ratio, nz, prm->lz,
+                      c->h_dzf_global.data());
+  c->h_dzf.assign(m, 0.0);
+  c->h_dzf_inv.assign(m, 0.0);
+  c->h_dzc.assign(m, 0.0);
+  c->h_dzc_inv.assign(m, 0.0);
+  c->h_dzflzi.assign(m, 0.0);
+  c->h_zc_global.assign(m, 0.0);
+  host_mesh_derived(nz, prm->lz, c->h_dzf_global.data(), c->h_dzf.data(), c->h_dzf_inv.data(),
+                    c->h_dzc.data(), c->h_dzc_inv.data(), c->h_dzflzi.data(),
+                    c->h_zc_global.data());
+  e = cudaMalloc(&c->d_mesh, 4 * m * sizeof(double));
+  if (e != cudaSuccess) return fail(set_error(c, PLC_ERR_NOMEM, "cudaMalloc mesh"));
+  const std::vector<double> *parts[4] = {&c->h_dzf, &c->h_dzf_inv, &c->h_dzc_inv, &c->h_dzflzi};
+  for (int q = 0; q < 4; ++q) {
+    e = cudaMemcpy(c->d_mesh + q * m, parts[q]->data(), m * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(cuda_status(c, e, "upload mesh"));
+  }
+  // fields (mod_variables.cc:4-12) and the spectral array, zero-initialised
+  for (int f = 0; f < 8; ++f) {
+    const size_t n = (f == PLC_SPEC) ? c->nspec : c->nfield;
+    e = cudaMalloc(&c->d_field[f], n * sizeof(double));
+    if (e != cudaSuccess) return fail(set_error(c, PLC_ERR_NOMEM, "cudaMalloc field"));
+    e = cudaMemset(c->d_field[f], 0, n * sizeof(double));
+    if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaMemset field"));
+  }
+  // scalars and scratch
+  if ((e = cudaMalloc(&c->d_sc, sizeof(StepConst))) != cudaSuccess ||
+      (e = cudaMemset(c->d_sc, 0, sizeof(StepConst))) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_partials, 4 * kMaxBlocksReduce * sizeof(double))) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_counter, 8 * sizeof(unsigned int))) != cudaSuccess ||
+      (e = cudaMemset(c->d_counter, 0, 8 * sizeof(unsigned int))) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_check, sizeof(CheckResult))) != cudaSuccess ||
+      (e = cudaMallocHost(&c->h_check, sizeof(CheckResult))) != cudaSuccess ||
+      (e = cudaMallocHost(&c->h_scal, 16 * sizeof(double))) != cudaSuccess)
+    return fail(cuda_status(c, e, "scratch allocation"));
+  if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
+  if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
+  *out = c;
+  return PLC_OK;
+}
+
+int plc_destroy(plc_ctx *c) {
+  if (!c) return PLC_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  free_poisson(c);
+  for (auto &f : c->d_field) cudaFree(f);
+  cudaFree(c->d_mesh);
+  cudaFree(c->d_sc);
+  cudaFree(c->d_partials);
+  cudaFree(c->d_counter);
+  cudaFree(c->d_check);
+  if (c->h_check) cudaFreeHost(c->h_check);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PLC_OK;
+}
+
+const char *plc_last_error(const plc_ctx *c) { return c ? c->err.c_str() : g_err.c_str(); }
+
+int plc_sync(plc_ctx *c) {
+  PLC_CHECK_CTX(c);
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
+int plc_get_mesh(const plc_ctx *c, int which, double *h_out) {
+  if (!c || !h_out) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  const std::vector<double> *arr[7] = {&c->h_dzf_global, &c->h_dzf,    &c->h_dzf_inv, &c->h_dzc,
+                                       &c->h_dzc_inv,    &c->h_dzflzi, &c->h_zc_global};
+  if (which < 0 || which > 6) return set_error(nullptr, PLC_ERR_ARG, "bad mesh array id");
+  memcpy(h_out, arr[which]->data(), arr[which]->size() * sizeof(double));
+  return PLC_OK;
+}
+
+int plc_field_ptr(plc_ctx *c, int field, double **d_ptr, size_t *count) {
+  PLC_CHECK_CTX(c);
+  if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
+  if (d_ptr) *d_ptr = c->d_field[field];
+  if (count) *count = (field == PLC_SPEC) ? c->nspec : c->nfield;
+  return PLC_OK;
+}
+
+int plc_upload(plc_ctx *c, int field, const double *h_src) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, h_src);
+  if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
+  const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
+  PLC_CUDA(c, cudaMemcpyAsync(c->d_field[field], h_src, n * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
+int plc_download(plc_ctx *c, int field, double *h_dst) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, h_dst);
+  if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
+  const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
+  PLC_CUDA(c, cudaMemcpyAsync(h_dst, c->d_field[field], n * sizeof(double),
+                              cudaMemcpyDeviceToHost, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
+int plc_get_dt(plc_ctx *c, double *dt) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, dt);
+  *dt = c->dt_host;
+  return PLC_OK;
+}
+
+int plc_set_dt(plc_ctx *c, double dt) {
+  PLC_CHECK_CTX(c);
+  if (!(dt > 0.0)) return set_error(c, PLC_ERR_ARG, "dt must be positive");
+  c->prm.dt = dt;
+  return upload_step_consts(c, dt);
+}
+
+// ---- mod_calcVel ----------------------------------------------------------
+int plc_transform2crf(plc_ctx *c, double vel_crf, double *d_vel, double *vel_force) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_vel);
+  if (vel_crf != 0) {
+    PLC_CUDA(c, launch_shift(c, d_vel, vel_crf, c->stream));
+    if (vel_force) *vel_force -= vel_crf;
+  }
+  return PLC_OK;
+}
+
+int plc_time_int_vel_rk1(plc_ctx *c, double u_crf, const double *d_u, const double *d_v,
+                         const double *d_w, double *d_u1, double *d_v1, double *d_w1) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_REQ(c, d_u1);
+  PLC_REQ(c, d_v1);
+  PLC_REQ(c, d_w1);
+  PLC_CUDA(c, launch_rk(c, 1, false, u_crf, d_u, d_v, d_w, d_u1, d_v1, d_w1, c->stream));
+  return PLC_OK;
+}
+
+int plc_time_int_vel_rk2(plc_ctx *c, double u_crf, double *d_u, double *d_v, double *d_w,
+                         const double *d_u1, const double *d_v1, const double *d_w1) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_REQ(c, d_u1);
+  PLC_REQ(c, d_v1);
+  PLC_REQ(c, d_w1);
+  PLC_CUDA(c, launch_rk(c, 2, false, u_crf, d_u1, d_v1, d_w1, d_u, d_v, d_w, c->stream));
+  return PLC_OK;
+}
+
+int plc_correct_vel(plc_ctx *c, const double *d_p, double *d_u, double *d_v, double *d_w) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_p);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_CUDA(c, launch_correct(c, false, d_p, d_u, d_v, d_w, c->stream));
+  return PLC_OK;
+}
+
+int plc_force_vel(plc_ctx *c, double *d_u, double *d_v, double *d_w, double *force_out) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  double *q[3] = {d_u, d_v, d_w};
+  for (int d = 0; d < 3; ++d)
+    if (c->prm.is_forced[d]) PLC_CUDA(c, launch_mean(c, d, c->nx, c->ny, q[d], c->stream));
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_scal, c->d_sc, sizeof(StepConst), cudaMemcpyDeviceToHost,
+                              c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  StepConst sc;
+  memcpy(&sc, c->h_scal, sizeof sc);
+  double force[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < 3; ++d)
+    if (c->prm.is_forced[d]) force[d] = c->prm.vel_force[d] - sc.mean[d];  // mod_calcVel.cc:297
+  memcpy(c->h_scal, force, sizeof force);
+  PLC_CUDA(c, cudaMemcpyAsync(reinterpret_cast<char *>(c->d_sc) + offsetof(StepConst, force),
+                              c->h_scal, sizeof force, cudaMemcpyHostToDevice, c->stream));
+  PLC_CUDA(c, launch_force_apply(c, false, d_u, d_v, d_w, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (force_out) memcpy(force_out, force, sizeof force);
+  return PLC_OK;
+}
+
+// ---- mod_calcRHS ----------------------------------------------------------
+int plc_calc_rhs(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
+                 double *d_rhs) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_REQ(c, d_rhs);
+  PLC_CUDA(c, launch_calc_rhs(c, d_u, d_v, d_w, d_rhs, c->stream));
+  return PLC_OK;
+}
+
+// ---- mod_updateBound ------------------------------------------------------
+int plc_update_bound_vel(plc_ctx *c, double u_crf, double *d_u, double *d_v, double *d_w) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_CUDA(c, launch_bound_vel(c, u_crf, d_u, d_v, d_w, c->stream));
+  return PLC_OK;
+}
+
+int plc_impose_bc_vel(plc_ctx *c, double *d_u, double *d_v, double *d_w, double u_crf) {
+  return plc_update_bound_vel(c, u_crf, d_u, d_v, d_w);
+}
+
+int plc_update_bound_p(plc_ctx *c, double *d_p) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_p);
+  PLC_CUDA(c, launch_bound_p(c, d_p, c->stream));
+  return PLC_OK;
+}
+
+// ---- mod_poisson_solver ---------------------------------------------------
+int plc_init_poisson_solver(plc_ctx *c, const double *h_dzf_global, const char *bctype_x,
+                            const char *bctype_y, const char *bctype_z) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, h_dzf_global);
+  if (!bctype_x || !bctype_y || !bctype_z || strcmp(bctype_x, "PP") || strcmp(bctype_y, "PP") ||
+      strcmp(bctype_z, "NN"))
+    return set_error(c, PLC_ERR_ARG, "only bctype PP, PP, NN is supported (mod_fft.cc:20-26)");
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return init_poisson(c, h_dzf_global);
+}
+
+int plc_free_poisson_solver(plc_ctx *c) {
+  PLC_CHECK_CTX(c);
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  free_poisson(c);
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return PLC_OK;
+}
+
+#define PLC_NEED_POISSON(c) \
+  if (!(c)->poisson_ready) return set_error(c, PLC_ERR_STATE, "Poisson solver not initialised")
+
+int plc_execute_poisson_solver(plc_ctx *c, double *d_p) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_p);
+  PLC_NEED_POISSON(c);
+  double *spec = c->d_field[PLC_SPEC];
+  PLC_CUDA(c, launch_fft_x_fwd(c, d_p, nullptr, nullptr, nullptr, spec, c->stream));
+  PLC_CUDA(c, launch_fft_y(c, spec, false, c->stream));
+  PLC_CUDA(c, launch_trid(c, spec, c->stream));
+  PLC_CUDA(c, launch_fft_y(c, spec, true, c->stream));
+  PLC_CUDA(c, launch_fft_x_bwd(c, spec, d_p, false, c->stream));
+  return PLC_OK;
+}
+
+int plc_solve_trid(plc_ctx *c, double *d_var) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_var);
+  PLC_NEED_POISSON(c);
+  PLC_CUDA(c, launch_trid(c, d_var, c->stream));
+  return PLC_OK;
+}
+
+// ---- mod_fft --------------------------------------------------------------
+int plc_fft_fwd_xpen(plc_ctx *c, const double *d_p, double *d_var) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_p);
+  PLC_REQ(c, d_var);
+  PLC_NEED_POISSON(c);
+  PLC_CUDA(c, launch_fft_x_fwd(c, d_p, nullptr, nullptr, nullptr, d_var, c->stream));
+  return PLC_OK;
+}
+
+int plc_fft_bwd_xpen(plc_ctx *c, const double *d_var, double *d_p) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_p);
+  PLC_REQ(c, d_var);
+  PLC_NEED_POISSON(c);
+  PLC_CUDA(c, launch_fft_x_bwd(c, d_var, d_p, false, c->stream));
+  return PLC_OK;
+}
+
+int plc_fft_fwd_ypen(plc_ctx *c, double *d_var) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_var);
+  PLC_NEED_POISSON(c);
+  PLC_CUDA(c, launch_fft_y(c, d_var, false, c->stream));
+  return PLC_OK;
+}
+
+int plc_fft_bwd_ypen(plc_ctx *c, double *d_var) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_var);
+  PLC_NEED_POISSON(c);
+  PLC_CUDA(c, launch_fft_y(c, d_var, true, c->stream));
+  return PLC_OK;
+}
+
+int plc_get_eigen_values(int ist, int isz, int isz_global, const char *bctype, double *h_lambda) {
+  if (!bctype || strcmp(bctype, "PP") || !h_lambda || isz_global < 2 || ist < 1 ||
+      ist + isz - 1 > isz_global)
+    return set_error(nullptr, PLC_ERR_ARG, "bad arguments to get_eigen_values (PP only)");
+  host_eigen_values(ist, isz, isz_global, h_lambda);
+  return PLC_OK;
+}
+
+// ---- mod_utils ------------------------------------------------------------
+int plc_mean(plc_ctx *c, int nx_global, int ny_global, const double *d_var, double *mean) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_var);
+  PLC_REQ(c, mean);
+  PLC_CUDA(c, launch_mean(c, 0, nx_global, ny_global, d_var, c->stream));
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_scal, reinterpret_cast<char *>(c->d_sc) + offsetof(StepConst, mean),
+                              sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  *mean = c->h_scal[0];
+  return PLC_OK;
+}
+
+int plc_check_nan(plc_ctx *c, const double *d_var, int *passed) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_var);
+  PLC_REQ(c, passed);
+  if (int rc = run_check(c, 1, d_var, d_var, d_var)) return rc;
+  *passed = c->h_check->nan_found ? 0 : 1;
+  return PLC_OK;
+}
+
+int plc_calc_max_cfl(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
+                     plc_value_index *cfl_max) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_REQ(c, cfl_max);
+  if (int rc = run_check(c, 2, d_u, d_v, d_w)) return rc;
+  to_ijk(c, c->h_check->cfl_idx, cfl_max, c->h_check->cfl * c->dt_host);  // mod_utils.cc:144
+  return PLC_OK;
+}
+
+int plc_calc_max_div(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
+                     plc_value_index *div_max) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, d_u);
+  PLC_REQ(c, d_v);
+  PLC_REQ(c, d_w);
+  PLC_REQ(c, div_max);
+  if (int rc = run_check(c, 4, d_u, d_v, d_w)) return rc;
+  to_ijk(c, c->h_check->div_idx, div_max, c->h_check->div);
+  return PLC_OK;
+}
+
+int plc_check(plc_ctx *c, int *nan_passed, plc_value_index *cfl_max, plc_value_index *div_max) {
+  PLC_CHECK_CTX(c);
+  if (int rc = run_check(c, 7, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W])) return rc;
+  c->last_nan_passed = c->h_check->nan_found ? 0 : 1;
+  to_ijk(c, c->h_check->cfl_idx, &c->last_cfl, c->h_check->cfl * c->dt_host);
+  to_ijk(c, c->h_check->div_idx, &c->last_div, c->h_check->div);
+  if (nan_passed) *nan_passed = c->last_nan_passed;
+  if (cfl_max) *cfl_max = c->last_cfl;
+  if (div_max) *div_max = c->last_div;
+  return PLC_OK;
+}
+
+int plc_last_check(plc_ctx *c, int *nan_passed, plc_value_index *cfl_max,
+                   plc_value_index *div_max) {
+  PLC_CHECK_CTX(c);
+  if (nan_passed) *nan_passed = c->last_nan_passed;
+  if (cfl_max) *cfl_max = c->last_cfl;
+  if (div_max) *div_max = c->last_div;
+  return PLC_OK;
+}
+
+// ---- mod_initFlow ---------------------------------------------------------
+int plc_init_flow(plc_ctx *c) {
+  PLC_CHECK_CTX(c);
+  const plc_params &P = c->prm;
+  const int nz = c->nz;
+  std::vector<double> prof(nz + 2, 0.0);
+  bool is_mean = false;
+  if (P.initial_field == PLC_INIT_UNI) {
+    for (int k = 1; k <= nz; ++k) prof[k] = P.u0;
+  } else if (P.initial_field == PLC_INIT_POI) {  // mod_initFlow.cc:16-21
+    for (int k = 1; k <= nz; ++k) {
+      const double z = c->h_zc_global[k] / P.lz;
+      prof[k] = 6.0 * (1.0 - z) * z * P.u_ref;
+    }
+    is_mean = true;
+  } else if (P.initial_field == PLC_INIT_LOG) {  // mod_initFlow.cc:23-30
+    const double retau = 0.09 * pow(P.re, 0.88);
+    for (int k = 1; k <= nz; ++k) {
+      const double zn = c->h_zc_global[k] / P.lz;
+      const double z = fmin(zn, 1.0 - zn) * 2.0 * retau;
+      prof[k] = (z <= 11.6 ? z : 2.5 * log(z) + 5.5);
+    }
+    is_mean = true;
+  } else if (P.initial_field == PLC_INIT_MPI) {
+    for (int k = 1; k <= nz; ++k) prof[k] = 0.0;  // rank 0
+  } else {
+    return set_error(c, PLC_ERR_ARG, "unknown initial_field");
+  }
+  double *u = c->d_field[PLC_U], *v = c->d_field[PLC_V], *w = c->d_field[PLC_W];
+  double *scratch = c->d_field[PLC_SPEC];  // nx*ny*nz >= nz+2
+  PLC_CUDA(c, cudaMemcpyAsync(scratch, prof.data(), prof.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+  PLC_CUDA(c, launch_init_flow(c, u, v, w, scratch, c->stream));
+  if (is_mean) {
+    double meanold = 0.0;
+    // the reference passes (nz, ny) as the global sizes here (mod_initFlow.cc:92)
+    if (int rc = plc_mean(c, c->nz, c->ny, u, &meanold)) return rc;
+    if (meanold != 0.0) {
+      c->h_scal[0] = 1.0 / (meanold * P.u_ref);
+      PLC_CUDA(c, cudaMemcpyAsync(scratch, c->h_scal, sizeof(double), cudaMemcpyHostToDevice,
+                                  c->stream));
+      PLC_CUDA(c, launch_scale(c, u, scratch, c->stream));
+    }
+  }
+  // main.cc:78-82
+  if (int rc = plc_transform2crf(c, P.u_crf, u, &c->prm.vel_force[0])) return rc;
+  PLC_CUDA(c, launch_bound_vel(c, P.u_crf, u, v, w, c->stream));
+  PLC_CUDA(c, launch_bound_p(c, c->d_field[PLC_P], c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  // the graph bakes the forcing configuration in: rebuild it on the next step
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return PLC_OK;
+}
+
+// ---- fused time step ------------------------------------------------------
+int plc_step(plc_ctx *c, int nsteps) {
+  PLC_CHECK_CTX(c);
+  if (nsteps < 0) return set_error(c, PLC_ERR_ARG, "nsteps < 0");
+  PLC_NEED_POISSON(c);
+  if (int rc = build_graph(c)) return rc;
+  const plc_params &P = c->prm;
+  if (P.cfl_target > 0.0 && c->nstep == 0) {
+    int passed;
+    plc_value_index cm, dm;
+    if (int rc = plc_check(c, &passed, &cm, &dm)) return rc;
+    if (c->h_check->cfl > 0.0)
+      if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    PLC_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
+    ++c->nstep;
+    if (P.nt_check > 0 && c->nstep % P.nt_check == 0) {
+      // main.cc:156-178
+      int passed;
+      plc_value_index cm, dm;
+      if (int rc = plc_check(c, &passed, &cm, &dm)) return rc;
+      bool ok = passed != 0;
+      std::string msg;
+      if (!passed) msg += "PowerLLEL.ERROR.checkNaN: NaN has been detected in <u>!\n";
+      if (cm.value > P.cfl_limit || std::isnan(cm.value)) {
+        ok = false;
+        msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
+      }
+      if (dm.value > P.div_limit || std::isnan(dm.value)) {
+        ok = false;
+        msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
+      }
+      if (!ok) {
+        char buf[256];
+        snprintf(buf, sizeof buf,
+                 "PowerLLEL.ERROR: nt = %9lld, cfl_max = %10.3e at (%5d,%5d,%5d), div_max = %10.3e at (%5d,%5d,%5d)",
+                 c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
+        return set_error(c, PLC_ERR_CHECK, msg + buf);
+      }
+      if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
+        if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+    }
+  }
+  return PLC_OK;
+}
+
+int plc_step_count(plc_ctx *c, long long *count) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, count);
+  *count = c->nstep;
+  return PLC_OK;
+}
+
+int plc_step_timed(plc_ctx *c, int nsteps, double *ms) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, ms);
+  PLC_NEED_POISSON(c);
+  if (int rc = build_graph(c)) return rc;
+  cudaEvent_t e0, e1;
+  PLC_CUDA(c, cudaEventCreate(&e0));
+  PLC_CUDA(c, cudaEventCreate(&e1));
+  int rc = PLC_OK;
+  cudaError_t e = cudaEventRecord(e0, c->stream);
+  if (e == cudaSuccess) {
+    rc = plc_step(c, nsteps);
+    e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float f = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, e0, e1);
+    *ms = f;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != PLC_OK) return rc;
+  if (e != cudaSuccess) return cuda_status(c, e, "step timing events");
+  return PLC_OK;
+}
+
+int plc_get_stream(plc_ctx *c, void **stream) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, stream);
+  *stream = (void *)c->stream;
+  return PLC_OK;
+}
+
+int plc_profile_step(plc_ctx *c, int nsteps, float *ms_per_kernel, int *count) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, ms_per_kernel);
+  PLC_NEED_POISSON(c);
+  cudaEvent_t ev[kStepKernels + 1];
+  for (auto &e : ev) PLC_CUDA(c, cudaEventCreate(&e));
+  int rc = PLC_OK;
+  for (int s = 0; s < nsteps && rc == PLC_OK; ++s) {
+    rc = enqueue_step(c, c->stream, ev);
+    if (rc != PLC_OK) break;
+    cudaError_t e = cudaEventSynchronize(ev[kStepKernels]);
+    if (e != cudaSuccess) {
+      rc = cuda_status(c, e, "cudaEventSynchronize");
+      break;
+    }
+    for (int q = 0; q < kStepKernels; ++q) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
+      ms_per_kernel[q] += ms;
+    }
+    ++c->nstep;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (count) *count = kStepKernels;
+  return rc;
+}
+
+const char *plc_step_kernel_name(int i) {
+  return (i >= 0 && i < kStepKernels) ? kStepKernelNames[i] : "";
+}
+
+int plc_mesh_by_func(int mesh_type, int stretch_func, double stretch_ratio, int nz, double lz,
+                     double *h_dzf_global) {
+  if (!h_dzf_global || nz < 1 || !(lz > 0.0))
+    return set_error(nullptr, PLC_ERR_ARG, "bad arguments to plc_mesh_by_func");
+  host_mesh_by_func(mesh_type, stretch_func, stretch_ratio, nz, lz, h_dzf_global);
+  return PLC_OK;
+}
+
+int plc_trid_tables(int nx, int ny, int nz, double lx, double ly, const double *h_dzf_global,
+                    double *h_rpiv, double *h_a, double *h_c) {
+  if (!h_dzf_global || !h_rpiv || nx < 2 || ny < 2 || nz < 2 || nx % 2 || ny % 2)
+    return set_error(nullptr, PLC_ERR_ARG, "bad arguments to plc_trid_tables");
+  std::vector<double> rpiv, a, cc;
+  host_trid_tables(nx, ny, nz, lx / nx, ly / ny, h_dzf_global, rpiv, a, cc);
+  memcpy(h_rpiv, rpiv.data(), rpiv.size() * sizeof(double));
+  if (h_a) memcpy(h_a, a.data(), a.size() * sizeof(double));
+  if (h_c) memcpy(h_c, cc.data(), cc.size() * sizeof(double));
+  return PLC_OK;
+}
+
+int plc_host_alloc(size_t bytes, void **ptr) {
+  if (!ptr) return set_error(nullptr, PLC_ERR_ARG, "null pointer");
+  cudaError_t e = cudaMallocHost(ptr, bytes);
+  if (e != cudaSuccess) return cuda_status(nullptr, e, "cudaMallocHost");
+  return PLC_OK;
+}
+
+int plc_host_free(void *ptr) {
+  if (ptr) {
+    cudaError_t e = cudaFreeHost(ptr);
+    if (e != cudaSuccess) return cuda_status(nullptr, e, "cudaFreeHost");
+  }
+  return PLC_OK;
+}
+
+int plc_kernels_per_step(plc_ctx *c, int *count) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, count);
+  if (int rc = build_graph(c)) return rc;
+  *count = c->graph_kernels;
+  return PLC_OK;
+}
+
+}  // extern "C"

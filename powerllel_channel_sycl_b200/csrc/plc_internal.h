@@ -1,0 +1,162 @@
+// Internal declarations shared by the translation units of libplc.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "plc.h"
+
+namespace plc {
+
+// ---------------------------------------------------------------------------
+// Geometry passed by value to every kernel.
+// ---------------------------------------------------------------------------
+struct Geo {
+  int nx, ny, nz;
+  int X, Y;           // halo'd x and y lengths (nx+2, ny+2)
+  long long XY;       // X*Y
+  double dx_inv, dy_inv, re_inv;
+  const double *dzf, *dzf_inv, *dzc_inv, *dzflzi;  // device, nz+2 each
+  __host__ __device__ long long at(int i, int j, int k) const {
+    return (long long)i + (long long)X * j + XY * k;
+  }
+};
+
+// Per-step scalars that may change on the device (CFL-controlled dt, the
+// bulk forcing of the step).  Kernels read them through a device pointer so
+// that a captured graph stays valid when they change.
+struct StepConst {
+  double dt, dti, dtidxi, dtidyi, dtdxi, dtdyi;
+  double force[3];   // vel_force - mean of the last forcing
+  double mean[3];
+  double cfl_rate;   // max |u|/dx + |v|/dy + |w|/dz of the last check (no dt)
+};
+
+// Result of the device-side NaN/CFL/divergence check.
+struct CheckResult {
+  int nan_found;
+  int pad;
+  double cfl;        // max CFL rate (without dt)
+  long long cfl_idx; // halo'd linear index, -1 if none
+  double div;
+  long long div_idx;
+};
+
+// Complex FFT plan for a line length n = 2^a 3^b.
+struct FftPlan {
+  int n = 0;
+  int npass = 0;
+  int radix[16] = {0};
+  double2 *tw = nullptr;  // device, n entries: exp(-2 pi i t / n)
+};
+
+constexpr int kMaxBlocksReduce = 4096;
+
+}  // namespace plc
+
+struct plc_ctx {
+  plc_params prm;
+  int device = 0;
+  int nx = 0, ny = 0, nz = 0;
+  double dx = 0, dy = 0, dx_inv = 0, dy_inv = 0, re_inv = 0;
+  size_t nfield = 0;  // (nx+2)(ny+2)(nz+2)
+  size_t nspec = 0;   // nx*ny*nz
+  // host copies of the mesh (nz+2 each)
+  std::vector<double> h_dzf_global, h_dzf, h_dzf_inv, h_dzc, h_dzc_inv, h_dzflzi,
+      h_zc_global;
+  double *d_mesh = nullptr;  // dzf | dzf_inv | dzc_inv | dzflzi
+  double *d_field[8] = {nullptr};
+  // Poisson solver state
+  bool poisson_ready = false;
+  double *d_rpiv = nullptr;   // 1/b, (nz, ny/2+1, nx/2+1)
+  double *d_ac = nullptr;     // a[nz] | c[nz]
+  plc::FftPlan plan_x, plan_y;
+  int fft_lines_x = 1, fft_lines_y = 1;
+  // scalars and scratch
+  plc::StepConst *d_sc = nullptr;
+  double *d_partials = nullptr;        // 4 * kMaxBlocksReduce
+  unsigned int *d_counter = nullptr;   // last-block counters
+  plc::CheckResult *d_check = nullptr;
+  plc::CheckResult *h_check = nullptr;  // pinned
+  double *h_scal = nullptr;             // pinned scalars
+  double dt_host = 0;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_kernels = 0;
+  long long nstep = 0;
+  int last_nan_passed = 1;
+  plc_value_index last_cfl{0, 1, 1, 1}, last_div{0, 1, 1, 1};
+  std::string err;
+  plc::Geo geo() const;
+};
+
+namespace plc {
+
+// error helpers ---------------------------------------------------------------
+int set_error(plc_ctx *ctx, int code, const std::string &msg);
+int cuda_status(plc_ctx *ctx, cudaError_t e, const char *what);
+#define PLC_CUDA(ctx, call)                                     \
+  do {                                                          \
+    cudaError_t _e = (call);                                    \
+    if (_e != cudaSuccess) return plc::cuda_status(ctx, _e, #call); \
+  } while (0)
+#define PLC_LAUNCH(ctx, what)                                   \
+  do {                                                          \
+    cudaError_t _e = cudaGetLastError();                        \
+    if (_e != cudaSuccess) return plc::cuda_status(ctx, _e, what); \
+  } while (0)
+
+// host-side mesh and solver set-up (plc_host.cc, compiled without FMA
+// contraction so that the arithmetic follows the reference's host loops)
+void host_mesh_by_func(int mesh_type, int stretch_func, double stretch_ratio,
+                       int nz, double lz, double *dzf_global);
+void host_mesh_derived(int nz, double lz, const double *dzf_global, double *dzf,
+                       double *dzf_inv, double *dzc, double *dzc_inv,
+                       double *dzflzi, double *zc_global);
+void host_eigen_values(int ist, int isz, int isz_global, double *lambda);
+// Reciprocal pre-factored pivots 1/b (0 where b == 0), table layout
+// (nz, ny/2+1, nx/2+1), plus a[nz] and c[nz].
+void host_trid_tables(int nx, int ny, int nz, double dx, double dy,
+                      const double *dzf_global, std::vector<double> &rpiv,
+                      std::vector<double> &a, std::vector<double> &c);
+void host_twiddles(int n, std::vector<double> &re_im);
+bool host_fft_factor(int n, int *radix, int *npass);
+int host_parse_param_json(const char *path, plc_params *prm, std::string &err);
+
+// kernel launchers (return cudaError_t of the launch) ---------------------------
+cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf,
+                      const double *qu, const double *qv, const double *qw,
+                      double *ou, double *ov, double *ow, cudaStream_t s);
+cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v,
+                            const double *w, double *rhs, cudaStream_t s);
+cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p,
+                           double *u, double *v, double *w, cudaStream_t s);
+cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u,
+                               double *v, double *w, cudaStream_t s);
+cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg,
+                        const double *var, cudaStream_t s);
+cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, double *u,
+                             double *v, double *w, cudaStream_t s);
+cudaError_t launch_bound_p(const plc_ctx *c, double *p, cudaStream_t s);
+cudaError_t launch_shift(const plc_ctx *c, double *var, double delta,
+                         cudaStream_t s);
+cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u,
+                             const double *v, const double *w, double *var,
+                             cudaStream_t s);
+cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p,
+                             bool fuse_bc, cudaStream_t s);
+cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse,
+                         cudaStream_t s);
+cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s);
+cudaError_t launch_check(const plc_ctx *c, const double *u, const double *v,
+                         const double *w, int what, cudaStream_t s);
+cudaError_t launch_init_flow(const plc_ctx *c, double *u, double *v, double *w,
+                             const double *d_prof, cudaStream_t s);
+cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult,
+                         cudaStream_t s);
+size_t fft_smem_bytes(int n, int lines);
+cudaError_t fft_configure(size_t max_bytes);
+
+}  // namespace plc

@@ -1,0 +1,701 @@
+// Stencil, boundary, forcing and reduction kernels of the FP64 time step.
+//
+// Fields use the reference's halo'd layout (one ghost cell per side, x
+// fastest).  Kernels that end a stage of the fused step ("fused BC") also
+// write the halo images of every interior value they produce, so the
+// separate boundary update of the reference (mod_updateBound.cc) costs no
+// extra pass over the field:
+//   x and y periodic images:  (0,j)=(nx,j), (nx+1,j)=(1,j), same in y and for
+//                             the corners (the y self-exchange of
+//                             mod_type.hh:219-289 followed by the x copy of
+//                             mod_updateBound.cc:32-73);
+//   z walls, centred u and v: q(0) = 2*bc - q(1), q(nz+1) = 2*bc - q(nz),
+//                             bc = -u_crf for u and 0 for v (:75-144);
+//   z walls, face w:          w(0) = w(nz) = w(nz+1) = 0;
+//   pressure:                 p(0) = p(1), p(nz+1) = p(nz) (:146-180).
+
+#include <cuda_runtime.h>
+
+#include "plc_device.cuh"
+#include "plc_internal.h"
+
+namespace plc {
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+struct Rhs3 {
+  double u, v, w;
+};
+
+// (visc - conv) of the three momentum components at (i,j,k),
+// mod_calcVel.cc:61-125 (the same expression for RK1 and RK2).
+__device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf,
+                                             const double *__restrict__ qu,
+                                             const double *__restrict__ qv,
+                                             const double *__restrict__ qw,
+                                             int i, int j, int k) {
+  const double _dx_inv = g.dx_inv, _dy_inv = g.dy_inv, _re_inv = g.re_inv;
+  const long long X = g.X, XY = g.XY;
+  const long long c = g.at(i, j, k);
+#define U(di, dj, dk) __ldg(qu + c + (di) + (dj) * X + (dk) * XY)
+#define V(di, dj, dk) __ldg(qv + c + (di) + (dj) * X + (dk) * XY)
+#define W(di, dj, dk) __ldg(qw + c + (di) + (dj) * X + (dk) * XY)
+  const double dzf_m = __ldg(g.dzf + k - 1), dzf_0 = __ldg(g.dzf + k),
+               dzf_p = __ldg(g.dzf + k + 1);
+  const double dzfi_0 = __ldg(g.dzf_inv + k), dzfi_p = __ldg(g.dzf_inv + k + 1);
+  const double dzci_m = __ldg(g.dzc_inv + k - 1), dzci_0 = __ldg(g.dzc_inv + k);
+  double uw, ue, us, un, ub, ut;
+  double ww, we, ws, wn, wb, wt;
+  double vw, ve, vs, vn, vb, vt;
+  double dqw, dqe, dqs, dqn, dqb, dqt;
+  double conv, visc;
+  Rhs3 r;
+  const double u000 = U(0, 0, 0), v000 = V(0, 0, 0), w000 = W(0, 0, 0);
+  // u component
+  {
+    const double up00 = U(1, 0, 0), um00 = U(-1, 0, 0), u0p0 = U(0, 1, 0),
+                 u0m0 = U(0, -1, 0), u00p = U(0, 0, 1), u00m = U(0, 0, -1);
+    ue = (u000 + up00);
+    uw = (um00 + u000);
+    un = (u000 + u0p0);
+    us = (u0m0 + u000);
+    ut = (u000 * dzf_p + u00p * dzf_0) * dzci_0;
+    ub = (u000 * dzf_m + u00m * dzf_0) * dzci_m;
+    vn = (v000 + V(1, 0, 0));
+    vs = (V(0, -1, 0) + V(1, -1, 0));
+    wt = (w000 + W(1, 0, 0));
+    wb = (W(0, 0, -1) + W(1, 0, -1));
+    dqe = (up00 - u000) * _dx_inv;
+    dqw = (u000 - um00) * _dx_inv;
+    dqn = (u0p0 - u000) * _dy_inv;
+    dqs = (u000 - u0m0) * _dy_inv;
+    dqt = (u00p - u000) * dzci_0;
+    dqb = (u000 - u00m) * dzci_m;
+    conv = 0.25 * ((ue * ue - uw * uw) * _dx_inv + (un * vn - us * vs) * _dy_inv +
+                   (ut * wt - ub * wb) * dzfi_0);
+    conv = conv + 0.5 * u_crf * (ue - uw) * _dx_inv;
+    visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzfi_0) * _re_inv;
+    r.u = visc - conv;
+  }
+  // v component
+  {
+    const double vp00 = V(1, 0, 0), vm00 = V(-1, 0, 0), v0p0 = V(0, 1, 0),
+                 v0m0 = V(0, -1, 0), v00p = V(0, 0, 1), v00m = V(0, 0, -1);
+    ve = (v000 + vp00);
+    vw = (vm00 + v000);
+    vn = (v000 + v0p0);
+    vs = (v0m0 + v000);
+    vt = (v000 * dzf_p + v00p * dzf_0) * dzci_0;
+    vb = (v000 * dzf_m + v00m * dzf_0) * dzci_m;
+    ue = (u000 + U(0, 1, 0));
+    uw = (U(-1, 0, 0) + U(-1, 1, 0));
+    wt = (w000 + W(0, 1, 0));
+    wb = (W(0, 0, -1) + W(0, 1, -1));
+    dqe = (vp00 - v000) * _dx_inv;
+    dqw = (v000 - vm00) * _dx_inv;
+    dqn = (v0p0 - v000) * _dy_inv;
+    dqs = (v000 - v0m0) * _dy_inv;
+    dqt = (v00p - v000) * dzci_0;
+    dqb = (v000 - v00m) * dzci_m;
+    conv = 0.25 * ((ue * ve - uw * vw) * _dx_inv + (vn * vn - vs * vs) * _dy_inv +
+                   (wt * vt - wb * vb) * dzfi_0);
+    conv = conv + 0.5 * u_crf * (ve - vw) * _dx_inv;
+    visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzfi_0) * _re_inv;
+    r.v = visc - conv;
+  }
+  // w component
+  {
+    const double wp00 = W(1, 0, 0), wm00 = W(-1, 0, 0), w0p0 = W(0, 1, 0),
+                 w0m0 = W(0, -1, 0), w00p = W(0, 0, 1), w00m = W(0, 0, -1);
+    we = (w000 + wp00);
+    ww = (wm00 + w000);
+    wn = (w000 + w0p0);
+    ws = (w0m0 + w000);
+    wt = (w000 + w00p);
+    wb = (w000 + w00m);
+    ue = (u000 * dzf_p + U(0, 0, 1) * dzf_0) * dzci_0;
+    uw = (U(-1, 0, 0) * dzf_p + U(-1, 0, 1) * dzf_0) * dzci_0;
+    vn = (v000 * dzf_p + V(0, 0, 1) * dzf_0) * dzci_0;
+    vs = (V(0, -1, 0) * dzf_p + V(0, -1, 1) * dzf_0) * dzci_0;
+    dqe = (wp00 - w000) * _dx_inv;
+    dqw = (w000 - wm00) * _dx_inv;
+    dqn = (w0p0 - w000) * _dy_inv;
+    dqs = (w000 - w0m0) * _dy_inv;
+    dqt = (w00p - w000) * dzfi_p;
+    dqb = (w000 - w00m) * dzfi_0;
+    conv = 0.25 * ((ue * we - uw * ww) * _dx_inv + (vn * wn - vs * ws) * _dy_inv +
+                   (wt * wt - wb * wb) * dzci_0);
+    conv = conv + 0.5 * u_crf * (we - ww) * _dx_inv;
+    visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzci_0) * _re_inv;
+    r.w = visc - conv;
+  }
+#undef U
+#undef V
+#undef W
+  return r;
+}
+
+// RK1 (STAGE 1, mod_calcVel.cc:27-129):  o = q + dt*F(q)
+// RK2 (STAGE 2, mod_calcVel.cc:140-242): o = (q + dt*F(q) + o)*0.5, q = u1
+template <int STAGE, bool FUSE>
+__global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restrict__ sc,
+                                               double u_crf, const double *__restrict__ qu,
+                                               const double *__restrict__ qv,
+                                               const double *__restrict__ qw, double *ou,
+                                               double *ov, double *ow) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const double dt = sc->dt;
+  const Rhs3 r = momentum_rhs(g, u_crf, qu, qv, qw, i, j, k);
+  const long long c = g.at(i, j, k);
+  double nu, nv, nw;
+  if (STAGE == 1) {
+    nu = qu[c] + dt * r.u;
+    nv = qv[c] + dt * r.v;
+    nw = qw[c] + dt * r.w;
+  } else {
+    nu = (qu[c] + dt * r.u + ou[c]) * 0.5;
+    nv = (qv[c] + dt * r.v + ov[c]) * 0.5;
+    nw = (qw[c] + dt * r.w + ow[c]) * 0.5;
+  }
+  if (FUSE) {
+    store_with_halo(ou, g, i, j, k, nu, BC_CENTRED, 0.0 - u_crf);
+    store_with_halo(ov, g, i, j, k, nv, BC_CENTRED, 0.0);
+    store_with_halo(ow, g, i, j, k, nw, BC_FACE, 0.0);
+  } else {
+    ou[c] = nu;
+    ov[c] = nv;
+    ow[c] = nw;
+  }
+}
+
+// calcRHS, mod_calcRHS.cc:7-33
+__global__ void __launch_bounds__(BX *BY) k_calc_rhs(Geo g, const StepConst *__restrict__ sc,
+                                                     const double *__restrict__ u,
+                                                     const double *__restrict__ v,
+                                                     const double *__restrict__ w,
+                                                     double *__restrict__ rhs) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const double dti = sc->dti, dtidxi = sc->dtidxi, dtidyi = sc->dtidyi;
+  const long long c = g.at(i, j, k);
+  rhs[c] = (u[c] - u[c - 1]) * dtidxi + (v[c] - v[c - g.X]) * dtidyi +
+           (w[c] - w[c - g.XY]) * dti * __ldg(g.dzf_inv + k);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic block and grid reductions
+// ---------------------------------------------------------------------------
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /*NV*32*/) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) smem[q * 32 + wid] = x;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double x = (lane < nw) ? smem[q * 32 + lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      v[q] = x;  // valid in thread 0
+    }
+  }
+  __syncthreads();
+}
+
+// After every block wrote its partial sums, the last block to arrive sums the
+// partials in block order and returns true in thread 0 with the totals.
+template <int NV>
+__device__ bool grid_sum_last(double (&v)[NV], double *partials, unsigned int *counter,
+                              int nblocks, double *smem) {
+  __shared__ bool am_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) partials[q * kMaxBlocksReduce + blockIdx.x] = v[q];
+    __threadfence();
+    const unsigned int t = atomicAdd(counter, 1u);
+    am_last = (t == (unsigned)nblocks - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    acc[q] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+      acc[q] += __ldcg(partials + q * kMaxBlocksReduce + b);
+  }
+  block_sum<NV>(acc, smem);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = acc[q];
+    *counter = 0u;  // ready for the next launch
+  }
+  return threadIdx.x == 0;
+}
+
+__device__ __forceinline__ void interior_coords(const Geo &g, long long t, int &i, int &j,
+                                                int &k) {
+  const long long nxy = (long long)g.nx * g.ny;
+  k = (int)(t / nxy);
+  const long long r = t - (long long)k * nxy;
+  j = (int)(r / g.nx);
+  i = (int)(r - (long long)j * g.nx);
+  ++i;
+  ++j;
+  ++k;
+}
+
+// Mean (mod_utils.cc:30-51): sum(var*dzflzi) / nxg / nyg -> sc->mean[comp]
+__global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, int nxg, int nyg,
+                                              const double *__restrict__ var, double *partials,
+                                              unsigned int *counter) {
+  __shared__ double smem[32];
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  double s[1] = {0.0};
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    interior_coords(g, t, i, j, k);
+    s[0] += var[g.at(i, j, k)] * __ldg(g.dzflzi + k);
+  }
+  block_sum<1>(s, smem);
+  if (grid_sum_last<1>(s, partials, counter, gridDim.x, smem)) {
+    sc->mean[comp] = s[0] / nxg / nyg;
+  }
+}
+
+// correctVel (mod_calcVel.cc:253-278), interior only.
+__global__ void __launch_bounds__(BX *BY) k_correct(Geo g, const StepConst *__restrict__ sc,
+                                                    const double *__restrict__ p, double *u,
+                                                    double *v, double *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const long long c = g.at(i, j, k);
+  const double pc = p[c];
+  u[c] -= (p[c + 1] - pc) * sc->dtdxi;
+  v[c] -= (p[c + g.X] - pc) * sc->dtdyi;
+  w[c] -= (p[c + g.XY] - pc) * sc->dt * __ldg(g.dzc_inv + k);
+}
+
+// Fused correction of the step: correctVel, the halo images of every
+// component that is not forced, and the bulk mean of every forced component
+// (after correction).  The last block turns the means into the forcing values
+// sc->force[d] = vel_force[d] - mean[d] (mod_calcVel.cc:280-301).
+struct ForceCfg {
+  int forced[3];
+  double vel_force[3];
+  double u_crf;
+};
+
+__global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
+                                                       const double *__restrict__ p, double *u,
+                                                       double *v, double *w, double *partials,
+                                                       unsigned int *counter) {
+  __shared__ double smem[3 * 32];
+  const double dtdxi = sc->dtdxi, dtdyi = sc->dtdyi, dt = sc->dt;
+  const int tiles_x = (g.nx + 31) / 32;
+  const int tiles_y = (g.ny + 7) / 8;
+  const long long ntiles = (long long)tiles_x * tiles_y * g.nz;
+  double s[3] = {0.0, 0.0, 0.0};
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int kt = (int)(tile / ((long long)tiles_x * tiles_y));
+    const int r = (int)(tile - (long long)kt * tiles_x * tiles_y);
+    const int jt = r / tiles_x, it = r - jt * tiles_x;
+    const int i = it * 32 + tx + 1, j = jt * 8 + ty + 1, k = kt + 1;
+    if (i > g.nx || j > g.ny) continue;
+    const long long c = g.at(i, j, k);
+    const double pc = p[c];
+    const double nu = u[c] - (p[c + 1] - pc) * dtdxi;
+    const double nv = v[c] - (p[c + g.X] - pc) * dtdyi;
+    const double nw = w[c] - (p[c + g.XY] - pc) * dt * __ldg(g.dzc_inv + k);
+    const double dzl = __ldg(g.dzflzi + k);
+    if (fc.forced[0]) {
+      u[c] = nu;
+      s[0] += nu * dzl;
+    } else {
+      store_with_halo(u, g, i, j, k, nu, BC_CENTRED, 0.0 - fc.u_crf);
+    }
+    if (fc.forced[1]) {
+      v[c] = nv;
+      s[1] += nv * dzl;
+    } else {
+      store_with_halo(v, g, i, j, k, nv, BC_CENTRED, 0.0);
+    }
+    if (fc.forced[2]) {
+      w[c] = nw;
+      s[2] += nw * dzl;
+    } else {
+      store_with_halo(w, g, i, j, k, nw, BC_FACE, 0.0);
+    }
+  }
+  block_sum<3>(s, smem);
+  if (grid_sum_last<3>(s, partials, counter, gridDim.x, smem)) {
+    for (int d = 0; d < 3; ++d) {
+      if (fc.forced[d]) {
+        const double mean = s[d] / g.nx / g.ny;
+        sc->mean[d] = mean;
+        sc->force[d] = fc.vel_force[d] - mean;
+      } else {
+        sc->mean[d] = 0.0;
+        sc->force[d] = 0.0;
+      }
+    }
+  }
+}
+
+// Adds sc->force[d] to the interior of each forced component
+// (mod_calcVel.cc:296-316); with FUSE the halos of those components are
+// refreshed from the new interior values (the final updateBoundVel of
+// main.cc:153).
+template <bool FUSE>
+__global__ void __launch_bounds__(BX *BY) k_force_apply(Geo g, const StepConst *__restrict__ sc,
+                                                        ForceCfg fc, double *u, double *v,
+                                                        double *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const long long c = g.at(i, j, k);
+  double *q[3] = {u, v, w};
+  const int kind[3] = {BC_CENTRED, BC_CENTRED, BC_FACE};
+  const double bc[3] = {0.0 - fc.u_crf, 0.0, 0.0};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (!fc.forced[d]) continue;
+    const double nv = q[d][c] + sc->force[d];
+    if (FUSE)
+      store_with_halo(q[d], g, i, j, k, nv, kind[d], bc[d]);
+    else
+      q[d][c] = nv;
+  }
+}
+
+// Boundary update of the velocity (mod_updateBound.cc:263-285) as one kernel
+// over the interior: every interior point rewrites its own halo images.
+__global__ void __launch_bounds__(BX *BY) k_bound_vel(Geo g, double u_crf, double *u, double *v,
+                                                      double *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  // only points that own an image do any work
+  if (!(i == 1 || i == g.nx || j == 1 || j == g.ny || k == 1 || k == g.nz)) return;
+  const long long c = g.at(i, j, k);
+  store_with_halo(u, g, i, j, k, u[c], BC_CENTRED, 0.0 - u_crf);
+  store_with_halo(v, g, i, j, k, v[c], BC_CENTRED, 0.0);
+  store_with_halo(w, g, i, j, k, w[c], BC_FACE, 0.0);
+}
+
+__global__ void __launch_bounds__(BX *BY) k_bound_p(Geo g, double *p) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  if (!(i == 1 || i == g.nx || j == 1 || j == g.ny || k == 1 || k == g.nz)) return;
+  store_with_halo(p, g, i, j, k, p[g.at(i, j, k)], BC_ZEROGRAD, 0.0);
+}
+
+// var -= delta on the interior (transform2CRF, mod_calcVel.cc:13-25)
+__global__ void k_shift(Geo g, double *var, double delta) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  var[g.at(i, j, k)] -= delta;
+}
+
+// var *= *mult on the interior (bulk rescale of initFlow, mod_initFlow.cc:108-118)
+__global__ void k_scale(Geo g, double *var, const double *mult) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const double m = *mult;
+  var[g.at(i, j, k)] *= m;
+}
+
+// Project noise generator: minstd (48271, 2^31-1) seeded with `seed` and
+// jumped ahead to output number offset+1, mapped to [0,1).
+__device__ __forceinline__ double noise_uniform(int seed, long long offset) {
+  const unsigned long long m = 2147483647ull;
+  unsigned long long x = (unsigned long long)((long long)seed % (long long)m);
+  if (x == 0) x = 1;
+  unsigned long long e = (unsigned long long)offset + 1ull, base = 48271ull, mult = 1ull;
+  while (e) {
+    if (e & 1ull) mult = (mult * base) % m;
+    base = (base * base) % m;
+    e >>= 1;
+  }
+  x = (x * mult) % m;
+  return (double)(x - 1ull) / (double)(m - 1ull);
+}
+
+// initFlow (mod_initFlow.cc:47-106) before the bulk rescale: u = profile(k)
+// plus noise, v and w noise only; halos untouched (zero).
+__global__ void k_init_flow(Geo g, const double *__restrict__ prof, int with_noise, double norm,
+                            double *u, double *v, double *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const long long c = g.at(i, j, k);
+  double uu = prof[k], vv = 0.0, ww = 0.0;
+  if (with_noise) {
+    const long long off = ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
+    // explicit roundings (no contraction) so that the field is bit-identical
+    // to var += 2.0*(x - 0.5)*norm evaluated term by term
+    uu = __dadd_rn(uu, __dmul_rn(__dmul_rn(2.0, __dsub_rn(noise_uniform(123, off), 0.5)), norm));
+    vv = __dadd_rn(vv, __dmul_rn(__dmul_rn(2.0, __dsub_rn(noise_uniform(456, off), 0.5)), norm));
+    ww = __dadd_rn(ww, __dmul_rn(__dmul_rn(2.0, __dsub_rn(noise_uniform(789, off), 0.5)), norm));
+  }
+  u[c] = uu;
+  v[c] = vv;
+  w[c] = ww;
+}
+
+// ---------------------------------------------------------------------------
+// NaN / CFL / divergence check (mod_utils.cc:77-205).  what: bit 0 NaN of u
+// (halos included), bit 1 CFL, bit 2 divergence.  Max with the smallest
+// linear index on ties, i.e. the first maximum of the reference's k,j,i scan.
+// ---------------------------------------------------------------------------
+struct MaxIdx {
+  double v;
+  long long i;
+};
+__device__ __forceinline__ void max_combine(MaxIdx &a, double v, long long i) {
+  if (v > a.v || (v == a.v && i < a.i)) {
+    a.v = v;
+    a.i = i;
+  }
+}
+
+__device__ void block_max(MaxIdx &a, MaxIdx *smem) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_down_sync(0xffffffffu, a.v, o);
+    long long i = __shfl_down_sync(0xffffffffu, a.i, o);
+    max_combine(a, v, i);
+  }
+  if (lane == 0) smem[wid] = a;
+  __syncthreads();
+  if (wid == 0) {
+    MaxIdx b = (lane < nw) ? smem[lane] : MaxIdx{0.0, 0x7fffffffffffffffll};
+    for (int o = 16; o > 0; o >>= 1) {
+      double v = __shfl_down_sync(0xffffffffu, b.v, o);
+      long long i = __shfl_down_sync(0xffffffffu, b.i, o);
+      max_combine(b, v, i);
+    }
+    a = b;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_check(Geo g, int what, const double *__restrict__ u,
+                                               const double *__restrict__ v,
+                                               const double *__restrict__ w, double *partials,
+                                               unsigned int *counter, CheckResult *out) {
+  __shared__ MaxIdx smem[32];
+  __shared__ int nan_s;
+  __shared__ bool am_last;
+  if (threadIdx.x == 0) nan_s = 0;
+  __syncthreads();
+  const long long first = g.at(1, 1, 1);
+  MaxIdx cfl{0.0, first}, div{0.0, first};
+  int nan_found = 0;
+  if (what & 1) {
+    const long long nall = (long long)g.XY * (g.nz + 2);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nall;
+         t += (long long)gridDim.x * blockDim.x)
+      if (isnan(u[t])) nan_found = 1;
+  }
+  if (what & 6) {
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+      int i, j, k;
+      interior_coords(g, t, i, j, k);
+      const long long c = g.at(i, j, k);
+      const double dzfi = __ldg(g.dzf_inv + k);
+      if (what & 2) {
+        const double r = fabs((u[c] + u[c - 1]) * 0.5) * g.dx_inv +
+                         fabs((v[c] + v[c - g.X]) * 0.5) * g.dy_inv +
+                         fabs((w[c] + w[c - g.XY]) * 0.5) * dzfi;
+        max_combine(cfl, r, c);
+      }
+      if (what & 4) {
+        const double d = fabs((u[c] - u[c - 1]) * g.dx_inv + (v[c] - v[c - g.X]) * g.dy_inv +
+                              (w[c] - w[c - g.XY]) * dzfi);
+        max_combine(div, d, c);
+      }
+    }
+  }
+  if (nan_found) atomicOr(&nan_s, 1);
+  block_max(cfl, smem);
+  block_max(div, smem);
+  // partial layout: [0] cfl value, [1] cfl index, [2] div value, [3] div index (as double bits)
+  if (threadIdx.x == 0) {
+    partials[0 * kMaxBlocksReduce + blockIdx.x] = cfl.v;
+    partials[1 * kMaxBlocksReduce + blockIdx.x] = __longlong_as_double(cfl.i);
+    partials[2 * kMaxBlocksReduce + blockIdx.x] = div.v;
+    partials[3 * kMaxBlocksReduce + blockIdx.x] = __longlong_as_double(div.i);
+    if (nan_s) atomicOr(&out->nan_found, 1);
+    __threadfence();
+    const unsigned int t = atomicAdd(counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  MaxIdx c2{0.0, first}, d2{0.0, first};
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    max_combine(c2, __ldcg(partials + b), __double_as_longlong(__ldcg(partials + kMaxBlocksReduce + b)));
+    max_combine(d2, __ldcg(partials + 2 * kMaxBlocksReduce + b),
+                __double_as_longlong(__ldcg(partials + 3 * kMaxBlocksReduce + b)));
+  }
+  block_max(c2, smem);
+  block_max(d2, smem);
+  if (threadIdx.x == 0) {
+    out->cfl = c2.v;
+    out->cfl_idx = c2.i;
+    out->div = d2.v;
+    out->div_idx = d2.i;
+    *counter = 0u;
+  }
+}
+
+inline dim3 interior_grid(const plc_ctx *c) {
+  return dim3((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, c->nz);
+}
+
+inline int reduce_blocks(const plc_ctx *c) {
+  long long n = (long long)c->nx * c->ny * c->nz;
+  long long b = (n + 255) / 256;
+  if (b > 148 * 8) b = 148 * 8;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+inline ForceCfg force_cfg(const plc_ctx *c) {
+  ForceCfg fc;
+  for (int d = 0; d < 3; ++d) {
+    fc.forced[d] = c->prm.is_forced[d] ? 1 : 0;
+    fc.vel_force[d] = c->prm.vel_force[d];
+  }
+  fc.u_crf = c->prm.u_crf;
+  return fc;
+}
+
+}  // namespace
+
+cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const double *qu,
+                      const double *qv, const double *qw, double *ou, double *ov, double *ow,
+                      cudaStream_t s) {
+  const Geo g = c->geo();
+  dim3 grid = interior_grid(c), block(BX, BY);
+  if (stage == 1) {
+    if (fuse_bc)
+      k_rk<1, true><<<grid, block, 0, s>>>(g, c->d_sc, u_crf, qu, qv, qw, ou, ov, ow);
+    else
+      k_rk<1, false><<<grid, block, 0, s>>>(g, c->d_sc, u_crf, qu, qv, qw, ou, ov, ow);
+  } else {
+    if (fuse_bc)
+      k_rk<2, true><<<grid, block, 0, s>>>(g, c->d_sc, u_crf, qu, qv, qw, ou, ov, ow);
+    else
+      k_rk<2, false><<<grid, block, 0, s>>>(g, c->d_sc, u_crf, qu, qv, qw, ou, ov, ow);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v, const double *w,
+                            double *rhs, cudaStream_t s) {
+  k_calc_rhs<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, u, v, w, rhs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p, double *u, double *v,
+                           double *w, cudaStream_t s) {
+  const Geo g = c->geo();
+  if (!fused) {
+    k_correct<<<interior_grid(c), dim3(BX, BY), 0, s>>>(g, c->d_sc, p, u, v, w);
+  } else {
+    long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
+    int nb = (int)(tiles < 148 * 8 ? tiles : 148 * 8);
+    k_correct_fused<<<nb, 256, 0, s>>>(g, c->d_sc, force_cfg(c), p, u, v, w, c->d_partials,
+                                       c->d_counter);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u, double *v, double *w,
+                               cudaStream_t s) {
+  const ForceCfg fc = force_cfg(c);
+  if (!fc.forced[0] && !fc.forced[1] && !fc.forced[2]) return cudaSuccess;
+  if (fuse_bc)
+    k_force_apply<true><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w);
+  else
+    k_force_apply<false><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg, const double *var,
+                        cudaStream_t s) {
+  k_mean<<<reduce_blocks(c), 256, 0, s>>>(c->geo(), c->d_sc, comp, nxg, nyg, var, c->d_partials,
+                                          c->d_counter + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, double *u, double *v, double *w,
+                             cudaStream_t s) {
+  k_bound_vel<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), u_crf, u, v, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bound_p(const plc_ctx *c, double *p, cudaStream_t s) {
+  k_bound_p<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shift(const plc_ctx *c, double *var, double delta, cudaStream_t s) {
+  k_shift<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, delta);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult, cudaStream_t s) {
+  k_scale<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, d_mult);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_check(const plc_ctx *c, const double *u, const double *v, const double *w,
+                         int what, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(c->d_check, 0, sizeof(CheckResult), s);
+  if (e != cudaSuccess) return e;
+  k_check<<<reduce_blocks(c), 256, 0, s>>>(c->geo(), what, u, v, w, c->d_partials,
+                                           c->d_counter + 2, c->d_check);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_flow(const plc_ctx *c, double *u, double *v, double *w,
+                             const double *d_prof, cudaStream_t s) {
+  k_init_flow<<<interior_grid(c), dim3(BX, BY), 0, s>>>(
+      c->geo(), d_prof, c->prm.init_with_noise, c->prm.noise_intensity, u, v, w);
+  return cudaGetLastError();
+}
+
+}  // namespace plc

@@ -1,0 +1,278 @@
+"""GPU parity: every entry point of libplc.so against the CPU oracle on the
+same seeded inputs (FP64).
+
+Tolerances: pure copies / boundary rules are bit-exact; stencils agree to a
+few ulp of the field magnitude (FMA contraction on the GPU); FFT-based
+results agree to 1e-13 relative L2; the 10-step run of the channel agrees to
+1e-12 relative L2 in u, v, w and in p - mean(p) (the reference's p carries an
+arbitrary constant from the singular (0,0) mode).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import case_kwargs, channel_params, demean, interior, random_fields, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(32, 24, 16), (48, 32, 8), (6, 4, 2), (16, 12, 6)]
+
+
+def make_pair(nx, ny, nz, **kw):
+    from powerllel_channel_sycl_b200 import Channel
+    kwargs = case_kwargs(nx, ny, nz, **kw)
+    case = oracle.Case(**kwargs)
+    ch = Channel(channel_params(**kwargs))
+    return case, ch
+
+
+def bc_fields(case, seed):
+    u, v, w = random_fields(case, seed)
+    case.update_bound_vel(u, v, w)
+    return u, v, w
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_mesh_identical(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    for name in ["dzf_global", "dzf", "dzf_inv", "dzc", "dzc_inv", "dzflzi", "zc_global"]:
+        np.testing.assert_array_equal(ch.mesh(name), getattr(case, name))
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_update_bound_vel_exact(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz, u_crf=0.25)
+    u, v, w = random_fields(case, 1)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    case.update_bound_vel(u, v, w)
+    ch.updateBoundVel(0.25)
+    for name, a in zip("uvw", (u, v, w)):
+        np.testing.assert_array_equal(ch.download(name), a)
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_update_bound_p_exact(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    (p,) = random_fields(case, 2, n=1)
+    ch.upload("p", p)
+    case.update_bound_p(p)
+    ch.updateBoundP()
+    np.testing.assert_array_equal(ch.download("p"), p)
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+@pytest.mark.parametrize("u_crf", [0.0, 0.3])
+def test_rk1_rk2(nx, ny, nz, u_crf):
+    case, ch = make_pair(nx, ny, nz, u_crf=u_crf)
+    u, v, w = bc_fields(case, 3)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    u1, v1, w1 = case.zeros(), case.zeros(), case.zeros()
+    case.rk1(u, v, w, u1, v1, w1)
+    ch.timeIntVelRK1(u_crf)
+    for name, a in zip(("u1", "v1", "w1"), (u1, v1, w1)):
+        g = ch.download(name)
+        err = np.abs(interior(g) - interior(a)).max() / np.abs(interior(a)).max()
+        assert err < 1e-14, (name, err)
+    # RK2 from the same u1 (after its boundary update)
+    case.update_bound_vel(u1, v1, w1)
+    for name, a in zip(("u1", "v1", "w1"), (u1, v1, w1)):
+        ch.upload(name, a)
+    case.rk2(u, v, w, u1, v1, w1)
+    ch.timeIntVelRK2(u_crf)
+    for name, a in zip("uvw", (u, v, w)):
+        g = ch.download(name)
+        err = np.abs(interior(g) - interior(a)).max() / np.abs(interior(a)).max()
+        assert err < 1e-14, (name, err)
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_calc_rhs_and_correct(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    u, v, w = bc_fields(case, 4)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    p = case.zeros()
+    case.calc_rhs(u, v, w, p)
+    ch.calcRHS()
+    gp = ch.download("p")
+    assert rel_l2(interior(gp), interior(p)) < 1e-14
+    # correctVel on a random pressure with valid halos
+    (q,) = random_fields(case, 5, n=1)
+    case.update_bound_p(q)
+    ch.upload("p", q)
+    case.correct_vel(q, u, v, w)
+    ch.correctVel()
+    for name, a in zip("uvw", (u, v, w)):
+        g = ch.download(name)
+        assert np.abs(interior(g) - interior(a)).max() <= 4e-16 * np.abs(interior(a)).max(), name
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_mean_and_force(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    u, v, w = bc_fields(case, 6)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    m_ref = case.mean(u)
+    m_gpu = ch.Mean(var="u")
+    assert abs(m_gpu - m_ref) <= 1e-14 * max(1.0, abs(m_ref))
+    f_ref = case.force_vel(u, v, w)
+    f_gpu = ch.forceVel()
+    assert abs(f_gpu[0] - f_ref[0]) <= 1e-14
+    assert f_gpu[1] == 0.0 and f_gpu[2] == 0.0
+    g = ch.download("u")
+    assert np.abs(interior(g) - interior(u)).max() <= 1e-14
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES + [(128, 64, 8), (96, 48, 4), (768, 12, 2), (8, 384, 2)])
+def test_fft_each_direction(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    (p,) = random_fields(case, 7, n=1)
+    ch.upload("p", p)
+    var = np.zeros(nx * ny * nz)
+    case.fft_fwd_x(p, var)
+    ch.execute_fft_fwd_xpen()
+    gs = ch.download("spec").ravel()
+    assert rel_l2(gs, var) < 1e-14
+    case.fft_fwd_y(var)
+    ch.upload("spec", gs.reshape(nz, ny, nx))
+    ch.execute_fft_fwd_ypen()
+    gs = ch.download("spec").ravel()
+    assert rel_l2(gs, var) < 1e-14
+    case.fft_bwd_y(var)
+    ch.upload("spec", gs.reshape(nz, ny, nx))
+    ch.execute_fft_bwd_ypen()
+    gs = ch.download("spec").ravel()
+    assert rel_l2(gs, var) < 1e-14
+    q = case.zeros()
+    case.fft_bwd_x(var, q)
+    ch.upload("spec", gs.reshape(nz, ny, nx))
+    ch.execute_fft_bwd_xpen()
+    gq = ch.download("p")
+    assert rel_l2(interior(gq), interior(q)) < 1e-14
+    # round trip returns the input
+    assert rel_l2(interior(gq), interior(p)) < 1e-13
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES + [(64, 48, 64)])
+def test_trid(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    rng = np.random.default_rng(8)
+    var = rng.standard_normal(nx * ny * nz)
+    # the (0,0) system of the spectral array is singular (Neumann in z): give it
+    # a compatible right-hand side, as a divergence field does
+    v3 = var.reshape(nz, ny, nx)
+    v3[:, 0, 0] -= np.sum(v3[:, 0, 0] * case.dzf[1:-1]) / np.sum(case.dzf[1:-1]) * 0.0
+    ch.upload("spec", v3)
+    ref = var.copy()
+    case.trid(ref)
+    ch.solve_trid()
+    g = ch.download("spec").ravel()
+    r3, g3 = ref.reshape(nz, ny, nx), g.reshape(nz, ny, nx)
+    mask = np.ones((ny, nx), bool)
+    mask[0, 0] = False
+    assert rel_l2(g3[:, mask], r3[:, mask]) < 1e-13
+    # the singular system agrees up to round-off of its (large) constant
+    assert rel_l2(g3[:, 0, 0], r3[:, 0, 0]) < 1e-9
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES + [(128, 64, 64)])
+def test_poisson_solve(nx, ny, nz):
+    case, ch = make_pair(nx, ny, nz)
+    u, v, w = bc_fields(case, 9)
+    p = case.zeros()
+    case.calc_rhs(u, v, w, p)
+    ch.upload("p", p)
+    case.poisson(p)
+    ch.execute_poisson_solver()
+    gp = ch.download("p")
+    assert rel_l2(demean(gp), demean(p)) < 1e-12
+
+
+@pytest.mark.parametrize("field,u_crf", [("poi", 0.0), ("log", 0.0), ("uni", 0.2)])
+def test_init_flow(field, u_crf):
+    from powerllel_channel_sycl_b200 import Channel
+    kwargs = case_kwargs(32, 24, 16, u_crf=u_crf)
+    case = oracle.Case(**kwargs)
+    prm = channel_params(**kwargs)
+    prm.initial_field = {"uni": 0, "poi": 1, "log": 2}[field]
+    prm.u0 = 1.0
+    ch = Channel(prm)
+    ch.initFlow()
+    u, v, w = case.init_flow(field, u0=1.0, noise_intensity=0.1)
+    for name, a in zip("uvw", (u, v, w)):
+        g = ch.download(name)
+        assert np.abs(g - a).max() <= 1e-15 * max(1.0, np.abs(a).max()), name
+
+
+def test_checks():
+    case, ch = make_pair(32, 24, 16)
+    u, v, w = bc_fields(case, 10)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    assert ch.checkNaN("u")
+    cfl = ch.calcMaxCFL()
+    cref = case.max_cfl(u, v, w)
+    assert cfl[1] == cref[1] and abs(cfl[0] - cref[0]) <= 1e-15 * cref[0]
+    div = ch.calcMaxDiv()
+    dref = case.max_div(u, v, w)
+    assert div[1] == dref[1] and abs(div[0] - dref[0]) <= 1e-14 * dref[0]
+    u2 = u.copy()
+    u2[3, 4, 5] = np.nan
+    ch.upload("u", u2)
+    assert not ch.checkNaN("u")
+
+
+@pytest.mark.parametrize("nx,ny,nz,nsteps", [(32, 24, 16, 5), (128, 64, 64, 10)])
+def test_step_parity(nx, ny, nz, nsteps):
+    """main.cc:116-154 for nsteps: fused GPU step vs the oracle loop."""
+    case, ch = make_pair(nx, ny, nz)
+    u, v, w = case.init_flow("poi", noise_intensity=0.1)
+    for name, a in zip("uvw", (u, v, w)):
+        ch.upload(name, a)
+    ch.upload("p", case.zeros())
+    u1, v1, w1, p = case.zeros(), case.zeros(), case.zeros(), case.zeros()
+    case.step(u, v, w, u1, v1, w1, p, nsteps=nsteps)
+    ch.step(nsteps)
+    for name, a in zip("uvw", (u, v, w)):
+        g = ch.download(name)
+        e = rel_l2(g, a)
+        assert e <= 1e-12, (name, e)
+    gp = ch.download("p")
+    assert rel_l2(demean(gp), demean(p)) <= 1e-12
+    div, _ = ch.calcMaxDiv()
+    assert div < 1e-10
+    # bulk velocity held at vel_force by the forcing
+    assert abs(ch.Mean(var="u") - 1.0) < 1e-12
+
+
+def test_step_matches_module_sequence():
+    """The fused graph step equals the reference's call sequence of entry points."""
+    from powerllel_channel_sycl_b200 import Channel
+    kwargs = case_kwargs(48, 32, 16)
+    a = Channel(channel_params(**kwargs))
+    b = Channel(channel_params(**kwargs))
+    a.initFlow()
+    b.initFlow()
+    for _ in range(3):
+        a.step(1)
+        b.timeIntVelRK1()
+        b.updateBoundVel(None, "u1", "v1", "w1")
+        b.timeIntVelRK2()
+        b.updateBoundVel()
+        b.calcRHS()
+        b.execute_poisson_solver()
+        b.updateBoundP()
+        b.correctVel()
+        b.forceVel()
+        b.updateBoundVel()
+    for name in "uvw":
+        assert rel_l2(a.download(name), b.download(name)) < 1e-13
+    assert rel_l2(demean(a.download("p")), demean(b.download("p"))) < 1e-12
+
+
+def test_kernels_per_step():
+    case, ch = make_pair(32, 24, 16)
+    assert ch.kernels_per_step == 9
