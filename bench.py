@@ -42,6 +42,9 @@ WORKLOADS = {
     # Re_tau ~ 550 channel (the headline throughput configuration)
     "re550": dict(nx=768, ny=384, nz=256, lx=2 * math.pi, ly=math.pi, lz=2.0, stretch_ratio=1.8,
                   re=10000.0, dt=1e-3, cfl_target=0.5),
+    # same physics on 512 x 256 x 128 (fields 138 MB, > L2): the ncu capture case
+    "prof": dict(nx=512, ny=256, nz=128, lx=2 * math.pi, ly=math.pi, lz=2.0, stretch_ratio=1.8,
+                 re=10000.0, dt=1e-3, cfl_target=0.5),
     # Re_tau ~ 180 channel, 128 x 64 x 64 (the reference's CPU-runnable case)
     "re180": dict(nx=128, ny=64, nz=64, lx=4 * math.pi, ly=2 * math.pi, lz=2.0, stretch_ratio=1.5,
                   re=2800.0, dt=2e-3, cfl_target=0.0),

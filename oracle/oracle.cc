@@ -36,6 +36,15 @@ struct Idx {
 
 inline Idx make_idx(const orc_grid *g) { return Idx{g->nx + 2, g->ny + 2}; }
 
+// Double-double accumulation: (hi, lo) += x with Knuth's error-free TwoSum.
+inline void two_sum_acc(double &hi, double &lo, double x) {
+  const double s = hi + x;
+  const double bb = s - hi;
+  const double e = (hi - (s - bb)) + (x - bb);
+  hi = s;
+  lo += e;
+}
+
 // ---------------------------------------------------------------------------
 // Mixed-radix complex DFT (recursive decimation in time by the smallest prime
 // factor).  Independent of the GPU implementation, which uses a Stockham
@@ -451,20 +460,31 @@ void orc_correct_vel(const orc_grid *g, const double *p, double *u, double *v,
 
 double orc_mean(const orc_grid *g, int nx_global, int ny_global,
                 const double *var) {
-  // mod_utils.cc:30-51.  The reference sums with sycl::reduction in an
-  // unspecified order; here each z plane is summed in (j,i) order and the
-  // planes are then summed in k order, so the value is deterministic.
+  // mod_utils.cc:30-51.  The reference sums var*dzflzi with sycl::reduction in
+  // an unspecified order.  Here every product var*dzflzi is rounded to double
+  // (as in the reference) and the products are accumulated in double-double
+  // (error-free TwoSum), which makes the rounded total independent of the
+  // summation order; the GPU reduction uses the same accumulation and so
+  // reproduces this value exactly.
   const Idx I = make_idx(g);
-  std::vector<double> plane(g->nz + 2, 0.0);
+  std::vector<double> plane_hi(g->nz + 2, 0.0), plane_lo(g->nz + 2, 0.0);
 #pragma omp parallel for
   for (int k = 1; k <= g->nz; ++k) {
-    double s = 0.0;
+    double hi = 0.0, lo = 0.0;
     for (int j = 1; j <= g->ny; ++j)
-      for (int i = 1; i <= g->nx; ++i) s += var[I(i, j, k)] * g->dzflzi[k];
-    plane[k] = s;
+      for (int i = 1; i <= g->nx; ++i) {
+        const double x = var[I(i, j, k)] * g->dzflzi[k];
+        two_sum_acc(hi, lo, x);
+      }
+    plane_hi[k] = hi;
+    plane_lo[k] = lo;
   }
-  double mean = 0.0;
-  for (int k = 1; k <= g->nz; ++k) mean += plane[k];
+  double hi = 0.0, lo = 0.0;
+  for (int k = 1; k <= g->nz; ++k) {
+    two_sum_acc(hi, lo, plane_hi[k]);
+    lo += plane_lo[k];
+  }
+  const double mean = hi + lo;
   return mean / nx_global / ny_global;
 }
 

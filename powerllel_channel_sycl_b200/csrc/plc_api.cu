@@ -132,7 +132,9 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
   PLC_CUDA(c, cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
   if (need > (size_t)dev_max)
     return set_error(c, PLC_ERR_SIZE, "FFT line too long for shared memory");
-  PLC_CUDA(c, fft_configure(need > 48 * 1024 ? need : 48 * 1024));
+  // the limit is a per-kernel attribute shared by all contexts: raise it to the
+  // device maximum so that no context can lower it under another one
+  PLC_CUDA(c, fft_configure((size_t)dev_max));
   c->poisson_ready = true;
   return PLC_OK;
 }
@@ -347,7 +349,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   // scalars and scratch
   if ((e = cudaMalloc(&c->d_sc, sizeof(StepConst))) != cudaSuccess ||
       (e = cudaMemset(c->d_sc, 0, sizeof(StepConst))) != cudaSuccess ||
-      (e = cudaMalloc(&c->d_partials, 4 * kMaxBlocksReduce * sizeof(double))) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_partials, 8 * kMaxBlocksReduce * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc(&c->d_counter, 8 * sizeof(unsigned int))) != cudaSuccess ||
       (e = cudaMemset(c->d_counter, 0, 8 * sizeof(unsigned int))) != cudaSuccess ||
       (e = cudaMalloc(&c->d_check, sizeof(CheckResult))) != cudaSuccess ||

@@ -218,6 +218,20 @@ __device__ __forceinline__ void pack_pair(double2 *Z, int n, int m, const double
   if (m != 0 && m != (n >> 1)) Z[padi(n - m)] = make_double2(reA + imB, reB - imA);
 }
 
+// div(u)/dt at halo'd index c exactly as calcRHS evaluates it
+// (mod_calcRHS.cc:27-29), every operation rounded separately (no contraction)
+// so that the value is bit-identical to the reference expression.
+__device__ __forceinline__ double div_dt(const double *__restrict__ u,
+                                         const double *__restrict__ v,
+                                         const double *__restrict__ w, long long c, int X,
+                                         long long XY, double dtidxi, double dtidyi, double dti,
+                                         double dzfi) {
+  const double tx = __dmul_rn(__dsub_rn(u[c], u[c - 1]), dtidxi);
+  const double ty = __dmul_rn(__dsub_rn(v[c], v[c - X]), dtidyi);
+  const double tz = __dmul_rn(__dmul_rn(__dsub_rn(w[c], w[c - XY]), dti), dzfi);
+  return __dadd_rn(__dadd_rn(tx, ty), tz);
+}
+
 // Forward x transform: rows (j0+2l, j0+2l+1) of plane k -> packed spectra.
 // FUSED: the rows are div(u)/dt evaluated on the fly (calcRHS).
 template <bool FUSED>
@@ -246,10 +260,8 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, FftDev P, int nl,
     const long long cb = ca + g.X;
     double a, b;
     if (FUSED) {
-      a = (u[ca] - u[ca - 1]) * dtidxi + (v[ca] - v[ca - g.X]) * dtidyi +
-          (w[ca] - w[ca - g.XY]) * dti * dzfi;
-      b = (u[cb] - u[cb - 1]) * dtidxi + (v[cb] - v[cb - g.X]) * dtidyi +
-          (w[cb] - w[cb - g.XY]) * dti * dzfi;
+      a = div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
+      b = div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
     } else {
       a = p[ca];
       b = p[cb];

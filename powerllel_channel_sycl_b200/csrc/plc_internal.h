@@ -76,7 +76,7 @@ struct plc_ctx {
   int fft_lines_x = 1, fft_lines_y = 1;
   // scalars and scratch
   plc::StepConst *d_sc = nullptr;
-  double *d_partials = nullptr;        // 4 * kMaxBlocksReduce
+  double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
   unsigned int *d_counter = nullptr;   // last-block counters
   plc::CheckResult *d_check = nullptr;
   plc::CheckResult *h_check = nullptr;  // pinned

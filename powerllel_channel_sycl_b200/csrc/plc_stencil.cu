@@ -190,39 +190,78 @@ __global__ void __launch_bounds__(BX *BY) k_calc_rhs(Geo g, const StepConst *__r
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic block and grid reductions
+// Order-independent block and grid sums.  Values are accumulated in
+// double-double (Knuth's error-free TwoSum); the rounded total hi + lo is the
+// correctly rounded sum except when the exact sum lies within ~n*2^-106 of a
+// rounding boundary, so it does not depend on the summation order and equals
+// the CPU restatement's value bit for bit.
 // ---------------------------------------------------------------------------
+struct DD {
+  double hi, lo;
+};
+
+__device__ __forceinline__ void dd_add(DD &a, double x) {
+  const double s = a.hi + x;
+  const double bb = s - a.hi;
+  const double e = (a.hi - (s - bb)) + (x - bb);
+  a.hi = s;
+  a.lo += e;
+}
+
+__device__ __forceinline__ void dd_merge(DD &a, double bhi, double blo) {
+  const double s = a.hi + bhi;
+  const double bb = s - a.hi;
+  const double e = (a.hi - (s - bb)) + (bhi - bb);
+  a.hi = s;
+  a.lo = (a.lo + blo) + e;
+}
+
 template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /*NV*32*/) {
+__device__ __forceinline__ void block_sum(DD (&v)[NV], double *smem /*2*NV*32*/) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
-    double x = v[q];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) smem[q * 32 + wid] = x;
+    DD x = v[q];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double h = __shfl_down_sync(0xffffffffu, x.hi, o);
+      const double l = __shfl_down_sync(0xffffffffu, x.lo, o);
+      dd_merge(x, h, l);
+    }
+    if (lane == 0) {
+      smem[(2 * q) * 32 + wid] = x.hi;
+      smem[(2 * q + 1) * 32 + wid] = x.lo;
+    }
   }
   __syncthreads();
   if (wid == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
-      double x = (lane < nw) ? smem[q * 32 + lane] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      DD x{0.0, 0.0};
+      if (lane < nw) x = DD{smem[(2 * q) * 32 + lane], smem[(2 * q + 1) * 32 + lane]};
+      for (int o = 16; o > 0; o >>= 1) {
+        const double h = __shfl_down_sync(0xffffffffu, x.hi, o);
+        const double l = __shfl_down_sync(0xffffffffu, x.lo, o);
+        dd_merge(x, h, l);
+      }
       v[q] = x;  // valid in thread 0
     }
   }
   __syncthreads();
 }
 
-// After every block wrote its partial sums, the last block to arrive sums the
-// partials in block order and returns true in thread 0 with the totals.
+// After every block wrote its partial sums, the last block to arrive merges
+// the partials and returns true in thread 0 with the totals.
 template <int NV>
-__device__ bool grid_sum_last(double (&v)[NV], double *partials, unsigned int *counter,
-                              int nblocks, double *smem) {
+__device__ bool grid_sum_last(DD (&v)[NV], double *partials, unsigned int *counter, int nblocks,
+                              double *smem) {
   __shared__ bool am_last;
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int q = 0; q < NV; ++q) partials[q * kMaxBlocksReduce + blockIdx.x] = v[q];
+    for (int q = 0; q < NV; ++q) {
+      partials[(2 * q) * kMaxBlocksReduce + blockIdx.x] = v[q].hi;
+      partials[(2 * q + 1) * kMaxBlocksReduce + blockIdx.x] = v[q].lo;
+    }
     __threadfence();
     const unsigned int t = atomicAdd(counter, 1u);
     am_last = (t == (unsigned)nblocks - 1);
@@ -230,12 +269,13 @@ __device__ bool grid_sum_last(double (&v)[NV], double *partials, unsigned int *c
   __syncthreads();
   if (!am_last) return false;
   __threadfence();
-  double acc[NV];
+  DD acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
-    acc[q] = 0.0;
+    acc[q] = DD{0.0, 0.0};
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-      acc[q] += __ldcg(partials + q * kMaxBlocksReduce + b);
+      dd_merge(acc[q], __ldcg(partials + (2 * q) * kMaxBlocksReduce + b),
+               __ldcg(partials + (2 * q + 1) * kMaxBlocksReduce + b));
   }
   block_sum<NV>(acc, smem);
   if (threadIdx.x == 0) {
@@ -262,18 +302,19 @@ __device__ __forceinline__ void interior_coords(const Geo &g, long long t, int &
 __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, int nxg, int nyg,
                                               const double *__restrict__ var, double *partials,
                                               unsigned int *counter) {
-  __shared__ double smem[32];
+  __shared__ double smem[2 * 32];
   const long long n = (long long)g.nx * g.ny * g.nz;
-  double s[1] = {0.0};
+  DD s[1] = {{0.0, 0.0}};
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
     interior_coords(g, t, i, j, k);
-    s[0] += var[g.at(i, j, k)] * __ldg(g.dzflzi + k);
+    dd_add(s[0], var[g.at(i, j, k)] * __ldg(g.dzflzi + k));
   }
   block_sum<1>(s, smem);
   if (grid_sum_last<1>(s, partials, counter, gridDim.x, smem)) {
-    sc->mean[comp] = s[0] / nxg / nyg;
+    const double total = s[0].hi + s[0].lo;
+    sc->mean[comp] = total / nxg / nyg;
   }
 }
 
@@ -306,12 +347,12 @@ __global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, For
                                                        const double *__restrict__ p, double *u,
                                                        double *v, double *w, double *partials,
                                                        unsigned int *counter) {
-  __shared__ double smem[3 * 32];
+  __shared__ double smem[2 * 3 * 32];
   const double dtdxi = sc->dtdxi, dtdyi = sc->dtdyi, dt = sc->dt;
   const int tiles_x = (g.nx + 31) / 32;
   const int tiles_y = (g.ny + 7) / 8;
   const long long ntiles = (long long)tiles_x * tiles_y * g.nz;
-  double s[3] = {0.0, 0.0, 0.0};
+  DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int kt = (int)(tile / ((long long)tiles_x * tiles_y));
@@ -327,19 +368,19 @@ __global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, For
     const double dzl = __ldg(g.dzflzi + k);
     if (fc.forced[0]) {
       u[c] = nu;
-      s[0] += nu * dzl;
+      dd_add(s[0], nu * dzl);
     } else {
       store_with_halo(u, g, i, j, k, nu, BC_CENTRED, 0.0 - fc.u_crf);
     }
     if (fc.forced[1]) {
       v[c] = nv;
-      s[1] += nv * dzl;
+      dd_add(s[1], nv * dzl);
     } else {
       store_with_halo(v, g, i, j, k, nv, BC_CENTRED, 0.0);
     }
     if (fc.forced[2]) {
       w[c] = nw;
-      s[2] += nw * dzl;
+      dd_add(s[2], nw * dzl);
     } else {
       store_with_halo(w, g, i, j, k, nw, BC_FACE, 0.0);
     }
@@ -348,7 +389,7 @@ __global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, For
   if (grid_sum_last<3>(s, partials, counter, gridDim.x, smem)) {
     for (int d = 0; d < 3; ++d) {
       if (fc.forced[d]) {
-        const double mean = s[d] / g.nx / g.ny;
+        const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
         sc->mean[d] = mean;
         sc->force[d] = fc.vel_force[d] - mean;
       } else {
