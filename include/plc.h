@@ -273,6 +273,26 @@ int plc_trid_tables(int nx, int ny, int nz, double lx, double ly,
 int plc_host_alloc(size_t bytes, void **ptr);
 int plc_host_free(void *ptr);
 
+/* ---- allocation-free entry point ---- */
+/* No counterpart in the reference.  The bulk mean of plc_mean
+ * (sum(var*dzflzi)/nx_global/ny_global over the interior) for callers that
+ * cannot allocate device memory -- for example a host application that keeps
+ * all GPU memory in its own pool and forbids allocation after start-up, or a
+ * time loop that must not take the implicit device synchronisation of
+ * cudaMalloc/cudaFree -- and that therefore have no plc context.  The caller
+ * passes the halo'd field d_var (nx, ny, nz interior), d_dzflzi (nz+2
+ * entries) and d_mean (one double), all device memory, and a cudaStream_t
+ * (NULL = default stream); the result is written to d_mean on that stream.
+ * Nothing is allocated: the partial sums live in a static 128 KiB array of
+ * the library (one double-double per z plane), held by every GPU that loads
+ * the library until exit, so nz is limited to 8192 (PLC_ERR_SIZE beyond).
+ * All calls share that array: calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's address (once per device); make it
+ * before any stream capture.  Errors: plc_last_error(NULL). */
+int plc_mean_noalloc(const double *d_var, const double *d_dzflzi, int nx, int ny,
+                     int nz, int nx_global, int ny_global, double *d_mean,
+                     void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -127,6 +127,7 @@ _SIGS = {
     "plc_trid_tables": [_int, _int, _int, _dbl, _dbl, _hp, _hp, _hp, _hp],
     "plc_host_alloc": [C.c_size_t, C.POINTER(_vp)],
     "plc_host_free": [_vp],
+    "plc_mean_noalloc": [_dp, _dp, _int, _int, _int, _int, _int, _dp, _vp],
 }
 
 
