@@ -157,6 +157,18 @@ void to_ijk(const plc_ctx *c, long long idx, plc_value_index *out, double value)
   out->ig = (int)(idx % X);
 }
 
+// Reads the error word that kernels with bounded device-side waits raise when
+// a wait gives up (synchronises the stream).
+int device_error(plc_ctx *c) {
+  int flag = 0;
+  PLC_CUDA(c, cudaMemcpyAsync(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (flag)
+    return set_error(c, PLC_ERR_CUDA,
+                     "a device-side wait for a tensor copy timed out (kernel left early)");
+  return PLC_OK;
+}
+
 int run_check(plc_ctx *c, int what, const double *u, const double *v, const double *w) {
   PLC_CUDA(c, launch_check(c, u, v, w, what, c->stream));
   PLC_CUDA(c, cudaMemcpyAsync(c->h_check, c->d_check, sizeof(CheckResult), cudaMemcpyDeviceToHost,
@@ -356,6 +368,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
       (e = cudaMallocHost(&c->h_check, sizeof(CheckResult))) != cudaSuccess ||
       (e = cudaMallocHost(&c->h_scal, 16 * sizeof(double))) != cudaSuccess)
     return fail(cuda_status(c, e, "scratch allocation"));
+  c->d_err = reinterpret_cast<int *>(c->d_counter + 4);  // zeroed with the counters
   if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
   if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
   *out = c;
@@ -385,7 +398,7 @@ const char *plc_last_error(const plc_ctx *c) { return c ? c->err.c_str() : g_err
 int plc_sync(plc_ctx *c) {
   PLC_CHECK_CTX(c);
   PLC_CUDA(c, cudaStreamSynchronize(c->stream));
-  return PLC_OK;
+  return device_error(c);
 }
 
 int plc_get_mesh(const plc_ctx *c, int which, double *h_out) {
@@ -761,7 +774,9 @@ int plc_init_flow(plc_ctx *c) {
 }
 
 // ---- fused time step ------------------------------------------------------
-int plc_step(plc_ctx *c, int nsteps) {
+// nsteps graph launches with the checks of main.cc:156-178 every nt_check
+// steps; the device error word is not read here.
+static int step_launches(plc_ctx *c, int nsteps) {
   PLC_CHECK_CTX(c);
   if (nsteps < 0) return set_error(c, PLC_ERR_ARG, "nsteps < 0");
   PLC_NEED_POISSON(c);
@@ -807,6 +822,11 @@ int plc_step(plc_ctx *c, int nsteps) {
   return PLC_OK;
 }
 
+int plc_step(plc_ctx *c, int nsteps) {
+  if (int rc = step_launches(c, nsteps)) return rc;
+  return device_error(c);
+}
+
 int plc_step_count(plc_ctx *c, long long *count) {
   PLC_CHECK_CTX(c);
   PLC_REQ(c, count);
@@ -825,7 +845,7 @@ int plc_step_timed(plc_ctx *c, int nsteps, double *ms) {
   int rc = PLC_OK;
   cudaError_t e = cudaEventRecord(e0, c->stream);
   if (e == cudaSuccess) {
-    rc = plc_step(c, nsteps);
+    rc = step_launches(c, nsteps);
     e = cudaEventRecord(e1, c->stream);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float f = 0.f;
@@ -836,7 +856,7 @@ int plc_step_timed(plc_ctx *c, int nsteps, double *ms) {
   cudaEventDestroy(e1);
   if (rc != PLC_OK) return rc;
   if (e != cudaSuccess) return cuda_status(c, e, "step timing events");
-  return PLC_OK;
+  return device_error(c);
 }
 
 int plc_get_stream(plc_ctx *c, void **stream) {

@@ -78,6 +78,7 @@ struct plc_ctx {
   plc::StepConst *d_sc = nullptr;
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
   unsigned int *d_counter = nullptr;   // last-block counters
+  int *d_err = nullptr;                // set by a kernel whose bounded wait gave up
   plc::CheckResult *d_check = nullptr;
   plc::CheckResult *h_check = nullptr;  // pinned
   double *h_scal = nullptr;             // pinned scalars

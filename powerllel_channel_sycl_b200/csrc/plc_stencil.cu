@@ -14,6 +14,8 @@
 //   z walls, face w:          w(0) = w(nz) = w(nz+1) = 0;
 //   pressure:                 p(0) = p(1), p(nz+1) = p(nz) (:146-180).
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "plc_device.cuh"
@@ -29,19 +31,32 @@ struct Rhs3 {
   double u, v, w;
 };
 
+// Operand access straight from global memory (read-only path).
+struct GlobalAcc {
+  const double *__restrict__ qu;
+  const double *__restrict__ qv;
+  const double *__restrict__ qw;
+  long long c, X, XY;
+  __device__ __forceinline__ double U(int di, int dj, int dk) const {
+    return __ldg(qu + c + di + dj * X + dk * XY);
+  }
+  __device__ __forceinline__ double V(int di, int dj, int dk) const {
+    return __ldg(qv + c + di + dj * X + dk * XY);
+  }
+  __device__ __forceinline__ double W(int di, int dj, int dk) const {
+    return __ldg(qw + c + di + dj * X + dk * XY);
+  }
+};
+
 // (visc - conv) of the three momentum components at (i,j,k),
-// mod_calcVel.cc:61-125 (the same expression for RK1 and RK2).
-__device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf,
-                                             const double *__restrict__ qu,
-                                             const double *__restrict__ qv,
-                                             const double *__restrict__ qw,
-                                             int i, int j, int k) {
+// mod_calcVel.cc:61-125 (the same expression for RK1 and RK2).  Acc gives the
+// operand values at offsets (di,dj,dk) from the point.
+template <class Acc>
+__device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const Acc &a, int k) {
   const double _dx_inv = g.dx_inv, _dy_inv = g.dy_inv, _re_inv = g.re_inv;
-  const long long X = g.X, XY = g.XY;
-  const long long c = g.at(i, j, k);
-#define U(di, dj, dk) __ldg(qu + c + (di) + (dj) * X + (dk) * XY)
-#define V(di, dj, dk) __ldg(qv + c + (di) + (dj) * X + (dk) * XY)
-#define W(di, dj, dk) __ldg(qw + c + (di) + (dj) * X + (dk) * XY)
+#define U(di, dj, dk) a.U(di, dj, dk)
+#define V(di, dj, dk) a.V(di, dj, dk)
+#define W(di, dj, dk) a.W(di, dj, dk)
   const double dzf_m = __ldg(g.dzf + k - 1), dzf_0 = __ldg(g.dzf + k),
                dzf_p = __ldg(g.dzf + k + 1);
   const double dzfi_0 = __ldg(g.dzf_inv + k), dzfi_p = __ldg(g.dzf_inv + k + 1);
@@ -150,8 +165,8 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
   const int k = blockIdx.z + 1;
   if (i > g.nx || j > g.ny) return;
   const double dt = sc->dt;
-  const Rhs3 r = momentum_rhs(g, u_crf, qu, qv, qw, i, j, k);
   const long long c = g.at(i, j, k);
+  const Rhs3 r = momentum_rhs(g, u_crf, GlobalAcc{qu, qv, qw, c, g.X, g.XY}, k);
   double nu, nv, nw;
   if (STAGE == 1) {
     nu = qu[c] + dt * r.u;
@@ -170,6 +185,199 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
     ou[c] = nu;
     ov[c] = nv;
     ow[c] = nw;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RK stages as z-marching kernels fed by TMA.
+//
+// A block owns a 32 x 8 tile of interior (i, j) columns and a chunk of z
+// planes.  For each operand field the (32+2) x (8+2) halo tile of every plane
+// is brought into a 5-slot shared-memory ring by one 3-D bulk tensor copy
+// (cp.async.bulk.tensor, completion on an mbarrier), two planes ahead of the
+// plane being computed, so every operand value crosses HBM once per block and
+// the copies overlap the arithmetic.  Thread 0 issues the copies and waits on
+// the barriers (bounded: on a timeout it raises *err and the whole block
+// leaves together); the expression trees are those of momentum_rhs, so the
+// results are bit-identical to the global-load kernel above.
+// ---------------------------------------------------------------------------
+constexpr int RX = 32, RY = 8;                  // interior tile
+constexpr int HX = RX + 2, HY = RY + 2;         // halo tile (34 x 10)
+constexpr int PLANE = HX * HY;                  // doubles per field-plane
+constexpr int SLOT = ((PLANE * 8 + 127) / 128) * 128 / 8;  // doubles, 128-B aligned
+constexpr int NSLOT = 5;
+constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 8u;  // three fields per plane
+constexpr long long kWaitLimit = 1ll << 22;            // try_wait polls before giving up
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_plane(double *dst, const CUtensorMap *map, int x, int y,
+                                               int z, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z),
+      "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Operand access from the three plane slots (k-1, k, k+1) of each field: the
+// u slots start at base, the v and w slots NSLOT*SLOT and 2*NSLOT*SLOT later.
+struct SmemAcc {
+  const double *base;
+  int off[3];  // slot offset of planes k-1, k, k+1 plus the thread's point
+  __device__ __forceinline__ double U(int di, int dj, int dk) const {
+    return base[off[dk + 1] + di + dj * HX];
+  }
+  __device__ __forceinline__ double V(int di, int dj, int dk) const {
+    return base[NSLOT * SLOT + off[dk + 1] + di + dj * HX];
+  }
+  __device__ __forceinline__ double W(int di, int dj, int dk) const {
+    return base[2 * NSLOT * SLOT + off[dk + 1] + di + dj * HX];
+  }
+};
+
+size_t rk_tma_smem_bytes() { return (size_t)3 * NSLOT * SLOT * 8 + NSLOT * 8 + 128; }
+
+template <int STAGE, bool FUSE>
+__global__ void __launch_bounds__(RX *RY, 3)
+    k_rk_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
+             const __grid_constant__ CUtensorMap mw, Geo g, const StepConst *__restrict__ sc,
+             double u_crf, double *ou, double *ov, double *ow, int kchunk, int *err) {
+  extern __shared__ unsigned char smem_raw[];
+  double *base = reinterpret_cast<double *>(
+      (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
+  double *slot_u = base, *slot_v = base + NSLOT * SLOT, *slot_w = base + 2 * NSLOT * SLOT;
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(base + 3 * NSLOT * SLOT);
+  __shared__ int ok_s;
+
+  const int tid = threadIdx.x;
+  const int tx = tid & (RX - 1), ty = tid / RX;
+  const int x0 = blockIdx.x * RX, y0 = blockIdx.y * RY;  // halo'd coords of the tile corner
+  const int i = x0 + tx + 1, j = y0 + ty + 1;
+  const bool active = (i <= g.nx) && (j <= g.ny);
+  const int kb = blockIdx.z * kchunk + 1;
+  const int ke = min(kb + kchunk - 1, g.nz);
+  const int plast = ke + 1;  // last plane to bring in
+
+  auto issue = [&](int p) {  // thread 0 only
+    const int rel = p - (kb - 1);
+    const int s = rel % NSLOT;
+    mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
+    tma_load_plane(slot_u + s * SLOT, &mu, x0, y0, p, &bar[s]);
+    tma_load_plane(slot_v + s * SLOT, &mv, x0, y0, p, &bar[s]);
+    tma_load_plane(slot_w + s * SLOT, &mw, x0, y0, p, &bar[s]);
+  };
+  auto wait_plane = [&](int p) -> bool {  // thread 0 only
+    const int rel = p - (kb - 1);
+    const int s = rel % NSLOT;
+    const unsigned parity = (unsigned)((rel / NSLOT) & 1);
+    for (long long it = 0; it < kWaitLimit; ++it)
+      if (mbar_try_wait(&bar[s], parity)) return true;
+    return false;
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < NSLOT; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int p = kb - 1; p <= min(kb + 2, plast); ++p) issue(p);
+  }
+  __syncthreads();
+
+  const double dt = sc->dt;
+  const long long XY = g.XY;
+  long long c = g.at(active ? i : 1, active ? j : 1, kb);
+  double bu = 0.0, bv = 0.0, bw = 0.0;  // RK2 base values (u, v, w) of plane k
+  if (STAGE == 2 && active) {
+    bu = ou[c];
+    bv = ov[c];
+    bw = ow[c];
+  }
+  const int o = (ty + 1) * HX + (tx + 1);
+  for (int k = kb; k <= ke; ++k) {
+    __syncthreads();  // every thread is done with plane k-2's slot
+    if (tid == 0) {
+      bool ok = true;
+      if (k + 3 <= plast) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(k + 3);
+      }
+      if (k == kb) ok = wait_plane(kb - 1) && wait_plane(kb);
+      ok = ok && wait_plane(k + 1);
+      ok_s = ok ? 1 : 0;
+      if (!ok) {
+        atomicExch(err, 1);
+        // give the copies still in flight a bounded chance to land before
+        // the block leaves
+        for (int p = k + 2; p <= min(k + 3, plast); ++p) {
+          const int rel = p - (kb - 1);
+          for (int it = 0; it < (1 << 20); ++it)
+            if (mbar_try_wait(&bar[rel % NSLOT], (unsigned)((rel / NSLOT) & 1))) break;
+        }
+      }
+    }
+    __syncthreads();
+    if (!ok_s) return;  // the whole block leaves together
+    double nbu = 0.0, nbv = 0.0, nbw = 0.0;
+    if (STAGE == 2 && active && k < ke) {
+      nbu = ou[c + XY];
+      nbv = ov[c + XY];
+      nbw = ow[c + XY];
+    }
+    if (active) {
+      const int rm = (k - 1 - (kb - 1)) % NSLOT, r0 = (k - (kb - 1)) % NSLOT,
+                rp = (k + 1 - (kb - 1)) % NSLOT;
+      SmemAcc a;
+      a.base = slot_u;
+      a.off[0] = rm * SLOT + o;
+      a.off[1] = r0 * SLOT + o;
+      a.off[2] = rp * SLOT + o;
+      const Rhs3 r = momentum_rhs(g, u_crf, a, k);
+      const double qu = a.U(0, 0, 0), qv = a.V(0, 0, 0), qw = a.W(0, 0, 0);
+      double nu, nv, nw;
+      if (STAGE == 1) {
+        nu = qu + dt * r.u;
+        nv = qv + dt * r.v;
+        nw = qw + dt * r.w;
+      } else {
+        nu = (qu + dt * r.u + bu) * 0.5;
+        nv = (qv + dt * r.v + bv) * 0.5;
+        nw = (qw + dt * r.w + bw) * 0.5;
+      }
+      if (FUSE) {
+        store_with_halo(ou, g, i, j, k, nu, BC_CENTRED, 0.0 - u_crf);
+        store_with_halo(ov, g, i, j, k, nv, BC_CENTRED, 0.0);
+        store_with_halo(ow, g, i, j, k, nw, BC_FACE, 0.0);
+      } else {
+        ou[c] = nu;
+        ov[c] = nv;
+        ow[c] = nw;
+      }
+    }
+    bu = nbu;
+    bv = nbv;
+    bw = nbw;
+    c += XY;
   }
 }
 
@@ -643,12 +851,65 @@ inline ForceCfg force_cfg(const plc_ctx *c) {
   return fc;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda directly).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of one halo'd field: dims (X, Y, Z), box = one 34 x 10 halo tile
+// of one plane.  Base and strides are multiples of 16 bytes (X is even); the
+// tile's x origin 32*bx is even, i.e. 16-byte aligned.
+bool field_tensor_map(CUtensorMap *m, const double *ptr, const Geo &g) {
+  auto enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<unsigned long long>(ptr) & 15ull)) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)g.X, (cuuint64_t)g.Y, (cuuint64_t)(g.nz + 2)};
+  cuuint64_t strides[2] = {(cuuint64_t)g.X * 8ull, (cuuint64_t)g.XY * 8ull};
+  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)HY, 1u};
+  cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r =
+      enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(ptr), dims, strides, box,
+          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int STAGE, bool FUSE>
+cudaError_t launch_rk_tma(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
+                          const CUtensorMap &mw, double u_crf, double *ou, double *ov, double *ow,
+                          cudaStream_t s) {
+  const int kchunk = c->nz < 32 ? c->nz : 32;
+  dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
+  k_rk_tma<STAGE, FUSE><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
+      mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const double *qu,
                       const double *qv, const double *qw, double *ou, double *ov, double *ow,
                       cudaStream_t s) {
   const Geo g = c->geo();
+  CUtensorMap mu, mv, mw;
+  if (field_tensor_map(&mu, qu, g) && field_tensor_map(&mv, qv, g) &&
+      field_tensor_map(&mw, qw, g)) {
+    if (stage == 1)
+      return fuse_bc ? launch_rk_tma<1, true>(c, mu, mv, mw, u_crf, ou, ov, ow, s)
+                     : launch_rk_tma<1, false>(c, mu, mv, mw, u_crf, ou, ov, ow, s);
+    return fuse_bc ? launch_rk_tma<2, true>(c, mu, mv, mw, u_crf, ou, ov, ow, s)
+                   : launch_rk_tma<2, false>(c, mu, mv, mw, u_crf, ou, ov, ow, s);
+  }
+  // operands not 16-byte aligned: the global-load kernel
   dim3 grid = interior_grid(c), block(BX, BY);
   if (stage == 1) {
     if (fuse_bc)
