@@ -59,15 +59,6 @@ bool fft_length_ok(int n) {
   return n >= 2 && (n % 2 == 0) && host_fft_factor(n, r, &np);
 }
 
-// Largest number of line pairs per block that divides `pairs` and keeps the
-// two shared-memory buffers under `cap` bytes.
-int choose_lines(int n, int pairs, size_t cap) {
-  int best = 1;
-  for (int d = 1; d <= pairs; ++d)
-    if (pairs % d == 0 && fft_smem_bytes(n, d) <= cap) best = d;
-  return best;
-}
-
 int upload_step_consts(plc_ctx *c, double dt) {
   StepConst sc;
   memset(&sc, 0, sizeof sc);
@@ -122,19 +113,13 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
     PLC_CUDA(c, cudaMalloc(&p.tw, tw.size() * sizeof(double)));
     PLC_CUDA(c, cudaMemcpy(p.tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
-  const size_t cap = 64 * 1024;
-  c->fft_lines_x = choose_lines(c->nx, c->ny / 2, cap);
-  c->fft_lines_y = choose_lines(c->ny, c->nx / 2, cap);
-  size_t need = fft_smem_bytes(c->nx, c->fft_lines_x);
-  const size_t need_y = fft_smem_bytes(c->ny, c->fft_lines_y);
-  if (need_y > need) need = need_y;
   int dev_max = 0;
   PLC_CUDA(c, cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-  if (need > (size_t)dev_max)
-    return set_error(c, PLC_ERR_SIZE, "FFT line too long for shared memory");
   // the limit is a per-kernel attribute shared by all contexts: raise it to the
   // device maximum so that no context can lower it under another one
   PLC_CUDA(c, fft_configure((size_t)dev_max));
+  if (fft_setup(c, 76 * 1024, (size_t)dev_max) != cudaSuccess)
+    return set_error(c, PLC_ERR_SIZE, "FFT line too long for shared memory");
   c->poisson_ready = true;
   return PLC_OK;
 }

@@ -15,7 +15,7 @@
 //    (calcRHS fused, mod_calcRHS.cc:23-30).
 //  * y lines pair adjacent packed-x columns i, i+1 and are read and written in
 //    place with x-contiguous row segments: no transpose buffer.
-//  * The complex FFT is a mixed-radix (8, 4, 2, 3) Stockham transform between
+//  * The complex FFT is a mixed-radix (16, 8, 4, 2, 3) Stockham transform between
 //    two shared-memory buffers, one butterfly per thread and pass; element e
 //    of a line lives at e + e/8 to spread the strided accesses over banks.
 //  * Both transforms are unscaled; the backward x transform multiplies by
@@ -38,7 +38,7 @@ namespace {
 
 struct FftDev {
   int n, npass;
-  int radix[16];
+  unsigned long long radices;  // radix - 1, 4 bits per pass, pass 0 in the low bits
   const double2 *tw;
 };
 
@@ -112,6 +112,34 @@ struct Dft<8, INV> {
 };
 
 template <bool INV>
+struct Dft<16, INV> {
+  __device__ __forceinline__ static void run(double2 (&v)[16]) {
+    // radix-2 step over two 8-point transforms: X_k = E_k + W16^k O_k,
+    // X_{k+8} = E_k - W16^k O_k, W16 = exp(-+ 2 pi i / 16)
+    const double c1 = 0.92387953251128675613;  // cos(pi/8)
+    const double s1 = 0.38268343236508977173;  // sin(pi/8)
+    const double h = 0.70710678118654752440;   // 1/sqrt(2)
+    double2 e[8], o[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      e[m] = v[2 * m];
+      o[m] = v[2 * m + 1];
+    }
+    Dft<8, INV>::run(e);
+    Dft<8, INV>::run(o);
+    const double2 w[8] = {make_double2(1.0, 0.0), make_double2(c1, -s1), make_double2(h, -h),
+                          make_double2(s1, -c1),  make_double2(0.0, -1.0), make_double2(-s1, -c1),
+                          make_double2(-h, -h),   make_double2(-c1, -s1)};
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double2 t = INV ? cmulc(o[k], w[k]) : cmul(o[k], w[k]);
+      v[k] = cadd(e[k], t);
+      v[k + 8] = csub(e[k], t);
+    }
+  }
+};
+
+template <bool INV>
 struct Dft<3, INV> {
   __device__ __forceinline__ static void run(double2 (&v)[3]) {
     const double h = 0.86602540378443864676;  // sqrt(3)/2
@@ -161,8 +189,9 @@ template <bool INV>
 __device__ double2 *fft_run(double2 *A, double2 *B, int nl, int LS, const FftDev &P) {
   int Ns = 1;
   for (int p = 0; p < P.npass; ++p) {
-    const int R = P.radix[p];
+    const int R = (int)((P.radices >> (4 * p)) & 15ull) + 1;
     switch (R) {
+      case 16: fft_pass<16, INV>(A, B, nl, P.n, LS, Ns, P.tw); break;
       case 8: fft_pass<8, INV>(A, B, nl, P.n, LS, Ns, P.tw); break;
       case 4: fft_pass<4, INV>(A, B, nl, P.n, LS, Ns, P.tw); break;
       case 2: fft_pass<2, INV>(A, B, nl, P.n, LS, Ns, P.tw); break;
@@ -179,19 +208,20 @@ __device__ double2 *fft_run(double2 *A, double2 *B, int nl, int LS, const FftDev
 
 __host__ __device__ __forceinline__ int line_stride(int n) { return n + (n >> 3) + 1; }
 
-// Packed output q of the two real lines encoded in Z (line of length n):
-// A for the real part sequence, B for the imaginary part sequence.
-__device__ __forceinline__ void unpack_pair(const double2 *Z, int n, int q, double &a, double &b) {
-  const int m = (q == 0) ? 0 : ((q == 1) ? (n >> 1) : (q >> 1));
-  const int part = (q < 2) ? 0 : (q & 1);
-  const double2 zm = Z[padi(m)];
-  const double2 zc = Z[padi(m == 0 ? 0 : n - m)];
-  if (part == 0) {
-    a = (zm.x + zc.x) * 0.5;
-    b = (zm.y + zc.y) * 0.5;
+// The four packed outputs owned by the conjugate pair (m, n-m), 0 <= m < n/2:
+// packed indices q0 = 2m and q1 = 2m+1 (q0 = 0 and q1 = 1 for m = 0, i.e.
+// X_0 and X_{n/2}), for the sequence a (real parts) and b (imaginary parts).
+// A_m = (Z_m + conj Z_{n-m})/2, B_m = (Z_m - conj Z_{n-m})/(2i).
+__device__ __forceinline__ void unpack_four(const double2 *Z, int n, int m, double2 &a,
+                                            double2 &b) {
+  if (m == 0) {
+    const double2 z0 = Z[0], zh = Z[padi(n >> 1)];
+    a = make_double2((z0.x + z0.x) * 0.5, (zh.x + zh.x) * 0.5);
+    b = make_double2((z0.y + z0.y) * 0.5, (zh.y + zh.y) * 0.5);
   } else {
-    a = (zm.y - zc.y) * 0.5;
-    b = (zc.x - zm.x) * 0.5;
+    const double2 zm = Z[padi(m)], zc = Z[padi(n - m)];
+    a = make_double2((zm.x + zc.x) * 0.5, (zm.y - zc.y) * 0.5);
+    b = make_double2((zm.y + zc.y) * 0.5, (zc.x - zm.x) * 0.5);
   }
 }
 
@@ -232,10 +262,11 @@ __device__ __forceinline__ double div_dt(const double *__restrict__ u,
   return __dadd_rn(__dadd_rn(tx, ty), tz);
 }
 
-// Forward x transform: rows (j0+2l, j0+2l+1) of plane k -> packed spectra.
-// FUSED: the rows are div(u)/dt evaluated on the fly (calcRHS).
+// Forward x transform fused with calcRHS, one tile per block: rows
+// (j0+2l, j0+2l+1) of plane k are div(u)/dt evaluated from global memory while
+// loading (many resident blocks hide the load latency), then transformed.
 template <bool FUSED>
-__global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, FftDev P, int nl,
+__global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
                                                    const StepConst *__restrict__ sc,
                                                    const double *__restrict__ p,
                                                    const double *__restrict__ u,
@@ -270,93 +301,190 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd(Geo g, FftDev P, int nl,
   }
   __syncthreads();
   const double2 *Z = fft_run<false>(A, B, nl, LS, P);
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int l = e / n, q = e - l * n;
-    double a, b;
-    unpack_pair(Z + l * LS, n, q, a, b);
+  const int half = n >> 1;
+  for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
+    const int l = e / half, m = e - l * half;
+    double2 a, b;
+    unpack_four(Z + l * LS, n, m, a, b);
     const long long row = (long long)k * g.ny + j0 + 2 * l;
-    var[row * n + q] = a;
-    var[(row + 1) * n + q] = b;
+    reinterpret_cast<double2 *>(var + row * n)[m] = a;
+    reinterpret_cast<double2 *>(var + (row + 1) * n)[m] = b;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent transform kernels.  Each block takes tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the raw rows of the next tile are copied into
+// a staging buffer S with cp.async (16-byte chunks, L2 only) as soon as the
+// current tile has been packed into the FFT buffers, so the copy overlaps the
+// radix passes and the stores of the current tile.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<unsigned>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Copies `rows` rows of `len` doubles (len even, 16-byte aligned rows) from
+// src (row stride `stride` doubles) to dst (row stride `len`).
+__device__ __forceinline__ void stage_rows(double *dst, const double *src, int rows, int len,
+                                           long long stride) {
+  const int cpr = len >> 1;  // 16-byte chunks per row
+  for (int e = threadIdx.x; e < rows * cpr; e += blockDim.x) {
+    const int r = e / cpr, ch = e - r * cpr;
+    cp_async16(dst + r * len + 2 * ch, src + r * stride + 2 * ch);
+  }
+}
+
+// Forward x transform (persistent): rows (j0+2l, j0+2l+1) of p at plane k ->
+// packed spectra.  The halo'd rows are staged whole (16-byte aligned).
+__global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
+                                                   const double *__restrict__ p,
+                                                   double *__restrict__ var) {
+  extern __shared__ double2 smem[];
+  const int n = g.nx, LS = line_stride(n), X = g.X, R = 2 * nl;
+  double2 *A = smem, *B = smem + nl * LS;
+  double *S = reinterpret_cast<double *>(B + nl * LS);  // R halo'd rows
+  const int tiles_y = g.ny / R;
+  const int ntiles = tiles_y * g.nz;
+  auto issue = [&](int tile) {
+    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;  // 0-based
+    stage_rows(S, p + g.at(0, j0 + 1, k + 1), R, X, X);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile);
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
+    cp_async_wait_all();
+    __syncthreads();
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int l = e / n, t = e - l * n;
+      A[l * LS + padi(t)] = make_double2(S[(2 * l) * X + t + 1], S[(2 * l + 1) * X + t + 1]);
+    }
+    __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    const double2 *Z = fft_run<false>(A, B, nl, LS, P);
+    const int half = n >> 1;
+    for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
+      const int l = e / half, m = e - l * half;
+      double2 a, b;
+      unpack_four(Z + l * LS, n, m, a, b);
+      const long long row = (long long)k * g.ny + j0 + 2 * l;
+      reinterpret_cast<double2 *>(var + row * n)[m] = a;
+      reinterpret_cast<double2 *>(var + (row + 1) * n)[m] = b;
+    }
   }
 }
 
 // Backward x transform: packed spectra -> p interior scaled by nf; with
 // FUSE_BC the pressure halos are written as well (updateBoundP).
 template <bool FUSE_BC>
-__global__ void __launch_bounds__(256) k_fft_x_bwd(Geo g, FftDev P, int nl, double nf,
+__global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, double nf,
                                                    const double *__restrict__ var, double *p) {
   extern __shared__ double2 smem[];
-  const int n = g.nx, LS = line_stride(n);
+  const int n = g.nx, LS = line_stride(n), R = 2 * nl;
   double2 *A = smem, *B = smem + nl * LS;
-  double *raw = reinterpret_cast<double *>(B);  // 2*nl rows of n doubles
-  const int j0 = blockIdx.x * 2 * nl;
-  const int k = blockIdx.y;
-  const double *src = var + ((long long)k * g.ny + j0) * n;
-  for (int e = threadIdx.x; e < 2 * nl * n; e += blockDim.x) raw[e] = src[e];
-  __syncthreads();
+  double *S = reinterpret_cast<double *>(B + nl * LS);  // R rows of n doubles
+  const int tiles_y = g.ny / R;
+  const int ntiles = tiles_y * g.nz;
+  auto issue = [&](int tile) {
+    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
+    stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile);
   const int half = n >> 1;
-  for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
-    const int l = e / (half + 1), m = e - l * (half + 1);
-    pack_pair(A + l * LS, n, m, raw + (2 * l) * n, raw + (2 * l + 1) * n, 1);
-  }
-  __syncthreads();
-  const double2 *Z = fft_run<true>(A, B, nl, LS, P);
-  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
-    const int l = e / n, t = e - l * n;
-    const double2 z = Z[l * LS + padi(t)];
-    const double a = nf * z.x, b = nf * z.y;
-    const int i = t + 1, ja = j0 + 2 * l + 1, kk = k + 1;
-    if (FUSE_BC) {
-      store_with_halo(p, g, i, ja, kk, a, BC_ZEROGRAD, 0.0);
-      store_with_halo(p, g, i, ja + 1, kk, b, BC_ZEROGRAD, 0.0);
-    } else {
-      const long long ca = g.at(i, ja, kk);
-      p[ca] = a;
-      p[ca + g.X] = b;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
+    cp_async_wait_all();
+    __syncthreads();
+    for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
+      const int l = e / (half + 1), m = e - l * (half + 1);
+      pack_pair(A + l * LS, n, m, S + (2 * l) * n, S + (2 * l + 1) * n, 1);
+    }
+    __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    const double2 *Z = fft_run<true>(A, B, nl, LS, P);
+    for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+      const int l = e / n, t = e - l * n;
+      const double2 z = Z[l * LS + padi(t)];
+      const double a = nf * z.x, b = nf * z.y;
+      const int i = t + 1, ja = j0 + 2 * l + 1, kk = k + 1;
+      if (FUSE_BC) {
+        store_with_halo(p, g, i, ja, kk, a, BC_ZEROGRAD, 0.0);
+        store_with_halo(p, g, i, ja + 1, kk, b, BC_ZEROGRAD, 0.0);
+      } else {
+        const long long ca = g.at(i, ja, kk);
+        p[ca] = a;
+        p[ca + g.X] = b;
+      }
     }
   }
 }
 
-// y transform in place on the spectral array: columns i0..i0+2nl-1 of plane k.
+// y transform in place on the spectral array: tile = columns i0..i0+2nl-1 of
+// plane k (TX = 2nl x-contiguous doubles per row, row stride nx).
 template <bool INV>
-__global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, FftDev P, int nl,
+__global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P, int nl,
                                                double *__restrict__ var) {
   extern __shared__ double2 smem[];
   const int n = ny, LS = line_stride(n), TX = 2 * nl;
   double2 *A = smem, *B = smem + nl * LS;
-  const int i0 = blockIdx.x * TX;
-  double *plane = var + (long long)blockIdx.y * nx * ny + i0;
-  if (!INV) {
-    for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-      const int t = e / TX, c = e - t * TX;
-      reinterpret_cast<double *>(A + (c >> 1) * LS + padi(t))[c & 1] = plane[(long long)t * nx + c];
+  double *S = reinterpret_cast<double *>(B + nl * LS);  // n rows of TX doubles
+  const int tiles_x = nx / TX;
+  const int ntiles = tiles_x * nz;
+  auto issue = [&](int tile) {
+    const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
+    stage_rows(S, var + (long long)k * nx * ny + i0, n, TX, nx);
+    cp_async_commit();
+  };
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile);
+  const int half = n >> 1;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
+    double *plane = var + (long long)k * nx * ny + i0;
+    cp_async_wait_all();
+    __syncthreads();
+    if (!INV) {
+      for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
+        const int t = e / TX, c = e - t * TX;
+        reinterpret_cast<double *>(A + (c >> 1) * LS + padi(t))[c & 1] = S[e];
+      }
+    } else {
+      for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
+        const int l = e / (half + 1), m = e - l * (half + 1);
+        pack_pair(A + l * LS, n, m, S + 2 * l, S + 2 * l + 1, TX);
+      }
     }
     __syncthreads();
-    const double2 *Z = fft_run<false>(A, B, nl, LS, P);
-    for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-      const int q = e / TX, c = e - q * TX;
-      double a, b;
-      unpack_pair(Z + (c >> 1) * LS, n, q, a, b);
-      plane[(long long)q * nx + c] = (c & 1) ? b : a;
-    }
-  } else {
-    double *raw = reinterpret_cast<double *>(B);  // n rows of TX doubles
-    for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-      const int t = e / TX, c = e - t * TX;
-      raw[e] = plane[(long long)t * nx + c];
-    }
-    __syncthreads();
-    const int half = n >> 1;
-    for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
-      const int l = e / (half + 1), m = e - l * (half + 1);
-      pack_pair(A + l * LS, n, m, raw + 2 * l, raw + 2 * l + 1, TX);
-    }
-    __syncthreads();
-    const double2 *Z = fft_run<true>(A, B, nl, LS, P);
-    for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-      const int t = e / TX, c = e - t * TX;
-      const double2 z = Z[(c >> 1) * LS + padi(t)];
-      plane[(long long)t * nx + c] = (c & 1) ? z.y : z.x;
+    if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    const double2 *Z = fft_run<INV>(A, B, nl, LS, P);
+    if (!INV) {
+      for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
+        const int m = e / nl, l = e - m * nl;
+        double2 a, b;
+        unpack_four(Z + l * LS, n, m, a, b);
+        const int q0 = (m == 0) ? 0 : 2 * m;
+        // row q0: (A, B) of columns 2l, 2l+1; row q0+1 likewise
+        reinterpret_cast<double2 *>(plane + (long long)q0 * nx)[l] = make_double2(a.x, b.x);
+        reinterpret_cast<double2 *>(plane + (long long)(q0 + 1) * nx)[l] = make_double2(a.y, b.y);
+      }
+    } else {
+      for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
+        const int t = e / TX, c = e - t * TX;
+        const double2 z = Z[(c >> 1) * LS + padi(t)];
+        plane[(long long)t * nx + c] = (c & 1) ? z.y : z.x;
+      }
     }
   }
 }
@@ -401,7 +529,8 @@ FftDev dev_plan(const FftPlan &p) {
   FftDev d;
   d.n = p.n;
   d.npass = p.npass;
-  for (int r = 0; r < 16; ++r) d.radix[r] = p.radix[r];
+  d.radices = 0ull;
+  for (int r = 0; r < p.npass; ++r) d.radices |= (unsigned long long)(p.radix[r] - 1) << (4 * r);
   d.tw = p.tw;
   return d;
 }
@@ -412,14 +541,46 @@ size_t fft_smem_bytes(int n, int lines) {
   return 2ull * (size_t)lines * (size_t)line_stride(n) * sizeof(double2);
 }
 
+namespace {
+size_t smem_x_fwd(int nx, int nl) {
+  return fft_smem_bytes(nx, nl) + (size_t)2 * nl * (nx + 2) * sizeof(double);
+}
+size_t smem_x_bwd(int nx, int nl) {
+  return fft_smem_bytes(nx, nl) + (size_t)2 * nl * nx * sizeof(double);
+}
+size_t smem_y(int ny, int nl) {
+  return fft_smem_bytes(ny, nl) + (size_t)ny * 2 * nl * sizeof(double);
+}
+// Largest number of line pairs per tile that divides `pairs` and keeps the
+// kernel's shared memory under `cap` bytes.
+template <class F>
+int pick_lines(int pairs, size_t cap, F bytes) {
+  int best = 1;
+  for (int d = 1; d <= pairs && d <= 16; ++d)
+    if (pairs % d == 0 && bytes(d) <= cap) best = d;
+  return best;
+}
+template <class K>
+int persistent_grid(K kernel, int threads, size_t smem, int sms, long long ntiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  long long g = (long long)per_sm * sms;
+  if (g > ntiles) g = ntiles;
+  return (int)(g < 1 ? 1 : g);
+}
+}  // namespace
+
 // Raises the dynamic shared-memory limit of every FFT kernel (once per process).
 cudaError_t fft_configure(size_t max_bytes) {
   cudaError_t e;
 #define PLC_SMEM(kern)                                                                    \
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes); \
   if (e != cudaSuccess) return e;
-  PLC_SMEM(k_fft_x_fwd<true>);
-  PLC_SMEM(k_fft_x_fwd<false>);
+  PLC_SMEM(k_fft_x_fwd);
+  PLC_SMEM(k_fft_x_fwd_div<true>);
   PLC_SMEM(k_fft_x_bwd<true>);
   PLC_SMEM(k_fft_x_bwd<false>);
   PLC_SMEM(k_fft_y<true>);
@@ -428,41 +589,62 @@ cudaError_t fft_configure(size_t max_bytes) {
   return cudaSuccess;
 }
 
+// Tile sizes (line pairs per tile) and persistent grid sizes of the
+// transforms, from the shared memory each needs and the occupancy it gets.
+cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max) {
+  int sms = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e != cudaSuccess) return e;
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  c->fft_lines_x = pick_lines(ny / 2, smem_cap_per_block, [&](int d) { return smem_x_bwd(nx, d); });
+  c->fft_lines_xf = pick_lines(ny / 2, 64 * 1024, [&](int d) { return fft_smem_bytes(nx, d); });
+  c->fft_lines_y = pick_lines(nx / 2, smem_cap_per_block, [&](int d) { return smem_y(ny, d); });
+  const size_t need[4] = {smem_x_fwd(nx, c->fft_lines_x), fft_smem_bytes(nx, c->fft_lines_xf),
+                          smem_x_bwd(nx, c->fft_lines_x), smem_y(ny, c->fft_lines_y)};
+  for (size_t b : need)
+    if (b > dev_max) return cudaErrorInvalidValue;
+  const long long tiles_x = (long long)(ny / (2 * c->fft_lines_x)) * nz;
+  const long long tiles_y = (long long)(nx / (2 * c->fft_lines_y)) * nz;
+  c->grid_xf = persistent_grid(k_fft_x_fwd, 128, need[0], sms, tiles_x);
+  c->grid_xb = persistent_grid(k_fft_x_bwd<true>, 128, need[2], sms, tiles_x);
+  c->grid_y = persistent_grid(k_fft_y<false>, 256, need[3], sms, tiles_y);
+  return cudaSuccess;
+}
+
 cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u, const double *v,
                              const double *w, double *var, cudaStream_t s) {
-  const int nl = c->fft_lines_x;
-  dim3 grid(c->ny / (2 * nl), c->nz);
-  const size_t sm = fft_smem_bytes(c->nx, nl);
-  if (p)
-    k_fft_x_fwd<false><<<grid, 256, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, c->d_sc, p,
-                                              nullptr, nullptr, nullptr, var);
-  else
-    k_fft_x_fwd<true><<<grid, 256, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, c->d_sc, nullptr,
-                                             u, v, w, var);
+  if (p) {
+    const int nl = c->fft_lines_x;
+    k_fft_x_fwd<<<c->grid_xf, 128, smem_x_fwd(c->nx, nl), s>>>(c->geo(), dev_plan(c->plan_x), nl,
+                                                                p, var);
+  } else {
+    const int nl = c->fft_lines_xf;
+    dim3 grid(c->ny / (2 * nl), c->nz);
+    k_fft_x_fwd_div<true><<<grid, 256, fft_smem_bytes(c->nx, nl), s>>>(
+        c->geo(), dev_plan(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p, bool fuse_bc,
                              cudaStream_t s) {
   const int nl = c->fft_lines_x;
-  dim3 grid(c->ny / (2 * nl), c->nz);
-  const size_t sm = fft_smem_bytes(c->nx, nl);
+  const size_t sm = smem_x_bwd(c->nx, nl);
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
   if (fuse_bc)
-    k_fft_x_bwd<true><<<grid, 256, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
+    k_fft_x_bwd<true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
   else
-    k_fft_x_bwd<false><<<grid, 256, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
+    k_fft_x_bwd<false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse, cudaStream_t s) {
   const int nl = c->fft_lines_y;
-  dim3 grid(c->nx / (2 * nl), c->nz);
-  const size_t sm = fft_smem_bytes(c->ny, nl);
+  const size_t sm = smem_y(c->ny, nl);
   if (inverse)
-    k_fft_y<true><<<grid, 256, sm, s>>>(c->nx, c->ny, dev_plan(c->plan_y), nl, var);
+    k_fft_y<true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl, var);
   else
-    k_fft_y<false><<<grid, 256, sm, s>>>(c->nx, c->ny, dev_plan(c->plan_y), nl, var);
+    k_fft_y<false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl, var);
   return cudaGetLastError();
 }
 

@@ -144,7 +144,7 @@ void host_twiddles(int n, std::vector<double> &re_im) {
   }
 }
 
-// Radix sequence for a complex FFT of length n = 2^a 3^b (radices 8, 4, 2, 3).
+// Radix sequence for a complex FFT of length n = 2^a 3^b (radices 16, 8, 4, 2, 3).
 bool host_fft_factor(int n, int *radix, int *npass) {
   if (n < 1) return false;
   int m = n, a = 0, b = 0;
@@ -152,7 +152,8 @@ bool host_fft_factor(int n, int *radix, int *npass) {
   while (m % 3 == 0) { m /= 3; ++b; }
   if (m != 1) return false;
   int p = 0;
-  while (a >= 3) { radix[p++] = 8; a -= 3; }
+  while (a >= 4) { radix[p++] = 16; a -= 4; }
+  if (a == 3) radix[p++] = 8;
   if (a == 2) radix[p++] = 4;
   if (a == 1) radix[p++] = 2;
   while (b-- > 0) radix[p++] = 3;

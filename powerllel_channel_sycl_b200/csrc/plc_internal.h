@@ -73,7 +73,8 @@ struct plc_ctx {
   double *d_rpiv = nullptr;   // 1/b, (nz, ny/2+1, nx/2+1)
   double *d_ac = nullptr;     // a[nz] | c[nz]
   plc::FftPlan plan_x, plan_y;
-  int fft_lines_x = 1, fft_lines_y = 1;
+  int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
+  int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids
   // scalars and scratch
   plc::StepConst *d_sc = nullptr;
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
@@ -159,5 +160,6 @@ cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult,
                          cudaStream_t s);
 size_t fft_smem_bytes(int n, int lines);
 cudaError_t fft_configure(size_t max_bytes);
+cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);
 
 }  // namespace plc
