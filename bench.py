@@ -284,7 +284,7 @@ def run_ours(args, wl, rank, world, local, pg):
     barrier(pg, local)
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
-    ok, cfl, div = ch.last_check()
+    ok, cfl, div = ch.check()  # NaN / CFL / divergence of the state after the timed steps
 
     # per-kernel device times of the same fused kernels (plain launches with
     # CUDA events between them on the library's stream)

@@ -354,6 +354,9 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
       (e = cudaMallocHost(&c->h_scal, 16 * sizeof(double))) != cudaSuccess)
     return fail(cuda_status(c, e, "scratch allocation"));
   c->d_err = reinterpret_cast<int *>(c->d_counter + 4);  // zeroed with the counters
+  if ((e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) !=
+      cudaSuccess)
+    return fail(cuda_status(c, e, "cudaDeviceGetAttribute"));
   if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
   if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
   *out = c;

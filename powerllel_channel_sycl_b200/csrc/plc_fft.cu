@@ -507,21 +507,79 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
   const long long PS = (long long)MX * ((ny >> 1) + 1);
   const double *rp = rpiv + (long long)my * MX + mx;
   double *q = var + t;
+  // The sweeps are sequential in k, but their loads are not: batches of PF
+  // planes of the right-hand side and of the pivots are loaded one batch
+  // ahead of the elimination, so 2*PF loads per thread are in flight.
+  constexpr int PF = 8;
   double prev = q[0];
-#pragma unroll 4
-  for (int k = 1; k < nz; ++k) {
-    double cur = q[k * plane];
-    cur -= (__ldg(a + k) * __ldg(rp + (k - 1) * PS)) * prev;
-    q[k * plane] = cur;
-    prev = cur;
+  {
+    // forward elimination over k = 1 .. nz-1
+    double xn[PF], rn[PF];
+    int k = 1;
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (k + s < nz) {
+        xn[s] = q[(long long)(k + s) * plane];
+        rn[s] = __ldg(rp + (long long)(k + s - 1) * PS);
+      }
+    for (; k < nz; k += PF) {
+      double x[PF], r[PF];
+#pragma unroll
+      for (int s = 0; s < PF; ++s) {
+        x[s] = xn[s];
+        r[s] = rn[s];
+      }
+      const int kn = k + PF;
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (kn + s < nz) {
+          xn[s] = q[(long long)(kn + s) * plane];
+          rn[s] = __ldg(rp + (long long)(kn + s - 1) * PS);
+        }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k + s < nz) {
+          double cur = x[s];
+          cur -= (__ldg(a + k + s) * r[s]) * prev;
+          q[(long long)(k + s) * plane] = cur;
+          prev = cur;
+        }
+    }
   }
-  prev *= __ldg(rp + (nz - 1) * PS);
-  q[(nz - 1) * plane] = prev;
-#pragma unroll 4
-  for (int k = nz - 2; k >= 0; --k) {
-    const double cur = (q[k * plane] - __ldg(c + k) * prev) * __ldg(rp + k * PS);
-    q[k * plane] = cur;
-    prev = cur;
+  prev *= __ldg(rp + (long long)(nz - 1) * PS);
+  q[(long long)(nz - 1) * plane] = prev;
+  {
+    // back substitution over k = nz-2 .. 0
+    double xn[PF], rn[PF];
+    int k = nz - 2;
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (k - s >= 0) {
+        xn[s] = q[(long long)(k - s) * plane];
+        rn[s] = __ldg(rp + (long long)(k - s) * PS);
+      }
+    for (; k >= 0; k -= PF) {
+      double x[PF], r[PF];
+#pragma unroll
+      for (int s = 0; s < PF; ++s) {
+        x[s] = xn[s];
+        r[s] = rn[s];
+      }
+      const int kn = k - PF;
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (kn - s >= 0) {
+          xn[s] = q[(long long)(kn - s) * plane];
+          rn[s] = __ldg(rp + (long long)(kn - s) * PS);
+        }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k - s >= 0) {
+          const double cur = (x[s] - __ldg(c + k - s) * prev) * r[s];
+          q[(long long)(k - s) * plane] = cur;
+          prev = cur;
+        }
+    }
   }
 }
 

@@ -52,6 +52,7 @@ struct FftPlan {
   double2 *tw = nullptr;  // device, n entries: exp(-2 pi i t / n)
 };
 
+// capacity (blocks) of each plane of the reduction partials array
 constexpr int kMaxBlocksReduce = 4096;
 
 }  // namespace plc
@@ -80,6 +81,7 @@ struct plc_ctx {
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
   unsigned int *d_counter = nullptr;   // last-block counters
   int *d_err = nullptr;                // set by a kernel whose bounded wait gave up
+  int num_sms = 148;
   plc::CheckResult *d_check = nullptr;
   plc::CheckResult *h_check = nullptr;  // pinned
   double *h_scal = nullptr;             // pinned scalars

@@ -462,13 +462,13 @@ __device__ __forceinline__ void block_sum(DD (&v)[NV], double *smem /*2*NV*32*/)
 // the partials and returns true in thread 0 with the totals.
 template <int NV>
 __device__ bool grid_sum_last(DD (&v)[NV], double *partials, unsigned int *counter, int nblocks,
-                              double *smem) {
+                              int blin, double *smem) {
   __shared__ bool am_last;
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
-      partials[(2 * q) * kMaxBlocksReduce + blockIdx.x] = v[q].hi;
-      partials[(2 * q + 1) * kMaxBlocksReduce + blockIdx.x] = v[q].lo;
+      partials[(2 * q) * kMaxBlocksReduce + blin] = v[q].hi;
+      partials[(2 * q + 1) * kMaxBlocksReduce + blin] = v[q].lo;
     }
     __threadfence();
     const unsigned int t = atomicAdd(counter, 1u);
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, in
     dd_add(s[0], var[g.at(i, j, k)] * __ldg(g.dzflzi + k));
   }
   block_sum<1>(s, smem);
-  if (grid_sum_last<1>(s, partials, counter, gridDim.x, smem)) {
+  if (grid_sum_last<1>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
     const double total = s[0].hi + s[0].lo;
     sc->mean[comp] = total / nxg / nyg;
   }
@@ -551,50 +551,96 @@ struct ForceCfg {
   double u_crf;
 };
 
-__global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
-                                                       const double *__restrict__ p, double *u,
-                                                       double *v, double *w, double *partials,
-                                                       unsigned int *counter) {
+// One wave of persistent blocks (grid-stride over 32 x 8 tiles of the
+// interior, plane by plane); each thread keeps the loads of its next tile in
+// flight while it finishes the current one, and the block reduces once at the
+// end (a reduction tail per short-lived block would cost more than the
+// correction itself).
+struct CorrIn {
+  double pc, px, py, pz, u, v, w;
+};
+
+__device__ __forceinline__ bool tile_point(const Geo &g, long long tile, int tiles_x, int tiles_y,
+                                           int &i, int &j, int &k) {
+  const long long per_plane = (long long)tiles_x * tiles_y;
+  k = (int)(tile / per_plane);
+  const int r = (int)(tile - (long long)k * per_plane);
+  const int jt = r / tiles_x, it = r - jt * tiles_x;
+  i = it * 32 + (threadIdx.x & 31) + 1;
+  j = jt * 8 + (threadIdx.x >> 5) + 1;
+  ++k;
+  return i <= g.nx && j <= g.ny;
+}
+
+__device__ __forceinline__ CorrIn corr_load(const Geo &g, const double *__restrict__ p,
+                                            const double *u, const double *v, const double *w,
+                                            long long c) {
+  CorrIn x;
+  x.pc = p[c];
+  x.px = p[c + 1];
+  x.py = p[c + g.X];
+  x.pz = p[c + g.XY];
+  x.u = u[c];
+  x.v = v[c];
+  x.w = w[c];
+  return x;
+}
+
+__global__ void __launch_bounds__(256, 4) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
+                                                          const double *__restrict__ p, double *u,
+                                                          double *v, double *w, double *partials,
+                                                          unsigned int *counter) {
   __shared__ double smem[2 * 3 * 32];
   const double dtdxi = sc->dtdxi, dtdyi = sc->dtdyi, dt = sc->dt;
-  const int tiles_x = (g.nx + 31) / 32;
-  const int tiles_y = (g.ny + 7) / 8;
+  const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 7) / 8;
   const long long ntiles = (long long)tiles_x * tiles_y * g.nz;
   DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int kt = (int)(tile / ((long long)tiles_x * tiles_y));
-    const int r = (int)(tile - (long long)kt * tiles_x * tiles_y);
-    const int jt = r / tiles_x, it = r - jt * tiles_x;
-    const int i = it * 32 + tx + 1, j = jt * 8 + ty + 1, k = kt + 1;
-    if (i > g.nx || j > g.ny) continue;
-    const long long c = g.at(i, j, k);
-    const double pc = p[c];
-    const double nu = u[c] - (p[c + 1] - pc) * dtdxi;
-    const double nv = v[c] - (p[c + g.X] - pc) * dtdyi;
-    const double nw = w[c] - (p[c + g.XY] - pc) * dt * __ldg(g.dzc_inv + k);
-    const double dzl = __ldg(g.dzflzi + k);
-    if (fc.forced[0]) {
-      u[c] = nu;
-      dd_add(s[0], nu * dzl);
-    } else {
-      store_with_halo(u, g, i, j, k, nu, BC_CENTRED, 0.0 - fc.u_crf);
+  long long tile = blockIdx.x;
+  int i = 0, j = 0, k = 0;
+  bool ok = tile < ntiles && tile_point(g, tile, tiles_x, tiles_y, i, j, k);
+  CorrIn cur{};
+  if (ok) cur = corr_load(g, p, u, v, w, g.at(i, j, k));
+  for (; tile < ntiles; tile += gridDim.x) {
+    // issue the next tile's loads before finishing this one
+    const long long nt = tile + gridDim.x;
+    int ni = 0, nj = 0, nk = 0;
+    const bool nok = nt < ntiles && tile_point(g, nt, tiles_x, tiles_y, ni, nj, nk);
+    CorrIn nxt{};
+    if (nok) nxt = corr_load(g, p, u, v, w, g.at(ni, nj, nk));
+    if (ok) {
+      const long long c = g.at(i, j, k);
+      // correctVel, mod_calcVel.cc:272-274
+      const double nu = cur.u - (cur.px - cur.pc) * dtdxi;
+      const double nv = cur.v - (cur.py - cur.pc) * dtdyi;
+      const double nw = cur.w - (cur.pz - cur.pc) * dt * __ldg(g.dzc_inv + k);
+      const double dzl = __ldg(g.dzflzi + k);
+      if (fc.forced[0]) {
+        u[c] = nu;
+        dd_add(s[0], nu * dzl);
+      } else {
+        store_with_halo(u, g, i, j, k, nu, BC_CENTRED, 0.0 - fc.u_crf);
+      }
+      if (fc.forced[1]) {
+        v[c] = nv;
+        dd_add(s[1], nv * dzl);
+      } else {
+        store_with_halo(v, g, i, j, k, nv, BC_CENTRED, 0.0);
+      }
+      if (fc.forced[2]) {
+        w[c] = nw;
+        dd_add(s[2], nw * dzl);
+      } else {
+        store_with_halo(w, g, i, j, k, nw, BC_FACE, 0.0);
+      }
     }
-    if (fc.forced[1]) {
-      v[c] = nv;
-      dd_add(s[1], nv * dzl);
-    } else {
-      store_with_halo(v, g, i, j, k, nv, BC_CENTRED, 0.0);
-    }
-    if (fc.forced[2]) {
-      w[c] = nw;
-      dd_add(s[2], nw * dzl);
-    } else {
-      store_with_halo(w, g, i, j, k, nw, BC_FACE, 0.0);
-    }
+    cur = nxt;
+    ok = nok;
+    i = ni;
+    j = nj;
+    k = nk;
   }
   block_sum<3>(s, smem);
-  if (grid_sum_last<3>(s, partials, counter, gridDim.x, smem)) {
+  if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
     for (int d = 0; d < 3; ++d) {
       if (fc.forced[d]) {
         const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
@@ -612,26 +658,40 @@ __global__ void __launch_bounds__(256) k_correct_fused(Geo g, StepConst *sc, For
 // (mod_calcVel.cc:296-316); with FUSE the halos of those components are
 // refreshed from the new interior values (the final updateBoundVel of
 // main.cc:153).
+// Each thread walks kz planes of one column; all its loads are issued first.
 template <bool FUSE>
 __global__ void __launch_bounds__(BX *BY) k_force_apply(Geo g, const StepConst *__restrict__ sc,
                                                         ForceCfg fc, double *u, double *v,
-                                                        double *w) {
+                                                        double *w, int kz) {
+  constexpr int KMAX = 8;
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
+  const int kb = blockIdx.z * kz + 1;
+  const int nk = min(kz, g.nz - kb + 1);
   if (i > g.nx || j > g.ny) return;
-  const long long c = g.at(i, j, k);
+  const long long c0 = g.at(i, j, kb);
   double *q[3] = {u, v, w};
   const int kind[3] = {BC_CENTRED, BC_CENTRED, BC_FACE};
   const double bc[3] = {0.0 - fc.u_crf, 0.0, 0.0};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (!fc.forced[d]) continue;
-    const double nv = q[d][c] + sc->force[d];
-    if (FUSE)
-      store_with_halo(q[d], g, i, j, k, nv, kind[d], bc[d]);
-    else
-      q[d][c] = nv;
+    const double f = sc->force[d];
+    for (int k0 = 0; k0 < nk; k0 += KMAX) {
+      double x[KMAX];
+#pragma unroll
+      for (int s = 0; s < KMAX; ++s)
+        if (k0 + s < nk) x[s] = q[d][c0 + (long long)(k0 + s) * g.XY];
+#pragma unroll
+      for (int s = 0; s < KMAX; ++s)
+        if (k0 + s < nk) {
+          const double nv = x[s] + f;
+          if (FUSE)
+            store_with_halo(q[d], g, i, j, kb + k0 + s, nv, kind[d], bc[d]);
+          else
+            q[d][c0 + (long long)(k0 + s) * g.XY] = nv;
+        }
+    }
   }
 }
 
@@ -937,10 +997,13 @@ cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p, double
   if (!fused) {
     k_correct<<<interior_grid(c), dim3(BX, BY), 0, s>>>(g, c->d_sc, p, u, v, w);
   } else {
-    long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
-    int nb = (int)(tiles < 148 * 8 ? tiles : 148 * 8);
-    k_correct_fused<<<nb, 256, 0, s>>>(g, c->d_sc, force_cfg(c), p, u, v, w, c->d_partials,
-                                       c->d_counter);
+    // one wave: 4 resident blocks per SM (launch bounds), at most the tiles
+    const long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
+    long long nb = 4ll * c->num_sms;
+    if (nb > tiles) nb = tiles;
+    if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
+    k_correct_fused<<<(unsigned)nb, 256, 0, s>>>(g, c->d_sc, force_cfg(c), p, u, v, w,
+                                                  c->d_partials, c->d_counter);
   }
   return cudaGetLastError();
 }
@@ -949,10 +1012,12 @@ cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u, double
                                cudaStream_t s) {
   const ForceCfg fc = force_cfg(c);
   if (!fc.forced[0] && !fc.forced[1] && !fc.forced[2]) return cudaSuccess;
+  const int kz = 8;
+  dim3 grid((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, (c->nz + kz - 1) / kz);
   if (fuse_bc)
-    k_force_apply<true><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w);
+    k_force_apply<true><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
   else
-    k_force_apply<false><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w);
+    k_force_apply<false><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
   return cudaGetLastError();
 }
 
