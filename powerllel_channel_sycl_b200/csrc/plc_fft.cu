@@ -29,6 +29,8 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "plc_device.cuh"
 #include "plc_internal.h"
 
@@ -206,7 +208,99 @@ __device__ double2 *fft_run(double2 *A, double2 *B, int nl, int LS, const FftDev
   return A;
 }
 
-__host__ __device__ __forceinline__ int line_stride(int n) { return n + (n >> 3) + 1; }
+__host__ __device__ __forceinline__ constexpr int line_stride(int n) { return n + (n >> 3) + 1; }
+
+// ---------------------------------------------------------------------------
+// Compile-time plans.  For the line lengths of the supported grids the radix
+// sequence (the rule of host_fft_factor: 16s, then one 8/4/2, then 3s) and
+// all index arithmetic are constants, the passes are unrolled and the
+// integer divisions become multiplications; N = 0 selects the runtime plan.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int count2(int n) {
+  int a = 0;
+  while (n > 0 && n % 2 == 0) {
+    n /= 2;
+    ++a;
+  }
+  return a;
+}
+__host__ __device__ constexpr int count3(int n) {
+  int b = 0;
+  while (n > 0 && n % 3 == 0) {
+    n /= 3;
+    ++b;
+  }
+  return b;
+}
+__host__ __device__ constexpr int plan_npass(int n) {
+  const int a = count2(n), b = count3(n >> a);
+  return a / 4 + (a % 4 != 0 ? 1 : 0) + b;
+}
+__host__ __device__ constexpr int plan_radix(int n, int p) {
+  const int a = count2(n);
+  if (p < a / 4) return 16;
+  p -= a / 4;
+  if (a % 4 != 0) {
+    if (p == 0) return a % 4 == 3 ? 8 : (a % 4 == 2 ? 4 : 2);
+    p -= 1;
+  }
+  return 3;
+}
+
+template <int R, bool INV, int N, int NS>
+__device__ __forceinline__ void fft_pass_t(const double2 *__restrict__ src,
+                                           double2 *__restrict__ dst, int nl,
+                                           const double2 *__restrict__ tw) {
+  constexpr int nb = N / R, LS = line_stride(N), tws = N / (NS * R);
+  const int tot = nl * nb;
+  for (int b = threadIdx.x; b < tot; b += blockDim.x) {
+    const int l = b / nb;
+    const int j = b - l * nb;
+    const double2 *s = src + l * LS;
+    double2 *d = dst + l * LS;
+    const int jm = j % NS;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = s[padi(j + r * nb)];
+    if (NS > 1 && jm != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const double2 w = __ldg(tw + r * jm * tws);
+        v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+      }
+    }
+    Dft<R, INV>::run(v);
+    const int idxD = (j / NS) * NS * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[padi(idxD + r * NS)] = v[r];
+  }
+}
+
+template <int N, int NS, int P, bool INV>
+__device__ __forceinline__ void passes_t(double2 *&A, double2 *&B, int nl,
+                                         const double2 *__restrict__ tw) {
+  if constexpr (P < plan_npass(N)) {
+    constexpr int R = plan_radix(N, P);
+    fft_pass_t<R, INV, N, NS>(A, B, nl, tw);
+    __syncthreads();
+    double2 *t = A;
+    A = B;
+    B = t;
+    passes_t<N, NS * R, P + 1, INV>(A, B, nl, tw);
+  }
+}
+
+// Complex FFT of nl lines held in A (compile-time plan for N > 0).
+template <int N, bool INV>
+__device__ __forceinline__ double2 *fft_run_n(double2 *A, double2 *B, int nl, int LS,
+                                              const FftDev &P) {
+  if constexpr (N > 0) {
+    passes_t<N, 1, 0, INV>(A, B, nl, P.tw);
+    return A;
+  } else {
+    return fft_run<INV>(A, B, nl, LS, P);
+  }
+}
 
 // The four packed outputs owned by the conjugate pair (m, n-m), 0 <= m < n/2:
 // packed indices q0 = 2m and q1 = 2m+1 (q0 = 0 and q1 = 1 for m = 0, i.e.
@@ -265,7 +359,7 @@ __device__ __forceinline__ double div_dt(const double *__restrict__ u,
 // Forward x transform fused with calcRHS, one tile per block: rows
 // (j0+2l, j0+2l+1) of plane k are div(u)/dt evaluated from global memory while
 // loading (many resident blocks hide the load latency), then transformed.
-template <bool FUSED>
+template <int N, bool FUSED>
 __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
                                                    const StepConst *__restrict__ sc,
                                                    const double *__restrict__ p,
@@ -274,7 +368,7 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
                                                    const double *__restrict__ w,
                                                    double *__restrict__ var) {
   extern __shared__ double2 smem[];
-  const int n = g.nx, LS = line_stride(n);
+  const int n = N > 0 ? N : g.nx, LS = line_stride(n);
   double2 *A = smem, *B = smem + nl * LS;
   const int j0 = blockIdx.x * 2 * nl;  // 0-based row in the plane
   const int k = blockIdx.y;            // 0-based plane
@@ -300,7 +394,7 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
     A[l * LS + padi(t)] = make_double2(a, b);
   }
   __syncthreads();
-  const double2 *Z = fft_run<false>(A, B, nl, LS, P);
+  const double2 *Z = fft_run_n<N, false>(A, B, nl, LS, P);
   const int half = n >> 1;
   for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
     const int l = e / half, m = e - l * half;
@@ -345,11 +439,12 @@ __device__ __forceinline__ void stage_rows(double *dst, const double *src, int r
 
 // Forward x transform (persistent): rows (j0+2l, j0+2l+1) of p at plane k ->
 // packed spectra.  The halo'd rows are staged whole (16-byte aligned).
+template <int N>
 __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
                                                    const double *__restrict__ p,
                                                    double *__restrict__ var) {
   extern __shared__ double2 smem[];
-  const int n = g.nx, LS = line_stride(n), X = g.X, R = 2 * nl;
+  const int n = N > 0 ? N : g.nx, LS = line_stride(n), X = g.X, R = 2 * nl;
   double2 *A = smem, *B = smem + nl * LS;
   double *S = reinterpret_cast<double *>(B + nl * LS);  // R halo'd rows
   const int tiles_y = g.ny / R;
@@ -371,7 +466,7 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run<false>(A, B, nl, LS, P);
+    const double2 *Z = fft_run_n<N, false>(A, B, nl, LS, P);
     const int half = n >> 1;
     for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
       const int l = e / half, m = e - l * half;
@@ -386,11 +481,11 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
 
 // Backward x transform: packed spectra -> p interior scaled by nf; with
 // FUSE_BC the pressure halos are written as well (updateBoundP).
-template <bool FUSE_BC>
+template <int N, bool FUSE_BC>
 __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, double nf,
                                                    const double *__restrict__ var, double *p) {
   extern __shared__ double2 smem[];
-  const int n = g.nx, LS = line_stride(n), R = 2 * nl;
+  const int n = N > 0 ? N : g.nx, LS = line_stride(n), R = 2 * nl;
   double2 *A = smem, *B = smem + nl * LS;
   double *S = reinterpret_cast<double *>(B + nl * LS);  // R rows of n doubles
   const int tiles_y = g.ny / R;
@@ -413,7 +508,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, doub
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run<true>(A, B, nl, LS, P);
+    const double2 *Z = fft_run_n<N, true>(A, B, nl, LS, P);
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
       const int l = e / n, t = e - l * n;
       const double2 z = Z[l * LS + padi(t)];
@@ -433,11 +528,11 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, doub
 
 // y transform in place on the spectral array: tile = columns i0..i0+2nl-1 of
 // plane k (TX = 2nl x-contiguous doubles per row, row stride nx).
-template <bool INV>
+template <int N, bool INV>
 __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P, int nl,
                                                double *__restrict__ var) {
   extern __shared__ double2 smem[];
-  const int n = ny, LS = line_stride(n), TX = 2 * nl;
+  const int n = N > 0 ? N : ny, LS = line_stride(n), TX = 2 * nl;
   double2 *A = smem, *B = smem + nl * LS;
   double *S = reinterpret_cast<double *>(B + nl * LS);  // n rows of TX doubles
   const int tiles_x = nx / TX;
@@ -468,7 +563,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P,
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run<INV>(A, B, nl, LS, P);
+    const double2 *Z = fft_run_n<N, INV>(A, B, nl, LS, P);
     if (!INV) {
       for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
         const int m = e / nl, l = e - m * nl;
@@ -631,19 +726,46 @@ int persistent_grid(K kernel, int threads, size_t smem, int sms, long long ntile
 }
 }  // namespace
 
+// Line lengths with compile-time plans (the grids of the supported channel
+// cases); any other 2^a 3^b length runs the runtime plan (N = 0).
+template <class F>
+cudaError_t with_size(int n, F &&f) {
+  switch (n) {
+    case 32: return f(std::integral_constant<int, 32>{});
+    case 48: return f(std::integral_constant<int, 48>{});
+    case 64: return f(std::integral_constant<int, 64>{});
+    case 96: return f(std::integral_constant<int, 96>{});
+    case 128: return f(std::integral_constant<int, 128>{});
+    case 192: return f(std::integral_constant<int, 192>{});
+    case 256: return f(std::integral_constant<int, 256>{});
+    case 384: return f(std::integral_constant<int, 384>{});
+    case 512: return f(std::integral_constant<int, 512>{});
+    case 768: return f(std::integral_constant<int, 768>{});
+    default: return f(std::integral_constant<int, 0>{});
+  }
+}
+constexpr int kPlanSizes[] = {0, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768};
+
 // Raises the dynamic shared-memory limit of every FFT kernel (once per process).
 cudaError_t fft_configure(size_t max_bytes) {
-  cudaError_t e;
-#define PLC_SMEM(kern)                                                                    \
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes); \
-  if (e != cudaSuccess) return e;
-  PLC_SMEM(k_fft_x_fwd);
-  PLC_SMEM(k_fft_x_fwd_div<true>);
-  PLC_SMEM(k_fft_x_bwd<true>);
-  PLC_SMEM(k_fft_x_bwd<false>);
-  PLC_SMEM(k_fft_y<true>);
-  PLC_SMEM(k_fft_y<false>);
+  for (int n : kPlanSizes) {
+    const cudaError_t e = with_size(n, [&](auto NC) -> cudaError_t {
+      constexpr int N = decltype(NC)::value;
+      cudaError_t r;
+#define PLC_SMEM(kern)                                                                        \
+  r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes); \
+  if (r != cudaSuccess) return r;
+      PLC_SMEM(k_fft_x_fwd<N>);
+      PLC_SMEM((k_fft_x_fwd_div<N, true>));
+      PLC_SMEM((k_fft_x_bwd<N, true>));
+      PLC_SMEM((k_fft_x_bwd<N, false>));
+      PLC_SMEM((k_fft_y<N, true>));
+      PLC_SMEM((k_fft_y<N, false>));
 #undef PLC_SMEM
+      return cudaSuccess;
+    });
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 
@@ -663,25 +785,36 @@ cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max) {
     if (b > dev_max) return cudaErrorInvalidValue;
   const long long tiles_x = (long long)(ny / (2 * c->fft_lines_x)) * nz;
   const long long tiles_y = (long long)(nx / (2 * c->fft_lines_y)) * nz;
-  c->grid_xf = persistent_grid(k_fft_x_fwd, 128, need[0], sms, tiles_x);
-  c->grid_xb = persistent_grid(k_fft_x_bwd<true>, 128, need[2], sms, tiles_x);
-  c->grid_y = persistent_grid(k_fft_y<false>, 256, need[3], sms, tiles_y);
-  return cudaSuccess;
+  e = with_size(nx, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    c->grid_xf = persistent_grid(k_fft_x_fwd<N>, 128, need[0], sms, tiles_x);
+    c->grid_xb = persistent_grid(k_fft_x_bwd<N, true>, 128, need[2], sms, tiles_x);
+    return cudaSuccess;
+  });
+  if (e != cudaSuccess) return e;
+  return with_size(ny, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    c->grid_y = persistent_grid(k_fft_y<N, false>, 256, need[3], sms, tiles_y);
+    return cudaSuccess;
+  });
 }
 
 cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u, const double *v,
                              const double *w, double *var, cudaStream_t s) {
-  if (p) {
-    const int nl = c->fft_lines_x;
-    k_fft_x_fwd<<<c->grid_xf, 128, smem_x_fwd(c->nx, nl), s>>>(c->geo(), dev_plan(c->plan_x), nl,
-                                                                p, var);
-  } else {
-    const int nl = c->fft_lines_xf;
-    dim3 grid(c->ny / (2 * nl), c->nz);
-    k_fft_x_fwd_div<true><<<grid, 256, fft_smem_bytes(c->nx, nl), s>>>(
-        c->geo(), dev_plan(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
-  }
-  return cudaGetLastError();
+  return with_size(c->nx, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    if (p) {
+      const int nl = c->fft_lines_x;
+      k_fft_x_fwd<N><<<c->grid_xf, 128, smem_x_fwd(c->nx, nl), s>>>(
+          c->geo(), dev_plan(c->plan_x), nl, p, var);
+    } else {
+      const int nl = c->fft_lines_xf;
+      dim3 grid(c->ny / (2 * nl), c->nz);
+      k_fft_x_fwd_div<N, true><<<grid, 256, fft_smem_bytes(c->nx, nl), s>>>(
+          c->geo(), dev_plan(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
+    }
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p, bool fuse_bc,
@@ -689,21 +822,31 @@ cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p, boo
   const int nl = c->fft_lines_x;
   const size_t sm = smem_x_bwd(c->nx, nl);
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
-  if (fuse_bc)
-    k_fft_x_bwd<true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
-  else
-    k_fft_x_bwd<false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf, var, p);
-  return cudaGetLastError();
+  return with_size(c->nx, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    if (fuse_bc)
+      k_fft_x_bwd<N, true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf,
+                                                        var, p);
+    else
+      k_fft_x_bwd<N, false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf,
+                                                         var, p);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse, cudaStream_t s) {
   const int nl = c->fft_lines_y;
   const size_t sm = smem_y(c->ny, nl);
-  if (inverse)
-    k_fft_y<true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl, var);
-  else
-    k_fft_y<false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl, var);
-  return cudaGetLastError();
+  return with_size(c->ny, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    if (inverse)
+      k_fft_y<N, true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl,
+                                                   var);
+    else
+      k_fft_y<N, false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl,
+                                                    var);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
