@@ -7,7 +7,9 @@ NaN/CFL/divergence checks every nt_check steps) on the Re_tau ~ 550 channel
 768 x 384 x 256 (domain 2pi x pi x 2, tanh stretching 1.8, Re_b = 20000,
 CFL-controlled dt with CFL 0.5), FP64, seeded laminar + noise initial field
 generated on the device.  Every field (613 MB) is larger than the 126 MB L2,
-so no L2 flush is needed between steps.
+so no L2 flush is needed between steps.  The line's "mixed" object reports
+the mixed-precision form on the same workload (FP32 fields) with its
+speed-up over the FP64 form and its 10-step error against it.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -65,6 +67,10 @@ KERNEL_BYTES_PER_POINT = {
     "force+bound(u)": 16,         # read u; write u
 }
 STEP_BYTES_PER_POINT = sum(KERNEL_BYTES_PER_POINT.values())  # 288
+# the mixed form stores every field in FP32: half the bytes of each kernel
+# (its FP64 pivot table of the tridiagonal sweep excluded, as above)
+MIXED_BYTES_PER_POINT = {k: v // 2 for k, v in KERNEL_BYTES_PER_POINT.items()}
+MIXED_STEP_BYTES_PER_POINT = sum(MIXED_BYTES_PER_POINT.values())  # 144
 
 
 def load_peaks():
@@ -145,14 +151,77 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def channel_params(wl, nt_check):
+def channel_params(wl, nt_check, precision="fp64", cfl_target=None):
     from powerllel_channel_sycl_b200 import make_params
     return make_params(
         nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], lx=wl["lx"], ly=wl["ly"], lz=wl["lz"],
         mesh_type=1, stretch_func=0, stretch_ratio=wl["stretch_ratio"], re=wl["re"], u_ref=1.0,
         l_ref=1.0, dt=wl["dt"], nt_check=nt_check, cfl_limit=1.0, div_limit=1e-9,
         initial_field="poi", init_with_noise=1, noise_intensity=0.1, is_forced=[1, 0, 0],
-        vel_force=[1.0, 0.0, 0.0], cfl_target=wl["cfl_target"])
+        vel_force=[1.0, 0.0, 0.0],
+        cfl_target=wl["cfl_target"] if cfl_target is None else cfl_target, precision=precision)
+
+
+def run_mixed(args, wl, world, local, pg, fp64_ms):
+    """The mixed-precision form on the same workload: throughput, per-kernel
+    times, and its 10-step error against the FP64 form from the same initial
+    field (fixed dt, so that both forms take identical steps)."""
+    import torch
+    from powerllel_channel_sycl_b200 import Channel
+
+    npts = wl["nx"] * wl["ny"] * wl["nz"]
+    ch = Channel(channel_params(wl, args.nt_check, precision="mixed"), device=local)
+    ch.initFlow()
+    ch.step(args.warmup)
+    ch.sync()
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    ms = ch.step_timed(args.steps)
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    ms_max = max_over_ranks(ms, pg, local)
+    value = world * npts * args.steps / (ms_max / 1e3)
+    ok, cfl, div = ch.check()
+    prof_steps = max(2, min(5, args.steps))
+    prof = ch.profile_step(prof_steps)
+    total = sum(prof.values())
+    kernels = {k: {"ms": v / prof_steps, "share": v / total,
+                   "gbs": MIXED_BYTES_PER_POINT[k] * npts / (v / prof_steps / 1e3) / 1e9}
+               for k, v in prof.items()}
+    ch.close()
+    peak, _ = load_peaks()
+
+    # accuracy: 10 steps of both forms from the same laminar + noise field
+    nerr = 10
+    a = Channel(channel_params(wl, 0, precision="fp64", cfl_target=0.0), device=local)
+    b = Channel(channel_params(wl, 0, precision="mixed", cfl_target=0.0), device=local)
+    a.initFlow()
+    b.initFlow()
+    a.step(nerr)
+    b.step(nerr)
+    err = {}
+    for name in "uvw":
+        x = a.download(name)[1:-1, 1:-1, 1:-1]
+        y = b.download(name)[1:-1, 1:-1, 1:-1]
+        err[name] = float(np.linalg.norm((y - x).ravel()) / np.linalg.norm(x.ravel()))
+        if name == "u":
+            mx, my = x.mean(axis=(1, 2)), y.mean(axis=(1, 2))
+            err["u_mean_profile_max_rel"] = float(np.max(np.abs(my - mx)) / np.max(np.abs(mx)))
+        del x, y
+    _, _, div_b = b.check()
+    a.close()
+    b.close()
+    return {
+        "value": value, "unit": "grid-pt*step/s", "ms_per_step": ms_max / args.steps,
+        "speedup_vs_fp64": fp64_ms / ms_max, "dtype": "f32 fields, f64 scalars/reductions/trid",
+        "step_roofline": {"bytes_per_point_step": MIXED_STEP_BYTES_PER_POINT,
+                          "achieved_gbs": MIXED_STEP_BYTES_PER_POINT * value / world / 1e9,
+                          "frac": MIXED_STEP_BYTES_PER_POINT * value / world / 1e9 / peak},
+        "kernels": kernels,
+        "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0]},
+        "error_vs_fp64": {"steps": nerr, "dt": wl["dt"], "vel_rel_l2": err,
+                          "div_max_mixed": div_b[0]},
+    }
 
 
 def cpu_oracle_rate(wl, budget_s: float, max_steps: int, warmup: int):
@@ -357,6 +426,9 @@ def run_ours(args, wl, rank, world, local, pg):
         "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0], "dt": ch.dt},
     }
     ch.close()
+    if not args.no_mixed:
+        line["mixed"] = run_mixed(args, wl, world, local, pg, ms_max)
+        line["gpu_launches"] += args.steps * 9
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, nsteps, threads = cpu_oracle_rate(wl, budget_s=args.cpu_budget, max_steps=1,
                                                 warmup=0)
@@ -378,6 +450,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=60.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision measurement")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

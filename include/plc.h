@@ -53,7 +53,16 @@ extern "C" {
 
 /* ---- precision forms ---- */
 #define PLC_FP64 0  /* plain FP64, parity with the reference */
-#define PLC_MIXED 1 /* FP32 stencils/FFTs, FP64 scalars and low modes */
+/* No counterpart in the reference.  FP32 fields, FP32 stencils and FFTs; FP64
+ * time step, forcing sum, NaN/CFL/divergence checks and tridiagonal sweep
+ * (with FP64 intermediates for the lowest wavenumbers and the singular (0,0)
+ * mode pinned).  nx and ny must be divisible by 4.  A mixed context runs
+ * through plc_step / plc_step_timed / plc_profile_step, plc_init_flow,
+ * plc_check, plc_upload / plc_download (FP64 host arrays in the reference
+ * layout, converted on the device) and plc_field_ptr_f32; the FP64 module
+ * entry points return PLC_ERR_STATE.  Its divergence check uses
+ * div_limit * 2^29 (the FP32/FP64 unit round-off ratio). */
+#define PLC_MIXED 1
 
 /* ---- initial fields (mod_initFlow.cc:47-102) ---- */
 #define PLC_INIT_UNI 0
@@ -141,6 +150,10 @@ int plc_sync(plc_ctx *ctx);
 int plc_get_mesh(const plc_ctx *ctx, int which, double *h_out);
 /* Device pointer and element count of a context-owned array (PLC_U..PLC_SPEC). */
 int plc_field_ptr(plc_ctx *ctx, int field, double **d_ptr, size_t *count);
+/* The same for a PLC_MIXED context: FP32 arrays; halo'd fields have rows of
+ * *pitch elements (nx+2 rounded up to a multiple of 4), the spectral array
+ * rows of nx.  No counterpart in the reference. */
+int plc_field_ptr_f32(plc_ctx *ctx, int field, float **d_ptr, size_t *count, int *pitch);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

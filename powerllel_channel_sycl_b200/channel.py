@@ -100,6 +100,7 @@ class Channel:
         check(rc)
         self._ctx = ctx
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
+        self.mixed = params.precision == PRECISION["mixed"]
 
     # -- lifetime ---------------------------------------------------------------
     def close(self):
@@ -139,6 +140,16 @@ class Channel:
         n = C.c_size_t()
         self._check(lib().plc_field_ptr(self._ctx, fid, C.byref(p), C.byref(n)))
         return p.value
+
+    def ptr_f32(self, f):
+        """(device pointer, element count, row pitch) of an FP32 field of a mixed context."""
+        fid = FIELDS[f] if isinstance(f, str) else int(f)
+        p = C.c_void_p()
+        n = C.c_size_t()
+        pitch = C.c_int()
+        self._check(lib().plc_field_ptr_f32(self._ctx, fid, C.byref(p), C.byref(n),
+                                            C.byref(pitch)))
+        return p.value, n.value, pitch.value
 
     def upload(self, field: str, arr: np.ndarray):
         fid = FIELDS[field]

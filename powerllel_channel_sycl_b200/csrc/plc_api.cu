@@ -10,6 +10,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "plc_internal.h"
@@ -23,7 +24,7 @@ plc::Geo plc_ctx::geo() const {
   g.nx = nx;
   g.ny = ny;
   g.nz = nz;
-  g.X = nx + 2;
+  g.X = pitch;
   g.Y = ny + 2;
   g.XY = (long long)g.X * g.Y;
   g.dx_inv = dx_inv;
@@ -81,12 +82,18 @@ int upload_step_consts(plc_ctx *c, double dt) {
 void free_poisson(plc_ctx *c) {
   cudaFree(c->d_rpiv);
   cudaFree(c->d_ac);
+  cudaFree(c->d_low);
   cudaFree(c->plan_x.tw);
   cudaFree(c->plan_y.tw);
+  cudaFree(c->plan_x.tw32);
+  cudaFree(c->plan_y.tw32);
   c->d_rpiv = nullptr;
   c->d_ac = nullptr;
+  c->d_low = nullptr;
   c->plan_x.tw = nullptr;
   c->plan_y.tw = nullptr;
+  c->plan_x.tw32 = nullptr;
+  c->plan_y.tw32 = nullptr;
   c->poisson_ready = false;
 }
 
@@ -94,6 +101,17 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
   free_poisson(c);
   std::vector<double> rpiv, a, cc;
   host_trid_tables(c->nx, c->ny, c->nz, c->dx, c->dy, dzf_global, rpiv, a, cc);
+  if (c->mixed) {
+    // The (0,0) system is singular (Neumann in z): its last pivot is zero up
+    // to rounding and its right-hand side sums to zero only up to FP32
+    // rounding.  The mixed form pins it: the reciprocal of the last pivot is
+    // set to 0, so the top value of the (0,0) mode is 0 and the rest follow
+    // by back substitution (the pressure is defined up to a constant).
+    const size_t plane = (size_t)(c->nx / 2 + 1) * (c->ny / 2 + 1);
+    rpiv[(size_t)(c->nz - 1) * plane] = 0.0;
+    const size_t nlow = (size_t)c->nz * kLowModes * kLowModes;
+    PLC_CUDA(c, cudaMalloc(&c->d_low, nlow * sizeof(double)));
+  }
   PLC_CUDA(c, cudaMalloc(&c->d_rpiv, rpiv.size() * sizeof(double)));
   PLC_CUDA(c, cudaMemcpy(c->d_rpiv, rpiv.data(), rpiv.size() * sizeof(double),
                          cudaMemcpyHostToDevice));
@@ -112,6 +130,12 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
     host_twiddles(p.n, tw);
     PLC_CUDA(c, cudaMalloc(&p.tw, tw.size() * sizeof(double)));
     PLC_CUDA(c, cudaMemcpy(p.tw, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (c->mixed) {
+      std::vector<float> tw32(tw.begin(), tw.end());
+      PLC_CUDA(c, cudaMalloc(&p.tw32, tw32.size() * sizeof(float)));
+      PLC_CUDA(c, cudaMemcpy(p.tw32, tw32.data(), tw32.size() * sizeof(float),
+                             cudaMemcpyHostToDevice));
+    }
   }
   int dev_max = 0;
   PLC_CUDA(c, cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
@@ -134,8 +158,10 @@ int check_ptr(plc_ctx *c, const void *p, const char *name) {
 #define PLC_REQ(c, p) \
   if (int _r = check_ptr(c, p, #p)) return _r
 
+// halo'd linear index of the context's layout -> 0-based (i, j, k) with the
+// halo, i.e. the reference's 1-based global indices of the interior
 void to_ijk(const plc_ctx *c, long long idx, plc_value_index *out, double value) {
-  const long long X = c->nx + 2, XY = X * (c->ny + 2);
+  const long long X = c->pitch, XY = X * (c->ny + 2);
   out->value = value;
   out->kg = (int)(idx / XY);
   out->jg = (int)((idx % XY) / X);
@@ -154,7 +180,8 @@ int device_error(plc_ctx *c) {
   return PLC_OK;
 }
 
-int run_check(plc_ctx *c, int what, const double *u, const double *v, const double *w) {
+template <class T>
+int run_check(plc_ctx *c, int what, const T *u, const T *v, const T *w) {
   PLC_CUDA(c, launch_check(c, u, v, w, what, c->stream));
   PLC_CUDA(c, cudaMemcpyAsync(c->h_check, c->d_check, sizeof(CheckResult), cudaMemcpyDeviceToHost,
                               c->stream));
@@ -162,18 +189,27 @@ int run_check(plc_ctx *c, int what, const double *u, const double *v, const doub
   return PLC_OK;
 }
 
+// the checks of the context's own u, v, w in either precision form
+int run_check_fields(plc_ctx *c, int what) {
+  if (c->mixed)
+    return run_check(c, what, c->f_field[PLC_U], c->f_field[PLC_V], c->f_field[PLC_W]);
+  return run_check(c, what, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W]);
+}
+
 const char *const kStepKernelNames[] = {
     "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
     "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+mean", "force+bound(u)"};
 constexpr int kStepKernels = 9;
 
-// Launches of one fused step (main.cc:116-154) on the context's fields.  With
-// ev != nullptr, ev[0] is recorded before the first kernel and ev[q+1] after
-// kernel q (per-kernel timing; not used inside graph capture).
-int enqueue_step(plc_ctx *c, cudaStream_t s, cudaEvent_t *ev = nullptr) {
-  double *u = c->d_field[PLC_U], *v = c->d_field[PLC_V], *w = c->d_field[PLC_W];
-  double *u1 = c->d_field[PLC_U1], *v1 = c->d_field[PLC_V1], *w1 = c->d_field[PLC_W1];
-  double *p = c->d_field[PLC_P], *spec = c->d_field[PLC_SPEC];
+// Launches of one fused step (main.cc:116-154) on the context's fields, in
+// the context's storage type T.  With ev != nullptr, ev[0] is recorded before
+// the first kernel and ev[q+1] after kernel q (per-kernel timing; not used
+// inside graph capture).
+template <class T>
+int enqueue_step_t(plc_ctx *c, T *const *f, cudaStream_t s, cudaEvent_t *ev) {
+  T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W];
+  T *u1 = f[PLC_U1], *v1 = f[PLC_V1], *w1 = f[PLC_W1];
+  T *p = f[PLC_P], *spec = f[PLC_SPEC];
   const double u_crf = c->prm.u_crf;
   int q = 0;
   auto mark = [&]() -> cudaError_t {
@@ -184,7 +220,10 @@ int enqueue_step(plc_ctx *c, cudaStream_t s, cudaEvent_t *ev = nullptr) {
   PLC_CUDA(c, mark());
   PLC_CUDA(c, launch_rk(c, 2, true, u_crf, u1, v1, w1, u, v, w, s));     // RK2 + bound(u)
   PLC_CUDA(c, mark());
-  PLC_CUDA(c, launch_fft_x_fwd(c, nullptr, u, v, w, spec, s));           // calcRHS + x-FFT
+  if constexpr (std::is_same<T, double>::value)
+    PLC_CUDA(c, launch_fft_x_fwd(c, nullptr, u, v, w, spec, s));         // calcRHS + x-FFT
+  else
+    PLC_CUDA(c, launch_fft_x_fwd(c, u, v, w, spec, s));
   PLC_CUDA(c, mark());
   PLC_CUDA(c, launch_fft_y(c, spec, false, s));                          // y-FFT
   PLC_CUDA(c, mark());
@@ -199,6 +238,11 @@ int enqueue_step(plc_ctx *c, cudaStream_t s, cudaEvent_t *ev = nullptr) {
   PLC_CUDA(c, launch_force_apply(c, true, u, v, w, s));                  // force + bound(u)
   PLC_CUDA(c, mark());
   return PLC_OK;
+}
+
+int enqueue_step(plc_ctx *c, cudaStream_t s, cudaEvent_t *ev = nullptr) {
+  if (c->mixed) return enqueue_step_t<float>(c, c->f_field, s, ev);
+  return enqueue_step_t<double>(c, c->d_field, s, ev);
 }
 
 int build_graph(plc_ctx *c) {
@@ -218,6 +262,51 @@ int build_graph(plc_ctx *c) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_status(c, e, "cudaGraphInstantiate");
   c->graph_kernels = (int)nodes;
+  return PLC_OK;
+}
+
+// Mean (mod_utils.cc:30-51) of a device field in the context's layout.
+template <class T>
+int mean_of(plc_ctx *c, int nxg, int nyg, const T *var, double *mean) {
+  PLC_CUDA(c, launch_mean(c, 0, nxg, nyg, var, c->stream));
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_scal, reinterpret_cast<char *>(c->d_sc) + offsetof(StepConst, mean),
+                              sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  *mean = c->h_scal[0];
+  return PLC_OK;
+}
+
+// initFlow (mod_initFlow.cc:47-118) on the context's u, v, w from the profile
+// prof[k], then transform2CRF and the boundary update (main.cc:78-82).  The
+// spectral array serves as device scratch for the profile (its nx*ny*nz
+// elements hold more than nz+2 doubles).
+template <class T>
+int init_fields(plc_ctx *c, const std::vector<double> &prof, bool is_mean, T *const *f) {
+  const plc_params &P = c->prm;
+  T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W];
+  double *scratch = reinterpret_cast<double *>(f[PLC_SPEC]);
+  PLC_CUDA(c, cudaMemcpyAsync(scratch, prof.data(), prof.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+  PLC_CUDA(c, launch_init_flow(c, u, v, w, scratch, c->stream));
+  if (is_mean) {
+    double meanold = 0.0;
+    // the reference passes (nz, ny) as the global sizes here (mod_initFlow.cc:92)
+    if (int rc = mean_of(c, c->nz, c->ny, u, &meanold)) return rc;
+    if (meanold != 0.0) {
+      c->h_scal[0] = 1.0 / (meanold * P.u_ref);
+      PLC_CUDA(c, cudaMemcpyAsync(scratch, c->h_scal, sizeof(double), cudaMemcpyHostToDevice,
+                                  c->stream));
+      PLC_CUDA(c, launch_scale(c, u, scratch, c->stream));
+    }
+  }
+  // transform2CRF (mod_calcVel.cc:13-25)
+  if (P.u_crf != 0.0) {
+    PLC_CUDA(c, launch_shift(c, u, P.u_crf, c->stream));
+    c->prm.vel_force[0] -= P.u_crf;
+  }
+  PLC_CUDA(c, launch_bound_vel(c, P.u_crf, u, v, w, c->stream));
+  PLC_CUDA(c, launch_bound_p(c, f[PLC_P], c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
   return PLC_OK;
 }
 
@@ -275,8 +364,9 @@ int plc_params_check(const plc_params *prm) {
     return set_error(nullptr, PLC_ERR_ARG, "dt, re, lx, ly, lz, u_ref and l_ref must be positive");
   if (prm->precision != PLC_FP64 && prm->precision != PLC_MIXED)
     return set_error(nullptr, PLC_ERR_ARG, "unknown precision form");
-  if (prm->precision == PLC_MIXED)
-    return set_error(nullptr, PLC_ERR_ARG, "the mixed-precision form is not built into this library");
+  // the FP32 transforms stage 16-byte chunks of 4 elements along x and y rows
+  if (prm->precision == PLC_MIXED && (prm->nx % 4 || prm->ny % 4))
+    return set_error(nullptr, PLC_ERR_SIZE, "the mixed-precision form needs nx and ny divisible by 4");
   return PLC_OK;
 }
 
@@ -299,7 +389,10 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   c->dx_inv = 1.0 / c->dx;
   c->dy_inv = 1.0 / c->dy;
   c->re_inv = prm->u_ref * prm->l_ref / prm->re;
-  c->nfield = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  c->mixed = (prm->precision == PLC_MIXED);
+  // FP64 fields keep the reference's row length; FP32 rows are padded to 16 bytes
+  c->pitch = c->mixed ? ((c->nx + 2 + 3) / 4) * 4 : c->nx + 2;
+  c->nfield = (size_t)c->pitch * (c->ny + 2) * (c->nz + 2);
   c->nspec = (size_t)c->nx * c->ny * c->nz;
   auto fail = [&](int rc) {
     std::string msg = c->err;
@@ -336,12 +429,26 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     if (e != cudaSuccess) return fail(cuda_status(c, e, "upload mesh"));
   }
   // fields (mod_variables.cc:4-12) and the spectral array, zero-initialised
+  const size_t esize = c->mixed ? sizeof(float) : sizeof(double);
   for (int f = 0; f < 8; ++f) {
     const size_t n = (f == PLC_SPEC) ? c->nspec : c->nfield;
-    e = cudaMalloc(&c->d_field[f], n * sizeof(double));
+    void *ptr = nullptr;
+    e = cudaMalloc(&ptr, n * esize);
     if (e != cudaSuccess) return fail(set_error(c, PLC_ERR_NOMEM, "cudaMalloc field"));
-    e = cudaMemset(c->d_field[f], 0, n * sizeof(double));
+    if (c->mixed)
+      c->f_field[f] = static_cast<float *>(ptr);
+    else
+      c->d_field[f] = static_cast<double *>(ptr);
+    e = cudaMemset(ptr, 0, n * esize);
     if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaMemset field"));
+  }
+  if (c->mixed) {
+    std::vector<float> coef;
+    host_rk32_coef(c, coef);
+    if ((e = cudaMalloc(&c->d_coef32, coef.size() * sizeof(float))) != cudaSuccess ||
+        (e = cudaMemcpy(c->d_coef32, coef.data(), coef.size() * sizeof(float),
+                        cudaMemcpyHostToDevice)) != cudaSuccess)
+      return fail(cuda_status(c, e, "RK coefficient table"));
   }
   // scalars and scratch
   if ((e = cudaMalloc(&c->d_sc, sizeof(StepConst))) != cudaSuccess ||
@@ -369,6 +476,8 @@ int plc_destroy(plc_ctx *c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   free_poisson(c);
   for (auto &f : c->d_field) cudaFree(f);
+  for (auto &f : c->f_field) cudaFree(f);
+  cudaFree(c->d_coef32);
   cudaFree(c->d_mesh);
   cudaFree(c->d_sc);
   cudaFree(c->d_partials);
@@ -398,22 +507,68 @@ int plc_get_mesh(const plc_ctx *c, int which, double *h_out) {
   return PLC_OK;
 }
 
+#define PLC_NEED_FP64(c)                                                              \
+  if ((c)->mixed)                                                                     \
+  return set_error(c, PLC_ERR_STATE,                                                  \
+                   "the module entry points take FP64 fields; this context holds the " \
+                   "mixed-precision form (use plc_step, plc_upload/plc_download)")
+
 int plc_field_ptr(plc_ctx *c, int field, double **d_ptr, size_t *count) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
   if (d_ptr) *d_ptr = c->d_field[field];
   if (count) *count = (field == PLC_SPEC) ? c->nspec : c->nfield;
   return PLC_OK;
 }
 
+int plc_field_ptr_f32(plc_ctx *c, int field, float **d_ptr, size_t *count, int *pitch) {
+  PLC_CHECK_CTX(c);
+  if (!c->mixed) return set_error(c, PLC_ERR_STATE, "the context holds FP64 fields");
+  if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
+  if (d_ptr) *d_ptr = c->f_field[field];
+  if (count) *count = (field == PLC_SPEC) ? c->nspec : c->nfield;
+  if (pitch) *pitch = (field == PLC_SPEC) ? c->nx : c->pitch;
+  return PLC_OK;
+}
+
+// rows and row length of a field in the reference's layout
+static void ref_shape(const plc_ctx *c, int field, long long *rows, int *len) {
+  if (field == PLC_SPEC) {
+    *rows = (long long)c->ny * c->nz;
+    *len = c->nx;
+  } else {
+    *rows = (long long)(c->ny + 2) * (c->nz + 2);
+    *len = c->nx + 2;
+  }
+}
+
 int plc_upload(plc_ctx *c, int field, const double *h_src) {
   PLC_CHECK_CTX(c);
   PLC_REQ(c, h_src);
   if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
-  const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
-  PLC_CUDA(c, cudaMemcpyAsync(c->d_field[field], h_src, n * sizeof(double),
-                              cudaMemcpyHostToDevice, c->stream));
-  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (!c->mixed) {
+    const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
+    PLC_CUDA(c, cudaMemcpyAsync(c->d_field[field], h_src, n * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream));
+    PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return PLC_OK;
+  }
+  // mixed form: FP64 host field -> stream-ordered FP64 staging -> FP32 field
+  long long rows;
+  int len;
+  ref_shape(c, field, &rows, &len);
+  const size_t n = (size_t)rows * len;
+  double *tmp = nullptr;
+  PLC_CUDA(c, cudaMallocAsync(&tmp, n * sizeof(double), c->stream));
+  cudaError_t e = cudaMemcpyAsync(tmp, h_src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = launch_to_f32(c, tmp, c->f_field[field], rows, len,
+                      field == PLC_SPEC ? c->nx : c->pitch, c->stream);
+  const cudaError_t ef = cudaFreeAsync(tmp, c->stream);
+  if (e == cudaSuccess) e = ef;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(c, e, "plc_upload (FP64 -> FP32)");
   return PLC_OK;
 }
 
@@ -421,10 +576,27 @@ int plc_download(plc_ctx *c, int field, double *h_dst) {
   PLC_CHECK_CTX(c);
   PLC_REQ(c, h_dst);
   if (field < 0 || field > PLC_SPEC) return set_error(c, PLC_ERR_ARG, "bad field id");
-  const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
-  PLC_CUDA(c, cudaMemcpyAsync(h_dst, c->d_field[field], n * sizeof(double),
-                              cudaMemcpyDeviceToHost, c->stream));
-  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (!c->mixed) {
+    const size_t n = (field == PLC_SPEC) ? c->nspec : c->nfield;
+    PLC_CUDA(c, cudaMemcpyAsync(h_dst, c->d_field[field], n * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return PLC_OK;
+  }
+  long long rows;
+  int len;
+  ref_shape(c, field, &rows, &len);
+  const size_t n = (size_t)rows * len;
+  double *tmp = nullptr;
+  PLC_CUDA(c, cudaMallocAsync(&tmp, n * sizeof(double), c->stream));
+  cudaError_t e = launch_to_f64(c, c->f_field[field], tmp, rows, len,
+                                field == PLC_SPEC ? c->nx : c->pitch, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h_dst, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  const cudaError_t ef = cudaFreeAsync(tmp, c->stream);
+  if (e == cudaSuccess) e = ef;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(c, e, "plc_download (FP32 -> FP64)");
   return PLC_OK;
 }
 
@@ -445,6 +617,7 @@ int plc_set_dt(plc_ctx *c, double dt) {
 // ---- mod_calcVel ----------------------------------------------------------
 int plc_transform2crf(plc_ctx *c, double vel_crf, double *d_vel, double *vel_force) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_vel);
   if (vel_crf != 0) {
     PLC_CUDA(c, launch_shift(c, d_vel, vel_crf, c->stream));
@@ -456,6 +629,7 @@ int plc_transform2crf(plc_ctx *c, double vel_crf, double *d_vel, double *vel_for
 int plc_time_int_vel_rk1(plc_ctx *c, double u_crf, const double *d_u, const double *d_v,
                          const double *d_w, double *d_u1, double *d_v1, double *d_w1) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -469,6 +643,7 @@ int plc_time_int_vel_rk1(plc_ctx *c, double u_crf, const double *d_u, const doub
 int plc_time_int_vel_rk2(plc_ctx *c, double u_crf, double *d_u, double *d_v, double *d_w,
                          const double *d_u1, const double *d_v1, const double *d_w1) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -481,6 +656,7 @@ int plc_time_int_vel_rk2(plc_ctx *c, double u_crf, double *d_u, double *d_v, dou
 
 int plc_correct_vel(plc_ctx *c, const double *d_p, double *d_u, double *d_v, double *d_w) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_p);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
@@ -491,6 +667,7 @@ int plc_correct_vel(plc_ctx *c, const double *d_p, double *d_u, double *d_v, dou
 
 int plc_force_vel(plc_ctx *c, double *d_u, double *d_v, double *d_w, double *force_out) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -518,6 +695,7 @@ int plc_force_vel(plc_ctx *c, double *d_u, double *d_v, double *d_w, double *for
 int plc_calc_rhs(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
                  double *d_rhs) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -529,6 +707,7 @@ int plc_calc_rhs(plc_ctx *c, const double *d_u, const double *d_v, const double 
 // ---- mod_updateBound ------------------------------------------------------
 int plc_update_bound_vel(plc_ctx *c, double u_crf, double *d_u, double *d_v, double *d_w) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -542,6 +721,7 @@ int plc_impose_bc_vel(plc_ctx *c, double *d_u, double *d_v, double *d_w, double 
 
 int plc_update_bound_p(plc_ctx *c, double *d_p) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_p);
   PLC_CUDA(c, launch_bound_p(c, d_p, c->stream));
   return PLC_OK;
@@ -575,6 +755,7 @@ int plc_free_poisson_solver(plc_ctx *c) {
 
 int plc_execute_poisson_solver(plc_ctx *c, double *d_p) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_p);
   PLC_NEED_POISSON(c);
   double *spec = c->d_field[PLC_SPEC];
@@ -588,6 +769,7 @@ int plc_execute_poisson_solver(plc_ctx *c, double *d_p) {
 
 int plc_solve_trid(plc_ctx *c, double *d_var) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_var);
   PLC_NEED_POISSON(c);
   PLC_CUDA(c, launch_trid(c, d_var, c->stream));
@@ -597,6 +779,7 @@ int plc_solve_trid(plc_ctx *c, double *d_var) {
 // ---- mod_fft --------------------------------------------------------------
 int plc_fft_fwd_xpen(plc_ctx *c, const double *d_p, double *d_var) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_p);
   PLC_REQ(c, d_var);
   PLC_NEED_POISSON(c);
@@ -606,6 +789,7 @@ int plc_fft_fwd_xpen(plc_ctx *c, const double *d_p, double *d_var) {
 
 int plc_fft_bwd_xpen(plc_ctx *c, const double *d_var, double *d_p) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_p);
   PLC_REQ(c, d_var);
   PLC_NEED_POISSON(c);
@@ -615,6 +799,7 @@ int plc_fft_bwd_xpen(plc_ctx *c, const double *d_var, double *d_p) {
 
 int plc_fft_fwd_ypen(plc_ctx *c, double *d_var) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_var);
   PLC_NEED_POISSON(c);
   PLC_CUDA(c, launch_fft_y(c, d_var, false, c->stream));
@@ -623,6 +808,7 @@ int plc_fft_fwd_ypen(plc_ctx *c, double *d_var) {
 
 int plc_fft_bwd_ypen(plc_ctx *c, double *d_var) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_var);
   PLC_NEED_POISSON(c);
   PLC_CUDA(c, launch_fft_y(c, d_var, true, c->stream));
@@ -640,18 +826,15 @@ int plc_get_eigen_values(int ist, int isz, int isz_global, const char *bctype, d
 // ---- mod_utils ------------------------------------------------------------
 int plc_mean(plc_ctx *c, int nx_global, int ny_global, const double *d_var, double *mean) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_var);
   PLC_REQ(c, mean);
-  PLC_CUDA(c, launch_mean(c, 0, nx_global, ny_global, d_var, c->stream));
-  PLC_CUDA(c, cudaMemcpyAsync(c->h_scal, reinterpret_cast<char *>(c->d_sc) + offsetof(StepConst, mean),
-                              sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
-  *mean = c->h_scal[0];
-  return PLC_OK;
+  return mean_of(c, nx_global, ny_global, d_var, mean);
 }
 
 int plc_check_nan(plc_ctx *c, const double *d_var, int *passed) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_var);
   PLC_REQ(c, passed);
   if (int rc = run_check(c, 1, d_var, d_var, d_var)) return rc;
@@ -662,6 +845,7 @@ int plc_check_nan(plc_ctx *c, const double *d_var, int *passed) {
 int plc_calc_max_cfl(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
                      plc_value_index *cfl_max) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -674,6 +858,7 @@ int plc_calc_max_cfl(plc_ctx *c, const double *d_u, const double *d_v, const dou
 int plc_calc_max_div(plc_ctx *c, const double *d_u, const double *d_v, const double *d_w,
                      plc_value_index *div_max) {
   PLC_CHECK_CTX(c);
+  PLC_NEED_FP64(c);
   PLC_REQ(c, d_u);
   PLC_REQ(c, d_v);
   PLC_REQ(c, d_w);
@@ -685,7 +870,7 @@ int plc_calc_max_div(plc_ctx *c, const double *d_u, const double *d_v, const dou
 
 int plc_check(plc_ctx *c, int *nan_passed, plc_value_index *cfl_max, plc_value_index *div_max) {
   PLC_CHECK_CTX(c);
-  if (int rc = run_check(c, 7, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W])) return rc;
+  if (int rc = run_check_fields(c, 7)) return rc;
   c->last_nan_passed = c->h_check->nan_found ? 0 : 1;
   to_ijk(c, c->h_check->cfl_idx, &c->last_cfl, c->h_check->cfl * c->dt_host);
   to_ijk(c, c->h_check->div_idx, &c->last_div, c->h_check->div);
@@ -732,27 +917,9 @@ int plc_init_flow(plc_ctx *c) {
   } else {
     return set_error(c, PLC_ERR_ARG, "unknown initial_field");
   }
-  double *u = c->d_field[PLC_U], *v = c->d_field[PLC_V], *w = c->d_field[PLC_W];
-  double *scratch = c->d_field[PLC_SPEC];  // nx*ny*nz >= nz+2
-  PLC_CUDA(c, cudaMemcpyAsync(scratch, prof.data(), prof.size() * sizeof(double),
-                              cudaMemcpyHostToDevice, c->stream));
-  PLC_CUDA(c, launch_init_flow(c, u, v, w, scratch, c->stream));
-  if (is_mean) {
-    double meanold = 0.0;
-    // the reference passes (nz, ny) as the global sizes here (mod_initFlow.cc:92)
-    if (int rc = plc_mean(c, c->nz, c->ny, u, &meanold)) return rc;
-    if (meanold != 0.0) {
-      c->h_scal[0] = 1.0 / (meanold * P.u_ref);
-      PLC_CUDA(c, cudaMemcpyAsync(scratch, c->h_scal, sizeof(double), cudaMemcpyHostToDevice,
-                                  c->stream));
-      PLC_CUDA(c, launch_scale(c, u, scratch, c->stream));
-    }
-  }
-  // main.cc:78-82
-  if (int rc = plc_transform2crf(c, P.u_crf, u, &c->prm.vel_force[0])) return rc;
-  PLC_CUDA(c, launch_bound_vel(c, P.u_crf, u, v, w, c->stream));
-  PLC_CUDA(c, launch_bound_p(c, c->d_field[PLC_P], c->stream));
-  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int rc = c->mixed ? init_fields(c, prof, is_mean, c->f_field)
+                          : init_fields(c, prof, is_mean, c->d_field);
+  if (rc != PLC_OK) return rc;
   // the graph bakes the forcing configuration in: rebuild it on the next step
   if (c->graph) {
     cudaGraphExecDestroy(c->graph);
@@ -792,7 +959,10 @@ static int step_launches(plc_ctx *c, int nsteps) {
         ok = false;
         msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
       }
-      if (dm.value > P.div_limit || std::isnan(dm.value)) {
+      // The mixed form's divergence is at FP32 rounding level: its limit is
+      // div_limit scaled by the ratio of the unit round-offs, 2^-24 / 2^-53.
+      const double div_limit = c->mixed ? P.div_limit * 536870912.0 : P.div_limit;
+      if (dm.value > div_limit || std::isnan(dm.value)) {
         ok = false;
         msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
       }

@@ -1,5 +1,6 @@
 // Batched real FFTs and the wall-normal tridiagonal solve of the Poisson
-// projection (FP64).
+// projection, in FP64 (the reference's arithmetic) and in FP32 storage for
+// the mixed-precision form.
 //
 // The reference (mod_fft.cc) copies p into a padded buffer, calls oneMKL's
 // batched real DFT and repacks the result; the y transform goes through an
@@ -17,15 +18,21 @@
 //    place with x-contiguous row segments: no transpose buffer.
 //  * The complex FFT is a mixed-radix (16, 8, 4, 2, 3) Stockham transform between
 //    two shared-memory buffers, one butterfly per thread and pass; element e
-//    of a line lives at e + e/8 to spread the strided accesses over banks.
+//    of a line lives at e + e/8 (FP64) or e + e/16 (FP32) to spread the
+//    strided accesses over the banks.
 //  * Both transforms are unscaled; the backward x transform multiplies by
 //    1/(nx*ny) (mod_fft.cc:57,116-117) and, in the fused step, also writes
 //    the pressure halos (updateBoundP, mod_updateBound.cc:287-330).
 //
+// Every kernel is a template on the storage type T (double, float); the
+// transform arithmetic runs in T with twiddles rounded once from long double.
+//
 // The tridiagonal solve (ssolve_trid, mod_poisson_solver.cc:317-357) is a
 // Thomas sweep per (kx,ky) system, one thread per system, coalesced over kx,
 // with the pre-factored reciprocal pivots read from a table indexed by the
-// distinct wavenumber pair.
+// distinct wavenumber pair.  The mixed form keeps FP32 storage but sweeps in
+// FP64, and the systems of the lowest wavenumbers keep their intermediate
+// values in an FP64 side buffer.
 
 #include <cuda_runtime.h>
 
@@ -38,31 +45,71 @@ namespace plc {
 
 namespace {
 
+template <class T>
+struct Cx;
+template <>
+struct Cx<double> {
+  using V = double2;
+  static constexpr int kPadShift = 3;  // one pad element per 128 bytes
+};
+template <>
+struct Cx<float> {
+  using V = float2;
+  static constexpr int kPadShift = 4;
+};
+template <class V>
+using ScalarOf = decltype(V::x);
+template <class V>
+constexpr int pad_shift() {
+  return Cx<ScalarOf<V>>::kPadShift;
+}
+
+template <class V>
+__device__ __forceinline__ V mk(ScalarOf<V> x, ScalarOf<V> y) {
+  V r;
+  r.x = x;
+  r.y = y;
+  return r;
+}
+
+template <class V>
 struct FftDev {
   int n, npass;
   unsigned long long radices;  // radix - 1, 4 bits per pass, pass 0 in the low bits
-  const double2 *tw;
+  const V *tw;
 };
 
-__device__ __forceinline__ int padi(int e) { return e + (e >> 3); }
+template <class V>
+__device__ __forceinline__ int padi(int e) {
+  return e + (e >> pad_shift<V>());
+}
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <class V>
+__host__ __device__ __forceinline__ constexpr int line_stride(int n) {
+  return n + (n >> pad_shift<V>()) + 1;
+}
+
+template <class V>
+__device__ __forceinline__ V cmul(V a, V b) {
+  return mk<V>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 // a * conj(b)
-__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
-  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+template <class V>
+__device__ __forceinline__ V cmulc(V a, V b) {
+  return mk<V>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
-  return make_double2(a.x + b.x, a.y + b.y);
+template <class V>
+__device__ __forceinline__ V cadd(V a, V b) {
+  return mk<V>(a.x + b.x, a.y + b.y);
 }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) {
-  return make_double2(a.x - b.x, a.y - b.y);
+template <class V>
+__device__ __forceinline__ V csub(V a, V b) {
+  return mk<V>(a.x - b.x, a.y - b.y);
 }
 // multiply by -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ double2 rot90(double2 a) {
-  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <bool INV, class V>
+__device__ __forceinline__ V rot90(V a) {
+  return INV ? mk<V>(-a.y, a.x) : mk<V>(a.y, -a.x);
 }
 
 template <int R, bool INV>
@@ -70,8 +117,9 @@ struct Dft;
 
 template <bool INV>
 struct Dft<2, INV> {
-  __device__ __forceinline__ static void run(double2 (&v)[2]) {
-    const double2 a = v[0], b = v[1];
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[2]) {
+    const V a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   }
@@ -79,9 +127,10 @@ struct Dft<2, INV> {
 
 template <bool INV>
 struct Dft<4, INV> {
-  __device__ __forceinline__ static void run(double2 (&v)[4]) {
-    const double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-    const double2 t2 = cadd(v[1], v[3]), t3 = rot90<INV>(csub(v[1], v[3]));
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[4]) {
+    const V t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const V t2 = cadd(v[1], v[3]), t3 = rot90<INV>(csub(v[1], v[3]));
     v[0] = cadd(t0, t2);
     v[2] = csub(t0, t2);
     v[1] = cadd(t1, t3);
@@ -91,20 +140,21 @@ struct Dft<4, INV> {
 
 template <bool INV>
 struct Dft<8, INV> {
-  __device__ __forceinline__ static void run(double2 (&v)[8]) {
-    const double s = 0.70710678118654752440;  // 1/sqrt(2)
-    double2 e[4] = {v[0], v[2], v[4], v[6]};
-    double2 o[4] = {v[1], v[3], v[5], v[7]};
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[8]) {
+    using S = ScalarOf<V>;
+    const S s = S(0.70710678118654752440);  // 1/sqrt(2)
+    V e[4] = {v[0], v[2], v[4], v[6]};
+    V o[4] = {v[1], v[3], v[5], v[7]};
     Dft<4, INV>::run(e);
     Dft<4, INV>::run(o);
     // o[m] *= W8^m, W8 = exp(-+ i pi/4)
-    double2 x = o[1];
-    o[1] = INV ? make_double2(s * (x.x - x.y), s * (x.x + x.y))
-               : make_double2(s * (x.x + x.y), s * (x.y - x.x));
+    V x = o[1];
+    o[1] = INV ? mk<V>(s * (x.x - x.y), s * (x.x + x.y)) : mk<V>(s * (x.x + x.y), s * (x.y - x.x));
     o[2] = rot90<INV>(o[2]);
     x = o[3];
-    o[3] = INV ? make_double2(-s * (x.x + x.y), s * (x.x - x.y))
-               : make_double2(s * (x.y - x.x), -s * (x.x + x.y));
+    o[3] = INV ? mk<V>(-s * (x.x + x.y), s * (x.x - x.y))
+               : mk<V>(s * (x.y - x.x), -s * (x.x + x.y));
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       v[m] = cadd(e[m], o[m]);
@@ -115,13 +165,15 @@ struct Dft<8, INV> {
 
 template <bool INV>
 struct Dft<16, INV> {
-  __device__ __forceinline__ static void run(double2 (&v)[16]) {
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[16]) {
     // radix-2 step over two 8-point transforms: X_k = E_k + W16^k O_k,
     // X_{k+8} = E_k - W16^k O_k, W16 = exp(-+ 2 pi i / 16)
-    const double c1 = 0.92387953251128675613;  // cos(pi/8)
-    const double s1 = 0.38268343236508977173;  // sin(pi/8)
-    const double h = 0.70710678118654752440;   // 1/sqrt(2)
-    double2 e[8], o[8];
+    using S = ScalarOf<V>;
+    const S c1 = S(0.92387953251128675613);  // cos(pi/8)
+    const S s1 = S(0.38268343236508977173);  // sin(pi/8)
+    const S h = S(0.70710678118654752440);   // 1/sqrt(2)
+    V e[8], o[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       e[m] = v[2 * m];
@@ -129,12 +181,11 @@ struct Dft<16, INV> {
     }
     Dft<8, INV>::run(e);
     Dft<8, INV>::run(o);
-    const double2 w[8] = {make_double2(1.0, 0.0), make_double2(c1, -s1), make_double2(h, -h),
-                          make_double2(s1, -c1),  make_double2(0.0, -1.0), make_double2(-s1, -c1),
-                          make_double2(-h, -h),   make_double2(-c1, -s1)};
+    const V w[8] = {mk<V>(S(1), S(0)), mk<V>(c1, -s1), mk<V>(h, -h),   mk<V>(s1, -c1),
+                    mk<V>(S(0), S(-1)), mk<V>(-s1, -c1), mk<V>(-h, -h), mk<V>(-c1, -s1)};
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const double2 t = INV ? cmulc(o[k], w[k]) : cmul(o[k], w[k]);
+      const V t = INV ? cmulc(o[k], w[k]) : cmul(o[k], w[k]);
       v[k] = cadd(e[k], t);
       v[k + 8] = csub(e[k], t);
     }
@@ -143,12 +194,14 @@ struct Dft<16, INV> {
 
 template <bool INV>
 struct Dft<3, INV> {
-  __device__ __forceinline__ static void run(double2 (&v)[3]) {
-    const double h = 0.86602540378443864676;  // sqrt(3)/2
-    const double2 t1 = cadd(v[1], v[2]);
-    const double2 t2 = make_double2(v[0].x - 0.5 * t1.x, v[0].y - 0.5 * t1.y);
-    const double2 d = csub(v[1], v[2]);
-    const double2 t3 = INV ? make_double2(-h * d.y, h * d.x) : make_double2(h * d.y, -h * d.x);
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[3]) {
+    using S = ScalarOf<V>;
+    const S h = S(0.86602540378443864676);  // sqrt(3)/2
+    const V t1 = cadd(v[1], v[2]);
+    const V t2 = mk<V>(v[0].x - S(0.5) * t1.x, v[0].y - S(0.5) * t1.y);
+    const V d = csub(v[1], v[2]);
+    const V t3 = INV ? mk<V>(-h * d.y, h * d.x) : mk<V>(h * d.y, -h * d.x);
     v[0] = cadd(v[0], t1);
     v[1] = cadd(t2, t3);
     v[2] = csub(t2, t3);
@@ -156,39 +209,38 @@ struct Dft<3, INV> {
 };
 
 // One Stockham pass of radix R over nl lines of length n (line stride LS).
-template <int R, bool INV>
-__device__ __forceinline__ void fft_pass(const double2 *__restrict__ src, double2 *__restrict__ dst,
-                                         int nl, int n, int LS, int Ns,
-                                         const double2 *__restrict__ tw) {
+template <int R, bool INV, class V>
+__device__ __forceinline__ void fft_pass(const V *__restrict__ src, V *__restrict__ dst, int nl,
+                                         int n, int LS, int Ns, const V *__restrict__ tw) {
   const int nb = n / R;
   const int tot = nl * nb;
   const int tws = n / (Ns * R);
   for (int b = threadIdx.x; b < tot; b += blockDim.x) {
     const int l = b / nb;
     const int j = b - l * nb;
-    const double2 *s = src + l * LS;
-    double2 *d = dst + l * LS;
+    const V *s = src + l * LS;
+    V *d = dst + l * LS;
     const int jm = j % Ns;
-    double2 v[R];
+    V v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[padi(j + r * nb)];
+    for (int r = 0; r < R; ++r) v[r] = s[padi<V>(j + r * nb)];
     if (jm != 0) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const double2 w = __ldg(tw + r * jm * tws);
+        const V w = __ldg(tw + r * jm * tws);
         v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
       }
     }
     Dft<R, INV>::run(v);
     const int idxD = (j / Ns) * Ns * R + jm;
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[padi(idxD + r * Ns)] = v[r];
+    for (int r = 0; r < R; ++r) d[padi<V>(idxD + r * Ns)] = v[r];
   }
 }
 
 // Complex FFT of nl lines held in A; returns the buffer holding the result.
-template <bool INV>
-__device__ double2 *fft_run(double2 *A, double2 *B, int nl, int LS, const FftDev &P) {
+template <bool INV, class V>
+__device__ V *fft_run(V *A, V *B, int nl, int LS, const FftDev<V> &P) {
   int Ns = 1;
   for (int p = 0; p < P.npass; ++p) {
     const int R = (int)((P.radices >> (4 * p)) & 15ull) + 1;
@@ -200,15 +252,13 @@ __device__ double2 *fft_run(double2 *A, double2 *B, int nl, int LS, const FftDev
       default: fft_pass<3, INV>(A, B, nl, P.n, LS, Ns, P.tw); break;
     }
     __syncthreads();
-    double2 *t = A;
+    V *t = A;
     A = B;
     B = t;
     Ns *= R;
   }
   return A;
 }
-
-__host__ __device__ __forceinline__ constexpr int line_stride(int n) { return n + (n >> 3) + 1; }
 
 // ---------------------------------------------------------------------------
 // Compile-time plans.  For the line lengths of the supported grids the radix
@@ -247,43 +297,41 @@ __host__ __device__ constexpr int plan_radix(int n, int p) {
   return 3;
 }
 
-template <int R, bool INV, int N, int NS>
-__device__ __forceinline__ void fft_pass_t(const double2 *__restrict__ src,
-                                           double2 *__restrict__ dst, int nl,
-                                           const double2 *__restrict__ tw) {
-  constexpr int nb = N / R, LS = line_stride(N), tws = N / (NS * R);
+template <int R, bool INV, int N, int NS, class V>
+__device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restrict__ dst, int nl,
+                                           const V *__restrict__ tw) {
+  constexpr int nb = N / R, LS = line_stride<V>(N), tws = N / (NS * R);
   const int tot = nl * nb;
   for (int b = threadIdx.x; b < tot; b += blockDim.x) {
     const int l = b / nb;
     const int j = b - l * nb;
-    const double2 *s = src + l * LS;
-    double2 *d = dst + l * LS;
+    const V *s = src + l * LS;
+    V *d = dst + l * LS;
     const int jm = j % NS;
-    double2 v[R];
+    V v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[padi(j + r * nb)];
+    for (int r = 0; r < R; ++r) v[r] = s[padi<V>(j + r * nb)];
     if (NS > 1 && jm != 0) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const double2 w = __ldg(tw + r * jm * tws);
+        const V w = __ldg(tw + r * jm * tws);
         v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
       }
     }
     Dft<R, INV>::run(v);
     const int idxD = (j / NS) * NS * R + jm;
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[padi(idxD + r * NS)] = v[r];
+    for (int r = 0; r < R; ++r) d[padi<V>(idxD + r * NS)] = v[r];
   }
 }
 
-template <int N, int NS, int P, bool INV>
-__device__ __forceinline__ void passes_t(double2 *&A, double2 *&B, int nl,
-                                         const double2 *__restrict__ tw) {
+template <int N, int NS, int P, bool INV, class V>
+__device__ __forceinline__ void passes_t(V *&A, V *&B, int nl, const V *__restrict__ tw) {
   if constexpr (P < plan_npass(N)) {
     constexpr int R = plan_radix(N, P);
     fft_pass_t<R, INV, N, NS>(A, B, nl, tw);
     __syncthreads();
-    double2 *t = A;
+    V *t = A;
     A = B;
     B = t;
     passes_t<N, NS * R, P + 1, INV>(A, B, nl, tw);
@@ -291,9 +339,8 @@ __device__ __forceinline__ void passes_t(double2 *&A, double2 *&B, int nl,
 }
 
 // Complex FFT of nl lines held in A (compile-time plan for N > 0).
-template <int N, bool INV>
-__device__ __forceinline__ double2 *fft_run_n(double2 *A, double2 *B, int nl, int LS,
-                                              const FftDev &P) {
+template <int N, bool INV, class V>
+__device__ __forceinline__ V *fft_run_n(V *A, V *B, int nl, int LS, const FftDev<V> &P) {
   if constexpr (N > 0) {
     passes_t<N, 1, 0, INV>(A, B, nl, P.tw);
     return A;
@@ -306,40 +353,44 @@ __device__ __forceinline__ double2 *fft_run_n(double2 *A, double2 *B, int nl, in
 // packed indices q0 = 2m and q1 = 2m+1 (q0 = 0 and q1 = 1 for m = 0, i.e.
 // X_0 and X_{n/2}), for the sequence a (real parts) and b (imaginary parts).
 // A_m = (Z_m + conj Z_{n-m})/2, B_m = (Z_m - conj Z_{n-m})/(2i).
-__device__ __forceinline__ void unpack_four(const double2 *Z, int n, int m, double2 &a,
-                                            double2 &b) {
+template <class V>
+__device__ __forceinline__ void unpack_four(const V *Z, int n, int m, V &a, V &b) {
+  using S = ScalarOf<V>;
+  const S half = S(0.5);
   if (m == 0) {
-    const double2 z0 = Z[0], zh = Z[padi(n >> 1)];
-    a = make_double2((z0.x + z0.x) * 0.5, (zh.x + zh.x) * 0.5);
-    b = make_double2((z0.y + z0.y) * 0.5, (zh.y + zh.y) * 0.5);
+    const V z0 = Z[0], zh = Z[padi<V>(n >> 1)];
+    a = mk<V>((z0.x + z0.x) * half, (zh.x + zh.x) * half);
+    b = mk<V>((z0.y + z0.y) * half, (zh.y + zh.y) * half);
   } else {
-    const double2 zm = Z[padi(m)], zc = Z[padi(n - m)];
-    a = make_double2((zm.x + zc.x) * 0.5, (zm.y - zc.y) * 0.5);
-    b = make_double2((zm.y + zc.y) * 0.5, (zc.x - zm.x) * 0.5);
+    const V zm = Z[padi<V>(m)], zc = Z[padi<V>(n - m)];
+    a = mk<V>((zm.x + zc.x) * half, (zm.y - zc.y) * half);
+    b = mk<V>((zm.y + zc.y) * half, (zc.x - zm.x) * half);
   }
 }
 
 // Builds Z_m and Z_{n-m} (0 <= m <= n/2) of the pair whose packed spectra are
 // ra[] (real sequence a) and rb[] (real sequence b), read with stride `st`.
-__device__ __forceinline__ void pack_pair(double2 *Z, int n, int m, const double *ra,
-                                          const double *rb, int st) {
-  double reA, imA, reB, imB;
+template <class V>
+__device__ __forceinline__ void pack_pair(V *Z, int n, int m, const ScalarOf<V> *ra,
+                                          const ScalarOf<V> *rb, int st) {
+  using S = ScalarOf<V>;
+  S reA, imA, reB, imB;
   if (m == 0) {
     reA = ra[0];
     reB = rb[0];
-    imA = imB = 0.0;
+    imA = imB = S(0);
   } else if (m == (n >> 1)) {
     reA = ra[st];
     reB = rb[st];
-    imA = imB = 0.0;
+    imA = imB = S(0);
   } else {
     reA = ra[(2 * m) * st];
     imA = ra[(2 * m + 1) * st];
     reB = rb[(2 * m) * st];
     imB = rb[(2 * m + 1) * st];
   }
-  Z[padi(m)] = make_double2(reA - imB, imA + reB);
-  if (m != 0 && m != (n >> 1)) Z[padi(n - m)] = make_double2(reA + imB, reB - imA);
+  Z[padi<V>(m)] = mk<V>(reA - imB, imA + reB);
+  if (m != 0 && m != (n >> 1)) Z[padi<V>(n - m)] = mk<V>(reA + imB, reB - imA);
 }
 
 // div(u)/dt at halo'd index c exactly as calcRHS evaluates it
@@ -355,35 +406,44 @@ __device__ __forceinline__ double div_dt(const double *__restrict__ u,
   const double tz = __dmul_rn(__dmul_rn(__dsub_rn(w[c], w[c - XY]), dti), dzfi);
   return __dadd_rn(__dadd_rn(tx, ty), tz);
 }
+// the mixed form: FP32 operands and arithmetic
+__device__ __forceinline__ float div_dt(const float *__restrict__ u, const float *__restrict__ v,
+                                        const float *__restrict__ w, long long c, int X,
+                                        long long XY, float dtidxi, float dtidyi, float dti,
+                                        float dzfi) {
+  return (u[c] - u[c - 1]) * dtidxi + (v[c] - v[c - X]) * dtidyi + (w[c] - w[c - XY]) * (dti * dzfi);
+}
 
 // Forward x transform fused with calcRHS, one tile per block: rows
 // (j0+2l, j0+2l+1) of plane k are div(u)/dt evaluated from global memory while
 // loading (many resident blocks hide the load latency), then transformed.
-template <int N, bool FUSED>
-__global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
-                                                   const StepConst *__restrict__ sc,
-                                                   const double *__restrict__ p,
-                                                   const double *__restrict__ u,
-                                                   const double *__restrict__ v,
-                                                   const double *__restrict__ w,
-                                                   double *__restrict__ var) {
-  extern __shared__ double2 smem[];
-  const int n = N > 0 ? N : g.nx, LS = line_stride(n);
-  double2 *A = smem, *B = smem + nl * LS;
+template <class T, int N, bool FUSED>
+__global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx<T>::V> P, int nl,
+                                                       const StepConst *__restrict__ sc,
+                                                       const T *__restrict__ p,
+                                                       const T *__restrict__ u,
+                                                       const T *__restrict__ v,
+                                                       const T *__restrict__ w,
+                                                       T *__restrict__ var) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : g.nx, LS = line_stride<V>(n);
+  V *A = smem, *B = smem + nl * LS;
   const int j0 = blockIdx.x * 2 * nl;  // 0-based row in the plane
   const int k = blockIdx.y;            // 0-based plane
-  double dti = 0, dtidxi = 0, dtidyi = 0, dzfi = 0;
+  T dti = 0, dtidxi = 0, dtidyi = 0, dzfi = 0;
   if (FUSED) {
-    dti = sc->dti;
-    dtidxi = sc->dtidxi;
-    dtidyi = sc->dtidyi;
-    dzfi = __ldg(g.dzf_inv + k + 1);
+    dti = T(sc->dti);
+    dtidxi = T(sc->dtidxi);
+    dtidyi = T(sc->dtidyi);
+    dzfi = T(__ldg(g.dzf_inv + k + 1));
   }
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
     const int l = e / n, t = e - l * n;
     const long long ca = g.at(t + 1, j0 + 2 * l + 1, k + 1);
     const long long cb = ca + g.X;
-    double a, b;
+    T a, b;
     if (FUSED) {
       a = div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
       b = div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
@@ -391,18 +451,18 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev P, int nl,
       a = p[ca];
       b = p[cb];
     }
-    A[l * LS + padi(t)] = make_double2(a, b);
+    A[l * LS + padi<V>(t)] = mk<V>(a, b);
   }
   __syncthreads();
-  const double2 *Z = fft_run_n<N, false>(A, B, nl, LS, P);
+  const V *Z = fft_run_n<N, false>(A, B, nl, LS, P);
   const int half = n >> 1;
   for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
     const int l = e / half, m = e - l * half;
-    double2 a, b;
+    V a, b;
     unpack_four(Z + l * LS, n, m, a, b);
     const long long row = (long long)k * g.ny + j0 + 2 * l;
-    reinterpret_cast<double2 *>(var + row * n)[m] = a;
-    reinterpret_cast<double2 *>(var + (row + 1) * n)[m] = b;
+    reinterpret_cast<V *>(var + row * n)[m] = a;
+    reinterpret_cast<V *>(var + (row + 1) * n)[m] = b;
   }
 }
 
@@ -426,27 +486,31 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-// Copies `rows` rows of `len` doubles (len even, 16-byte aligned rows) from
-// src (row stride `stride` doubles) to dst (row stride `len`).
-__device__ __forceinline__ void stage_rows(double *dst, const double *src, int rows, int len,
+// Copies `rows` rows of `len` elements (len a multiple of 16 bytes, 16-byte
+// aligned rows) from src (row stride `stride` elements) to dst (row stride
+// `len`).
+template <class T>
+__device__ __forceinline__ void stage_rows(T *dst, const T *src, int rows, int len,
                                            long long stride) {
-  const int cpr = len >> 1;  // 16-byte chunks per row
+  constexpr int per = 16 / sizeof(T);  // elements per 16-byte chunk
+  const int cpr = len / per;           // chunks per row
   for (int e = threadIdx.x; e < rows * cpr; e += blockDim.x) {
     const int r = e / cpr, ch = e - r * cpr;
-    cp_async16(dst + r * len + 2 * ch, src + r * stride + 2 * ch);
+    cp_async16(dst + r * len + per * ch, src + r * stride + per * ch);
   }
 }
 
 // Forward x transform (persistent): rows (j0+2l, j0+2l+1) of p at plane k ->
 // packed spectra.  The halo'd rows are staged whole (16-byte aligned).
-template <int N>
-__global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
-                                                   const double *__restrict__ p,
-                                                   double *__restrict__ var) {
-  extern __shared__ double2 smem[];
-  const int n = N > 0 ? N : g.nx, LS = line_stride(n), X = g.X, R = 2 * nl;
-  double2 *A = smem, *B = smem + nl * LS;
-  double *S = reinterpret_cast<double *>(B + nl * LS);  // R halo'd rows
+template <class T, int N>
+__global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>::V> P, int nl,
+                                                   const T *__restrict__ p, T *__restrict__ var) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : g.nx, LS = line_stride<V>(n), X = g.X, R = 2 * nl;
+  V *A = smem, *B = smem + nl * LS;
+  T *S = reinterpret_cast<T *>(B + nl * LS);  // R halo'd rows
   const int tiles_y = g.ny / R;
   const int ntiles = tiles_y * g.nz;
   auto issue = [&](int tile) {
@@ -462,34 +526,37 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev P, int nl,
     __syncthreads();
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
       const int l = e / n, t = e - l * n;
-      A[l * LS + padi(t)] = make_double2(S[(2 * l) * X + t + 1], S[(2 * l + 1) * X + t + 1]);
+      A[l * LS + padi<V>(t)] = mk<V>(S[(2 * l) * X + t + 1], S[(2 * l + 1) * X + t + 1]);
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run_n<N, false>(A, B, nl, LS, P);
+    const V *Z = fft_run_n<N, false>(A, B, nl, LS, P);
     const int half = n >> 1;
     for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
       const int l = e / half, m = e - l * half;
-      double2 a, b;
+      V a, b;
       unpack_four(Z + l * LS, n, m, a, b);
       const long long row = (long long)k * g.ny + j0 + 2 * l;
-      reinterpret_cast<double2 *>(var + row * n)[m] = a;
-      reinterpret_cast<double2 *>(var + (row + 1) * n)[m] = b;
+      reinterpret_cast<V *>(var + row * n)[m] = a;
+      reinterpret_cast<V *>(var + (row + 1) * n)[m] = b;
     }
   }
 }
 
 // Backward x transform: packed spectra -> p interior scaled by nf; with
 // FUSE_BC the pressure halos are written as well (updateBoundP).
-template <int N, bool FUSE_BC>
-__global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, double nf,
-                                                   const double *__restrict__ var, double *p) {
-  extern __shared__ double2 smem[];
-  const int n = N > 0 ? N : g.nx, LS = line_stride(n), R = 2 * nl;
-  double2 *A = smem, *B = smem + nl * LS;
-  double *S = reinterpret_cast<double *>(B + nl * LS);  // R rows of n doubles
+template <class T, int N, bool FUSE_BC>
+__global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>::V> P, int nl,
+                                                   double nf, const T *__restrict__ var, T *p) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : g.nx, LS = line_stride<V>(n), R = 2 * nl;
+  V *A = smem, *B = smem + nl * LS;
+  T *S = reinterpret_cast<T *>(B + nl * LS);  // R rows of n elements
   const int tiles_y = g.ny / R;
   const int ntiles = tiles_y * g.nz;
+  const T scale = T(nf);
   auto issue = [&](int tile) {
     const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
     stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n);
@@ -508,15 +575,15 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, doub
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run_n<N, true>(A, B, nl, LS, P);
+    const V *Z = fft_run_n<N, true>(A, B, nl, LS, P);
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
       const int l = e / n, t = e - l * n;
-      const double2 z = Z[l * LS + padi(t)];
-      const double a = nf * z.x, b = nf * z.y;
+      const V z = Z[l * LS + padi<V>(t)];
+      const T a = scale * z.x, b = scale * z.y;
       const int i = t + 1, ja = j0 + 2 * l + 1, kk = k + 1;
       if (FUSE_BC) {
-        store_with_halo(p, g, i, ja, kk, a, BC_ZEROGRAD, 0.0);
-        store_with_halo(p, g, i, ja + 1, kk, b, BC_ZEROGRAD, 0.0);
+        store_with_halo(p, g, i, ja, kk, a, BC_ZEROGRAD, T(0));
+        store_with_halo(p, g, i, ja + 1, kk, b, BC_ZEROGRAD, T(0));
       } else {
         const long long ca = g.at(i, ja, kk);
         p[ca] = a;
@@ -527,14 +594,17 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev P, int nl, doub
 }
 
 // y transform in place on the spectral array: tile = columns i0..i0+2nl-1 of
-// plane k (TX = 2nl x-contiguous doubles per row, row stride nx).
-template <int N, bool INV>
-__global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P, int nl,
-                                               double *__restrict__ var) {
-  extern __shared__ double2 smem[];
-  const int n = N > 0 ? N : ny, LS = line_stride(n), TX = 2 * nl;
-  double2 *A = smem, *B = smem + nl * LS;
-  double *S = reinterpret_cast<double *>(B + nl * LS);  // n rows of TX doubles
+// plane k (TX = 2nl x-contiguous elements per row, row stride nx).
+template <class T, int N, bool INV>
+__global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
+                                               FftDev<typename Cx<T>::V> P, int nl,
+                                               T *__restrict__ var) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : ny, LS = line_stride<V>(n), TX = 2 * nl;
+  V *A = smem, *B = smem + nl * LS;
+  T *S = reinterpret_cast<T *>(B + nl * LS);  // n rows of TX elements
   const int tiles_x = nx / TX;
   const int ntiles = tiles_x * nz;
   auto issue = [&](int tile) {
@@ -547,13 +617,13 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P,
   const int half = n >> 1;
   for (; tile < ntiles; tile += gridDim.x) {
     const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
-    double *plane = var + (long long)k * nx * ny + i0;
+    T *plane = var + (long long)k * nx * ny + i0;
     cp_async_wait_all();
     __syncthreads();
     if (!INV) {
       for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
         const int t = e / TX, c = e - t * TX;
-        reinterpret_cast<double *>(A + (c >> 1) * LS + padi(t))[c & 1] = S[e];
+        reinterpret_cast<T *>(A + (c >> 1) * LS + padi<V>(t))[c & 1] = S[e];
       }
     } else {
       for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
@@ -563,35 +633,45 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz, FftDev P,
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const double2 *Z = fft_run_n<N, INV>(A, B, nl, LS, P);
+    const V *Z = fft_run_n<N, INV>(A, B, nl, LS, P);
     if (!INV) {
       for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
         const int m = e / nl, l = e - m * nl;
-        double2 a, b;
+        V a, b;
         unpack_four(Z + l * LS, n, m, a, b);
         const int q0 = (m == 0) ? 0 : 2 * m;
         // row q0: (A, B) of columns 2l, 2l+1; row q0+1 likewise
-        reinterpret_cast<double2 *>(plane + (long long)q0 * nx)[l] = make_double2(a.x, b.x);
-        reinterpret_cast<double2 *>(plane + (long long)(q0 + 1) * nx)[l] = make_double2(a.y, b.y);
+        reinterpret_cast<V *>(plane + (long long)q0 * nx)[l] = mk<V>(a.x, b.x);
+        reinterpret_cast<V *>(plane + (long long)(q0 + 1) * nx)[l] = mk<V>(a.y, b.y);
       }
     } else {
       for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
         const int t = e / TX, c = e - t * TX;
-        const double2 z = Z[(c >> 1) * LS + padi(t)];
+        const V z = Z[(c >> 1) * LS + padi<V>(t)];
         plane[(long long)t * nx + c] = (c & 1) ? z.y : z.x;
       }
     }
   }
 }
 
+// ---------------------------------------------------------------------------
 // Thomas sweep per (i,j) system with the reciprocal pivot table
 // rpiv[(k*(ny/2+1) + my)*(nx/2+1) + mx]; the reference's divisions by b
 // become multiplications by 1/b (mod_poisson_solver.cc:334-354).
+//
+// T = double: the reference's solve.  T = float (mixed form): FP32 storage,
+// FP64 arithmetic; systems whose packed indices are both below kLowModes
+// (the lowest wavenumbers, which carry the largest amplification 1/lambda and
+// the singular (0,0) mode) keep the forward-elimination values in the FP64
+// buffer `low` [k][j][i] (kLowModes^2 per plane) instead of rounding them to
+// FP32 in place.
+// ---------------------------------------------------------------------------
+template <class T>
 __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
                                               const double *__restrict__ rpiv,
                                               const double *__restrict__ a,
-                                              const double *__restrict__ c,
-                                              double *__restrict__ var) {
+                                              const double *__restrict__ c, T *__restrict__ var,
+                                              double *__restrict__ low) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const long long plane = (long long)nx * ny;
   if (t >= plane) return;
@@ -601,12 +681,27 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
   const int MX = (nx >> 1) + 1;
   const long long PS = (long long)MX * ((ny >> 1) + 1);
   const double *rp = rpiv + (long long)my * MX + mx;
-  double *q = var + t;
+  T *q = var + t;
+  constexpr bool kMixed = std::is_same<T, float>::value;
+  const bool in_low = kMixed && i < kLowModes && j < kLowModes;
+  double *lq = in_low ? low + j * kLowModes + i : nullptr;
+  constexpr long long LP = (long long)kLowModes * kLowModes;  // low-buffer plane stride
+  // the forward values go to the FP64 buffer for the low systems
+  auto put_fwd = [&](int k, double x) {
+    if (kMixed && in_low)
+      lq[k * LP] = x;
+    else
+      q[(long long)k * plane] = T(x);
+  };
+  auto get_fwd = [&](int k) -> double {
+    if (kMixed && in_low) return lq[k * LP];
+    return double(q[(long long)k * plane]);
+  };
   // The sweeps are sequential in k, but their loads are not: batches of PF
   // planes of the right-hand side and of the pivots are loaded one batch
   // ahead of the elimination, so 2*PF loads per thread are in flight.
   constexpr int PF = 8;
-  double prev = q[0];
+  double prev = double(q[0]);
   {
     // forward elimination over k = 1 .. nz-1
     double xn[PF], rn[PF];
@@ -614,9 +709,10 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (k + s < nz) {
-        xn[s] = q[(long long)(k + s) * plane];
+        xn[s] = double(q[(long long)(k + s) * plane]);
         rn[s] = __ldg(rp + (long long)(k + s - 1) * PS);
       }
+    if (kMixed && in_low) lq[0] = prev;
     for (; k < nz; k += PF) {
       double x[PF], r[PF];
 #pragma unroll
@@ -628,7 +724,7 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (kn + s < nz) {
-          xn[s] = q[(long long)(kn + s) * plane];
+          xn[s] = double(q[(long long)(kn + s) * plane]);
           rn[s] = __ldg(rp + (long long)(kn + s - 1) * PS);
         }
 #pragma unroll
@@ -636,13 +732,13 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
         if (k + s < nz) {
           double cur = x[s];
           cur -= (__ldg(a + k + s) * r[s]) * prev;
-          q[(long long)(k + s) * plane] = cur;
+          put_fwd(k + s, cur);
           prev = cur;
         }
     }
   }
   prev *= __ldg(rp + (long long)(nz - 1) * PS);
-  q[(long long)(nz - 1) * plane] = prev;
+  q[(long long)(nz - 1) * plane] = T(prev);
   {
     // back substitution over k = nz-2 .. 0
     double xn[PF], rn[PF];
@@ -650,7 +746,7 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (k - s >= 0) {
-        xn[s] = q[(long long)(k - s) * plane];
+        xn[s] = get_fwd(k - s);
         rn[s] = __ldg(rp + (long long)(k - s) * PS);
       }
     for (; k >= 0; k -= PF) {
@@ -664,52 +760,63 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (kn - s >= 0) {
-          xn[s] = q[(long long)(kn - s) * plane];
+          xn[s] = get_fwd(kn - s);
           rn[s] = __ldg(rp + (long long)(kn - s) * PS);
         }
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (k - s >= 0) {
           const double cur = (x[s] - __ldg(c + k - s) * prev) * r[s];
-          q[(long long)(k - s) * plane] = cur;
+          q[(long long)(k - s) * plane] = T(cur);
           prev = cur;
         }
     }
   }
 }
 
-FftDev dev_plan(const FftPlan &p) {
-  FftDev d;
+template <class T>
+FftDev<typename Cx<T>::V> dev_plan(const FftPlan &p) {
+  FftDev<typename Cx<T>::V> d;
   d.n = p.n;
   d.npass = p.npass;
   d.radices = 0ull;
   for (int r = 0; r < p.npass; ++r) d.radices |= (unsigned long long)(p.radix[r] - 1) << (4 * r);
-  d.tw = p.tw;
+  if constexpr (std::is_same<T, double>::value)
+    d.tw = p.tw;
+  else
+    d.tw = p.tw32;
   return d;
+}
+
+template <class T>
+size_t fft_bytes(int n, int lines) {
+  using V = typename Cx<T>::V;
+  return 2ull * (size_t)lines * (size_t)line_stride<V>(n) * sizeof(V);
 }
 
 }  // namespace
 
-size_t fft_smem_bytes(int n, int lines) {
-  return 2ull * (size_t)lines * (size_t)line_stride(n) * sizeof(double2);
-}
+size_t fft_smem_bytes(int n, int lines) { return fft_bytes<double>(n, lines); }
 
 namespace {
+template <class T>
 size_t smem_x_fwd(int nx, int nl) {
-  return fft_smem_bytes(nx, nl) + (size_t)2 * nl * (nx + 2) * sizeof(double);
+  return fft_bytes<T>(nx, nl) + (size_t)2 * nl * (nx + 2) * sizeof(T);
 }
+template <class T>
 size_t smem_x_bwd(int nx, int nl) {
-  return fft_smem_bytes(nx, nl) + (size_t)2 * nl * nx * sizeof(double);
+  return fft_bytes<T>(nx, nl) + (size_t)2 * nl * nx * sizeof(T);
 }
+template <class T>
 size_t smem_y(int ny, int nl) {
-  return fft_smem_bytes(ny, nl) + (size_t)ny * 2 * nl * sizeof(double);
+  return fft_bytes<T>(ny, nl) + (size_t)ny * 2 * nl * sizeof(T);
 }
-// Largest number of line pairs per tile that divides `pairs` and keeps the
-// kernel's shared memory under `cap` bytes.
+// Largest number of line pairs per tile that divides `pairs`, is a multiple
+// of `step` and keeps the kernel's shared memory under `cap` bytes.
 template <class F>
-int pick_lines(int pairs, size_t cap, F bytes) {
-  int best = 1;
-  for (int d = 1; d <= pairs && d <= 16; ++d)
+int pick_lines(int pairs, size_t cap, F bytes, int step = 1) {
+  int best = step;
+  for (int d = step; d <= pairs && d <= 16; d += step)
     if (pairs % d == 0 && bytes(d) <= cap) best = d;
   return best;
 }
@@ -755,12 +862,18 @@ cudaError_t fft_configure(size_t max_bytes) {
 #define PLC_SMEM(kern)                                                                        \
   r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_bytes); \
   if (r != cudaSuccess) return r;
-      PLC_SMEM(k_fft_x_fwd<N>);
-      PLC_SMEM((k_fft_x_fwd_div<N, true>));
-      PLC_SMEM((k_fft_x_bwd<N, true>));
-      PLC_SMEM((k_fft_x_bwd<N, false>));
-      PLC_SMEM((k_fft_y<N, true>));
-      PLC_SMEM((k_fft_y<N, false>));
+      PLC_SMEM((k_fft_x_fwd<double, N>));
+      PLC_SMEM((k_fft_x_fwd_div<double, N, true>));
+      PLC_SMEM((k_fft_x_bwd<double, N, true>));
+      PLC_SMEM((k_fft_x_bwd<double, N, false>));
+      PLC_SMEM((k_fft_y<double, N, true>));
+      PLC_SMEM((k_fft_y<double, N, false>));
+      PLC_SMEM((k_fft_x_fwd<float, N>));
+      PLC_SMEM((k_fft_x_fwd_div<float, N, true>));
+      PLC_SMEM((k_fft_x_bwd<float, N, true>));
+      PLC_SMEM((k_fft_x_bwd<float, N, false>));
+      PLC_SMEM((k_fft_y<float, N, true>));
+      PLC_SMEM((k_fft_y<float, N, false>));
 #undef PLC_SMEM
       return cudaSuccess;
     });
@@ -769,92 +882,139 @@ cudaError_t fft_configure(size_t max_bytes) {
   return cudaSuccess;
 }
 
+namespace {
+template <class T>
+cudaError_t fft_setup_t(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max, int sms) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  // FP32 staging copies 16-byte chunks of 4 elements: tiles of the y
+  // transform then span a multiple of 4 columns (an even number of pairs)
+  const int ystep = sizeof(T) == 4 ? 2 : 1;
+  c->fft_lines_x =
+      pick_lines(ny / 2, smem_cap_per_block, [&](int d) { return smem_x_bwd<T>(nx, d); });
+  c->fft_lines_xf = pick_lines(ny / 2, 64 * 1024, [&](int d) { return fft_bytes<T>(nx, d); });
+  c->fft_lines_y = pick_lines(
+      nx / 2, smem_cap_per_block, [&](int d) { return smem_y<T>(ny, d); }, ystep);
+  const size_t need[4] = {smem_x_fwd<T>(nx, c->fft_lines_x), fft_bytes<T>(nx, c->fft_lines_xf),
+                          smem_x_bwd<T>(nx, c->fft_lines_x), smem_y<T>(ny, c->fft_lines_y)};
+  for (size_t b : need)
+    if (b > dev_max) return cudaErrorInvalidValue;
+  const long long tiles_x = (long long)(ny / (2 * c->fft_lines_x)) * nz;
+  const long long tiles_y = (long long)(nx / (2 * c->fft_lines_y)) * nz;
+  cudaError_t e = with_size(nx, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    c->grid_xf = persistent_grid(k_fft_x_fwd<T, N>, 128, need[0], sms, tiles_x);
+    c->grid_xb = persistent_grid(k_fft_x_bwd<T, N, true>, 128, need[2], sms, tiles_x);
+    return cudaSuccess;
+  });
+  if (e != cudaSuccess) return e;
+  return with_size(ny, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    c->grid_y = persistent_grid(k_fft_y<T, N, false>, 256, need[3], sms, tiles_y);
+    return cudaSuccess;
+  });
+}
+}  // namespace
+
 // Tile sizes (line pairs per tile) and persistent grid sizes of the
 // transforms, from the shared memory each needs and the occupancy it gets.
 cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max) {
   int sms = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   if (e != cudaSuccess) return e;
-  const int nx = c->nx, ny = c->ny, nz = c->nz;
-  c->fft_lines_x = pick_lines(ny / 2, smem_cap_per_block, [&](int d) { return smem_x_bwd(nx, d); });
-  c->fft_lines_xf = pick_lines(ny / 2, 64 * 1024, [&](int d) { return fft_smem_bytes(nx, d); });
-  c->fft_lines_y = pick_lines(nx / 2, smem_cap_per_block, [&](int d) { return smem_y(ny, d); });
-  const size_t need[4] = {smem_x_fwd(nx, c->fft_lines_x), fft_smem_bytes(nx, c->fft_lines_xf),
-                          smem_x_bwd(nx, c->fft_lines_x), smem_y(ny, c->fft_lines_y)};
-  for (size_t b : need)
-    if (b > dev_max) return cudaErrorInvalidValue;
-  const long long tiles_x = (long long)(ny / (2 * c->fft_lines_x)) * nz;
-  const long long tiles_y = (long long)(nx / (2 * c->fft_lines_y)) * nz;
-  e = with_size(nx, [&](auto NC) -> cudaError_t {
-    constexpr int N = decltype(NC)::value;
-    c->grid_xf = persistent_grid(k_fft_x_fwd<N>, 128, need[0], sms, tiles_x);
-    c->grid_xb = persistent_grid(k_fft_x_bwd<N, true>, 128, need[2], sms, tiles_x);
-    return cudaSuccess;
-  });
-  if (e != cudaSuccess) return e;
-  return with_size(ny, [&](auto NC) -> cudaError_t {
-    constexpr int N = decltype(NC)::value;
-    c->grid_y = persistent_grid(k_fft_y<N, false>, 256, need[3], sms, tiles_y);
-    return cudaSuccess;
-  });
+  return c->mixed ? fft_setup_t<float>(c, smem_cap_per_block, dev_max, sms)
+                  : fft_setup_t<double>(c, smem_cap_per_block, dev_max, sms);
 }
 
-cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u, const double *v,
-                             const double *w, double *var, cudaStream_t s) {
+namespace {
+template <class T>
+cudaError_t fft_x_fwd_t(const plc_ctx *c, const T *p, const T *u, const T *v, const T *w, T *var,
+                        cudaStream_t s) {
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
     if (p) {
       const int nl = c->fft_lines_x;
-      k_fft_x_fwd<N><<<c->grid_xf, 128, smem_x_fwd(c->nx, nl), s>>>(
-          c->geo(), dev_plan(c->plan_x), nl, p, var);
+      k_fft_x_fwd<T, N><<<c->grid_xf, 128, smem_x_fwd<T>(c->nx, nl), s>>>(
+          c->geo(), dev_plan<T>(c->plan_x), nl, p, var);
     } else {
       const int nl = c->fft_lines_xf;
       dim3 grid(c->ny / (2 * nl), c->nz);
-      k_fft_x_fwd_div<N, true><<<grid, 256, fft_smem_bytes(c->nx, nl), s>>>(
-          c->geo(), dev_plan(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
+      k_fft_x_fwd_div<T, N, true><<<grid, 256, fft_bytes<T>(c->nx, nl), s>>>(
+          c->geo(), dev_plan<T>(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
     }
     return cudaGetLastError();
   });
 }
 
-cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p, bool fuse_bc,
-                             cudaStream_t s) {
+template <class T>
+cudaError_t fft_x_bwd_t(const plc_ctx *c, const T *var, T *p, bool fuse_bc, cudaStream_t s) {
   const int nl = c->fft_lines_x;
-  const size_t sm = smem_x_bwd(c->nx, nl);
+  const size_t sm = smem_x_bwd<T>(c->nx, nl);
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
     if (fuse_bc)
-      k_fft_x_bwd<N, true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf,
-                                                        var, p);
+      k_fft_x_bwd<T, N, true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan<T>(c->plan_x), nl,
+                                                           nf, var, p);
     else
-      k_fft_x_bwd<N, false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan(c->plan_x), nl, nf,
-                                                         var, p);
+      k_fft_x_bwd<T, N, false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan<T>(c->plan_x), nl,
+                                                            nf, var, p);
     return cudaGetLastError();
   });
 }
 
-cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse, cudaStream_t s) {
+template <class T>
+cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
   const int nl = c->fft_lines_y;
-  const size_t sm = smem_y(c->ny, nl);
+  const size_t sm = smem_y<T>(c->ny, nl);
   return with_size(c->ny, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
     if (inverse)
-      k_fft_y<N, true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl,
-                                                   var);
+      k_fft_y<T, N, true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan<T>(c->plan_y),
+                                                      nl, var);
     else
-      k_fft_y<N, false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan(c->plan_y), nl,
-                                                    var);
+      k_fft_y<T, N, false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
+                                                       dev_plan<T>(c->plan_y), nl, var);
     return cudaGetLastError();
   });
 }
 
-cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
+template <class T>
+cudaError_t trid_t(const plc_ctx *c, T *var, cudaStream_t s) {
   const long long plane = (long long)c->nx * c->ny;
   const int bs = 128;
-  k_trid<<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(c->nx, c->ny, c->nz, c->d_rpiv,
-                                                          c->d_ac, c->d_ac + c->nz, var);
+  k_trid<T><<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(
+      c->nx, c->ny, c->nz, c->d_rpiv, c->d_ac, c->d_ac + c->nz, var, c->d_low);
   return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u, const double *v,
+                             const double *w, double *var, cudaStream_t s) {
+  return fft_x_fwd_t<double>(c, p, u, v, w, var, s);
+}
+cudaError_t launch_fft_x_fwd(const plc_ctx *c, const float *u, const float *v, const float *w,
+                             float *var, cudaStream_t s) {
+  return fft_x_fwd_t<float>(c, nullptr, u, v, w, var, s);
+}
+cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p, bool fuse_bc,
+                             cudaStream_t s) {
+  return fft_x_bwd_t<double>(c, var, p, fuse_bc, s);
+}
+cudaError_t launch_fft_x_bwd(const plc_ctx *c, const float *var, float *p, bool fuse_bc,
+                             cudaStream_t s) {
+  return fft_x_bwd_t<float>(c, var, p, fuse_bc, s);
+}
+cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse, cudaStream_t s) {
+  return fft_y_t<double>(c, var, inverse, s);
+}
+cudaError_t launch_fft_y(const plc_ctx *c, float *var, bool inverse, cudaStream_t s) {
+  return fft_y_t<float>(c, var, inverse, s);
+}
+cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
+  return trid_t<double>(c, var, s);
+}
+cudaError_t launch_trid(const plc_ctx *c, float *var, cudaStream_t s) {
+  return trid_t<float>(c, var, s);
 }
 
 }  // namespace plc

@@ -49,30 +49,41 @@ struct FftPlan {
   int n = 0;
   int npass = 0;
   int radix[16] = {0};
-  double2 *tw = nullptr;  // device, n entries: exp(-2 pi i t / n)
+  double2 *tw = nullptr;   // device, n entries: exp(-2 pi i t / n)
+  float2 *tw32 = nullptr;  // the same rounded to FP32 (mixed form)
 };
 
 // capacity (blocks) of each plane of the reduction partials array
 constexpr int kMaxBlocksReduce = 4096;
+
+// Mixed form: Thomas systems whose packed x and y indices are both below
+// kLowModes (wavenumbers |m| < kLowModes/2, the Nyquist line of each axis
+// included) sweep with FP64 intermediates.
+constexpr int kLowModes = 16;
 
 }  // namespace plc
 
 struct plc_ctx {
   plc_params prm;
   int device = 0;
+  bool mixed = false;  // PLC_MIXED: FP32 fields in f_field, d_field unused
   int nx = 0, ny = 0, nz = 0;
+  int pitch = 0;       // x stride of the halo'd fields: nx+2 (FP64), a multiple of 4 (FP32)
   double dx = 0, dy = 0, dx_inv = 0, dy_inv = 0, re_inv = 0;
-  size_t nfield = 0;  // (nx+2)(ny+2)(nz+2)
+  size_t nfield = 0;  // pitch*(ny+2)*(nz+2)
   size_t nspec = 0;   // nx*ny*nz
   // host copies of the mesh (nz+2 each)
   std::vector<double> h_dzf_global, h_dzf, h_dzf_inv, h_dzc, h_dzc_inv, h_dzflzi,
       h_zc_global;
   double *d_mesh = nullptr;  // dzf | dzf_inv | dzc_inv | dzflzi
   double *d_field[8] = {nullptr};
+  float *f_field[8] = {nullptr};  // mixed form: the same fields in FP32
   // Poisson solver state
   bool poisson_ready = false;
   double *d_rpiv = nullptr;   // 1/b, (nz, ny/2+1, nx/2+1)
   double *d_ac = nullptr;     // a[nz] | c[nz]
+  double *d_low = nullptr;    // mixed form: FP64 sweep values of the low modes
+  float *d_coef32 = nullptr;  // mixed form: per-plane RK coefficients
   plc::FftPlan plan_x, plan_y;
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
   int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids
@@ -133,32 +144,70 @@ int host_parse_param_json(const char *path, plc_params *prm, std::string &err);
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf,
                       const double *qu, const double *qv, const double *qw,
                       double *ou, double *ov, double *ow, cudaStream_t s);
+// mixed form (plc_mixed.cu): FP32 operands, FP32 arithmetic
+cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf,
+                      const float *qu, const float *qv, const float *qw,
+                      float *ou, float *ov, float *ow, cudaStream_t s);
+// FP64 rows of `len` elements (the reference's layout) <-> FP32 rows of
+// stride `pitch` (the context's layout)
+cudaError_t launch_to_f32(const plc_ctx *c, const double *src, float *dst, long long rows, int len,
+                          int pitch, cudaStream_t s);
+cudaError_t launch_to_f64(const plc_ctx *c, const float *src, double *dst, long long rows, int len,
+                          int pitch, cudaStream_t s);
+// per-plane coefficient rows of the FP32 RK kernels, rk32_coef_floats() per plane
+void host_rk32_coef(const plc_ctx *c, std::vector<float> &out);
+int rk32_coef_floats();
 cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v,
                             const double *w, double *rhs, cudaStream_t s);
 cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p,
                            double *u, double *v, double *w, cudaStream_t s);
+cudaError_t launch_correct(const plc_ctx *c, bool fused, const float *p,
+                           float *u, float *v, float *w, cudaStream_t s);
 cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u,
                                double *v, double *w, cudaStream_t s);
+cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, float *u,
+                               float *v, float *w, cudaStream_t s);
 cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg,
                         const double *var, cudaStream_t s);
+cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg,
+                        const float *var, cudaStream_t s);
 cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, double *u,
                              double *v, double *w, cudaStream_t s);
+cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, float *u,
+                             float *v, float *w, cudaStream_t s);
 cudaError_t launch_bound_p(const plc_ctx *c, double *p, cudaStream_t s);
+cudaError_t launch_bound_p(const plc_ctx *c, float *p, cudaStream_t s);
 cudaError_t launch_shift(const plc_ctx *c, double *var, double delta,
+                         cudaStream_t s);
+cudaError_t launch_shift(const plc_ctx *c, float *var, double delta,
                          cudaStream_t s);
 cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u,
                              const double *v, const double *w, double *var,
                              cudaStream_t s);
+// mixed form: calcRHS fused with the forward x transform only
+cudaError_t launch_fft_x_fwd(const plc_ctx *c, const float *u, const float *v,
+                             const float *w, float *var, cudaStream_t s);
 cudaError_t launch_fft_x_bwd(const plc_ctx *c, const double *var, double *p,
+                             bool fuse_bc, cudaStream_t s);
+cudaError_t launch_fft_x_bwd(const plc_ctx *c, const float *var, float *p,
                              bool fuse_bc, cudaStream_t s);
 cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse,
                          cudaStream_t s);
+cudaError_t launch_fft_y(const plc_ctx *c, float *var, bool inverse,
+                         cudaStream_t s);
 cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s);
+cudaError_t launch_trid(const plc_ctx *c, float *var, cudaStream_t s);
 cudaError_t launch_check(const plc_ctx *c, const double *u, const double *v,
                          const double *w, int what, cudaStream_t s);
+cudaError_t launch_check(const plc_ctx *c, const float *u, const float *v,
+                         const float *w, int what, cudaStream_t s);
 cudaError_t launch_init_flow(const plc_ctx *c, double *u, double *v, double *w,
                              const double *d_prof, cudaStream_t s);
+cudaError_t launch_init_flow(const plc_ctx *c, float *u, float *v, float *w,
+                             const double *d_prof, cudaStream_t s);
 cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult,
+                         cudaStream_t s);
+cudaError_t launch_scale(const plc_ctx *c, float *var, const double *d_mult,
                          cudaStream_t s);
 size_t fft_smem_bytes(int n, int lines);
 cudaError_t fft_configure(size_t max_bytes);

@@ -1,0 +1,428 @@
+// FP32 kernels of the mixed-precision form: the two RK stages and the
+// conversions between the reference's FP64 host layout and the context's
+// FP32 fields.
+//
+// The mixed form stores u, v, w, u1, v1, w1, p and the spectral array in
+// FP32; the halo'd fields keep the reference's (i, j, k) layout but with the
+// x row padded to a multiple of 4 elements (16 bytes), so that every row and
+// plane starts on a 16-byte boundary for the bulk tensor copies.  Scalars
+// (dt, the forcing), reductions (bulk mean, NaN/CFL/divergence checks) and
+// the tridiagonal sweep stay FP64.
+//
+// RK stages (mod_calcVel.cc:27-129 and :140-242): the same z-marching
+// structure as the FP64 kernel -- a 32 x 8 block of (i, j) columns walks a
+// chunk of z planes, each operand plane brought into a 5-slot shared-memory
+// ring by one cp.async.bulk.tensor copy per field two planes ahead -- but the
+// momentum right-hand side is evaluated in FP32 with fused multiply-adds and
+// with the z interpolation weights folded into ten per-plane coefficients
+// (an algebraic rearrangement of the reference's expressions).
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "plc_device.cuh"
+#include "plc_internal.h"
+
+namespace plc {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+namespace {
+
+constexpr int RX = 32, RY = 8;
+constexpr int HX = 36;                  // 34 columns used; TMA rows are whole 16-byte units
+constexpr int HY = RY + 2;              // 10
+constexpr int PLANE = HX * HY;          // floats per field-plane
+constexpr int SLOT = ((PLANE * 4 + 127) / 128) * 128 / 4;  // floats, 128-B aligned
+constexpr int NSLOT = 5;
+constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 4u;
+constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up
+constexpr int KCHUNK = 32;
+constexpr int NCOEF = 12;               // per-plane coefficient row (10 used), 3 float4
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_plane(float *dst, const CUtensorMap *map, int x, int y,
+                                               int z, unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z),
+      "r"(smem_addr(bar))
+      : "memory");
+}
+
+// x/y constants of the momentum right-hand side
+struct RkConst {
+  float qx, qy;    // 0.25/dx, 0.25/dy (convection)
+  float rx, ry;    // re_inv/dx^2, re_inv/dy^2 (diffusion)
+  float crf;       // 0.5*u_crf/dx (convecting frame; 0 when u_crf = 0)
+};
+
+// Per-plane coefficient row k (FP64 on the host, rounded once):
+//   [0] at = dzf(k+1)/dzc(k)   [1] bt = dzf(k)/dzc(k)      z interpolation to the
+//   [2] ab = dzf(k-1)/dzc(k-1) [3] bb = dzf(k)/dzc(k-1)    top/bottom faces
+//   [4] cz = 0.25/dzf(k)       [5] cw = 0.25/dzc(k)        convection, centred / w
+//   [6] vt = re_inv/(dzf(k) dzc(k))     [7] vb = re_inv/(dzf(k) dzc(k-1))
+//   [8] wt = re_inv/(dzc(k) dzf(k+1))   [9] wb = re_inv/(dzc(k) dzf(k))
+struct alignas(16) Coef {
+  float at, bt, ab, bb, cz, cw, vt, vb, wt, wb, pad0, pad1;
+};
+
+struct Rhs3f {
+  float u, v, w;
+};
+
+// (visc - conv) at one point; P(f, di, dj, dk) reads field f (0 u, 1 v, 2 w)
+// at offset (di, dj, dk) from the point.
+template <bool CRF, class Acc>
+__device__ __forceinline__ Rhs3f momentum_rhs32(const RkConst &K, const Coef &z, const Acc &P) {
+  const float u0 = P(0, 0, 0, 0), v0 = P(1, 0, 0, 0), w0 = P(2, 0, 0, 0);
+  Rhs3f r;
+  {
+    const float upx = P(0, 1, 0, 0), umx = P(0, -1, 0, 0), upy = P(0, 0, 1, 0),
+                umy = P(0, 0, -1, 0), uzp = P(0, 0, 0, 1), uzm = P(0, 0, 0, -1);
+    const float ue = u0 + upx, uw = umx + u0, un = u0 + upy, us = umy + u0;
+    const float ut = fmaf(u0, z.at, uzp * z.bt), ub = fmaf(u0, z.ab, uzm * z.bb);
+    const float vn = v0 + P(1, 1, 0, 0), vs = P(1, 0, -1, 0) + P(1, 1, -1, 0);
+    const float wt = w0 + P(2, 1, 0, 0), wb = P(2, 0, 0, -1) + P(2, 1, 0, -1);
+    float conv = K.qx * (ue * ue - uw * uw) + K.qy * (un * vn - us * vs) +
+                 z.cz * (ut * wt - ub * wb);
+    if (CRF) conv = fmaf(K.crf, ue - uw, conv);
+    const float visc = K.rx * ((upx - u0) - (u0 - umx)) + K.ry * ((upy - u0) - (u0 - umy)) +
+                       (z.vt * (uzp - u0) - z.vb * (u0 - uzm));
+    r.u = visc - conv;
+  }
+  {
+    const float vpx = P(1, 1, 0, 0), vmx = P(1, -1, 0, 0), vpy = P(1, 0, 1, 0),
+                vmy = P(1, 0, -1, 0), vzp = P(1, 0, 0, 1), vzm = P(1, 0, 0, -1);
+    const float ve = v0 + vpx, vw = vmx + v0, vn = v0 + vpy, vs = vmy + v0;
+    const float vt = fmaf(v0, z.at, vzp * z.bt), vb = fmaf(v0, z.ab, vzm * z.bb);
+    const float ue = u0 + P(0, 0, 1, 0), uw = P(0, -1, 0, 0) + P(0, -1, 1, 0);
+    const float wt = w0 + P(2, 0, 1, 0), wb = P(2, 0, 0, -1) + P(2, 0, 1, -1);
+    float conv = K.qx * (ue * ve - uw * vw) + K.qy * (vn * vn - vs * vs) +
+                 z.cz * (wt * vt - wb * vb);
+    if (CRF) conv = fmaf(K.crf, ve - vw, conv);
+    const float visc = K.rx * ((vpx - v0) - (v0 - vmx)) + K.ry * ((vpy - v0) - (v0 - vmy)) +
+                       (z.vt * (vzp - v0) - z.vb * (v0 - vzm));
+    r.v = visc - conv;
+  }
+  {
+    const float wpx = P(2, 1, 0, 0), wmx = P(2, -1, 0, 0), wpy = P(2, 0, 1, 0),
+                wmy = P(2, 0, -1, 0), wzp = P(2, 0, 0, 1), wzm = P(2, 0, 0, -1);
+    const float we = w0 + wpx, ww = wmx + w0, wn = w0 + wpy, ws = wmy + w0;
+    const float wt = w0 + wzp, wb = w0 + wzm;
+    const float ue = fmaf(u0, z.at, P(0, 0, 0, 1) * z.bt);
+    const float uw = fmaf(P(0, -1, 0, 0), z.at, P(0, -1, 0, 1) * z.bt);
+    const float vn = fmaf(v0, z.at, P(1, 0, 0, 1) * z.bt);
+    const float vs = fmaf(P(1, 0, -1, 0), z.at, P(1, 0, -1, 1) * z.bt);
+    float conv = K.qx * (ue * we - uw * ww) + K.qy * (vn * wn - vs * ws) +
+                 z.cw * (wt * wt - wb * wb);
+    if (CRF) conv = fmaf(K.crf, we - ww, conv);
+    const float visc = K.rx * ((wpx - w0) - (w0 - wmx)) + K.ry * ((wpy - w0) - (w0 - wmy)) +
+                       (z.wt * (wzp - w0) - z.wb * (w0 - wzm));
+    r.w = visc - conv;
+  }
+  return r;
+}
+
+// Operand access from the three plane slots (k-1, k, k+1) of each field.
+struct SmemAcc32 {
+  const float *base;
+  int off[3];  // slot offset of planes k-1, k, k+1 plus the thread's point
+  __device__ __forceinline__ float operator()(int f, int di, int dj, int dk) const {
+    return base[f * NSLOT * SLOT + off[dk + 1] + di + dj * HX];
+  }
+};
+
+size_t rk32_smem_bytes() {
+  return (size_t)3 * NSLOT * SLOT * 4 + (size_t)(KCHUNK + 2) * NCOEF * 4 + NSLOT * 8 + 128;
+}
+
+// RK1 (STAGE 1): o = q + dt*F(q);  RK2 (STAGE 2): o = (q + dt*F(q) + o)/2.
+// FUSE: the halo images and wall ghosts of the result are written as well.
+template <int STAGE, bool FUSE, bool CRF>
+__global__ void __launch_bounds__(RX *RY, 4)
+    k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
+           const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
+           const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
+           float *ou, float *ov, float *ow, int kchunk, int *err) {
+  extern __shared__ unsigned char smem_raw[];
+  float *base = reinterpret_cast<float *>(
+      (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
+  Coef *zc = reinterpret_cast<Coef *>(base + 3 * NSLOT * SLOT);  // planes kb-1 .. ke+1
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
+  __shared__ int ok_s;
+
+  const int tid = threadIdx.x;
+  const int tx = tid & (RX - 1), ty = tid / RX;
+  const int x0 = blockIdx.x * RX, y0 = blockIdx.y * RY;  // halo'd coords of the tile corner
+  const int i = x0 + tx + 1, j = y0 + ty + 1;
+  const bool active = (i <= g.nx) && (j <= g.ny);
+  const int kb = blockIdx.z * kchunk + 1;
+  const int ke = min(kb + kchunk - 1, g.nz);
+  const int plast = ke + 1;  // last plane to bring in
+  float *slot = base;
+
+  auto issue = [&](int p) {  // thread 0 only
+    const int rel = p - (kb - 1);
+    const int s = rel % NSLOT;
+    mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
+    tma_load_plane(slot + s * SLOT, &mu, x0, y0, p, &bar[s]);
+    tma_load_plane(slot + NSLOT * SLOT + s * SLOT, &mv, x0, y0, p, &bar[s]);
+    tma_load_plane(slot + 2 * NSLOT * SLOT + s * SLOT, &mw, x0, y0, p, &bar[s]);
+  };
+  auto wait_plane = [&](int p) -> bool {  // thread 0 only
+    const int rel = p - (kb - 1);
+    const int s = rel % NSLOT;
+    const unsigned parity = (unsigned)((rel / NSLOT) & 1);
+    for (long long it = 0; it < kWaitLimit; ++it)
+      if (mbar_try_wait(&bar[s], parity)) return true;
+    return false;
+  };
+
+  if (tid == 0) {
+    for (int s = 0; s < NSLOT; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int p = kb - 1; p <= min(kb + 2, plast); ++p) issue(p);
+  }
+  // coefficient rows of the block's planes
+  for (int e = tid; e < (ke - kb + 1) * NCOEF; e += blockDim.x)
+    reinterpret_cast<float *>(zc)[e] = __ldg(reinterpret_cast<const float *>(coef + kb) + e);
+  __syncthreads();
+
+  const float dt = float(sc->dt);
+  const long long XY = g.XY;
+  long long c = g.at(active ? i : 1, active ? j : 1, kb);
+  float bu = 0.f, bv = 0.f, bw = 0.f;  // RK2 base values (u, v, w) of plane k
+  if (STAGE == 2 && active) {
+    bu = ou[c];
+    bv = ov[c];
+    bw = ow[c];
+  }
+  const int o = (ty + 1) * HX + (tx + 1);
+  for (int k = kb; k <= ke; ++k) {
+    __syncthreads();  // every thread is done with plane k-2's slot
+    if (tid == 0) {
+      bool ok = true;
+      if (k + 3 <= plast) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(k + 3);
+      }
+      if (k == kb) ok = wait_plane(kb - 1) && wait_plane(kb);
+      ok = ok && wait_plane(k + 1);
+      ok_s = ok ? 1 : 0;
+      if (!ok) {
+        atomicExch(err, 1);
+        // give the copies still in flight a bounded chance to land before
+        // the block leaves
+        for (int p = k + 2; p <= min(k + 3, plast); ++p) {
+          const int rel = p - (kb - 1);
+          for (int it = 0; it < (1 << 20); ++it)
+            if (mbar_try_wait(&bar[rel % NSLOT], (unsigned)((rel / NSLOT) & 1))) break;
+        }
+      }
+    }
+    __syncthreads();
+    if (!ok_s) return;  // the whole block leaves together
+    float nbu = 0.f, nbv = 0.f, nbw = 0.f;
+    if (STAGE == 2 && active && k < ke) {
+      nbu = ou[c + XY];
+      nbv = ov[c + XY];
+      nbw = ow[c + XY];
+    }
+    if (active) {
+      const int rel = k - (kb - 1);
+      SmemAcc32 a;
+      a.base = slot;
+      a.off[0] = ((rel - 1) % NSLOT) * SLOT + o;
+      a.off[1] = (rel % NSLOT) * SLOT + o;
+      a.off[2] = ((rel + 1) % NSLOT) * SLOT + o;
+      const Coef z = zc[k - kb];
+      const Rhs3f r = momentum_rhs32<CRF>(K, z, a);
+      const float qu = a(0, 0, 0, 0), qv = a(1, 0, 0, 0), qw = a(2, 0, 0, 0);
+      float nu, nv, nw;
+      if (STAGE == 1) {
+        nu = fmaf(dt, r.u, qu);
+        nv = fmaf(dt, r.v, qv);
+        nw = fmaf(dt, r.w, qw);
+      } else {
+        nu = (fmaf(dt, r.u, qu) + bu) * 0.5f;
+        nv = (fmaf(dt, r.v, qv) + bv) * 0.5f;
+        nw = (fmaf(dt, r.w, qw) + bw) * 0.5f;
+      }
+      if (FUSE) {
+        store_with_halo(ou, g, i, j, k, nu, BC_CENTRED, bc_u);
+        store_with_halo(ov, g, i, j, k, nv, BC_CENTRED, 0.f);
+        store_with_halo(ow, g, i, j, k, nw, BC_FACE, 0.f);
+      } else {
+        ou[c] = nu;
+        ov[c] = nv;
+        ow[c] = nw;
+      }
+    }
+    bu = nbu;
+    bv = nbv;
+    bw = nbw;
+    c += XY;
+  }
+}
+
+// Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 10
+// tile of one plane.  The pitch is a multiple of 4 (16 bytes) and the tile's x
+// origin 32*bx is 128-byte aligned.
+bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g) {
+  auto enc = tensor_map_encoder();
+  if (!enc || (reinterpret_cast<unsigned long long>(ptr) & 15ull) || (g.X & 3)) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)g.X, (cuuint64_t)g.Y, (cuuint64_t)(g.nz + 2)};
+  cuuint64_t strides[2] = {(cuuint64_t)g.X * 4ull, (cuuint64_t)g.XY * 4ull};
+  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)HY, 1u};
+  cuuint32_t estr[3] = {1u, 1u, 1u};
+  const CUresult r =
+      enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box,
+          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int STAGE, bool FUSE, bool CRF>
+cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
+                          const CUtensorMap &mw, const RkConst &K, float bc_u, float *ou,
+                          float *ov, float *ow, cudaStream_t s) {
+  const size_t smem = rk32_smem_bytes();  // about 25 KB: below the default limit
+  const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
+  dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
+  k_rk32<STAGE, FUSE, CRF><<<grid, RX * RY, smem, s>>>(
+      mu, mv, mw, c->geo(), K, reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou,
+      ov, ow, kchunk, c->d_err);
+  return cudaGetLastError();
+}
+
+// FP64 (row length len) -> FP32 (row pitch), rows rows
+__global__ void k_to_f32(const double *__restrict__ src, float *__restrict__ dst, long long rows,
+                         int len, int pitch) {
+  const long long n = rows * len;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long r = t / len;
+    const int x = (int)(t - r * len);
+    dst[r * pitch + x] = (float)src[t];
+  }
+}
+
+__global__ void k_to_f64(const float *__restrict__ src, double *__restrict__ dst, long long rows,
+                         int len, int pitch) {
+  const long long n = rows * len;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long r = t / len;
+    const int x = (int)(t - r * len);
+    dst[t] = (double)src[r * pitch + x];
+  }
+}
+
+unsigned convert_blocks(const plc_ctx *c, long long n) {
+  long long b = (n + 255) / 256;
+  const long long cap = 16ll * c->num_sms;
+  return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace
+
+cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const float *qu,
+                      const float *qv, const float *qw, float *ou, float *ov, float *ow,
+                      cudaStream_t s) {
+  const Geo g = c->geo();
+  CUtensorMap mu, mv, mw;
+  if (!field_tensor_map32(&mu, qu, g) || !field_tensor_map32(&mv, qv, g) ||
+      !field_tensor_map32(&mw, qw, g))
+    return cudaErrorInvalidValue;  // FP32 fields are allocated 16-byte aligned and padded
+  RkConst K;
+  K.qx = float(0.25 * c->dx_inv);
+  K.qy = float(0.25 * c->dy_inv);
+  K.rx = float(c->re_inv * c->dx_inv * c->dx_inv);
+  K.ry = float(c->re_inv * c->dy_inv * c->dy_inv);
+  K.crf = float(0.5 * u_crf * c->dx_inv);
+  const float bc_u = float(0.0 - u_crf);
+  const bool crf = (u_crf != 0.0);
+#define PLC_RK32(S, F, C) return launch_rk32_t<S, F, C>(c, mu, mv, mw, K, bc_u, ou, ov, ow, s)
+  if (stage == 1) {
+    if (fuse_bc) {
+      if (crf) PLC_RK32(1, true, true);
+      PLC_RK32(1, true, false);
+    }
+    if (crf) PLC_RK32(1, false, true);
+    PLC_RK32(1, false, false);
+  }
+  if (fuse_bc) {
+    if (crf) PLC_RK32(2, true, true);
+    PLC_RK32(2, true, false);
+  }
+  if (crf) PLC_RK32(2, false, true);
+  PLC_RK32(2, false, false);
+#undef PLC_RK32
+}
+
+cudaError_t launch_to_f32(const plc_ctx *c, const double *src, float *dst, long long rows, int len,
+                          int pitch, cudaStream_t s) {
+  const long long n = rows * len;
+  k_to_f32<<<convert_blocks(c, n), 256, 0, s>>>(src, dst, rows, len, pitch);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_f64(const plc_ctx *c, const float *src, double *dst, long long rows, int len,
+                          int pitch, cudaStream_t s) {
+  const long long n = rows * len;
+  k_to_f64<<<convert_blocks(c, n), 256, 0, s>>>(src, dst, rows, len, pitch);
+  return cudaGetLastError();
+}
+
+// Per-plane coefficient rows of the FP32 RK kernels (k = 0 .. nz+1; the rows
+// of the ghost planes are not used).
+void host_rk32_coef(const plc_ctx *c, std::vector<float> &out) {
+  const int nz = c->nz;
+  out.assign((size_t)(nz + 2) * NCOEF, 0.f);
+  for (int k = 1; k <= nz; ++k) {
+    const double dzf_m = c->h_dzf[k - 1], dzf_0 = c->h_dzf[k], dzf_p = c->h_dzf[k + 1];
+    const double dzfi_0 = c->h_dzf_inv[k], dzfi_p = c->h_dzf_inv[k + 1];
+    const double dzci_m = c->h_dzc_inv[k - 1], dzci_0 = c->h_dzc_inv[k];
+    float *r = out.data() + (size_t)k * NCOEF;
+    r[0] = float(dzf_p * dzci_0);
+    r[1] = float(dzf_0 * dzci_0);
+    r[2] = float(dzf_m * dzci_m);
+    r[3] = float(dzf_0 * dzci_m);
+    r[4] = float(0.25 * dzfi_0);
+    r[5] = float(0.25 * dzci_0);
+    r[6] = float(c->re_inv * dzfi_0 * dzci_0);
+    r[7] = float(c->re_inv * dzfi_0 * dzci_m);
+    r[8] = float(c->re_inv * dzci_0 * dzfi_p);
+    r[9] = float(c->re_inv * dzci_0 * dzfi_0);
+  }
+}
+
+int rk32_coef_floats() { return NCOEF; }
+
+}  // namespace plc

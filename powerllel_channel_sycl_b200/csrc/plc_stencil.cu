@@ -507,8 +507,10 @@ __device__ __forceinline__ void interior_coords(const Geo &g, long long t, int &
 }
 
 // Mean (mod_utils.cc:30-51): sum(var*dzflzi) / nxg / nyg -> sc->mean[comp]
+// (products and sums in FP64 also for an FP32 field)
+template <class T>
 __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, int nxg, int nyg,
-                                              const double *__restrict__ var, double *partials,
+                                              const T *__restrict__ var, double *partials,
                                               unsigned int *counter) {
   __shared__ double smem[2 * 32];
   const long long n = (long long)g.nx * g.ny * g.nz;
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, in
        t += (long long)gridDim.x * blockDim.x) {
     int i, j, k;
     interior_coords(g, t, i, j, k);
-    dd_add(s[0], var[g.at(i, j, k)] * __ldg(g.dzflzi + k));
+    dd_add(s[0], double(var[g.at(i, j, k)]) * __ldg(g.dzflzi + k));
   }
   block_sum<1>(s, smem);
   if (grid_sum_last<1>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
@@ -556,8 +558,9 @@ struct ForceCfg {
 // flight while it finishes the current one, and the block reduces once at the
 // end (a reduction tail per short-lived block would cost more than the
 // correction itself).
+template <class T>
 struct CorrIn {
-  double pc, px, py, pz, u, v, w;
+  T pc, px, py, pz, u, v, w;
 };
 
 __device__ __forceinline__ bool tile_point(const Geo &g, long long tile, int tiles_x, int tiles_y,
@@ -572,10 +575,10 @@ __device__ __forceinline__ bool tile_point(const Geo &g, long long tile, int til
   return i <= g.nx && j <= g.ny;
 }
 
-__device__ __forceinline__ CorrIn corr_load(const Geo &g, const double *__restrict__ p,
-                                            const double *u, const double *v, const double *w,
-                                            long long c) {
-  CorrIn x;
+template <class T>
+__device__ __forceinline__ CorrIn<T> corr_load(const Geo &g, const T *__restrict__ p, const T *u,
+                                               const T *v, const T *w, long long c) {
+  CorrIn<T> x;
   x.pc = p[c];
   x.px = p[c + 1];
   x.py = p[c + g.X];
@@ -586,51 +589,54 @@ __device__ __forceinline__ CorrIn corr_load(const Geo &g, const double *__restri
   return x;
 }
 
+// T = double: the reference's arithmetic.  T = float (mixed form): the
+// correction in FP32, the bulk sums of the forced components in FP64.
+template <class T>
 __global__ void __launch_bounds__(256, 4) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
-                                                          const double *__restrict__ p, double *u,
-                                                          double *v, double *w, double *partials,
+                                                          const T *__restrict__ p, T *u, T *v,
+                                                          T *w, double *partials,
                                                           unsigned int *counter) {
   __shared__ double smem[2 * 3 * 32];
-  const double dtdxi = sc->dtdxi, dtdyi = sc->dtdyi, dt = sc->dt;
+  const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
   const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 7) / 8;
   const long long ntiles = (long long)tiles_x * tiles_y * g.nz;
   DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
   long long tile = blockIdx.x;
   int i = 0, j = 0, k = 0;
   bool ok = tile < ntiles && tile_point(g, tile, tiles_x, tiles_y, i, j, k);
-  CorrIn cur{};
+  CorrIn<T> cur{};
   if (ok) cur = corr_load(g, p, u, v, w, g.at(i, j, k));
   for (; tile < ntiles; tile += gridDim.x) {
     // issue the next tile's loads before finishing this one
     const long long nt = tile + gridDim.x;
     int ni = 0, nj = 0, nk = 0;
     const bool nok = nt < ntiles && tile_point(g, nt, tiles_x, tiles_y, ni, nj, nk);
-    CorrIn nxt{};
+    CorrIn<T> nxt{};
     if (nok) nxt = corr_load(g, p, u, v, w, g.at(ni, nj, nk));
     if (ok) {
       const long long c = g.at(i, j, k);
       // correctVel, mod_calcVel.cc:272-274
-      const double nu = cur.u - (cur.px - cur.pc) * dtdxi;
-      const double nv = cur.v - (cur.py - cur.pc) * dtdyi;
-      const double nw = cur.w - (cur.pz - cur.pc) * dt * __ldg(g.dzc_inv + k);
+      const T nu = cur.u - (cur.px - cur.pc) * dtdxi;
+      const T nv = cur.v - (cur.py - cur.pc) * dtdyi;
+      const T nw = cur.w - (cur.pz - cur.pc) * dt * T(__ldg(g.dzc_inv + k));
       const double dzl = __ldg(g.dzflzi + k);
       if (fc.forced[0]) {
         u[c] = nu;
-        dd_add(s[0], nu * dzl);
+        dd_add(s[0], double(nu) * dzl);
       } else {
-        store_with_halo(u, g, i, j, k, nu, BC_CENTRED, 0.0 - fc.u_crf);
+        store_with_halo(u, g, i, j, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
       }
       if (fc.forced[1]) {
         v[c] = nv;
-        dd_add(s[1], nv * dzl);
+        dd_add(s[1], double(nv) * dzl);
       } else {
-        store_with_halo(v, g, i, j, k, nv, BC_CENTRED, 0.0);
+        store_with_halo(v, g, i, j, k, nv, BC_CENTRED, T(0));
       }
       if (fc.forced[2]) {
         w[c] = nw;
-        dd_add(s[2], nw * dzl);
+        dd_add(s[2], double(nw) * dzl);
       } else {
-        store_with_halo(w, g, i, j, k, nw, BC_FACE, 0.0);
+        store_with_halo(w, g, i, j, k, nw, BC_FACE, T(0));
       }
     }
     cur = nxt;
@@ -659,10 +665,9 @@ __global__ void __launch_bounds__(256, 4) k_correct_fused(Geo g, StepConst *sc, 
 // refreshed from the new interior values (the final updateBoundVel of
 // main.cc:153).
 // Each thread walks kz planes of one column; all its loads are issued first.
-template <bool FUSE>
+template <class T, bool FUSE>
 __global__ void __launch_bounds__(BX *BY) k_force_apply(Geo g, const StepConst *__restrict__ sc,
-                                                        ForceCfg fc, double *u, double *v,
-                                                        double *w, int kz) {
+                                                        ForceCfg fc, T *u, T *v, T *w, int kz) {
   constexpr int KMAX = 8;
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
@@ -670,22 +675,22 @@ __global__ void __launch_bounds__(BX *BY) k_force_apply(Geo g, const StepConst *
   const int nk = min(kz, g.nz - kb + 1);
   if (i > g.nx || j > g.ny) return;
   const long long c0 = g.at(i, j, kb);
-  double *q[3] = {u, v, w};
+  T *q[3] = {u, v, w};
   const int kind[3] = {BC_CENTRED, BC_CENTRED, BC_FACE};
-  const double bc[3] = {0.0 - fc.u_crf, 0.0, 0.0};
+  const T bc[3] = {T(0.0 - fc.u_crf), T(0), T(0)};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (!fc.forced[d]) continue;
-    const double f = sc->force[d];
+    const T f = T(sc->force[d]);
     for (int k0 = 0; k0 < nk; k0 += KMAX) {
-      double x[KMAX];
+      T x[KMAX];
 #pragma unroll
       for (int s = 0; s < KMAX; ++s)
         if (k0 + s < nk) x[s] = q[d][c0 + (long long)(k0 + s) * g.XY];
 #pragma unroll
       for (int s = 0; s < KMAX; ++s)
         if (k0 + s < nk) {
-          const double nv = x[s] + f;
+          const T nv = x[s] + f;
           if (FUSE)
             store_with_halo(q[d], g, i, j, kb + k0 + s, nv, kind[d], bc[d]);
           else
@@ -697,8 +702,8 @@ __global__ void __launch_bounds__(BX *BY) k_force_apply(Geo g, const StepConst *
 
 // Boundary update of the velocity (mod_updateBound.cc:263-285) as one kernel
 // over the interior: every interior point rewrites its own halo images.
-__global__ void __launch_bounds__(BX *BY) k_bound_vel(Geo g, double u_crf, double *u, double *v,
-                                                      double *w) {
+template <class T>
+__global__ void __launch_bounds__(BX *BY) k_bound_vel(Geo g, double u_crf, T *u, T *v, T *w) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -706,37 +711,42 @@ __global__ void __launch_bounds__(BX *BY) k_bound_vel(Geo g, double u_crf, doubl
   // only points that own an image do any work
   if (!(i == 1 || i == g.nx || j == 1 || j == g.ny || k == 1 || k == g.nz)) return;
   const long long c = g.at(i, j, k);
-  store_with_halo(u, g, i, j, k, u[c], BC_CENTRED, 0.0 - u_crf);
-  store_with_halo(v, g, i, j, k, v[c], BC_CENTRED, 0.0);
-  store_with_halo(w, g, i, j, k, w[c], BC_FACE, 0.0);
+  store_with_halo(u, g, i, j, k, u[c], BC_CENTRED, T(0.0 - u_crf));
+  store_with_halo(v, g, i, j, k, v[c], BC_CENTRED, T(0));
+  store_with_halo(w, g, i, j, k, w[c], BC_FACE, T(0));
 }
 
-__global__ void __launch_bounds__(BX *BY) k_bound_p(Geo g, double *p) {
+template <class T>
+__global__ void __launch_bounds__(BX *BY) k_bound_p(Geo g, T *p) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   if (i > g.nx || j > g.ny) return;
   if (!(i == 1 || i == g.nx || j == 1 || j == g.ny || k == 1 || k == g.nz)) return;
-  store_with_halo(p, g, i, j, k, p[g.at(i, j, k)], BC_ZEROGRAD, 0.0);
+  store_with_halo(p, g, i, j, k, p[g.at(i, j, k)], BC_ZEROGRAD, T(0));
 }
 
 // var -= delta on the interior (transform2CRF, mod_calcVel.cc:13-25)
-__global__ void k_shift(Geo g, double *var, double delta) {
+template <class T>
+__global__ void k_shift(Geo g, T *var, double delta) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   if (i > g.nx || j > g.ny) return;
-  var[g.at(i, j, k)] -= delta;
+  const long long c = g.at(i, j, k);
+  var[c] = T(var[c] - delta);
 }
 
 // var *= *mult on the interior (bulk rescale of initFlow, mod_initFlow.cc:108-118)
-__global__ void k_scale(Geo g, double *var, const double *mult) {
+template <class T>
+__global__ void k_scale(Geo g, T *var, const double *mult) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   if (i > g.nx || j > g.ny) return;
   const double m = *mult;
-  var[g.at(i, j, k)] *= m;
+  const long long c = g.at(i, j, k);
+  var[c] = T(var[c] * m);
 }
 
 // Project noise generator: minstd (48271, 2^31-1) seeded with `seed` and
@@ -757,8 +767,10 @@ __device__ __forceinline__ double noise_uniform(int seed, long long offset) {
 
 // initFlow (mod_initFlow.cc:47-106) before the bulk rescale: u = profile(k)
 // plus noise, v and w noise only; halos untouched (zero).
+// (computed in FP64 and stored in T)
+template <class T>
 __global__ void k_init_flow(Geo g, const double *__restrict__ prof, int with_noise, double norm,
-                            double *u, double *v, double *w) {
+                            T *u, T *v, T *w) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -773,9 +785,9 @@ __global__ void k_init_flow(Geo g, const double *__restrict__ prof, int with_noi
     vv = __dadd_rn(vv, __dmul_rn(__dmul_rn(2.0, __dsub_rn(noise_uniform(456, off), 0.5)), norm));
     ww = __dadd_rn(ww, __dmul_rn(__dmul_rn(2.0, __dsub_rn(noise_uniform(789, off), 0.5)), norm));
   }
-  u[c] = uu;
-  v[c] = vv;
-  w[c] = ww;
+  u[c] = T(uu);
+  v[c] = T(vv);
+  w[c] = T(ww);
 }
 
 // ---------------------------------------------------------------------------
@@ -816,10 +828,12 @@ __device__ void block_max(MaxIdx &a, MaxIdx *smem) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_check(Geo g, int what, const double *__restrict__ u,
-                                               const double *__restrict__ v,
-                                               const double *__restrict__ w, double *partials,
-                                               unsigned int *counter, CheckResult *out) {
+// (an FP32 field is checked in FP64 arithmetic)
+template <class T>
+__global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restrict__ u,
+                                               const T *__restrict__ v, const T *__restrict__ w,
+                                               double *partials, unsigned int *counter,
+                                               CheckResult *out) {
   __shared__ MaxIdx smem[32];
   __shared__ int nan_s;
   __shared__ bool am_last;
@@ -842,15 +856,15 @@ __global__ void __launch_bounds__(256) k_check(Geo g, int what, const double *__
       interior_coords(g, t, i, j, k);
       const long long c = g.at(i, j, k);
       const double dzfi = __ldg(g.dzf_inv + k);
+      const double uc = u[c], um = u[c - 1], vc = v[c], vm = v[c - g.X], wc = w[c],
+                   wm = w[c - g.XY];
       if (what & 2) {
-        const double r = fabs((u[c] + u[c - 1]) * 0.5) * g.dx_inv +
-                         fabs((v[c] + v[c - g.X]) * 0.5) * g.dy_inv +
-                         fabs((w[c] + w[c - g.XY]) * 0.5) * dzfi;
+        const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
+                         fabs((wc + wm) * 0.5) * dzfi;
         max_combine(cfl, r, c);
       }
       if (what & 4) {
-        const double d = fabs((u[c] - u[c - 1]) * g.dx_inv + (v[c] - v[c - g.X]) * g.dy_inv +
-                              (w[c] - w[c - g.XY]) * dzfi);
+        const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
         max_combine(div, d, c);
       }
     }
@@ -911,6 +925,8 @@ inline ForceCfg force_cfg(const plc_ctx *c) {
   return fc;
 }
 
+}  // namespace
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (the
 // library does not link libcuda directly).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -925,6 +941,8 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   }();
   return fn;
 }
+
+namespace {
 
 // Tensor map of one halo'd field: dims (X, Y, Z), box = one 34 x 10 halo tile
 // of one plane.  Base and strides are multiples of 16 bytes (X is even); the
@@ -991,76 +1009,134 @@ cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p, double *u, double *v,
-                           double *w, cudaStream_t s) {
-  const Geo g = c->geo();
-  if (!fused) {
-    k_correct<<<interior_grid(c), dim3(BX, BY), 0, s>>>(g, c->d_sc, p, u, v, w);
-  } else {
-    // one wave: 4 resident blocks per SM (launch bounds), at most the tiles
-    const long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
-    long long nb = 4ll * c->num_sms;
-    if (nb > tiles) nb = tiles;
-    if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
-    k_correct_fused<<<(unsigned)nb, 256, 0, s>>>(g, c->d_sc, force_cfg(c), p, u, v, w,
-                                                  c->d_partials, c->d_counter);
-  }
+namespace {
+template <class T>
+cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cudaStream_t s) {
+  // one wave: 4 resident blocks per SM (launch bounds), at most the tiles
+  const long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
+  long long nb = 4ll * c->num_sms;
+  if (nb > tiles) nb = tiles;
+  if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
+  k_correct_fused<T><<<(unsigned)nb, 256, 0, s>>>(c->geo(), c->d_sc, force_cfg(c), p, u, v, w,
+                                                   c->d_partials, c->d_counter);
   return cudaGetLastError();
 }
 
-cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u, double *v, double *w,
-                               cudaStream_t s) {
+template <class T>
+cudaError_t force_apply_t(const plc_ctx *c, bool fuse_bc, T *u, T *v, T *w, cudaStream_t s) {
   const ForceCfg fc = force_cfg(c);
   if (!fc.forced[0] && !fc.forced[1] && !fc.forced[2]) return cudaSuccess;
   const int kz = 8;
   dim3 grid((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, (c->nz + kz - 1) / kz);
   if (fuse_bc)
-    k_force_apply<true><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
+    k_force_apply<T, true><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
   else
-    k_force_apply<false><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
+    k_force_apply<T, false><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, fc, u, v, w, kz);
   return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t check_t(const plc_ctx *c, const T *u, const T *v, const T *w, int what,
+                    cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(c->d_check, 0, sizeof(CheckResult), s);
+  if (e != cudaSuccess) return e;
+  k_check<T><<<reduce_blocks(c), 256, 0, s>>>(c->geo(), what, u, v, w, c->d_partials,
+                                              c->d_counter + 2, c->d_check);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p, double *u, double *v,
+                           double *w, cudaStream_t s) {
+  if (fused) return correct_fused_t<double>(c, p, u, v, w, s);
+  k_correct<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, p, u, v, w);
+  return cudaGetLastError();
+}
+// mixed form: the fused correction of the step only
+cudaError_t launch_correct(const plc_ctx *c, bool fused, const float *p, float *u, float *v,
+                           float *w, cudaStream_t s) {
+  if (!fused) return cudaErrorInvalidValue;
+  return correct_fused_t<float>(c, p, u, v, w, s);
+}
+
+cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u, double *v, double *w,
+                               cudaStream_t s) {
+  return force_apply_t<double>(c, fuse_bc, u, v, w, s);
+}
+cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, float *u, float *v, float *w,
+                               cudaStream_t s) {
+  return force_apply_t<float>(c, fuse_bc, u, v, w, s);
 }
 
 cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg, const double *var,
                         cudaStream_t s) {
-  k_mean<<<reduce_blocks(c), 256, 0, s>>>(c->geo(), c->d_sc, comp, nxg, nyg, var, c->d_partials,
-                                          c->d_counter + 1);
+  k_mean<double><<<reduce_blocks(c), 256, 0, s>>>(c->geo(), c->d_sc, comp, nxg, nyg, var,
+                                                  c->d_partials, c->d_counter + 1);
+  return cudaGetLastError();
+}
+cudaError_t launch_mean(const plc_ctx *c, int comp, int nxg, int nyg, const float *var,
+                        cudaStream_t s) {
+  k_mean<float><<<reduce_blocks(c), 256, 0, s>>>(c->geo(), c->d_sc, comp, nxg, nyg, var,
+                                                 c->d_partials, c->d_counter + 1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, double *u, double *v, double *w,
                              cudaStream_t s) {
-  k_bound_vel<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), u_crf, u, v, w);
+  k_bound_vel<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), u_crf, u, v, w);
+  return cudaGetLastError();
+}
+cudaError_t launch_bound_vel(const plc_ctx *c, double u_crf, float *u, float *v, float *w,
+                             cudaStream_t s) {
+  k_bound_vel<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), u_crf, u, v, w);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bound_p(const plc_ctx *c, double *p, cudaStream_t s) {
-  k_bound_p<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), p);
+  k_bound_p<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), p);
+  return cudaGetLastError();
+}
+cudaError_t launch_bound_p(const plc_ctx *c, float *p, cudaStream_t s) {
+  k_bound_p<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), p);
   return cudaGetLastError();
 }
 
 cudaError_t launch_shift(const plc_ctx *c, double *var, double delta, cudaStream_t s) {
-  k_shift<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, delta);
+  k_shift<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, delta);
+  return cudaGetLastError();
+}
+cudaError_t launch_shift(const plc_ctx *c, float *var, double delta, cudaStream_t s) {
+  k_shift<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, delta);
   return cudaGetLastError();
 }
 
 cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult, cudaStream_t s) {
-  k_scale<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, d_mult);
+  k_scale<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, d_mult);
+  return cudaGetLastError();
+}
+cudaError_t launch_scale(const plc_ctx *c, float *var, const double *d_mult, cudaStream_t s) {
+  k_scale<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), var, d_mult);
   return cudaGetLastError();
 }
 
 cudaError_t launch_check(const plc_ctx *c, const double *u, const double *v, const double *w,
                          int what, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(c->d_check, 0, sizeof(CheckResult), s);
-  if (e != cudaSuccess) return e;
-  k_check<<<reduce_blocks(c), 256, 0, s>>>(c->geo(), what, u, v, w, c->d_partials,
-                                           c->d_counter + 2, c->d_check);
-  return cudaGetLastError();
+  return check_t<double>(c, u, v, w, what, s);
+}
+cudaError_t launch_check(const plc_ctx *c, const float *u, const float *v, const float *w,
+                         int what, cudaStream_t s) {
+  return check_t<float>(c, u, v, w, what, s);
 }
 
 cudaError_t launch_init_flow(const plc_ctx *c, double *u, double *v, double *w,
                              const double *d_prof, cudaStream_t s) {
-  k_init_flow<<<interior_grid(c), dim3(BX, BY), 0, s>>>(
+  k_init_flow<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(
+      c->geo(), d_prof, c->prm.init_with_noise, c->prm.noise_intensity, u, v, w);
+  return cudaGetLastError();
+}
+cudaError_t launch_init_flow(const plc_ctx *c, float *u, float *v, float *w,
+                             const double *d_prof, cudaStream_t s) {
+  k_init_flow<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(
       c->geo(), d_prof, c->prm.init_with_noise, c->prm.noise_intensity, u, v, w);
   return cudaGetLastError();
 }

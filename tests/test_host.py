@@ -96,7 +96,9 @@ def test_param_json_missing_section_is_an_error(tmp_path):
 
 @pytest.mark.parametrize("kw,code", [
     (dict(nx=127), -2), (dict(nz=63), -2), (dict(nx=40), -2), (dict(ny=10), -2),
-    (dict(p_row=2), -3), (dict(dt=0.0), -1), (dict(precision=1), -1)])
+    (dict(p_row=2), -3), (dict(dt=0.0), -1), (dict(precision=2), -1),
+    (dict(precision=1, nx=96, ny=18), -2), (dict(precision=1, nx=6, ny=64), -2),
+    (dict(precision=1), 0), (dict(precision=0, nx=96, ny=18), 0)])
 def test_param_check_errors(kw, code):
     base = dict(nx=128, ny=64, nz=64, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, re=100.0, u_ref=1.0,
                 l_ref=1.0)
