@@ -83,6 +83,8 @@ void free_poisson(plc_ctx *c) {
   cudaFree(c->d_rpiv);
   cudaFree(c->d_ac);
   cudaFree(c->d_low);
+  cudaFree(c->d_rpiv32);
+  cudaFree(c->d_ac32);
   cudaFree(c->plan_x.tw);
   cudaFree(c->plan_y.tw);
   cudaFree(c->plan_x.tw32);
@@ -90,6 +92,8 @@ void free_poisson(plc_ctx *c) {
   c->d_rpiv = nullptr;
   c->d_ac = nullptr;
   c->d_low = nullptr;
+  c->d_rpiv32 = nullptr;
+  c->d_ac32 = nullptr;
   c->plan_x.tw = nullptr;
   c->plan_y.tw = nullptr;
   c->plan_x.tw32 = nullptr;
@@ -119,6 +123,16 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
   ac.insert(ac.end(), cc.begin(), cc.end());
   PLC_CUDA(c, cudaMalloc(&c->d_ac, ac.size() * sizeof(double)));
   PLC_CUDA(c, cudaMemcpy(c->d_ac, ac.data(), ac.size() * sizeof(double), cudaMemcpyHostToDevice));
+  if (c->mixed) {
+    // FP32 copies for the systems that sweep in FP32
+    const std::vector<float> rpiv32(rpiv.begin(), rpiv.end()), ac32(ac.begin(), ac.end());
+    PLC_CUDA(c, cudaMalloc(&c->d_rpiv32, rpiv32.size() * sizeof(float)));
+    PLC_CUDA(c, cudaMemcpy(c->d_rpiv32, rpiv32.data(), rpiv32.size() * sizeof(float),
+                           cudaMemcpyHostToDevice));
+    PLC_CUDA(c, cudaMalloc(&c->d_ac32, ac32.size() * sizeof(float)));
+    PLC_CUDA(c, cudaMemcpy(c->d_ac32, ac32.data(), ac32.size() * sizeof(float),
+                           cudaMemcpyHostToDevice));
+  }
   FftPlan *plans[2] = {&c->plan_x, &c->plan_y};
   const int ns[2] = {c->nx, c->ny};
   for (int d = 0; d < 2; ++d) {
@@ -443,6 +457,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaMemset field"));
   }
   if (c->mixed) {
+    if ((e = rk32_configure()) != cudaSuccess) return fail(cuda_status(c, e, "rk32_configure"));
     std::vector<float> coef;
     host_rk32_coef(c, coef);
     if ((e = cudaMalloc(&c->d_coef32, coef.size() * sizeof(float))) != cudaSuccess ||
@@ -947,6 +962,17 @@ static int step_launches(plc_ctx *c, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     PLC_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
     ++c->nstep;
+    // Under CFL control the first steps also re-evaluate dt (steps 1, 2, 4,
+    // ... below nt_check), without the limit checks: the first forcing step
+    // moves the bulk velocity from that of the initial field (the reference's
+    // rescale divides by nz*ny, mod_initFlow.cc:92) to vel_force, which changes
+    // the CFL rate by up to nx/nz.
+    if (P.cfl_target > 0.0 && c->nstep < P.nt_check && (c->nstep & (c->nstep - 1)) == 0) {
+      if (int rc = run_check_fields(c, 2)) return rc;
+      if (c->h_check->cfl > 0.0)
+        if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+      continue;
+    }
     if (P.nt_check > 0 && c->nstep % P.nt_check == 0) {
       // main.cc:156-178
       int passed;

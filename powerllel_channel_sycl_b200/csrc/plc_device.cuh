@@ -42,4 +42,62 @@ static __device__ __forceinline__ void store_with_halo(T *q, const Geo &g, int i
   if (k == nz) put(nz + 1, gv);
 }
 
+// The halo images of one interior column (i, j): the offsets from a point of
+// the column to its periodic x image, its y image and its xy corner image
+// (0 where the column has none).  Computed once per column, so that a kernel
+// writing many planes of the column pays for the image rules once.  The
+// offsets are within one plane (at most ny*pitch elements), so 32 bits hold
+// them.
+struct HaloCol {
+  int dx, dy;
+};
+static __device__ __forceinline__ HaloCol halo_col(const Geo &g, int i, int j) {
+  HaloCol h;
+  h.dx = (i == g.nx) ? -g.nx : ((i == 1) ? g.nx : 0);
+  h.dy = (j == g.ny) ? -g.ny * g.X : ((j == 1) ? g.ny * g.X : 0);
+  return h;
+}
+template <class T>
+static __device__ __forceinline__ void store_col(T *q, long long c, const HaloCol &h, T x) {
+  q[c] = x;
+  if (h.dx) q[c + h.dx] = x;
+  if (h.dy) {
+    q[c + h.dy] = x;
+    if (h.dx) q[c + (h.dx + h.dy)] = x;
+  }
+}
+// The image and ghost writes of store_point: rare (boundary columns and the
+// wall planes), so kept out of line, off the kernels' common path.
+template <class T>
+static __device__ __noinline__ void store_images(T *q, const Geo &g, HaloCol h, long long c,
+                                                 int k, T v, int kind, T bc) {
+  if (h.dx) q[c + h.dx] = v;
+  if (h.dy) {
+    q[c + h.dy] = v;
+    if (h.dx) q[c + (h.dx + h.dy)] = v;
+  }
+  if (k == 1 || k == g.nz) {
+    T gv;
+    if (kind == BC_CENTRED)
+      gv = T(2) * bc - v;
+    else if (kind == BC_FACE)
+      gv = bc;
+    else
+      gv = v;
+    if (k == 1) store_col(q, c - g.XY, h, gv);
+    if (k == g.nz) store_col(q, c + g.XY, h, gv);
+  }
+}
+
+// The same writes as store_with_halo for the point at halo'd index c of
+// column h, plane k.
+template <class T>
+static __device__ __forceinline__ void store_point(T *q, const Geo &g, const HaloCol &h,
+                                                   long long c, int k, T val, int kind, T bc) {
+  T v = val;
+  if (kind == BC_FACE && k == g.nz) v = bc;  // w(nz) = bcvalue
+  q[c] = v;
+  if ((h.dx | h.dy) != 0 || k == 1 || k == g.nz) store_images(q, g, h, c, k, v, kind, bc);
+}
+
 }  // namespace plc

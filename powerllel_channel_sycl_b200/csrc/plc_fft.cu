@@ -30,9 +30,9 @@
 // The tridiagonal solve (ssolve_trid, mod_poisson_solver.cc:317-357) is a
 // Thomas sweep per (kx,ky) system, one thread per system, coalesced over kx,
 // with the pre-factored reciprocal pivots read from a table indexed by the
-// distinct wavenumber pair.  The mixed form keeps FP32 storage but sweeps in
-// FP64, and the systems of the lowest wavenumbers keep their intermediate
-// values in an FP64 side buffer.
+// distinct wavenumber pair.  In the mixed form the systems of the lowest
+// wavenumbers sweep in FP64 (pivots, arithmetic and intermediate values), the
+// others in FP32.
 
 #include <cuda_runtime.h>
 
@@ -626,8 +626,11 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
         reinterpret_cast<T *>(A + (c >> 1) * LS + padi<V>(t))[c & 1] = S[e];
       }
     } else {
+      // consecutive threads take consecutive column pairs l: their reads of
+      // the staged rows are adjacent (a stride of 2*TX elements between
+      // threads would put every lane in one bank)
       for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
-        const int l = e / (half + 1), m = e - l * (half + 1);
+        const int m = e / nl, l = e - m * nl;
         pack_pair(A + l * LS, n, m, S + 2 * l, S + 2 * l + 1, TX);
       }
     }
@@ -659,62 +662,29 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
 // rpiv[(k*(ny/2+1) + my)*(nx/2+1) + mx]; the reference's divisions by b
 // become multiplications by 1/b (mod_poisson_solver.cc:334-354).
 //
-// T = double: the reference's solve.  T = float (mixed form): FP32 storage,
-// FP64 arithmetic; systems whose packed indices are both below kLowModes
-// (the lowest wavenumbers, which carry the largest amplification 1/lambda and
-// the singular (0,0) mode) keep the forward-elimination values in the FP64
-// buffer `low` [k][j][i] (kLowModes^2 per plane) instead of rounding them to
-// FP32 in place.
+// The sweeps are sequential in k, but their loads are not: batches of PF
+// planes of the right-hand side and of the pivots are loaded one batch ahead
+// of the elimination, so 2*PF loads per thread are in flight.  Sys gives the
+// loads and stores of one system: rhs(k), piv(k), a(k), c(k), the forward
+// values fwd_put(k, x) / fwd_get(k) and the solution out(k, x); A is the
+// arithmetic type.
 // ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
-                                              const double *__restrict__ rpiv,
-                                              const double *__restrict__ a,
-                                              const double *__restrict__ c, T *__restrict__ var,
-                                              double *__restrict__ low) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const long long plane = (long long)nx * ny;
-  if (t >= plane) return;
-  const int i = t % nx, j = t / nx;
-  const int mx = (i == 0) ? 0 : ((i == 1) ? (nx >> 1) : (i >> 1));
-  const int my = (j == 0) ? 0 : ((j == 1) ? (ny >> 1) : (j >> 1));
-  const int MX = (nx >> 1) + 1;
-  const long long PS = (long long)MX * ((ny >> 1) + 1);
-  const double *rp = rpiv + (long long)my * MX + mx;
-  T *q = var + t;
-  constexpr bool kMixed = std::is_same<T, float>::value;
-  const bool in_low = kMixed && i < kLowModes && j < kLowModes;
-  double *lq = in_low ? low + j * kLowModes + i : nullptr;
-  constexpr long long LP = (long long)kLowModes * kLowModes;  // low-buffer plane stride
-  // the forward values go to the FP64 buffer for the low systems
-  auto put_fwd = [&](int k, double x) {
-    if (kMixed && in_low)
-      lq[k * LP] = x;
-    else
-      q[(long long)k * plane] = T(x);
-  };
-  auto get_fwd = [&](int k) -> double {
-    if (kMixed && in_low) return lq[k * LP];
-    return double(q[(long long)k * plane]);
-  };
-  // The sweeps are sequential in k, but their loads are not: batches of PF
-  // planes of the right-hand side and of the pivots are loaded one batch
-  // ahead of the elimination, so 2*PF loads per thread are in flight.
-  constexpr int PF = 8;
-  double prev = double(q[0]);
+template <class A, int PF, class Sys>
+__device__ __forceinline__ void thomas_sweep(int nz, const Sys &sys) {
+  A prev = sys.rhs(0);
+  sys.fwd_put(0, prev);
   {
     // forward elimination over k = 1 .. nz-1
-    double xn[PF], rn[PF];
+    A xn[PF], rn[PF];
     int k = 1;
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (k + s < nz) {
-        xn[s] = double(q[(long long)(k + s) * plane]);
-        rn[s] = __ldg(rp + (long long)(k + s - 1) * PS);
+        xn[s] = sys.rhs(k + s);
+        rn[s] = sys.piv(k + s - 1);
       }
-    if (kMixed && in_low) lq[0] = prev;
     for (; k < nz; k += PF) {
-      double x[PF], r[PF];
+      A x[PF], r[PF];
 #pragma unroll
       for (int s = 0; s < PF; ++s) {
         x[s] = xn[s];
@@ -724,33 +694,33 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (kn + s < nz) {
-          xn[s] = double(q[(long long)(kn + s) * plane]);
-          rn[s] = __ldg(rp + (long long)(kn + s - 1) * PS);
+          xn[s] = sys.rhs(kn + s);
+          rn[s] = sys.piv(kn + s - 1);
         }
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (k + s < nz) {
-          double cur = x[s];
-          cur -= (__ldg(a + k + s) * r[s]) * prev;
-          put_fwd(k + s, cur);
+          A cur = x[s];
+          cur -= (sys.a(k + s) * r[s]) * prev;
+          sys.fwd_put(k + s, cur);
           prev = cur;
         }
     }
   }
-  prev *= __ldg(rp + (long long)(nz - 1) * PS);
-  q[(long long)(nz - 1) * plane] = T(prev);
+  prev *= sys.piv(nz - 1);
+  sys.out(nz - 1, prev);
   {
     // back substitution over k = nz-2 .. 0
-    double xn[PF], rn[PF];
+    A xn[PF], rn[PF];
     int k = nz - 2;
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (k - s >= 0) {
-        xn[s] = get_fwd(k - s);
-        rn[s] = __ldg(rp + (long long)(k - s) * PS);
+        xn[s] = sys.fwd_get(k - s);
+        rn[s] = sys.piv(k - s);
       }
     for (; k >= 0; k -= PF) {
-      double x[PF], r[PF];
+      A x[PF], r[PF];
 #pragma unroll
       for (int s = 0; s < PF; ++s) {
         x[s] = xn[s];
@@ -760,17 +730,111 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (kn - s >= 0) {
-          xn[s] = get_fwd(kn - s);
-          rn[s] = __ldg(rp + (long long)(kn - s) * PS);
+          xn[s] = sys.fwd_get(kn - s);
+          rn[s] = sys.piv(kn - s);
         }
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (k - s >= 0) {
-          const double cur = (x[s] - __ldg(c + k - s) * prev) * r[s];
-          q[(long long)(k - s) * plane] = T(cur);
+          const A cur = (x[s] - sys.c(k - s) * prev) * r[s];
+          sys.out(k - s, cur);
           prev = cur;
         }
     }
+  }
+}
+
+// A system solved in place in the spectral array, with data, pivots and
+// coefficients of type S.
+template <class S>
+struct InPlaceSys {
+  S *q;
+  long long plane;
+  const S *rp;
+  long long PS;
+  const S *ca, *cc;
+  __device__ __forceinline__ S rhs(int k) const { return q[(long long)k * plane]; }
+  __device__ __forceinline__ S piv(int k) const { return __ldg(rp + (long long)k * PS); }
+  __device__ __forceinline__ S a(int k) const { return __ldg(ca + k); }
+  __device__ __forceinline__ S c(int k) const { return __ldg(cc + k); }
+  __device__ __forceinline__ void fwd_put(int k, S x) const {
+    if (k > 0) q[(long long)k * plane] = x;  // the k = 0 value is the right-hand side
+  }
+  __device__ __forceinline__ S fwd_get(int k) const { return q[(long long)k * plane]; }
+  __device__ __forceinline__ void out(int k, S x) const { q[(long long)k * plane] = x; }
+};
+
+// A low-wavenumber system of the mixed form: FP32 right-hand side and
+// solution, FP64 pivots and arithmetic, forward values in the FP64 buffer
+// `lq` (plane stride LP).
+struct LowSys {
+  float *q;
+  long long plane;
+  double *lq;
+  long long LP;
+  const double *rp;
+  long long PS;
+  const double *ca, *cc;
+  __device__ __forceinline__ double rhs(int k) const { return double(q[(long long)k * plane]); }
+  __device__ __forceinline__ double piv(int k) const { return __ldg(rp + (long long)k * PS); }
+  __device__ __forceinline__ double a(int k) const { return __ldg(ca + k); }
+  __device__ __forceinline__ double c(int k) const { return __ldg(cc + k); }
+  __device__ __forceinline__ void fwd_put(int k, double x) const { lq[k * LP] = x; }
+  __device__ __forceinline__ double fwd_get(int k) const { return lq[k * LP]; }
+  __device__ __forceinline__ void out(int k, double x) const {
+    q[(long long)k * plane] = float(x);
+  }
+};
+
+// packed indices (i, j) of system t and the offset of its pivot column
+__device__ __forceinline__ void trid_index(int t, int nx, int ny, int &i, int &j,
+                                           long long &pivot) {
+  i = t % nx;
+  j = t / nx;
+  const int mx = (i == 0) ? 0 : ((i == 1) ? (nx >> 1) : (i >> 1));
+  const int my = (j == 0) ? 0 : ((j == 1) ? (ny >> 1) : (j >> 1));
+  pivot = (long long)my * ((nx >> 1) + 1) + mx;
+}
+
+// FP64: the reference's solve, in place.
+__global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
+                                              const double *__restrict__ rpiv,
+                                              const double *__restrict__ a,
+                                              const double *__restrict__ c,
+                                              double *__restrict__ var) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  if (t >= plane) return;
+  int i, j;
+  long long pv;
+  trid_index(t, nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  thomas_sweep<double, 8>(nz, InPlaceSys<double>{var + t, plane, rpiv + pv, PS, a, c});
+}
+
+// Mixed form: systems whose packed x and y indices are both below kLowModes
+// (the lowest wavenumbers, with the largest amplification 1/lambda, and the
+// pinned singular (0,0) mode) sweep in FP64 with FP64 pivots and FP64
+// forward values in `low` [k][j][i]; all other systems sweep in FP32 in
+// place with the FP32 pivot table, 16 planes of loads in flight.
+__global__ void __launch_bounds__(128) k_trid_mixed(
+    int nx, int ny, int nz, const float *__restrict__ rpiv32, const float *__restrict__ a32,
+    const float *__restrict__ c32, const double *__restrict__ rpiv,
+    const double *__restrict__ a, const double *__restrict__ c, float *__restrict__ var,
+    double *__restrict__ low) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  if (t >= plane) return;
+  int i, j;
+  long long pv;
+  trid_index(t, nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  if (i < kLowModes && j < kLowModes) {
+    constexpr long long LP = (long long)kLowModes * kLowModes;
+    thomas_sweep<double, 8>(
+        nz, LowSys{var + t, plane, low + j * kLowModes + i, LP, rpiv + pv, PS, a, c});
+  } else {
+    thomas_sweep<float, 16>(nz, InPlaceSys<float>{var + t, plane, rpiv32 + pv, PS, a32, c32});
   }
 }
 
@@ -978,14 +1042,6 @@ cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
   });
 }
 
-template <class T>
-cudaError_t trid_t(const plc_ctx *c, T *var, cudaStream_t s) {
-  const long long plane = (long long)c->nx * c->ny;
-  const int bs = 128;
-  k_trid<T><<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(
-      c->nx, c->ny, c->nz, c->d_rpiv, c->d_ac, c->d_ac + c->nz, var, c->d_low);
-  return cudaGetLastError();
-}
 }  // namespace
 
 cudaError_t launch_fft_x_fwd(const plc_ctx *c, const double *p, const double *u, const double *v,
@@ -1011,10 +1067,19 @@ cudaError_t launch_fft_y(const plc_ctx *c, float *var, bool inverse, cudaStream_
   return fft_y_t<float>(c, var, inverse, s);
 }
 cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
-  return trid_t<double>(c, var, s);
+  const long long plane = (long long)c->nx * c->ny;
+  const int bs = 128;
+  k_trid<<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(c->nx, c->ny, c->nz, c->d_rpiv,
+                                                          c->d_ac, c->d_ac + c->nz, var);
+  return cudaGetLastError();
 }
 cudaError_t launch_trid(const plc_ctx *c, float *var, cudaStream_t s) {
-  return trid_t<float>(c, var, s);
+  const long long plane = (long long)c->nx * c->ny;
+  const int bs = 128;
+  k_trid_mixed<<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(
+      c->nx, c->ny, c->nz, c->d_rpiv32, c->d_ac32, c->d_ac32 + c->nz, c->d_rpiv, c->d_ac,
+      c->d_ac + c->nz, var, c->d_low);
+  return cudaGetLastError();
 }
 
 }  // namespace plc

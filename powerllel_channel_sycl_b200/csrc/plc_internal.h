@@ -58,7 +58,7 @@ constexpr int kMaxBlocksReduce = 4096;
 
 // Mixed form: Thomas systems whose packed x and y indices are both below
 // kLowModes (wavenumbers |m| < kLowModes/2, the Nyquist line of each axis
-// included) sweep with FP64 intermediates.
+// included) sweep in FP64; the others in FP32.
 constexpr int kLowModes = 16;
 
 }  // namespace plc
@@ -83,6 +83,8 @@ struct plc_ctx {
   double *d_rpiv = nullptr;   // 1/b, (nz, ny/2+1, nx/2+1)
   double *d_ac = nullptr;     // a[nz] | c[nz]
   double *d_low = nullptr;    // mixed form: FP64 sweep values of the low modes
+  float *d_rpiv32 = nullptr;  // mixed form: the pivot table in FP32
+  float *d_ac32 = nullptr;    // mixed form: a[nz] | c[nz] in FP32
   float *d_coef32 = nullptr;  // mixed form: per-plane RK coefficients
   plc::FftPlan plan_x, plan_y;
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
@@ -154,6 +156,8 @@ cudaError_t launch_to_f32(const plc_ctx *c, const double *src, float *dst, long 
                           int pitch, cudaStream_t s);
 cudaError_t launch_to_f64(const plc_ctx *c, const float *src, double *dst, long long rows, int len,
                           int pitch, cudaStream_t s);
+// shared-memory limit of the FP32 RK kernels on the current device
+cudaError_t rk32_configure();
 // per-plane coefficient rows of the FP32 RK kernels, rk32_coef_floats() per plane
 void host_rk32_coef(const plc_ctx *c, std::vector<float> &out);
 int rk32_coef_floats();

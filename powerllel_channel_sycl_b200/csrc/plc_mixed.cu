@@ -10,9 +10,9 @@
 // the tridiagonal sweep stay FP64.
 //
 // RK stages (mod_calcVel.cc:27-129 and :140-242): the same z-marching
-// structure as the FP64 kernel -- a 32 x 8 block of (i, j) columns walks a
-// chunk of z planes, each operand plane brought into a 5-slot shared-memory
-// ring by one cp.async.bulk.tensor copy per field two planes ahead -- but the
+// structure as the FP64 kernel -- a block of (i, j) columns walks a chunk of
+// z planes, each operand plane brought into a shared-memory ring by one
+// cp.async.bulk.tensor copy per field three planes ahead -- but the
 // momentum right-hand side is evaluated in FP32 with fused multiply-adds and
 // with the z interpolation weights folded into ten per-plane coefficients
 // (an algebraic rearrangement of the reference's expressions).
@@ -32,12 +32,14 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 namespace {
 
-constexpr int RX = 32, RY = 8;
+constexpr int RX = 32;                  // interior columns of a tile (one warp)
+constexpr int TY = 8;                   // thread rows of a block
+constexpr int RY = 2 * TY;              // interior rows of a tile: two per thread
 constexpr int HX = 36;                  // 34 columns used; TMA rows are whole 16-byte units
-constexpr int HY = RY + 2;              // 10
+constexpr int HY = RY + 2;              // 18
 constexpr int PLANE = HX * HY;          // floats per field-plane
 constexpr int SLOT = ((PLANE * 4 + 127) / 128) * 128 / 4;  // floats, 128-B aligned
-constexpr int NSLOT = 5;
+constexpr int NSLOT = 6;
 constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 4u;
 constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr int KCHUNK = 32;
@@ -164,32 +166,39 @@ size_t rk32_smem_bytes() {
 
 // RK1 (STAGE 1): o = q + dt*F(q);  RK2 (STAGE 2): o = (q + dt*F(q) + o)/2.
 // FUSE: the halo images and wall ghosts of the result are written as well.
+//
+// A block of 32 x 8 threads owns a 32 x 16 tile of interior columns; each
+// thread computes the two rows j, j+1 of its column pair (the operands the two
+// points share are read from shared memory once).  Plane k+3 is copied into
+// the slot of plane k-3 while plane k is computed: that slot was last read in
+// iteration k-2, which every thread finished before it reached the barrier of
+// iteration k-1, so one barrier per plane orders the ring.
 template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *RY, 4)
+__global__ void __launch_bounds__(RX *TY, 2)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
            const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
            float *ou, float *ov, float *ow, int kchunk, int *err) {
   extern __shared__ unsigned char smem_raw[];
-  float *base = reinterpret_cast<float *>(
+  float *slot = reinterpret_cast<float *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
-  Coef *zc = reinterpret_cast<Coef *>(base + 3 * NSLOT * SLOT);  // planes kb-1 .. ke+1
+  Coef *zc = reinterpret_cast<Coef *>(slot + 3 * NSLOT * SLOT);  // planes kb .. ke
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
-  __shared__ int ok_s;
+  __shared__ int ok_s[2];  // by iteration parity: a fast thread 0 cannot overwrite a flag
+                           // that a slow thread has still to read
 
   const int tid = threadIdx.x;
   const int tx = tid & (RX - 1), ty = tid / RX;
   const int x0 = blockIdx.x * RX, y0 = blockIdx.y * RY;  // halo'd coords of the tile corner
-  const int i = x0 + tx + 1, j = y0 + ty + 1;
-  const bool active = (i <= g.nx) && (j <= g.ny);
+  const int i = x0 + tx + 1, ja = y0 + 2 * ty + 1, jb = ja + 1;
+  const bool act_a = (i <= g.nx) && (ja <= g.ny);
+  const bool act_b = act_a && (jb <= g.ny);
   const int kb = blockIdx.z * kchunk + 1;
   const int ke = min(kb + kchunk - 1, g.nz);
   const int plast = ke + 1;  // last plane to bring in
-  float *slot = base;
 
   auto issue = [&](int p) {  // thread 0 only
-    const int rel = p - (kb - 1);
-    const int s = rel % NSLOT;
+    const int s = (p - (kb - 1)) % NSLOT;
     mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
     tma_load_plane(slot + s * SLOT, &mu, x0, y0, p, &bar[s]);
     tma_load_plane(slot + NSLOT * SLOT + s * SLOT, &mv, x0, y0, p, &bar[s]);
@@ -215,17 +224,26 @@ __global__ void __launch_bounds__(RX *RY, 4)
   __syncthreads();
 
   const float dt = float(sc->dt);
-  const long long XY = g.XY;
-  long long c = g.at(active ? i : 1, active ? j : 1, kb);
-  float bu = 0.f, bv = 0.f, bw = 0.f;  // RK2 base values (u, v, w) of plane k
-  if (STAGE == 2 && active) {
-    bu = ou[c];
-    bv = ov[c];
-    bw = ow[c];
+  const long long X = g.X, XY = g.XY;
+  long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
+  float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};  // RK2 base values of plane k
+  if (STAGE == 2) {
+    if (act_a) {
+      ba[0] = ou[c];
+      ba[1] = ov[c];
+      ba[2] = ow[c];
+    }
+    if (act_b) {
+      bb[0] = ou[c + X];
+      bb[1] = ov[c + X];
+      bb[2] = ow[c + X];
+    }
   }
-  const int o = (ty + 1) * HX + (tx + 1);
+  const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
+  const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
+  int sm = 0, s0 = 1, sp = 2;                  // slots of planes k-1, k, k+1
   for (int k = kb; k <= ke; ++k) {
-    __syncthreads();  // every thread is done with plane k-2's slot
+    const int par = (k - kb) & 1;
     if (tid == 0) {
       bool ok = true;
       if (k + 3 <= plast) {
@@ -234,7 +252,7 @@ __global__ void __launch_bounds__(RX *RY, 4)
       }
       if (k == kb) ok = wait_plane(kb - 1) && wait_plane(kb);
       ok = ok && wait_plane(k + 1);
-      ok_s = ok ? 1 : 0;
+      ok_s[par] = ok ? 1 : 0;
       if (!ok) {
         atomicExch(err, 1);
         // give the copies still in flight a bounded chance to land before
@@ -247,51 +265,79 @@ __global__ void __launch_bounds__(RX *RY, 4)
       }
     }
     __syncthreads();
-    if (!ok_s) return;  // the whole block leaves together
-    float nbu = 0.f, nbv = 0.f, nbw = 0.f;
-    if (STAGE == 2 && active && k < ke) {
-      nbu = ou[c + XY];
-      nbv = ov[c + XY];
-      nbw = ow[c + XY];
+    if (!ok_s[par]) return;  // the whole block leaves together
+    float na[3] = {0.f, 0.f, 0.f}, nb[3] = {0.f, 0.f, 0.f};
+    if (STAGE == 2 && k < ke) {
+      if (act_a) {
+        na[0] = ou[c + XY];
+        na[1] = ov[c + XY];
+        na[2] = ow[c + XY];
+      }
+      if (act_b) {
+        nb[0] = ou[c + XY + X];
+        nb[1] = ov[c + XY + X];
+        nb[2] = ow[c + XY + X];
+      }
     }
-    if (active) {
-      const int rel = k - (kb - 1);
+    if (act_a) {
+      const Coef z = zc[k - kb];
       SmemAcc32 a;
       a.base = slot;
-      a.off[0] = ((rel - 1) % NSLOT) * SLOT + o;
-      a.off[1] = (rel % NSLOT) * SLOT + o;
-      a.off[2] = ((rel + 1) % NSLOT) * SLOT + o;
-      const Coef z = zc[k - kb];
-      const Rhs3f r = momentum_rhs32<CRF>(K, z, a);
-      const float qu = a(0, 0, 0, 0), qv = a(1, 0, 0, 0), qw = a(2, 0, 0, 0);
-      float nu, nv, nw;
-      if (STAGE == 1) {
-        nu = fmaf(dt, r.u, qu);
-        nv = fmaf(dt, r.v, qv);
-        nw = fmaf(dt, r.w, qw);
-      } else {
-        nu = (fmaf(dt, r.u, qu) + bu) * 0.5f;
-        nv = (fmaf(dt, r.v, qv) + bv) * 0.5f;
-        nw = (fmaf(dt, r.w, qw) + bw) * 0.5f;
+      a.off[0] = sm * SLOT + o;
+      a.off[1] = s0 * SLOT + o;
+      a.off[2] = sp * SLOT + o;
+      SmemAcc32 b = a;
+      b.off[0] += HX;
+      b.off[1] += HX;
+      b.off[2] += HX;
+      const Rhs3f ra = momentum_rhs32<CRF>(K, z, a);
+      const Rhs3f rb = momentum_rhs32<CRF>(K, z, b);
+      float va[3] = {a(0, 0, 0, 0), a(1, 0, 0, 0), a(2, 0, 0, 0)};
+      float vb[3] = {b(0, 0, 0, 0), b(1, 0, 0, 0), b(2, 0, 0, 0)};
+      const float fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (STAGE == 1) {
+          va[d] = fmaf(dt, fa[d], va[d]);
+          vb[d] = fmaf(dt, fb[d], vb[d]);
+        } else {
+          va[d] = (fmaf(dt, fa[d], va[d]) + ba[d]) * 0.5f;
+          vb[d] = (fmaf(dt, fb[d], vb[d]) + bb[d]) * 0.5f;
+        }
       }
       if (FUSE) {
-        store_with_halo(ou, g, i, j, k, nu, BC_CENTRED, bc_u);
-        store_with_halo(ov, g, i, j, k, nv, BC_CENTRED, 0.f);
-        store_with_halo(ow, g, i, j, k, nw, BC_FACE, 0.f);
+        store_point(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
+        store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
+        store_point(ow, g, ha, c, k, va[2], BC_FACE, 0.f);
+        if (act_b) {
+          store_point(ou, g, hb, c + X, k, vb[0], BC_CENTRED, bc_u);
+          store_point(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.f);
+          store_point(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.f);
+        }
       } else {
-        ou[c] = nu;
-        ov[c] = nv;
-        ow[c] = nw;
+        ou[c] = va[0];
+        ov[c] = va[1];
+        ow[c] = va[2];
+        if (act_b) {
+          ou[c + X] = vb[0];
+          ov[c + X] = vb[1];
+          ow[c + X] = vb[2];
+        }
       }
     }
-    bu = nbu;
-    bv = nbv;
-    bw = nbw;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ba[d] = na[d];
+      bb[d] = nb[d];
+    }
+    sm = s0;
+    s0 = sp;
+    sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
     c += XY;
   }
 }
 
-// Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 10
+// Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 18
 // tile of one plane.  The pitch is a multiple of 4 (16 bytes) and the tile's x
 // origin 32*bx is 128-byte aligned.
 bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g) {
@@ -312,10 +358,10 @@ template <int STAGE, bool FUSE, bool CRF>
 cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
                           const CUtensorMap &mw, const RkConst &K, float bc_u, float *ou,
                           float *ov, float *ow, cudaStream_t s) {
-  const size_t smem = rk32_smem_bytes();  // about 25 KB: below the default limit
+  const size_t smem = rk32_smem_bytes();
   const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
-  k_rk32<STAGE, FUSE, CRF><<<grid, RX * RY, smem, s>>>(
+  k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
       mu, mv, mw, c->geo(), K, reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou,
       ov, ow, kchunk, c->d_err);
   return cudaGetLastError();
@@ -351,6 +397,27 @@ unsigned convert_blocks(const plc_ctx *c, long long n) {
 }
 
 }  // namespace
+
+// Raises the dynamic shared-memory limit of the FP32 RK kernels (about 50 KB)
+// on the current device.
+cudaError_t rk32_configure() {
+  const int bytes = (int)rk32_smem_bytes();
+  cudaError_t e = cudaSuccess;
+#define PLC_RK32_ATTR(S, F, C)                                                            \
+  if (e == cudaSuccess)                                                                   \
+    e = cudaFuncSetAttribute(k_rk32<S, F, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             bytes);
+  PLC_RK32_ATTR(1, true, true)
+  PLC_RK32_ATTR(1, true, false)
+  PLC_RK32_ATTR(1, false, true)
+  PLC_RK32_ATTR(1, false, false)
+  PLC_RK32_ATTR(2, true, true)
+  PLC_RK32_ATTR(2, true, false)
+  PLC_RK32_ATTR(2, false, true)
+  PLC_RK32_ATTR(2, false, false)
+#undef PLC_RK32_ATTR
+  return e;
+}
 
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const float *qu,
                       const float *qv, const float *qw, float *ou, float *ov, float *ow,

@@ -313,6 +313,7 @@ __global__ void __launch_bounds__(RX *RY, 3)
     bv = ov[c];
     bw = ow[c];
   }
+  const HaloCol hc = halo_col(g, i, j);
   const int o = (ty + 1) * HX + (tx + 1);
   for (int k = kb; k <= ke; ++k) {
     __syncthreads();  // every thread is done with plane k-2's slot
@@ -365,9 +366,9 @@ __global__ void __launch_bounds__(RX *RY, 3)
         nw = (qw + dt * r.w + bw) * 0.5;
       }
       if (FUSE) {
-        store_with_halo(ou, g, i, j, k, nu, BC_CENTRED, 0.0 - u_crf);
-        store_with_halo(ov, g, i, j, k, nv, BC_CENTRED, 0.0);
-        store_with_halo(ow, g, i, j, k, nw, BC_FACE, 0.0);
+        store_point(ou, g, hc, c, k, nu, BC_CENTRED, 0.0 - u_crf);
+        store_point(ov, g, hc, c, k, nv, BC_CENTRED, 0.0);
+        store_point(ow, g, hc, c, k, nw, BC_FACE, 0.0);
       } else {
         ou[c] = nu;
         ov[c] = nv;
@@ -553,97 +554,80 @@ struct ForceCfg {
   double u_crf;
 };
 
-// One wave of persistent blocks (grid-stride over 32 x 8 tiles of the
-// interior, plane by plane); each thread keeps the loads of its next tile in
-// flight while it finishes the current one, and the block reduces once at the
-// end (a reduction tail per short-lived block would cost more than the
-// correction itself).
-template <class T>
-struct CorrIn {
-  T pc, px, py, pz, u, v, w;
-};
-
-__device__ __forceinline__ bool tile_point(const Geo &g, long long tile, int tiles_x, int tiles_y,
-                                           int &i, int &j, int &k) {
-  const long long per_plane = (long long)tiles_x * tiles_y;
-  k = (int)(tile / per_plane);
-  const int r = (int)(tile - (long long)k * per_plane);
-  const int jt = r / tiles_x, it = r - jt * tiles_x;
-  i = it * 32 + (threadIdx.x & 31) + 1;
-  j = jt * 8 + (threadIdx.x >> 5) + 1;
-  ++k;
-  return i <= g.nx && j <= g.ny;
-}
-
-template <class T>
-__device__ __forceinline__ CorrIn<T> corr_load(const Geo &g, const T *__restrict__ p, const T *u,
-                                               const T *v, const T *w, long long c) {
-  CorrIn<T> x;
-  x.pc = p[c];
-  x.px = p[c + 1];
-  x.py = p[c + g.X];
-  x.pz = p[c + g.XY];
-  x.u = u[c];
-  x.v = v[c];
-  x.w = w[c];
-  return x;
-}
-
+// One wave of persistent blocks walks work items of 32 x 8 interior columns
+// by KZ planes; each thread issues all loads of its column segment (p at
+// KZ+1 planes, its x and y neighbours, u, v, w) before the arithmetic, so
+// p(k+1) is read once for planes k and k+1 and ~6 loads per thread and plane
+// are in flight.  The block reduces once at the end (a reduction tail per
+// short-lived block would cost more than the correction itself).
 // T = double: the reference's arithmetic.  T = float (mixed form): the
 // correction in FP32, the bulk sums of the forced components in FP64.
-template <class T>
-__global__ void __launch_bounds__(256, 4) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
+template <class T, int KZ>
+__global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
                                                           const T *__restrict__ p, T *u, T *v,
                                                           T *w, double *partials,
                                                           unsigned int *counter) {
   __shared__ double smem[2 * 3 * 32];
   const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
   const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 7) / 8;
-  const long long ntiles = (long long)tiles_x * tiles_y * g.nz;
+  const int per_chunk = tiles_x * tiles_y;
+  const int items = per_chunk * ((g.nz + KZ - 1) / KZ);
+  const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+  const long long X = g.X, XY = g.XY;
   DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-  long long tile = blockIdx.x;
-  int i = 0, j = 0, k = 0;
-  bool ok = tile < ntiles && tile_point(g, tile, tiles_x, tiles_y, i, j, k);
-  CorrIn<T> cur{};
-  if (ok) cur = corr_load(g, p, u, v, w, g.at(i, j, k));
-  for (; tile < ntiles; tile += gridDim.x) {
-    // issue the next tile's loads before finishing this one
-    const long long nt = tile + gridDim.x;
-    int ni = 0, nj = 0, nk = 0;
-    const bool nok = nt < ntiles && tile_point(g, nt, tiles_x, tiles_y, ni, nj, nk);
-    CorrIn<T> nxt{};
-    if (nok) nxt = corr_load(g, p, u, v, w, g.at(ni, nj, nk));
-    if (ok) {
-      const long long c = g.at(i, j, k);
-      // correctVel, mod_calcVel.cc:272-274
-      const T nu = cur.u - (cur.px - cur.pc) * dtdxi;
-      const T nv = cur.v - (cur.py - cur.pc) * dtdyi;
-      const T nw = cur.w - (cur.pz - cur.pc) * dt * T(__ldg(g.dzc_inv + k));
-      const double dzl = __ldg(g.dzflzi + k);
-      if (fc.forced[0]) {
-        u[c] = nu;
-        dd_add(s[0], double(nu) * dzl);
-      } else {
-        store_with_halo(u, g, i, j, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int kc = item / per_chunk, r = item - kc * per_chunk;
+    const int jt = r / tiles_x, it = r - jt * tiles_x;
+    const int i = it * 32 + lx + 1, j = jt * 8 + ly + 1, k0 = kc * KZ + 1;
+    if (i > g.nx || j > g.ny) continue;
+    const int nk = min(KZ, g.nz - k0 + 1);
+    const long long c0 = g.at(i, j, k0);
+    const HaloCol h = halo_col(g, i, j);
+    T pc[KZ + 1], px[KZ], py[KZ], uu[KZ], vv[KZ], ww[KZ];
+#pragma unroll
+    for (int q = 0; q < KZ; ++q)
+      if (q < nk) {
+        const long long c = c0 + q * XY;
+        pc[q] = p[c];
+        px[q] = p[c + 1];
+        py[q] = p[c + X];
+        uu[q] = u[c];
+        vv[q] = v[c];
+        ww[q] = w[c];
       }
-      if (fc.forced[1]) {
-        v[c] = nv;
-        dd_add(s[1], double(nv) * dzl);
-      } else {
-        store_with_halo(v, g, i, j, k, nv, BC_CENTRED, T(0));
+    // p(k+1) of the last plane (k0+nk <= nz+1, a halo plane at most)
+#pragma unroll
+    for (int q = 1; q <= KZ; ++q)
+      if (q == nk) pc[q] = p[c0 + q * XY];
+#pragma unroll
+    for (int q = 0; q < KZ; ++q)
+      if (q < nk) {
+        const int k = k0 + q;
+        const long long c = c0 + q * XY;
+        // correctVel, mod_calcVel.cc:272-274
+        const T nu = uu[q] - (px[q] - pc[q]) * dtdxi;
+        const T nv = vv[q] - (py[q] - pc[q]) * dtdyi;
+        const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k));
+        const double dzl = __ldg(g.dzflzi + k);
+        if (fc.forced[0]) {
+          u[c] = nu;
+          dd_add(s[0], double(nu) * dzl);
+        } else {
+          store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
+        }
+        if (fc.forced[1]) {
+          v[c] = nv;
+          dd_add(s[1], double(nv) * dzl);
+        } else {
+          store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
+        }
+        if (fc.forced[2]) {
+          w[c] = nw;
+          dd_add(s[2], double(nw) * dzl);
+        } else {
+          store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+        }
       }
-      if (fc.forced[2]) {
-        w[c] = nw;
-        dd_add(s[2], double(nw) * dzl);
-      } else {
-        store_with_halo(w, g, i, j, k, nw, BC_FACE, T(0));
-      }
-    }
-    cur = nxt;
-    ok = nok;
-    i = ni;
-    j = nj;
-    k = nk;
   }
   block_sum<3>(s, smem);
   if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
@@ -1012,13 +996,17 @@ cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v, 
 namespace {
 template <class T>
 cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cudaStream_t s) {
-  // one wave: 4 resident blocks per SM (launch bounds), at most the tiles
-  const long long tiles = (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * c->nz;
-  long long nb = 4ll * c->num_sms;
-  if (nb > tiles) nb = tiles;
+  // KZ planes per work item: 6 in FP32, 4 in FP64 (the loads of one item
+  // live in registers)
+  constexpr int KZ = sizeof(T) == 4 ? 6 : 4;
+  // one wave: 2 resident blocks per SM (launch bounds), at most the items
+  const long long items =
+      (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * ((c->nz + KZ - 1) / KZ);
+  long long nb = 2ll * c->num_sms;
+  if (nb > items) nb = items;
   if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
-  k_correct_fused<T><<<(unsigned)nb, 256, 0, s>>>(c->geo(), c->d_sc, force_cfg(c), p, u, v, w,
-                                                   c->d_partials, c->d_counter);
+  k_correct_fused<T, KZ><<<(unsigned)nb, 256, 0, s>>>(c->geo(), c->d_sc, force_cfg(c), p, u, v,
+                                                       w, c->d_partials, c->d_counter);
   return cudaGetLastError();
 }
 

@@ -16,7 +16,11 @@ pytestmark = pytest.mark.gpu
 
 VEL_TOL = 1e-4        # 10-step velocity rel L2, mixed vs FP64
 PROFILE_TOL = 5e-3    # mean-profile relative error
-P_TOL = 1e-3          # pressure (up to a constant) rel L2
+# Pressure (up to a constant) rel L2.  The pressure of these noisy fields is
+# ill-conditioned: the FP64 oracle amplifies rounding of 1e-16 to ~1e-12
+# (test_pressure_roundoff_floor), i.e. ~1e4, so FP32 rounding (6e-8) puts it
+# near 1e-3.
+P_TOL = 5e-3
 DIV_TOL = 1e-3        # max |div u| after the projection, FP32 rounding level
 
 

@@ -122,7 +122,8 @@ def test_mean_and_force(nx, ny, nz):
     np.testing.assert_array_equal(interior(ch.download("u")), interior(u))
 
 
-@pytest.mark.parametrize("nx,ny,nz", SIZES + [(128, 64, 8), (96, 48, 4), (768, 12, 2), (8, 384, 2)])
+@pytest.mark.parametrize("nx,ny,nz", SIZES + [(128, 64, 8), (96, 48, 4), (768, 12, 2), (8, 384, 2),
+                                      (512, 8, 2), (8, 256, 2), (192, 192, 2)])
 def test_fft_each_direction(nx, ny, nz):
     case, ch = make_pair(nx, ny, nz)
     (p,) = random_fields(case, 7, n=1)
