@@ -182,6 +182,7 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
     ok, cfl, div = ch.check()
+    tiles = ch.fft_tiles
     prof_steps = max(2, min(5, args.steps))
     prof = ch.profile_step(prof_steps)
     total = sum(prof.values())
@@ -219,6 +220,7 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
                           "frac": MIXED_STEP_BYTES_PER_POINT * value / world / 1e9 / peak},
         "kernels": kernels,
         "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0]},
+        "fft_tiles": tiles,
         "error_vs_fp64": {"steps": nerr, "dt": wl["dt"], "vel_rel_l2": err,
                           "div_max_mixed": div_b[0]},
     }
@@ -354,6 +356,7 @@ def run_ours(args, wl, rank, world, local, pg):
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
     ok, cfl, div = ch.check()  # NaN / CFL / divergence of the state after the timed steps
+    tiles = ch.fft_tiles
 
     # per-kernel device times of the same fused kernels (plain launches with
     # CUDA events between them on the library's stream)
@@ -424,6 +427,7 @@ def run_ours(args, wl, rank, world, local, pg):
                                                             if args.nt_check else 0),
         "clocks": clk.summary(),
         "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0], "dt": ch.dt},
+        "fft_tiles": tiles,
     }
     ch.close()
     if not args.no_mixed:

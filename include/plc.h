@@ -154,6 +154,11 @@ int plc_field_ptr(plc_ctx *ctx, int field, double **d_ptr, size_t *count);
  * *pitch elements (nx+2 rounded up to a multiple of 4), the spectral array
  * rows of nx.  No counterpart in the reference. */
 int plc_field_ptr_f32(plc_ctx *ctx, int field, float **d_ptr, size_t *count, int *pitch);
+/* Line pairs per tile of the forward x (fused with calcRHS), backward x and
+ * y transforms, as the autotuner of plc_create chose them by timing every
+ * feasible size on the device (the choice changes speed, never results).
+ * No counterpart in the reference. */
+int plc_fft_tiles(const plc_ctx *ctx, int *lines_xf, int *lines_x, int *lines_y);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

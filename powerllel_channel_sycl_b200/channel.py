@@ -141,6 +141,13 @@ class Channel:
         self._check(lib().plc_field_ptr(self._ctx, fid, C.byref(p), C.byref(n)))
         return p.value
 
+    @property
+    def fft_tiles(self):
+        """Line pairs per tile (x forward, x backward, y) chosen by the autotuner."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(lib().plc_fft_tiles(self._ctx, C.byref(a), C.byref(b), C.byref(c)))
+        return {"x_fwd": a.value, "x_bwd": b.value, "y": c.value}
+
     def ptr_f32(self, f):
         """(device pointer, element count, row pitch) of an FP32 field of a mixed context."""
         fid = FIELDS[f] if isinstance(f, str) else int(f)

@@ -80,6 +80,12 @@ int upload_step_consts(plc_ctx *c, double dt) {
 }
 
 void free_poisson(plc_ctx *c) {
+  // the captured step holds the solver's tables and tile sizes
+  if (c->graph) {
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
   cudaFree(c->d_rpiv);
   cudaFree(c->d_ac);
   cudaFree(c->d_low);
@@ -481,6 +487,11 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     return fail(cuda_status(c, e, "cudaDeviceGetAttribute"));
   if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
   if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
+  // the fields hold zeros: time the transforms' tile sizes on them
+  if ((e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
+  c->tuned_lines[0] = c->fft_lines_xf;
+  c->tuned_lines[1] = c->fft_lines_x;
+  c->tuned_lines[2] = c->fft_lines_y;
   *out = c;
   return PLC_OK;
 }
@@ -488,8 +499,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
 int plc_destroy(plc_ctx *c) {
   if (!c) return PLC_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->graph) cudaGraphExecDestroy(c->graph);
-  free_poisson(c);
+  free_poisson(c);  // also releases the captured step
   for (auto &f : c->d_field) cudaFree(f);
   for (auto &f : c->f_field) cudaFree(f);
   cudaFree(c->d_coef32);
@@ -556,6 +566,14 @@ static void ref_shape(const plc_ctx *c, int field, long long *rows, int *len) {
     *rows = (long long)(c->ny + 2) * (c->nz + 2);
     *len = c->nx + 2;
   }
+}
+
+int plc_fft_tiles(const plc_ctx *c, int *lines_xf, int *lines_x, int *lines_y) {
+  if (!c) return set_error(nullptr, PLC_ERR_ARG, "null context");
+  if (lines_xf) *lines_xf = c->fft_lines_xf;
+  if (lines_x) *lines_x = c->fft_lines_x;
+  if (lines_y) *lines_y = c->fft_lines_y;
+  return PLC_OK;
 }
 
 int plc_upload(plc_ctx *c, int field, const double *h_src) {
@@ -751,7 +769,10 @@ int plc_init_poisson_solver(plc_ctx *c, const double *h_dzf_global, const char *
       strcmp(bctype_z, "NN"))
     return set_error(c, PLC_ERR_ARG, "only bctype PP, PP, NN is supported (mod_fft.cc:20-26)");
   PLC_CUDA(c, cudaStreamSynchronize(c->stream));
-  return init_poisson(c, h_dzf_global);
+  if (int rc = init_poisson(c, h_dzf_global)) return rc;
+  if (c->tuned_lines[0] > 0)
+    PLC_CUDA(c, fft_set_lines(c, c->tuned_lines[0], c->tuned_lines[1], c->tuned_lines[2]));
+  return PLC_OK;
 }
 
 int plc_free_poisson_solver(plc_ctx *c) {

@@ -297,10 +297,20 @@ __host__ __device__ constexpr int plan_radix(int n, int p) {
   return 3;
 }
 
+// Shared-memory index of element e0 + r*stride of a line when e0 >= 0 and
+// stride is a multiple of the padding period P = 2^pad_shift: padi(e0) plus
+// the constant r*(stride + stride/P), so that all R accesses of a butterfly
+// are one base register plus immediate offsets.
+template <class V, int STRIDE>
+__device__ __forceinline__ constexpr bool pad_linear() {
+  return STRIDE % (1 << pad_shift<V>()) == 0;
+}
+
 template <int R, bool INV, int N, int NS, class V>
 __device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restrict__ dst, int nl,
                                            const V *__restrict__ tw) {
   constexpr int nb = N / R, LS = line_stride<V>(N), tws = N / (NS * R);
+  constexpr int P = 1 << pad_shift<V>();
   const int tot = nl * nb;
   for (int b = threadIdx.x; b < tot; b += blockDim.x) {
     const int l = b / nb;
@@ -309,8 +319,14 @@ __device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restr
     V *d = dst + l * LS;
     const int jm = j % NS;
     V v[R];
+    if constexpr (pad_linear<V, nb>()) {
+      const V *sb = s + padi<V>(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[padi<V>(j + r * nb)];
+      for (int r = 0; r < R; ++r) v[r] = sb[r * (nb + nb / P)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = s[padi<V>(j + r * nb)];
+    }
     if (NS > 1 && jm != 0) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
@@ -319,9 +335,20 @@ __device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restr
       }
     }
     Dft<R, INV>::run(v);
-    const int idxD = (j / NS) * NS * R + jm;
+    if constexpr (pad_linear<V, NS>()) {
+      V *db = d + padi<V>((j / NS) * NS * R + jm);
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[padi<V>(idxD + r * NS)] = v[r];
+      for (int r = 0; r < R; ++r) db[r * (NS + NS / P)] = v[r];
+    } else if constexpr (NS == 1 && R % P == 0) {
+      // first pass: idxD = j*R, a multiple of P; offsets r < R
+      V *db = d + j * (R + R / P);
+#pragma unroll
+      for (int r = 0; r < R; ++r) db[r + r / P] = v[r];
+    } else {
+      const int idxD = (j / NS) * NS * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) d[padi<V>(idxD + r * NS)] = v[r];
+    }
   }
 }
 
@@ -621,9 +648,11 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
     cp_async_wait_all();
     __syncthreads();
     if (!INV) {
-      for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-        const int t = e / TX, c = e - t * TX;
-        reinterpret_cast<T *>(A + (c >> 1) * LS + padi<V>(t))[c & 1] = S[e];
+      // columns 2l, 2l+1 of row t form element t of line l: one vector
+      // load and store per pair
+      for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const int t = e / nl, l = e - t * nl;
+        A[l * LS + padi<V>(t)] = reinterpret_cast<const V *>(S + t * TX)[l];
       }
     } else {
       // consecutive threads take consecutive column pairs l: their reads of
@@ -648,10 +677,9 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
         reinterpret_cast<V *>(plane + (long long)(q0 + 1) * nx)[l] = mk<V>(a.y, b.y);
       }
     } else {
-      for (int e = threadIdx.x; e < n * TX; e += blockDim.x) {
-        const int t = e / TX, c = e - t * TX;
-        const V z = Z[(c >> 1) * LS + padi<V>(t)];
-        plane[(long long)t * nx + c] = (c & 1) ? z.y : z.x;
+      for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const int t = e / nl, l = e - t * nl;
+        reinterpret_cast<V *>(plane + (long long)t * nx)[l] = Z[l * LS + padi<V>(t)];
       }
     }
   }
@@ -947,17 +975,11 @@ cudaError_t fft_configure(size_t max_bytes) {
 }
 
 namespace {
+// Persistent grid sizes for the context's line counts; fails if a kernel's
+// shared memory exceeds the device limit.
 template <class T>
-cudaError_t fft_setup_t(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max, int sms) {
+cudaError_t fft_grids_t(plc_ctx *c, size_t dev_max, int sms) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
-  // FP32 staging copies 16-byte chunks of 4 elements: tiles of the y
-  // transform then span a multiple of 4 columns (an even number of pairs)
-  const int ystep = sizeof(T) == 4 ? 2 : 1;
-  c->fft_lines_x =
-      pick_lines(ny / 2, smem_cap_per_block, [&](int d) { return smem_x_bwd<T>(nx, d); });
-  c->fft_lines_xf = pick_lines(ny / 2, 64 * 1024, [&](int d) { return fft_bytes<T>(nx, d); });
-  c->fft_lines_y = pick_lines(
-      nx / 2, smem_cap_per_block, [&](int d) { return smem_y<T>(ny, d); }, ystep);
   const size_t need[4] = {smem_x_fwd<T>(nx, c->fft_lines_x), fft_bytes<T>(nx, c->fft_lines_xf),
                           smem_x_bwd<T>(nx, c->fft_lines_x), smem_y<T>(ny, c->fft_lines_y)};
   for (size_t b : need)
@@ -976,6 +998,20 @@ cudaError_t fft_setup_t(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max, i
     c->grid_y = persistent_grid(k_fft_y<T, N, false>, 256, need[3], sms, tiles_y);
     return cudaSuccess;
   });
+}
+
+template <class T>
+cudaError_t fft_setup_t(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max, int sms) {
+  const int nx = c->nx, ny = c->ny;
+  // FP32 staging copies 16-byte chunks of 4 elements: tiles of the y
+  // transform then span a multiple of 4 columns (an even number of pairs)
+  const int ystep = sizeof(T) == 4 ? 2 : 1;
+  c->fft_lines_x =
+      pick_lines(ny / 2, smem_cap_per_block, [&](int d) { return smem_x_bwd<T>(nx, d); });
+  c->fft_lines_xf = pick_lines(ny / 2, 64 * 1024, [&](int d) { return fft_bytes<T>(nx, d); });
+  c->fft_lines_y = pick_lines(
+      nx / 2, smem_cap_per_block, [&](int d) { return smem_y<T>(ny, d); }, ystep);
+  return fft_grids_t<T>(c, dev_max, sms);
 }
 }  // namespace
 
@@ -1066,6 +1102,109 @@ cudaError_t launch_fft_y(const plc_ctx *c, double *var, bool inverse, cudaStream
 cudaError_t launch_fft_y(const plc_ctx *c, float *var, bool inverse, cudaStream_t s) {
   return fft_y_t<float>(c, var, inverse, s);
 }
+// ---------------------------------------------------------------------------
+// Autotuner of the transforms' tile sizes.  Each transform processes its
+// lines independently, so the number of line pairs per tile changes only the
+// speed, never the result.  For each transform the feasible tile sizes
+// (divisors of the line-pair count, up to 16, within the device's shared
+// memory) are timed on the context's own buffers and the fastest is kept.
+// Call it while the fields hold no data to keep: it overwrites the spectral
+// array and the pressure with transforms of the current fields.
+// ---------------------------------------------------------------------------
+namespace {
+template <class T>
+cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
+  const int nx = c->nx, ny = c->ny;
+  cudaStream_t s = c->stream;
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  auto time_of = [&](auto launch) -> float {
+    // one untimed launch, then the best of three
+    if (launch() != cudaSuccess) return -1.f;
+    float best = -1.f;
+    for (int r = 0; r < 3; ++r) {
+      if (cudaEventRecord(e0, s) != cudaSuccess || launch() != cudaSuccess ||
+          cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+        return -1.f;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best < 0.f || ms < best) best = ms;
+    }
+    return best;
+  };
+  // tunes one line count *field over the divisors of `pairs` (multiples of
+  // `step`); `fits` says whether a value fits the device
+  auto tune = [&](int *field, int pairs, int step, auto fits, auto launch) {
+    int best_d = *field;
+    float best_t = -1.f;
+    for (int d = step; d <= pairs && d <= 16; d += step) {
+      if (pairs % d || !fits(d)) continue;
+      *field = d;
+      if (fft_grids_t<T>(c, dev_max, sms) != cudaSuccess) continue;
+      const float t = time_of(launch);
+      if (t >= 0.f && (best_t < 0.f || t < best_t)) {
+        best_t = t;
+        best_d = d;
+      }
+    }
+    *field = best_d;
+    cudaGetLastError();  // a candidate that failed to launch leaves no error behind
+  };
+  T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W], *p = f[PLC_P], *spec = f[PLC_SPEC];
+  tune(&c->fft_lines_xf, ny / 2, 1, [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
+       [&]() -> cudaError_t {
+         if constexpr (sizeof(T) == 8)
+           return launch_fft_x_fwd(c, nullptr, u, v, w, spec, s);
+         else
+           return launch_fft_x_fwd(c, u, v, w, spec, s);
+       });
+  tune(&c->fft_lines_y, nx / 2, sizeof(T) == 4 ? 2 : 1,
+       [&](int d) { return smem_y<T>(ny, d) <= dev_max; },
+       [&]() -> cudaError_t {
+         cudaError_t r = launch_fft_y(c, spec, false, s);
+         return r == cudaSuccess ? launch_fft_y(c, spec, true, s) : r;
+       });
+  tune(&c->fft_lines_x, ny / 2, 1,
+       [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
+       [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return fft_grids_t<T>(c, dev_max, sms);
+}
+}  // namespace
+
+cudaError_t fft_autotune(plc_ctx *c) {
+  int sms = 0, dev_max = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if (e != cudaSuccess) return e;
+  e = c->mixed ? fft_autotune_t<float>(c, c->f_field, (size_t)dev_max, sms)
+               : fft_autotune_t<double>(c, c->d_field, (size_t)dev_max, sms);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
+}
+
+// Applies line counts chosen earlier (a re-initialised solver keeps the
+// context's tuning).
+cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y) {
+  int sms = 0, dev_max = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  if (e != cudaSuccess) return e;
+  c->fft_lines_xf = lines_xf;
+  c->fft_lines_x = lines_x;
+  c->fft_lines_y = lines_y;
+  return c->mixed ? fft_grids_t<float>(c, (size_t)dev_max, sms)
+                  : fft_grids_t<double>(c, (size_t)dev_max, sms);
+}
+
 cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
   const long long plane = (long long)c->nx * c->ny;
   const int bs = 128;

@@ -89,6 +89,7 @@ struct plc_ctx {
   plc::FftPlan plan_x, plan_y;
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
   int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids
+  int tuned_lines[3] = {0, 0, 0};  // autotuned (xf, x, y) line pairs, 0 = not tuned
   // scalars and scratch
   plc::StepConst *d_sc = nullptr;
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
@@ -216,5 +217,9 @@ cudaError_t launch_scale(const plc_ctx *c, float *var, const double *d_mult,
 size_t fft_smem_bytes(int n, int lines);
 cudaError_t fft_configure(size_t max_bytes);
 cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);
+// times the feasible tile sizes of each transform on the context's buffers
+// and keeps the fastest (overwrites the spectral array and p)
+cudaError_t fft_autotune(plc_ctx *c);
+cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 }  // namespace plc
