@@ -273,8 +273,10 @@ int plc_get_stream(plc_ctx *ctx, void **stream);
  * ms_per_kernel[0..count-1]; *count receives the number of kernels per step
  * (at most 16).  Used for per-kernel roofline figures; advances the state. */
 int plc_profile_step(plc_ctx *ctx, int nsteps, float *ms_per_kernel, int *count);
-/* Name of kernel i of the fused step (static string). */
+/* Name of kernel i of the fused step of the FP64 form (static string). */
 const char *plc_step_kernel_name(int i);
+/* Name of kernel i of the context's fused step (either form). */
+const char *plc_step_kernel_name_ctx(const plc_ctx *ctx, int i);
 
 /* ---- host-only helpers (no GPU needed) ---- */
 /* initMeshByFunc (src/mod_mesh.cc:95-125): dzf_global[0..nz+1]. */

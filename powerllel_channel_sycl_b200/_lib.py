@@ -135,7 +135,8 @@ _SIGS = {
 
 def exported_symbols():
     """Names of the entry points this binding expects (all declared in plc.h)."""
-    return sorted(list(_SIGS) + ["plc_last_error", "plc_step_kernel_name"])
+    return sorted(list(_SIGS) + ["plc_last_error", "plc_step_kernel_name",
+                                 "plc_step_kernel_name_ctx"])
 
 
 def lib():
@@ -157,6 +158,8 @@ def lib():
         L.plc_last_error.restype = C.c_char_p
         L.plc_step_kernel_name.argtypes = [_int]
         L.plc_step_kernel_name.restype = C.c_char_p
+        L.plc_step_kernel_name_ctx.argtypes = [_vp, _int]
+        L.plc_step_kernel_name_ctx.restype = C.c_char_p
         _lib = L
         return L
 

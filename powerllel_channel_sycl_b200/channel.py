@@ -335,7 +335,8 @@ class Channel:
         ms = (C.c_float * 16)()
         n = C.c_int()
         self._check(lib().plc_profile_step(self._ctx, int(nsteps), ms, C.byref(n)))
-        return {lib().plc_step_kernel_name(i).decode(): float(ms[i]) for i in range(n.value)}
+        return {lib().plc_step_kernel_name_ctx(self._ctx, i).decode(): float(ms[i])
+                for i in range(n.value)}
 
     @property
     def kernels_per_step(self) -> int:

@@ -220,6 +220,13 @@ const char *const kStepKernelNames[] = {
     "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
     "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+mean", "force+bound(u)"};
 constexpr int kStepKernels = 9;
+// the mixed form reduces the bulk mean in the forward x transform and forces
+// in the correction
+const char *const kStepKernelNamesMixed[] = {
+    "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd+mean", "fft_y_fwd", "trid_z",
+    "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+force+bound(u)"};
+constexpr int kStepKernelsMixed = 8;  // the one-block bulk_force sum is timed with the x transform
+int step_kernels(const plc_ctx *c) { return c->mixed ? kStepKernelsMixed : kStepKernels; }
 
 // Launches of one fused step (main.cc:116-154) on the context's fields, in
 // the context's storage type T.  With ev != nullptr, ev[0] is recorded before
@@ -255,8 +262,10 @@ int enqueue_step_t(plc_ctx *c, T *const *f, cudaStream_t s, cudaEvent_t *ev) {
   PLC_CUDA(c, mark());
   PLC_CUDA(c, launch_correct(c, true, p, u, v, w, s));                   // correct + mean
   PLC_CUDA(c, mark());
-  PLC_CUDA(c, launch_force_apply(c, true, u, v, w, s));                  // force + bound(u)
-  PLC_CUDA(c, mark());
+  if constexpr (std::is_same<T, double>::value) {
+    PLC_CUDA(c, launch_force_apply(c, true, u, v, w, s));                // force + bound(u)
+    PLC_CUDA(c, mark());
+  }
   return PLC_OK;
 }
 
@@ -464,6 +473,10 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   }
   if (c->mixed) {
     if ((e = rk32_configure()) != cudaSuccess) return fail(cuda_status(c, e, "rk32_configure"));
+    // one partial per block of the forward x transform (at most ny/2 * nz)
+    if ((e = cudaMalloc(&c->d_mean_partials,
+                        3 * (size_t)(c->ny / 2) * c->nz * sizeof(double))) != cudaSuccess)
+      return fail(set_error(c, PLC_ERR_NOMEM, "cudaMalloc bulk-mean partials"));
     std::vector<float> coef;
     host_rk32_coef(c, coef);
     if ((e = cudaMalloc(&c->d_coef32, coef.size() * sizeof(float))) != cudaSuccess ||
@@ -503,6 +516,7 @@ int plc_destroy(plc_ctx *c) {
   for (auto &f : c->d_field) cudaFree(f);
   for (auto &f : c->f_field) cudaFree(f);
   cudaFree(c->d_coef32);
+  cudaFree(c->d_mean_partials);
   cudaFree(c->d_mesh);
   cudaFree(c->d_sc);
   cudaFree(c->d_partials);
@@ -1075,18 +1089,19 @@ int plc_profile_step(plc_ctx *c, int nsteps, float *ms_per_kernel, int *count) {
   PLC_CHECK_CTX(c);
   PLC_REQ(c, ms_per_kernel);
   PLC_NEED_POISSON(c);
+  const int nk = step_kernels(c);
   cudaEvent_t ev[kStepKernels + 1];
   for (auto &e : ev) PLC_CUDA(c, cudaEventCreate(&e));
   int rc = PLC_OK;
   for (int s = 0; s < nsteps && rc == PLC_OK; ++s) {
     rc = enqueue_step(c, c->stream, ev);
     if (rc != PLC_OK) break;
-    cudaError_t e = cudaEventSynchronize(ev[kStepKernels]);
+    cudaError_t e = cudaEventSynchronize(ev[nk]);
     if (e != cudaSuccess) {
       rc = cuda_status(c, e, "cudaEventSynchronize");
       break;
     }
-    for (int q = 0; q < kStepKernels; ++q) {
+    for (int q = 0; q < nk; ++q) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
       ms_per_kernel[q] += ms;
@@ -1094,12 +1109,17 @@ int plc_profile_step(plc_ctx *c, int nsteps, float *ms_per_kernel, int *count) {
     ++c->nstep;
   }
   for (auto &e : ev) cudaEventDestroy(e);
-  if (count) *count = kStepKernels;
+  if (count) *count = nk;
   return rc;
 }
 
 const char *plc_step_kernel_name(int i) {
   return (i >= 0 && i < kStepKernels) ? kStepKernelNames[i] : "";
+}
+
+const char *plc_step_kernel_name_ctx(const plc_ctx *c, int i) {
+  if (!c || !c->mixed) return plc_step_kernel_name(i);
+  return (i >= 0 && i < kStepKernelsMixed) ? kStepKernelNamesMixed[i] : "";
 }
 
 int plc_mesh_by_func(int mesh_type, int stretch_func, double stretch_ratio, int nz, double lz,

@@ -86,6 +86,7 @@ struct plc_ctx {
   float *d_rpiv32 = nullptr;  // mixed form: the pivot table in FP32
   float *d_ac32 = nullptr;    // mixed form: a[nz] | c[nz] in FP32
   float *d_coef32 = nullptr;  // mixed form: per-plane RK coefficients
+  double *d_mean_partials = nullptr;  // mixed form: bulk-mean partials, 3 * (ny/2)*nz
   plc::FftPlan plan_x, plan_y;
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
   int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids

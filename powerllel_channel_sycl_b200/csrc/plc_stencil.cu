@@ -18,6 +18,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "plc_device.cuh"
 #include "plc_internal.h"
 
@@ -562,19 +564,30 @@ struct ForceCfg {
 // short-lived block would cost more than the correction itself).
 // T = double: the reference's arithmetic.  T = float (mixed form): the
 // correction in FP32, the bulk sums of the forced components in FP64.
-template <class T, int KZ>
+template <class T, int KZ, bool PRE>
 __global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
                                                           const T *__restrict__ p, T *u, T *v,
                                                           T *w, double *partials,
                                                           unsigned int *counter) {
   __shared__ double smem[2 * 3 * 32];
   const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
+  // PRE: the forcing of this step, already reduced (0 for unforced components)
+  const T fu = PRE ? T(sc->force[0]) : T(0), fv = PRE ? T(sc->force[1]) : T(0),
+          fw = PRE ? T(sc->force[2]) : T(0);
   const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 7) / 8;
   const int per_chunk = tiles_x * tiles_y;
   const int items = per_chunk * ((g.nz + KZ - 1) / KZ);
   const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
   const long long X = g.X, XY = g.XY;
   DD s[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  // FP64: error-free double-double terms (the order-independent sum of the
+  // reference restatement); FP32 fields: a plain FP64 sum of the FP32 values
+  auto acc = [](DD &a, double x) {
+    if constexpr (sizeof(T) == 8)
+      dd_add(a, x);
+    else
+      a.hi += x;
+  };
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
     const int kc = item / per_chunk, r = item - kc * per_chunk;
     const int jt = r / tiles_x, it = r - jt * tiles_x;
@@ -609,36 +622,45 @@ __global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, 
         const T nv = vv[q] - (py[q] - pc[q]) * dtdyi;
         const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k));
         const double dzl = __ldg(g.dzflzi + k);
-        if (fc.forced[0]) {
-          u[c] = nu;
-          dd_add(s[0], double(nu) * dzl);
+        if constexpr (PRE) {
+          // the forcing is known: add it and write the final halos
+          store_point(u, g, h, c, k, nu + fu, BC_CENTRED, T(0.0 - fc.u_crf));
+          store_point(v, g, h, c, k, nv + fv, BC_CENTRED, T(0));
+          store_point(w, g, h, c, k, nw + fw, BC_FACE, T(0));
         } else {
-          store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
-        }
-        if (fc.forced[1]) {
-          v[c] = nv;
-          dd_add(s[1], double(nv) * dzl);
-        } else {
-          store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
-        }
-        if (fc.forced[2]) {
-          w[c] = nw;
-          dd_add(s[2], double(nw) * dzl);
-        } else {
-          store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+          if (fc.forced[0]) {
+            u[c] = nu;
+            acc(s[0], double(nu) * dzl);
+          } else {
+            store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
+          }
+          if (fc.forced[1]) {
+            v[c] = nv;
+            acc(s[1], double(nv) * dzl);
+          } else {
+            store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
+          }
+          if (fc.forced[2]) {
+            w[c] = nw;
+            acc(s[2], double(nw) * dzl);
+          } else {
+            store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+          }
         }
       }
   }
-  block_sum<3>(s, smem);
-  if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
-    for (int d = 0; d < 3; ++d) {
-      if (fc.forced[d]) {
-        const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
-        sc->mean[d] = mean;
-        sc->force[d] = fc.vel_force[d] - mean;
-      } else {
-        sc->mean[d] = 0.0;
-        sc->force[d] = 0.0;
+  if constexpr (!PRE) {
+    block_sum<3>(s, smem);
+    if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
+      for (int d = 0; d < 3; ++d) {
+        if (fc.forced[d]) {
+          const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
+          sc->mean[d] = mean;
+          sc->force[d] = fc.vel_force[d] - mean;
+        } else {
+          sc->mean[d] = 0.0;
+          sc->force[d] = 0.0;
+        }
       }
     }
   }
@@ -996,17 +1018,23 @@ cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v, 
 namespace {
 template <class T>
 cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cudaStream_t s) {
-  // KZ planes per work item: 6 in FP32, 4 in FP64 (the loads of one item
-  // live in registers)
+  // KZ planes per work item (the loads of one item live in registers): 6 in
+  // FP32, 4 in FP64; 2 resident blocks per SM (launch bounds)
   constexpr int KZ = sizeof(T) == 4 ? 6 : 4;
-  // one wave: 2 resident blocks per SM (launch bounds), at most the items
+  constexpr int kBlocksPerSm = 2;
+  // one wave of resident blocks, at most the items
   const long long items =
       (long long)((c->nx + 31) / 32) * ((c->ny + 7) / 8) * ((c->nz + KZ - 1) / KZ);
-  long long nb = 2ll * c->num_sms;
+  long long nb = (long long)kBlocksPerSm * c->num_sms;
   if (nb > items) nb = items;
   if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
-  k_correct_fused<T, KZ><<<(unsigned)nb, 256, 0, s>>>(c->geo(), c->d_sc, force_cfg(c), p, u, v,
-                                                       w, c->d_partials, c->d_counter);
+  // the mixed form's fused RK2 has reduced the forcing already
+  if (c->mixed)
+    k_correct_fused<T, KZ, true><<<(unsigned)nb, 256, 0, s>>>(
+        c->geo(), c->d_sc, force_cfg(c), p, u, v, w, c->d_partials, c->d_counter);
+  else
+    k_correct_fused<T, KZ, false><<<(unsigned)nb, 256, 0, s>>>(
+        c->geo(), c->d_sc, force_cfg(c), p, u, v, w, c->d_partials, c->d_counter);
   return cudaGetLastError();
 }
 

@@ -132,6 +132,9 @@ def test_cfl_controlled_dt():
 
 
 def test_step_graph_kernel_count():
+    """The forward x transform writes the bulk-mean partials, a one-block
+    kernel turns them into the forcing and the correction applies it: no
+    forcing pass over the field."""
     ch = mixed_channel(32, 24, 16)
     ch.initFlow()
     assert ch.kernels_per_step == 9
@@ -141,4 +144,5 @@ def test_profile_step_mixed():
     ch = mixed_channel(64, 48, 32)
     ch.initFlow()
     ms = ch.profile_step(2)
-    assert len(ms) == 9 and all(t > 0 for t in ms.values())
+    assert len(ms) == 8 and all(t > 0 for t in ms.values())
+    assert "correct+force+bound(u)" in ms
