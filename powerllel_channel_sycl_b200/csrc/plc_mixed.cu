@@ -41,6 +41,9 @@ constexpr int PLANE = HX * HY;          // floats per field-plane
 constexpr int SLOT = ((PLANE * 4 + 127) / 128) * 128 / 4;  // floats, 128-B aligned
 constexpr int NSLOT = 6;
 constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 4u;
+// RK2 base values (u, v, w of plane k): the interior rows of the tile, 36 x 16
+constexpr int BPLANE = HX * RY;         // 576 floats = 2304 bytes, a multiple of 128
+constexpr unsigned BASE_TX_BYTES = 3u * BPLANE * 4u;
 constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr int KCHUNK = 32;
 constexpr int NCOEF = 12;               // per-plane coefficient row (10 used), 3 float4
@@ -160,8 +163,9 @@ struct SmemAcc32 {
   }
 };
 
-size_t rk32_smem_bytes() {
-  return (size_t)3 * NSLOT * SLOT * 4 + (size_t)(KCHUNK + 2) * NCOEF * 4 + NSLOT * 8 + 128;
+size_t rk32_smem_bytes(int stage) {
+  return (size_t)3 * NSLOT * SLOT * 4 + (stage == 2 ? (size_t)3 * NSLOT * BPLANE * 4 : 0) +
+         (size_t)(KCHUNK + 2) * NCOEF * 4 + NSLOT * 8 + 128;
 }
 
 // RK1 (STAGE 1): o = q + dt*F(q);  RK2 (STAGE 2): o = (q + dt*F(q) + o)/2.
@@ -172,17 +176,22 @@ size_t rk32_smem_bytes() {
 // points share are read from shared memory once).  Plane k+3 is copied into
 // the slot of plane k-3 while plane k is computed: that slot was last read in
 // iteration k-2, which every thread finished before it reached the barrier of
-// iteration k-1, so one barrier per plane orders the ring.
+// iteration k-1, so one barrier per plane orders the ring.  RK2 also brings the
+// base values of each interior plane of its chunk (the interior rows of u, v,
+// w, with the operand planes and on the same barrier) into a second ring.
 template <int STAGE, bool FUSE, bool CRF>
 __global__ void __launch_bounds__(RX *TY, 2)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
-           const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
+           const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap bu,
+           const __grid_constant__ CUtensorMap bv, const __grid_constant__ CUtensorMap bw, Geo g,
+           RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
            float *ou, float *ov, float *ow, int kchunk, int *err) {
   extern __shared__ unsigned char smem_raw[];
   float *slot = reinterpret_cast<float *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
-  Coef *zc = reinterpret_cast<Coef *>(slot + 3 * NSLOT * SLOT);  // planes kb .. ke
+  float *bslot = slot + 3 * NSLOT * SLOT;  // RK2 base ring (3 * NSLOT * BPLANE)
+  Coef *zc = reinterpret_cast<Coef *>(bslot + (STAGE == 2 ? 3 * NSLOT * BPLANE : 0));
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
   __shared__ int ok_s[2];  // by iteration parity: a fast thread 0 cannot overwrite a flag
                            // that a slow thread has still to read
@@ -199,10 +208,16 @@ __global__ void __launch_bounds__(RX *TY, 2)
 
   auto issue = [&](int p) {  // thread 0 only
     const int s = (p - (kb - 1)) % NSLOT;
-    mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
+    const bool base = (STAGE == 2) && p >= kb && p <= ke;
+    mbar_expect_tx(&bar[s], PLANE_TX_BYTES + (base ? BASE_TX_BYTES : 0u));
     tma_load_plane(slot + s * SLOT, &mu, x0, y0, p, &bar[s]);
     tma_load_plane(slot + NSLOT * SLOT + s * SLOT, &mv, x0, y0, p, &bar[s]);
     tma_load_plane(slot + 2 * NSLOT * SLOT + s * SLOT, &mw, x0, y0, p, &bar[s]);
+    if (base) {
+      tma_load_plane(bslot + s * BPLANE, &bu, x0, y0 + 1, p, &bar[s]);
+      tma_load_plane(bslot + NSLOT * BPLANE + s * BPLANE, &bv, x0, y0 + 1, p, &bar[s]);
+      tma_load_plane(bslot + 2 * NSLOT * BPLANE + s * BPLANE, &bw, x0, y0 + 1, p, &bar[s]);
+    }
   };
   auto wait_plane = [&](int p) -> bool {  // thread 0 only
     const int rel = p - (kb - 1);
@@ -226,19 +241,7 @@ __global__ void __launch_bounds__(RX *TY, 2)
   const float dt = float(sc->dt);
   const long long X = g.X, XY = g.XY;
   long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
-  float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};  // RK2 base values of plane k
-  if (STAGE == 2) {
-    if (act_a) {
-      ba[0] = ou[c];
-      ba[1] = ov[c];
-      ba[2] = ow[c];
-    }
-    if (act_b) {
-      bb[0] = ou[c + X];
-      bb[1] = ov[c + X];
-      bb[2] = ow[c + X];
-    }
-  }
+  const int ob = (2 * ty) * HX + (tx + 1);  // point a in a base slot
   const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
   const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
   int sm = 0, s0 = 1, sp = 2;                  // slots of planes k-1, k, k+1
@@ -266,19 +269,6 @@ __global__ void __launch_bounds__(RX *TY, 2)
     }
     __syncthreads();
     if (!ok_s[par]) return;  // the whole block leaves together
-    float na[3] = {0.f, 0.f, 0.f}, nb[3] = {0.f, 0.f, 0.f};
-    if (STAGE == 2 && k < ke) {
-      if (act_a) {
-        na[0] = ou[c + XY];
-        na[1] = ov[c + XY];
-        na[2] = ow[c + XY];
-      }
-      if (act_b) {
-        nb[0] = ou[c + XY + X];
-        nb[1] = ov[c + XY + X];
-        nb[2] = ow[c + XY + X];
-      }
-    }
     if (act_a) {
       const Coef z = zc[k - kb];
       SmemAcc32 a;
@@ -295,6 +285,14 @@ __global__ void __launch_bounds__(RX *TY, 2)
       float va[3] = {a(0, 0, 0, 0), a(1, 0, 0, 0), a(2, 0, 0, 0)};
       float vb[3] = {b(0, 0, 0, 0), b(1, 0, 0, 0), b(2, 0, 0, 0)};
       const float fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
+      float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};  // RK2 base values
+      if (STAGE == 2) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          ba[d] = bslot[d * NSLOT * BPLANE + s0 * BPLANE + ob];
+          bb[d] = bslot[d * NSLOT * BPLANE + s0 * BPLANE + ob + HX];
+        }
+      }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         if (STAGE == 1) {
@@ -325,11 +323,7 @@ __global__ void __launch_bounds__(RX *TY, 2)
         }
       }
     }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      ba[d] = na[d];
-      bb[d] = nb[d];
-    }
+
     sm = s0;
     s0 = sp;
     sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
@@ -340,12 +334,12 @@ __global__ void __launch_bounds__(RX *TY, 2)
 // Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 18
 // tile of one plane.  The pitch is a multiple of 4 (16 bytes) and the tile's x
 // origin 32*bx is 128-byte aligned.
-bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g) {
+bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g, int box_rows = HY) {
   auto enc = tensor_map_encoder();
   if (!enc || (reinterpret_cast<unsigned long long>(ptr) & 15ull) || (g.X & 3)) return false;
   cuuint64_t dims[3] = {(cuuint64_t)g.X, (cuuint64_t)g.Y, (cuuint64_t)(g.nz + 2)};
   cuuint64_t strides[2] = {(cuuint64_t)g.X * 4ull, (cuuint64_t)g.XY * 4ull};
-  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)HY, 1u};
+  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)box_rows, 1u};
   cuuint32_t estr[3] = {1u, 1u, 1u};
   const CUresult r =
       enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box,
@@ -355,15 +349,14 @@ bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g) {
 }
 
 template <int STAGE, bool FUSE, bool CRF>
-cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
-                          const CUtensorMap &mw, const RkConst &K, float bc_u, float *ou,
-                          float *ov, float *ow, cudaStream_t s) {
-  const size_t smem = rk32_smem_bytes();
+cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[6], const RkConst &K,
+                          float bc_u, float *ou, float *ov, float *ow, cudaStream_t s) {
+  const size_t smem = rk32_smem_bytes(STAGE);
   const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
-      mu, mv, mw, c->geo(), K, reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou,
-      ov, ow, kchunk, c->d_err);
+      m[0], m[1], m[2], m[3], m[4], m[5], c->geo(), K,
+      reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err);
   return cudaGetLastError();
 }
 
@@ -401,7 +394,7 @@ unsigned convert_blocks(const plc_ctx *c, long long n) {
 // Raises the dynamic shared-memory limit of the FP32 RK kernels (about 50 KB)
 // on the current device.
 cudaError_t rk32_configure() {
-  const int bytes = (int)rk32_smem_bytes();
+  const int bytes = (int)rk32_smem_bytes(2);
   cudaError_t e = cudaSuccess;
 #define PLC_RK32_ATTR(S, F, C)                                                            \
   if (e == cudaSuccess)                                                                   \
@@ -423,10 +416,18 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
                       const float *qv, const float *qw, float *ou, float *ov, float *ow,
                       cudaStream_t s) {
   const Geo g = c->geo();
-  CUtensorMap mu, mv, mw;
-  if (!field_tensor_map32(&mu, qu, g) || !field_tensor_map32(&mv, qv, g) ||
-      !field_tensor_map32(&mw, qw, g))
+  // operand tiles (36 x 18) of q, and for RK2 the base tiles (36 x 16) of o
+  CUtensorMap m[6];
+  if (!field_tensor_map32(&m[0], qu, g) || !field_tensor_map32(&m[1], qv, g) ||
+      !field_tensor_map32(&m[2], qw, g))
     return cudaErrorInvalidValue;  // FP32 fields are allocated 16-byte aligned and padded
+  if (stage == 2) {
+    if (!field_tensor_map32(&m[3], ou, g, RY) || !field_tensor_map32(&m[4], ov, g, RY) ||
+        !field_tensor_map32(&m[5], ow, g, RY))
+      return cudaErrorInvalidValue;
+  } else {
+    m[3] = m[4] = m[5] = m[0];  // not read by RK1
+  }
   RkConst K;
   K.qx = float(0.25 * c->dx_inv);
   K.qy = float(0.25 * c->dy_inv);
@@ -435,7 +436,7 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
   K.crf = float(0.5 * u_crf * c->dx_inv);
   const float bc_u = float(0.0 - u_crf);
   const bool crf = (u_crf != 0.0);
-#define PLC_RK32(S, F, C) return launch_rk32_t<S, F, C>(c, mu, mv, mw, K, bc_u, ou, ov, ow, s)
+#define PLC_RK32(S, F, C) return launch_rk32_t<S, F, C>(c, m, K, bc_u, ou, ov, ow, s)
   if (stage == 1) {
     if (fuse_bc) {
       if (crf) PLC_RK32(1, true, true);

@@ -564,16 +564,13 @@ struct ForceCfg {
 // short-lived block would cost more than the correction itself).
 // T = double: the reference's arithmetic.  T = float (mixed form): the
 // correction in FP32, the bulk sums of the forced components in FP64.
-template <class T, int KZ, bool PRE>
+template <class T, int KZ>
 __global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, ForceCfg fc,
                                                           const T *__restrict__ p, T *u, T *v,
                                                           T *w, double *partials,
                                                           unsigned int *counter) {
   __shared__ double smem[2 * 3 * 32];
   const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
-  // PRE: the forcing of this step, already reduced (0 for unforced components)
-  const T fu = PRE ? T(sc->force[0]) : T(0), fv = PRE ? T(sc->force[1]) : T(0),
-          fw = PRE ? T(sc->force[2]) : T(0);
   const int tiles_x = (g.nx + 31) / 32, tiles_y = (g.ny + 7) / 8;
   const int per_chunk = tiles_x * tiles_y;
   const int items = per_chunk * ((g.nz + KZ - 1) / KZ);
@@ -622,48 +619,86 @@ __global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, 
         const T nv = vv[q] - (py[q] - pc[q]) * dtdyi;
         const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k));
         const double dzl = __ldg(g.dzflzi + k);
-        if constexpr (PRE) {
-          // the forcing is known: add it and write the final halos
-          store_point(u, g, h, c, k, nu + fu, BC_CENTRED, T(0.0 - fc.u_crf));
-          store_point(v, g, h, c, k, nv + fv, BC_CENTRED, T(0));
-          store_point(w, g, h, c, k, nw + fw, BC_FACE, T(0));
+        if (fc.forced[0]) {
+          u[c] = nu;
+          acc(s[0], double(nu) * dzl);
         } else {
-          if (fc.forced[0]) {
-            u[c] = nu;
-            acc(s[0], double(nu) * dzl);
-          } else {
-            store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
-          }
-          if (fc.forced[1]) {
-            v[c] = nv;
-            acc(s[1], double(nv) * dzl);
-          } else {
-            store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
-          }
-          if (fc.forced[2]) {
-            w[c] = nw;
-            acc(s[2], double(nw) * dzl);
-          } else {
-            store_point(w, g, h, c, k, nw, BC_FACE, T(0));
-          }
+          store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - fc.u_crf));
+        }
+        if (fc.forced[1]) {
+          v[c] = nv;
+          acc(s[1], double(nv) * dzl);
+        } else {
+          store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
+        }
+        if (fc.forced[2]) {
+          w[c] = nw;
+          acc(s[2], double(nw) * dzl);
+        } else {
+          store_point(w, g, h, c, k, nw, BC_FACE, T(0));
         }
       }
   }
-  if constexpr (!PRE) {
-    block_sum<3>(s, smem);
-    if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
-      for (int d = 0; d < 3; ++d) {
-        if (fc.forced[d]) {
-          const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
-          sc->mean[d] = mean;
-          sc->force[d] = fc.vel_force[d] - mean;
-        } else {
-          sc->mean[d] = 0.0;
-          sc->force[d] = 0.0;
-        }
+  block_sum<3>(s, smem);
+  if (grid_sum_last<3>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
+    for (int d = 0; d < 3; ++d) {
+      if (fc.forced[d]) {
+        const double mean = (s[d].hi + s[d].lo) / g.nx / g.ny;
+        sc->mean[d] = mean;
+        sc->force[d] = fc.vel_force[d] - mean;
+      } else {
+        sc->mean[d] = 0.0;
+        sc->force[d] = 0.0;
       }
     }
   }
+}
+
+// The mixed form's fused correction: correctVel (mod_calcVel.cc:272-274) plus
+// the forcing sc->force[d] that its forward x transform has already reduced
+// (0 for unforced components), written with the halo images and wall ghosts.
+// No reduction, so a plain grid: each thread takes KZ planes of one column
+// (p(k+1) of a plane is p(k) of the next) with all loads issued first.
+template <class T, int KZ>
+__global__ void __launch_bounds__(BX *BY) k_correct_forced(Geo g, const StepConst *__restrict__ sc,
+                                                           double u_crf, const T *__restrict__ p,
+                                                           T *u, T *v, T *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k0 = blockIdx.z * KZ + 1;
+  if (i > g.nx || j > g.ny) return;
+  const int nk = min(KZ, g.nz - k0 + 1);
+  const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
+  const T fu = T(sc->force[0]), fv = T(sc->force[1]), fw = T(sc->force[2]);
+  const long long c0 = g.at(i, j, k0), X = g.X, XY = g.XY;
+  const HaloCol h = halo_col(g, i, j);
+  T pc[KZ + 1], px[KZ], py[KZ], uu[KZ], vv[KZ], ww[KZ];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q)
+    if (q < nk) {
+      const long long c = c0 + q * XY;
+      pc[q] = p[c];
+      px[q] = p[c + 1];
+      py[q] = p[c + X];
+      uu[q] = u[c];
+      vv[q] = v[c];
+      ww[q] = w[c];
+    }
+#pragma unroll
+  for (int q = 1; q <= KZ; ++q)
+    if (q == nk) pc[q] = p[c0 + q * XY];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q)
+    if (q < nk) {
+      const int k = k0 + q;
+      const long long c = c0 + q * XY;
+      const T nu = uu[q] - (px[q] - pc[q]) * dtdxi + fu;
+      const T nv = vv[q] - (py[q] - pc[q]) * dtdyi + fv;
+      const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k)) + fw;
+      store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - u_crf));
+      store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
+      store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+    }
 }
 
 // Adds sc->force[d] to the interior of each forced component
@@ -1028,13 +1063,16 @@ cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cuda
   long long nb = (long long)kBlocksPerSm * c->num_sms;
   if (nb > items) nb = items;
   if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
-  // the mixed form's fused RK2 has reduced the forcing already
-  if (c->mixed)
-    k_correct_fused<T, KZ, true><<<(unsigned)nb, 256, 0, s>>>(
-        c->geo(), c->d_sc, force_cfg(c), p, u, v, w, c->d_partials, c->d_counter);
-  else
-    k_correct_fused<T, KZ, false><<<(unsigned)nb, 256, 0, s>>>(
-        c->geo(), c->d_sc, force_cfg(c), p, u, v, w, c->d_partials, c->d_counter);
+  if (c->mixed) {
+    // the mixed form's forward x transform has reduced the forcing already
+    constexpr int KZF = 4;
+    dim3 grid((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, (c->nz + KZF - 1) / KZF);
+    k_correct_forced<T, KZF><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, c->prm.u_crf, p, u,
+                                                          v, w);
+  } else {
+    k_correct_fused<T, KZ><<<(unsigned)nb, 256, 0, s>>>(c->geo(), c->d_sc, force_cfg(c), p, u, v,
+                                                         w, c->d_partials, c->d_counter);
+  }
   return cudaGetLastError();
 }
 
