@@ -68,12 +68,12 @@ KERNEL_BYTES_PER_POINT = {
 }
 STEP_BYTES_PER_POINT = sum(KERNEL_BYTES_PER_POINT.values())  # 288
 # the mixed form stores every field in FP32 (half the bytes; the pivot table
-# excluded, as above); its forward x transform also reduces the bulk mean and
-# its correction applies the forcing, so it has no separate forcing pass
+# excluded, as above); its RK2 also sums the bulk mean and its correction
+# applies the forcing, so it has no separate forcing pass
 MIXED_BYTES_PER_POINT = {
     "rk1+bound(u1)": 24,          # read u,v,w; write u1,v1,w1
-    "rk2+bound(u)": 36,           # read u1,v1,w1,u,v,w; write u,v,w
-    "calcRHS+fft_x_fwd+mean": 16,  # read u,v,w; write spectral array
+    "rk2+bound(u)+mean": 36,      # read u1,v1,w1,u,v,w; write u,v,w
+    "calcRHS+fft_x_fwd": 16,      # read u,v,w; write spectral array
     "fft_y_fwd": 8,
     "trid_z": 8,
     "fft_y_bwd": 8,
@@ -93,15 +93,22 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(workload):
-    """dram read+write bytes per launch of each kernel from the committed ncu summary."""
+def load_traffic(workload, form, kernel, npts):
+    """ncu DRAM read+write bytes per launch of a step kernel: the committed
+    bytes per point (from a capture of this workload, else of the 512x256x128
+    case -- the traffic of these streaming kernels grows with the points)
+    times the points of the workload.  Returns (bytes, source) or (None, None)."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(workload, {})
     except Exception:
-        return {}
+        return None, None
+    for wl in (workload, "prof"):
+        bpp = d.get(wl, {}).get(form, {}).get(kernel)
+        if bpp is not None:
+            return bpp * npts, f"ncu capture of the {wl} workload, {bpp:.1f} B/pt"
+    return None, None
 
 
 class ClockSampler:
@@ -161,6 +168,28 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class nvtx_range:
+    """NVTX range around a timed region (lets a profiler select the step's
+    kernels: ncu --nvtx --nvtx-include fp64_step/); a no-op without torch."""
+
+    def __init__(self, name):
+        self.name = name
+
+    def __enter__(self):
+        try:
+            import torch
+            torch.cuda.nvtx.range_push(self.name)
+            self.ok = True
+        except Exception:
+            self.ok = False
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            import torch
+            torch.cuda.nvtx.range_pop()
+
+
 def channel_params(wl, nt_check, precision="fp64", cfl_target=None):
     from powerllel_channel_sycl_b200 import make_params
     return make_params(
@@ -186,7 +215,8 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
     ch.sync()
     torch.cuda.synchronize(local)
     barrier(pg, local)
-    ms = ch.step_timed(args.steps)
+    with nvtx_range("mixed_step"):
+        ms = ch.step_timed(args.steps)
     torch.cuda.synchronize(local)
     barrier(pg, local)
     ms_max = max_over_ranks(ms, pg, local)
@@ -200,7 +230,10 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
                    "gbs": MIXED_BYTES_PER_POINT[k] * npts / (v / prof_steps / 1e3) / 1e9}
                for k, v in prof.items()}
     ch.close()
-    peak, _ = load_peaks()
+    peak, peak_kind = load_peaks()
+    dom = max(prof, key=prof.get)
+    achieved = kernels[dom]["gbs"]
+    traffic, traffic_src = load_traffic(args.workload, "mixed", dom, npts)
 
     # accuracy: 10 steps of both forms from the same laminar + noise field
     nerr = 10
@@ -228,6 +261,10 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
         "step_roofline": {"bytes_per_point_step": MIXED_STEP_BYTES_PER_POINT,
                           "achieved_gbs": MIXED_STEP_BYTES_PER_POINT * value / world / 1e9,
                           "frac": MIXED_STEP_BYTES_PER_POINT * value / world / 1e9 / peak},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_source": traffic_src,
+                     "bytes_per_point": MIXED_BYTES_PER_POINT[dom]},
         "kernels": kernels,
         "checks": {"nan_free": ok, "cfl_max": cfl[0], "div_max": div[0]},
         "fft_tiles": tiles,
@@ -359,7 +396,7 @@ def run_ours(args, wl, rank, world, local, pg):
     torch.cuda.synchronize(local)
     barrier(pg, local)
     torch.cuda.synchronize(local)
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk, nvtx_range("fp64_step"):
         ms = ch.step_timed(args.steps)
     torch.cuda.synchronize(local)
     barrier(pg, local)
@@ -377,7 +414,7 @@ def run_ours(args, wl, rank, world, local, pg):
     dom_ms = prof[dom] / prof_steps
     peak, peak_kind = load_peaks()
     achieved = KERNEL_BYTES_PER_POINT[dom] * npts / (dom_ms / 1e3) / 1e9
-    traffic = load_traffic(args.workload).get(dom)
+    traffic, traffic_src = load_traffic(args.workload, "fp64", dom, npts)
     kernels = {k: {"ms": v / prof_steps, "share": v / total,
                    "gbs": KERNEL_BYTES_PER_POINT[k] * npts / (v / prof_steps / 1e3) / 1e9}
                for k, v in prof.items()}
@@ -425,7 +462,7 @@ def run_ours(args, wl, rank, world, local, pg):
         "config": workload_config(args, wl),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic,
+                     "traffic": traffic, "traffic_source": traffic_src,
                      "bytes_per_point": KERNEL_BYTES_PER_POINT[dom]},
         "step_roofline": {"bytes_per_point_step": STEP_BYTES_PER_POINT,
                           "achieved_gbs": STEP_BYTES_PER_POINT * value / world / 1e9,

@@ -220,12 +220,11 @@ const char *const kStepKernelNames[] = {
     "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
     "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+mean", "force+bound(u)"};
 constexpr int kStepKernels = 9;
-// the mixed form reduces the bulk mean in the forward x transform and forces
-// in the correction
+// the mixed form sums the bulk mean in RK2 and forces in the correction
 const char *const kStepKernelNamesMixed[] = {
-    "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd+mean", "fft_y_fwd", "trid_z",
+    "rk1+bound(u1)", "rk2+bound(u)+mean", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
     "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+force+bound(u)"};
-constexpr int kStepKernelsMixed = 8;  // the one-block bulk_force sum is timed with the x transform
+constexpr int kStepKernelsMixed = 8;  // the one-block bulk_force sum is timed with RK2
 int step_kernels(const plc_ctx *c) { return c->mixed ? kStepKernelsMixed : kStepKernels; }
 
 // Launches of one fused step (main.cc:116-154) on the context's fields, in
@@ -473,9 +472,9 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   }
   if (c->mixed) {
     if ((e = rk32_configure()) != cudaSuccess) return fail(cuda_status(c, e, "rk32_configure"));
-    // one partial per block of the forward x transform (at most ny/2 * nz)
-    if ((e = cudaMalloc(&c->d_mean_partials,
-                        3 * (size_t)(c->ny / 2) * c->nz * sizeof(double))) != cudaSuccess)
+    // one partial per block of the fused RK2
+    if ((e = cudaMalloc(&c->d_mean_partials, 3 * (size_t)rk32_blocks(c) * sizeof(double))) !=
+        cudaSuccess)
       return fail(set_error(c, PLC_ERR_NOMEM, "cudaMalloc bulk-mean partials"));
     std::vector<float> coef;
     host_rk32_coef(c, coef);

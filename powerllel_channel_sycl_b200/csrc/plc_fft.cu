@@ -433,26 +433,20 @@ __device__ __forceinline__ double div_dt(const double *__restrict__ u,
   const double tz = __dmul_rn(__dmul_rn(__dsub_rn(w[c], w[c - XY]), dti), dzfi);
   return __dadd_rn(__dadd_rn(tx, ty), tz);
 }
-
-// Bulk mean of the forced components, reduced by the mixed form's fused
-// forward x transform (MEAN), which loads every interior u, v, w once.  The
-// correction that follows changes each x-line of u by -dt/dx times
-// sum_i (p(i+1) - p(i)), zero on the periodic line, so this mean of the
-// state after RK2 is the mean after the correction (forceVel,
-// mod_calcVel.cc:280-301, up to rounding) and the correction adds the force.
-// Each block writes its FP64 partial sums; k_bulk_force adds them up.
-struct BulkMean {
-  int forced[3];
-  double vel_force[3];
-  double *partials;        // 3 * blocks
-};
+// the mixed form: FP32 operands and arithmetic
+__device__ __forceinline__ float div_dt(const float *__restrict__ u, const float *__restrict__ v,
+                                        const float *__restrict__ w, long long c, int X,
+                                        long long XY, float dtidxi, float dtidyi, float dti,
+                                        float dzfi) {
+  return (u[c] - u[c - 1]) * dtidxi + (v[c] - v[c - X]) * dtidyi + (w[c] - w[c - XY]) * (dti * dzfi);
+}
 
 // Forward x transform fused with calcRHS, one tile per block: rows
 // (j0+2l, j0+2l+1) of plane k are div(u)/dt evaluated from global memory while
 // loading (many resident blocks hide the load latency), then transformed.
-template <class T, int N, bool FUSED, bool MEAN>
+template <class T, int N, bool FUSED>
 __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx<T>::V> P, int nl,
-                                                       StepConst *sc, BulkMean bm,
+                                                       const StepConst *__restrict__ sc,
                                                        const T *__restrict__ p,
                                                        const T *__restrict__ u,
                                                        const T *__restrict__ v,
@@ -472,24 +466,12 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx
     dtidyi = T(sc->dtidyi);
     dzfi = T(__ldg(g.dzf_inv + k + 1));
   }
-  // MEAN: per-thread sums of u, v, w over the few dozen points a thread loads
-  // (FP32; the block and grid sums are FP64)
-  T msum[3] = {T(0), T(0), T(0)};
   for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
     const int l = e / n, t = e - l * n;
     const long long ca = g.at(t + 1, j0 + 2 * l + 1, k + 1);
     const long long cb = ca + g.X;
     T a, b;
-    if constexpr (MEAN) {
-      const T ua = u[ca], va = v[ca], wa = w[ca], ub = u[cb], vb = v[cb], wb = w[cb];
-      a = (ua - u[ca - 1]) * dtidxi + (va - v[ca - g.X]) * dtidyi +
-          (wa - w[ca - g.XY]) * (dti * dzfi);
-      b = (ub - u[cb - 1]) * dtidxi + (vb - v[cb - g.X]) * dtidyi +
-          (wb - w[cb - g.XY]) * (dti * dzfi);
-      msum[0] += ua + ub;
-      msum[1] += va + vb;
-      msum[2] += wa + wb;
-    } else if (FUSED) {
+    if (FUSED) {
       a = div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
       b = div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
     } else {
@@ -508,56 +490,6 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx
     const long long row = (long long)k * g.ny + j0 + 2 * l;
     reinterpret_cast<V *>(var + row * n)[m] = a;
     reinterpret_cast<V *>(var + (row + 1) * n)[m] = b;
-  }
-  if constexpr (MEAN) {
-    __shared__ T red[8][3];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;  // 256 threads: 8 warps
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      if (bm.forced[d]) {  // uniform: only the forced components are reduced
-        T x = msum[d];
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) red[wid][d] = x;
-      }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-      const int d = threadIdx.x;
-      double x = 0.0;
-      if (bm.forced[d])
-        for (int w2 = 0; w2 < 8; ++w2) x += double(red[w2][d]);
-      const unsigned nblocks = gridDim.x * gridDim.y;
-      bm.partials[d * nblocks + blockIdx.x + gridDim.x * blockIdx.y] =
-          x * __ldg(g.dzflzi + k + 1);
-    }
-  }
-}
-
-// The forcing of the mixed form from the partial sums of its forward x
-// transform: sc->mean[d] = sum / (nx*ny), sc->force[d] = vel_force[d] - mean
-// (forceVel, mod_calcVel.cc:280-301).  One block; the partials are added in a
-// fixed order.
-__global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkMean bm,
-                                                     int nblocks) {
-  __shared__ double red[32][3];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double part[3] = {0.0, 0.0, 0.0};
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) part[d] += bm.partials[d * nblocks + b];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    double x = part[d];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) red[wid][d] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    const int d = threadIdx.x;
-    double tot = 0.0;
-    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot += red[w2][d];
-    const double mean = tot / g.nx / g.ny;
-    sc->mean[d] = bm.forced[d] ? mean : 0.0;
-    sc->force[d] = bm.forced[d] ? bm.vel_force[d] - mean : 0.0;
   }
 }
 
@@ -1030,13 +962,13 @@ cudaError_t fft_configure(size_t max_bytes) {
     if (r != cudaSuccess) return r;                                                       \
   }
       PLC_SMEM((k_fft_x_fwd<double, N>));
-      PLC_SMEM((k_fft_x_fwd_div<double, N, true, false>));
+      PLC_SMEM((k_fft_x_fwd_div<double, N, true>));
       PLC_SMEM((k_fft_x_bwd<double, N, true>));
       PLC_SMEM((k_fft_x_bwd<double, N, false>));
       PLC_SMEM((k_fft_y<double, N, true>));
       PLC_SMEM((k_fft_y<double, N, false>));
       PLC_SMEM((k_fft_x_fwd<float, N>));
-      PLC_SMEM((k_fft_x_fwd_div<float, N, true, true>));
+      PLC_SMEM((k_fft_x_fwd_div<float, N, true>));
       PLC_SMEM((k_fft_x_bwd<float, N, true>));
       PLC_SMEM((k_fft_x_bwd<float, N, false>));
       PLC_SMEM((k_fft_y<float, N, true>));
@@ -1113,21 +1045,8 @@ cudaError_t fft_x_fwd_t(const plc_ctx *c, const T *p, const T *u, const T *v, co
     } else {
       const int nl = c->fft_lines_xf;
       dim3 grid(c->ny / (2 * nl), c->nz);
-      // the mixed form also reduces the bulk mean of the forced components
-      BulkMean bm;
-      for (int d = 0; d < 3; ++d) {
-        bm.forced[d] = c->prm.is_forced[d] ? 1 : 0;
-        bm.vel_force[d] = c->prm.vel_force[d];
-      }
-      bm.partials = c->d_mean_partials;
-      constexpr bool kMean = sizeof(T) == 4;
-      k_fft_x_fwd_div<T, N, true, kMean><<<grid, 256, fft_bytes<T>(c->nx, nl), s>>>(
-          c->geo(), dev_plan<T>(c->plan_x), nl, c->d_sc, bm, nullptr, u, v, w, var);
-      if constexpr (kMean) {
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        k_bulk_force<<<1, 1024, 0, s>>>(c->geo(), c->d_sc, bm, (int)(grid.x * grid.y));
-      }
+      k_fft_x_fwd_div<T, N, true><<<grid, 256, fft_bytes<T>(c->nx, nl), s>>>(
+          c->geo(), dev_plan<T>(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
     }
     return cudaGetLastError();
   });

@@ -86,7 +86,7 @@ struct plc_ctx {
   float *d_rpiv32 = nullptr;  // mixed form: the pivot table in FP32
   float *d_ac32 = nullptr;    // mixed form: a[nz] | c[nz] in FP32
   float *d_coef32 = nullptr;  // mixed form: per-plane RK coefficients
-  double *d_mean_partials = nullptr;  // mixed form: bulk-mean partials, 3 * (ny/2)*nz
+  double *d_mean_partials = nullptr;  // mixed form: bulk-mean partials, 3 * RK blocks
   plc::FftPlan plan_x, plan_y;
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
   int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids
@@ -160,6 +160,8 @@ cudaError_t launch_to_f64(const plc_ctx *c, const float *src, double *dst, long 
                           int pitch, cudaStream_t s);
 // shared-memory limit of the FP32 RK kernels on the current device
 cudaError_t rk32_configure();
+// blocks of the FP32 RK grid
+long long rk32_blocks(const plc_ctx *c);
 // per-plane coefficient rows of the FP32 RK kernels, rk32_coef_floats() per plane
 void host_rk32_coef(const plc_ctx *c, std::vector<float> &out);
 int rk32_coef_floats();

@@ -15,7 +15,8 @@
 // cp.async.bulk.tensor copy per field three planes ahead -- but the
 // momentum right-hand side is evaluated in FP32 with fused multiply-adds and
 // with the z interpolation weights folded into ten per-plane coefficients
-// (an algebraic rearrangement of the reference's expressions).
+// (an algebraic rearrangement of the reference's expressions).  The fused RK2
+// stage also sums the forced components for the bulk forcing.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -168,6 +169,20 @@ size_t rk32_smem_bytes(int stage) {
          (size_t)(KCHUNK + 2) * NCOEF * 4 + NSLOT * 8 + 128;
 }
 
+// Bulk mean of the forced components, summed by the mixed form's fused RK2
+// stage (MEAN = STAGE 2 with FUSE) from the values it stores.  The correction
+// that follows changes each x-line of u by -dt/dx times
+// sum_i (p(i+1) - p(i)), zero on the periodic line, so this mean of the state
+// after RK2 is the mean after the correction (forceVel,
+// mod_calcVel.cc:280-301, up to rounding), and the correction adds the force.
+// Threads sum in FP32 (a few hundred values), blocks write FP64 partials and
+// k_bulk_force adds them in a fixed order.
+struct BulkMean {
+  int forced[3];
+  double vel_force[3];
+  double *partials;  // 3 * blocks
+};
+
 // RK1 (STAGE 1): o = q + dt*F(q);  RK2 (STAGE 2): o = (q + dt*F(q) + o)/2.
 // FUSE: the halo images and wall ghosts of the result are written as well.
 //
@@ -186,7 +201,7 @@ __global__ void __launch_bounds__(RX *TY, 2)
            const __grid_constant__ CUtensorMap bv, const __grid_constant__ CUtensorMap bw, Geo g,
            RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
-           float *ou, float *ov, float *ow, int kchunk, int *err) {
+           float *ou, float *ov, float *ow, int kchunk, int *err, BulkMean bm) {
   extern __shared__ unsigned char smem_raw[];
   float *slot = reinterpret_cast<float *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
@@ -196,6 +211,8 @@ __global__ void __launch_bounds__(RX *TY, 2)
   __shared__ int ok_s[2];  // by iteration parity: a fast thread 0 cannot overwrite a flag
                            // that a slow thread has still to read
 
+  constexpr bool kMean = (STAGE == 2 && FUSE);
+  float msum[3] = {0.f, 0.f, 0.f};  // kMean: the thread's dz-weighted sums
   const int tid = threadIdx.x;
   const int tx = tid & (RX - 1), ty = tid / RX;
   const int x0 = blockIdx.x * RX, y0 = blockIdx.y * RY;  // halo'd coords of the tile corner
@@ -233,9 +250,11 @@ __global__ void __launch_bounds__(RX *TY, 2)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int p = kb - 1; p <= min(kb + 2, plast); ++p) issue(p);
   }
-  // coefficient rows of the block's planes
+  // coefficient rows of the block's planes (and, for the bulk mean, dzf/lz)
+  __shared__ float zl[KCHUNK];
   for (int e = tid; e < (ke - kb + 1) * NCOEF; e += blockDim.x)
     reinterpret_cast<float *>(zc)[e] = __ldg(reinterpret_cast<const float *>(coef + kb) + e);
+  if (kMean && tid < ke - kb + 1) zl[tid] = float(__ldg(g.dzflzi + kb + tid));
   __syncthreads();
 
   const float dt = float(sc->dt);
@@ -268,7 +287,7 @@ __global__ void __launch_bounds__(RX *TY, 2)
       }
     }
     __syncthreads();
-    if (!ok_s[par]) return;  // the whole block leaves together
+    if (!ok_s[par]) break;  // the whole block leaves the loop together
     if (act_a) {
       const Coef z = zc[k - kb];
       SmemAcc32 a;
@@ -303,6 +322,17 @@ __global__ void __launch_bounds__(RX *TY, 2)
           vb[d] = (fmaf(dt, fb[d], vb[d]) + bb[d]) * 0.5f;
         }
       }
+      if (kMean) {
+        const float dzl = zl[k - kb];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (bm.forced[d]) {  // uniform
+            // the stored value: w(nz) is the wall value 0
+            const bool wall = (d == 2 && k == g.nz);
+            const float x = wall ? 0.f : va[d] + (act_b ? vb[d] : 0.f);
+            msum[d] = fmaf(x, dzl, msum[d]);
+          }
+      }
       if (FUSE) {
         store_point(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
         store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
@@ -329,6 +359,57 @@ __global__ void __launch_bounds__(RX *TY, 2)
     sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
     c += XY;
   }
+  if constexpr (kMean) {
+    __shared__ float red[RX * TY / 32][3];
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (bm.forced[d]) {  // uniform: only the forced components are reduced
+        float x = msum[d];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) x += __shfl_down_sync(0xffffffffu, x, o2);
+        if (lane == 0) red[wid][d] = x;
+      }
+    __syncthreads();
+    if (tid < 3) {
+      // (a parameter array indexed at run time would be copied to local memory)
+      const int forced = tid == 0 ? bm.forced[0] : (tid == 1 ? bm.forced[1] : bm.forced[2]);
+      double x = 0.0;
+      if (forced)
+        for (int w2 = 0; w2 < RX * TY / 32; ++w2) x += double(red[w2][tid]);
+      const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+      bm.partials[tid * nblocks + blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] =
+          x;
+    }
+  }
+}
+
+// The forcing of the mixed form from the fused RK2's partial sums:
+// sc->mean[d] = sum / (nx*ny), sc->force[d] = vel_force[d] - mean
+// (forceVel, mod_calcVel.cc:280-301).  One block; the partials are added in a
+// fixed order.
+__global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkMean bm,
+                                                     int nblocks) {
+  __shared__ double red[32][3];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double part[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) part[d] += bm.partials[d * nblocks + b];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double x = part[d];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[wid][d] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    double tot = 0.0;
+    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot += red[w2][d];
+    const double mean = tot / g.nx / g.ny;
+    sc->mean[d] = bm.forced[d] ? mean : 0.0;
+    sc->force[d] = bm.forced[d] ? bm.vel_force[d] - mean : 0.0;
+  }
 }
 
 // Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 18
@@ -354,9 +435,21 @@ cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[6], const RkC
   const size_t smem = rk32_smem_bytes(STAGE);
   const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
+  BulkMean bm;
+  for (int d = 0; d < 3; ++d) {
+    bm.forced[d] = c->prm.is_forced[d] ? 1 : 0;
+    bm.vel_force[d] = c->prm.vel_force[d];
+  }
+  bm.partials = c->d_mean_partials;
   k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
       m[0], m[1], m[2], m[3], m[4], m[5], c->geo(), K,
-      reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err);
+      reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err,
+      bm);
+  if constexpr (STAGE == 2 && FUSE) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_bulk_force<<<1, 1024, 0, s>>>(c->geo(), c->d_sc, bm, (int)(grid.x * grid.y * grid.z));
+  }
   return cudaGetLastError();
 }
 
@@ -391,7 +484,14 @@ unsigned convert_blocks(const plc_ctx *c, long long n) {
 
 }  // namespace
 
-// Raises the dynamic shared-memory limit of the FP32 RK kernels (about 50 KB)
+// Blocks of the FP32 RK grid (the number of bulk-mean partials).
+long long rk32_blocks(const plc_ctx *c) {
+  const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
+  return (long long)((c->nx + RX - 1) / RX) * ((c->ny + RY - 1) / RY) *
+         ((c->nz + kchunk - 1) / kchunk);
+}
+
+// Raises the dynamic shared-memory limit of the FP32 RK kernels (up to ~90 KB)
 // on the current device.
 cudaError_t rk32_configure() {
   const int bytes = (int)rk32_smem_bytes(2);

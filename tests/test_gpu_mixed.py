@@ -132,9 +132,8 @@ def test_cfl_controlled_dt():
 
 
 def test_step_graph_kernel_count():
-    """The forward x transform writes the bulk-mean partials, a one-block
-    kernel turns them into the forcing and the correction applies it: no
-    forcing pass over the field."""
+    """RK2 writes the bulk-mean partials, a one-block kernel turns them into
+    the forcing and the correction applies it: no forcing pass over the field."""
     ch = mixed_channel(32, 24, 16)
     ch.initFlow()
     assert ch.kernels_per_step == 9
