@@ -240,6 +240,56 @@ int plc_calc_max_cfl(plc_ctx *ctx, const double *d_u, const double *d_v,
 int plc_calc_max_div(plc_ctx *ctx, const double *d_u, const double *d_v,
                      const double *d_w, plc_value_index *div_max);
 
+/* ---- mod_statistics (src/mod_statistics.hh:8-16) on the context's fields ---- */
+/* Statistic ids of the running sums: cell-centred u (+ u_crf), v, w and their
+ * products, p, p*p; sampled when plc_params.stat_which_var[id] is set. */
+#define PLC_STAT_U 0
+#define PLC_STAT_V 1
+#define PLC_STAT_W 2
+#define PLC_STAT_UU 3
+#define PLC_STAT_VV 4
+#define PLC_STAT_WW 5
+#define PLC_STAT_UV 6
+#define PLC_STAT_UW 7
+#define PLC_STAT_VW 8
+#define PLC_STAT_P 9
+#define PLC_STAT_PP 10
+/* allocStat + initStat (mod_statistics.cc:7-28): zeroed device sums of the
+ * enabled statistics; nts = nt_init_stat+1, nte = nt_init_stat, nspl = 0. */
+int plc_stat_init(plc_ctx *ctx);
+/* freeStat (mod_statistics.cc:15-21). */
+int plc_stat_free(plc_ctx *ctx);
+/* calcStat (mod_statistics.cc:30-106): when (nt - nt_init_stat) is a multiple
+ * of sample_interval, adds one sample of the context's u, v, w, p to the sums
+ * (nte += sample_interval, nspl += 1).  The sums are FP64 in either form. */
+int plc_calc_stat(plc_ctx *ctx, int nt);
+/* stat_info (mod_statistics.hh:8-12). */
+int plc_stat_info(const plc_ctx *ctx, int *nts, int *nte, int *nspl);
+/* A running sum (nx*ny*nz doubles, x fastest, no halos) to / from the host;
+ * the upload also restores the counters (inputStatData, mod_dataIO.cc:232-252). */
+int plc_stat_download(plc_ctx *ctx, int which, double *h_dst);
+int plc_stat_upload(plc_ctx *ctx, int which, const double *h_src, int nts, int nte, int nspl);
+/* Plane averages of every statistic divided by the samples: h_prof[id*nz + k-1]
+ * (0 for statistics not sampled), the mean and second-moment profiles from
+ * which RMS profiles follow.  No counterpart in the reference (its profiles
+ * are post-processed from the stat files). */
+int plc_stat_profiles(plc_ctx *ctx, double *h_prof);
+
+/* ---- mod_monitor (src/mod_monitor.cc:57-205) on the context's fields ---- */
+/* calcAndWriteForcing (:57-75): Mean of each forced component (u + u_crf), 0 else. */
+int plc_monitor_forcing(plc_ctx *ctx, double *vel_mean3);
+/* extractAndWriteProbePoint (:77-91): u + u_crf, v, w, p at the 1-based point. */
+int plc_monitor_probe(plc_ctx *ctx, int ig, int jg, int kg, double *out4);
+/* calcAndWriteSkf (:93-113) at the bottom (wall 0, k = 1) or top (wall 1,
+ * k = nz) wall: tau_w = mean of re_inv*(u + u_crf)/(dzf/2) over the plane
+ * (double-double sum), u_tau = sqrt(tau_w), cf = tau_w/(u_ref^2/2).  With
+ * l_ref = 1 (the half height) Re_tau = u_tau / re_inv. */
+int plc_monitor_skf(plc_ctx *ctx, int wall, double *u_tau, double *cf);
+/* extractRegion (:117-158, :160-205): the box region_ijk = {i0,i1,j0,j1,k0,k1}
+ * (1-based, inclusive, clipped to the domain as initMonitor does) of u, v, w
+ * (centred along their own direction, u + u_crf) or p, into h_dst (x fastest). */
+int plc_extract_region(plc_ctx *ctx, const int *region_ijk, int field, double *h_dst);
+
 /* ---- initial field (mod_initFlow.cc:47-102) on the context's u, v, w ---- */
 /* Followed by transform2CRF and the boundary update, as main.cc:73-82. */
 int plc_init_flow(plc_ctx *ctx);

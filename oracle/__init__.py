@@ -94,6 +94,11 @@ def lib():
             "orc_init_flow": (None, [G, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.c_double, _dp, _dp, _dp, _dp]),
             "orc_step": (None, [G, vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+            "orc_calc_stat_sample": (None, [G, C.c_double, _dp, _dp, _dp, _dp,
+                                            C.POINTER(C.c_void_p)]),
+            "orc_wall_tau": (C.c_double, [G, C.c_int, C.c_double, _dp, C.c_double]),
+            "orc_extract_region": (None, [G, _dp, C.c_int, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), _dp]),
             "orc_set_threads": (None, [C.c_int]),
             "orc_get_threads": (C.c_int, []),
         }
@@ -262,6 +267,25 @@ class Case:
 
     def check_nan(self, var):
         return bool(lib().orc_check_nan(self.gp, var))
+
+    def calc_stat_sample(self, u, v, w, p, sums, u_crf=None):
+        """One calcStat sample into sums: a list of 11 arrays (nz, ny, nx) or None."""
+        ptrs = (C.c_void_p * 11)(*[None if a is None else a.ctypes.data for a in sums])
+        lib().orc_calc_stat_sample(self.gp, self.u_crf if u_crf is None else u_crf,
+                                   u, v, w, p, ptrs)
+
+    def wall_tau(self, vel, k_wall, vel_crf=None):
+        """calcAndWriteSkf's tau_w at k_wall (1 or nz), dz = dzf(k_wall)/2."""
+        dz = 0.5 * self.dzf[k_wall]
+        return lib().orc_wall_tau(self.gp, k_wall, dz, vel,
+                                  self.u_crf if vel_crf is None else vel_crf)
+
+    def extract_region(self, var, offset_dir, reg_st, reg_sz):
+        out = np.zeros((reg_sz[2], reg_sz[1], reg_sz[0]))
+        st = (C.c_int * 3)(*reg_st)
+        sz = (C.c_int * 3)(*reg_sz)
+        lib().orc_extract_region(self.gp, var, offset_dir, st, sz, out)
+        return out
 
     def step(self, u, v, w, u1, v1, w1, p, nsteps=1):
         lib().orc_step(self.gp, self.ps, nsteps, u, v, w, u1, v1, w1, p)

@@ -222,6 +222,66 @@ struct orc_poisson {
 
 extern "C" {
 
+// ---------------------------------------------------------------------------
+// mod_statistics::calcStat, src/mod_statistics.cc:30-106: one sample.  The
+// cell-centred velocities are (q(i-1) + q(i)) * 0.5 (+ u_crf for u) (:44-46);
+// each sum adds the value or the product of two of them (:50-99).
+// ---------------------------------------------------------------------------
+void orc_calc_stat_sample(const orc_grid *g, double u_crf, const double *u, const double *v,
+                          const double *w, const double *p, double *const *sums) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const long X = nx + 2, XY = X * (ny + 2);
+#pragma omp parallel for
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const long c = i + X * j + XY * k;
+        const long o = (i - 1) + (long)nx * ((j - 1) + (long)ny * (k - 1));
+        const double uc = (u[c - 1] + u[c]) * 0.5 + u_crf;
+        const double vc = (v[c - X] + v[c]) * 0.5;
+        const double wc = (w[c - XY] + w[c]) * 0.5;
+        const double pc = p[c];
+        const double val[11] = {uc, vc, wc, uc * uc, vc * vc, wc * wc,
+                                uc * vc, uc * wc, vc * wc, pc, pc * pc};
+        for (int q = 0; q < 11; ++q)
+          if (sums[q]) sums[q][o] += val[q];
+      }
+}
+
+// ---------------------------------------------------------------------------
+// mod_monitor::calcAndWriteSkf, src/mod_monitor.cc:93-113: the plane mean of
+// re_inv * (vel + vel_crf) / dz at k_wall.  The reference's sum runs in
+// (j, i) order with an MPI_Reduce over ranks; here it is double-double, so the
+// rounded total does not depend on the order.
+// ---------------------------------------------------------------------------
+double orc_wall_tau(const orc_grid *g, int k_wall, double dz, const double *vel,
+                    double vel_crf) {
+  const int nx = g->nx, ny = g->ny;
+  const long X = nx + 2, XY = X * (ny + 2);
+  double hi = 0.0, lo = 0.0;
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      two_sum_acc(hi, lo, g->re_inv * (vel[i + X * j + XY * k_wall] + vel_crf) / dz);
+  return (hi + lo) / nx / ny;
+}
+
+// ---------------------------------------------------------------------------
+// mod_monitor::extractRegion, src/mod_monitor.cc:117-158.
+// ---------------------------------------------------------------------------
+void orc_extract_region(const orc_grid *g, const double *var, int offset_dir,
+                        const int *reg_st, const int *reg_sz, double *out) {
+  const long X = g->nx + 2, XY = X * (g->ny + 2);
+  const int is = reg_st[0] - 1, js = reg_st[1] - 1, ks = reg_st[2] - 1;
+  const long d = offset_dir == 1 ? 1 : (offset_dir == 2 ? X : (offset_dir == 3 ? XY : 0));
+  for (int k = 1; k <= reg_sz[2]; ++k)
+    for (int j = 1; j <= reg_sz[1]; ++j)
+      for (int i = 1; i <= reg_sz[0]; ++i) {
+        const long c = (i + is) + X * (j + js) + XY * (k + ks);
+        const long o = (i - 1) + (long)reg_sz[0] * ((j - 1) + (long)reg_sz[1] * (k - 1));
+        out[o] = offset_dir == 0 ? var[c] : 0.5 * (var[c - d] + var[c]);
+      }
+}
+
 void orc_set_threads(int n) {
 #ifdef _OPENMP
   if (n > 0) omp_set_num_threads(n);

@@ -129,6 +129,24 @@ void orc_step(const orc_grid *g, orc_poisson *ps, int nsteps, double *u,
               double *v, double *w, double *u1, double *v1, double *w1,
               double *p);
 
+/* ---- mod_statistics (src/mod_statistics.cc:30-106) ---- */
+/* One sample of calcStat: adds to the enabled running sums (sums[q] != NULL,
+ * nx*ny*nz doubles, x fastest, no halos): q = 0 u, 1 v, 2 w (cell-centred,
+ * u + u_crf), 3 u*u, 4 v*v, 5 w*w, 6 u*v, 7 u*w, 8 v*w, 9 p, 10 p*p. */
+void orc_calc_stat_sample(const orc_grid *g, double u_crf, const double *u, const double *v,
+                          const double *w, const double *p, double *const *sums);
+
+/* ---- mod_monitor (src/mod_monitor.cc:93-113, 117-158) ---- */
+/* calcAndWriteSkf's plane mean: sum over (i,j) of re_inv*(vel(i,j,k_wall)+vel_crf)/dz,
+ * divided by nx and ny (the sum in double-double, i.e. order independent). */
+double orc_wall_tau(const orc_grid *g, int k_wall, double dz, const double *vel,
+                    double vel_crf);
+/* extractRegion: the box of size reg_sz starting at the 1-based interior
+ * index reg_st, staggered -> centred along offset_dir (0 none, 1 x, 2 y,
+ * 3 z); out is reg_sz[0]*reg_sz[1]*reg_sz[2], x fastest. */
+void orc_extract_region(const orc_grid *g, const double *var, int offset_dir,
+                        const int *reg_st, const int *reg_sz, double *out);
+
 void orc_set_threads(int n);
 int orc_get_threads(void);
 

@@ -117,6 +117,17 @@ _SIGS = {
     "plc_calc_max_cfl": [_vp, _dp, _dp, _dp, C.POINTER(PlcValueIndex)],
     "plc_calc_max_div": [_vp, _dp, _dp, _dp, C.POINTER(PlcValueIndex)],
     "plc_init_flow": [_vp],
+    "plc_stat_init": [_vp],
+    "plc_stat_free": [_vp],
+    "plc_calc_stat": [_vp, _int],
+    "plc_stat_info": [_vp, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
+    "plc_stat_download": [_vp, _int, _hp],
+    "plc_stat_upload": [_vp, _int, _hp, _int, _int, _int],
+    "plc_stat_profiles": [_vp, _hp],
+    "plc_monitor_forcing": [_vp, _hp],
+    "plc_monitor_probe": [_vp, _int, _int, _int, _hp],
+    "plc_monitor_skf": [_vp, _int, C.POINTER(_dbl), C.POINTER(_dbl)],
+    "plc_extract_region": [_vp, C.POINTER(_int), _int, _hp],
     "plc_step": [_vp, _int],
     "plc_last_check": [_vp, C.POINTER(_int), C.POINTER(PlcValueIndex), C.POINTER(PlcValueIndex)],
     "plc_check": [_vp, C.POINTER(_int), C.POINTER(PlcValueIndex), C.POINTER(PlcValueIndex)],

@@ -293,6 +293,81 @@ class Channel:
         return _vi(r)
 
     # -- initial field and the fused step -------------------------------------------
+    # -- mod_statistics -----------------------------------------------------------
+    STAT_NAMES = ("u", "v", "w", "u2", "v2", "w2", "uv", "uw", "vw", "p", "p2")
+
+    def initStat(self):
+        """allocStat + initStat: zeroed sums of the statistics enabled by stat_which_var."""
+        self._check(lib().plc_stat_init(self._ctx))
+
+    def freeStat(self):
+        self._check(lib().plc_stat_free(self._ctx))
+
+    def calcStat(self, nt: int):
+        """calcStat: one sample when (nt - nt_init_stat) % sample_interval == 0."""
+        self._check(lib().plc_calc_stat(self._ctx, int(nt)))
+
+    @property
+    def stat_info(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(lib().plc_stat_info(self._ctx, C.byref(a), C.byref(b), C.byref(c)))
+        return {"nts": a.value, "nte": b.value, "nspl": c.value}
+
+    def stat(self, which) -> np.ndarray:
+        """A running sum, (nz, ny, nx)."""
+        q = self.STAT_NAMES.index(which) if isinstance(which, str) else int(which)
+        out = np.empty((self.nz, self.ny, self.nx))
+        self._check(lib().plc_stat_download(self._ctx, q, out.ctypes.data))
+        return out
+
+    def set_stat(self, which, arr, nts: int, nte: int, nspl: int):
+        q = self.STAT_NAMES.index(which) if isinstance(which, str) else int(which)
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != (self.nz, self.ny, self.nx):
+            raise ValueError("statistic arrays are (nz, ny, nx)")
+        self._check(lib().plc_stat_upload(self._ctx, q, a.ctypes.data, nts, nte, nspl))
+
+    def stat_profiles(self) -> dict:
+        """Plane means of each statistic divided by the samples, name -> (nz,)."""
+        out = np.zeros((len(self.STAT_NAMES), self.nz))
+        self._check(lib().plc_stat_profiles(self._ctx, out.ctypes.data))
+        return dict(zip(self.STAT_NAMES, out))
+
+    # -- mod_monitor --------------------------------------------------------------
+    def monitor_forcing(self) -> np.ndarray:
+        out = np.zeros(3)
+        self._check(lib().plc_monitor_forcing(self._ctx, out.ctypes.data))
+        return out
+
+    def monitor_probe(self, ig: int, jg: int, kg: int) -> np.ndarray:
+        """u + u_crf, v, w, p at the 1-based interior point."""
+        out = np.zeros(4)
+        self._check(lib().plc_monitor_probe(self._ctx, ig, jg, kg, out.ctypes.data))
+        return out
+
+    def monitor_skf(self, wall: int = 0):
+        """(u_tau, cf) at the bottom (0) or top (1) wall."""
+        ut, cf = C.c_double(), C.c_double()
+        self._check(lib().plc_monitor_skf(self._ctx, wall, C.byref(ut), C.byref(cf)))
+        return ut.value, cf.value
+
+    def re_tau(self) -> float:
+        """Friction Reynolds number u_tau * h / nu from both walls' u_tau, h = lz/2."""
+        ut = 0.5 * (self.monitor_skf(0)[0] + self.monitor_skf(1)[0])
+        nu = self.params.u_ref * self.params.l_ref / self.params.re  # re_inv
+        return ut * (0.5 * self.params.lz) / nu
+
+    def extract_region(self, region_ijk, field: str = "u") -> np.ndarray:
+        """The box {i0,i1,j0,j1,k0,k1} (1-based, clipped), shape (nk, nj, ni)."""
+        r = [int(x) for x in region_ijk]
+        r[0], r[1] = max(r[0], 1), min(r[1], self.nx)
+        r[2], r[3] = max(r[2], 1), min(r[3], self.ny)
+        r[4], r[5] = max(r[4], 1), min(r[5], self.nz)
+        out = np.zeros((r[5] - r[4] + 1, r[3] - r[2] + 1, r[1] - r[0] + 1))
+        arr = (C.c_int * 6)(*r)
+        self._check(lib().plc_extract_region(self._ctx, arr, FIELDS[field], out.ctypes.data))
+        return out
+
     def initFlow(self):
         self._check(lib().plc_init_flow(self._ctx))
 

@@ -512,6 +512,7 @@ int plc_destroy(plc_ctx *c) {
   if (!c) return PLC_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_poisson(c);  // also releases the captured step
+  plc_stat_free(c);
   for (auto &f : c->d_field) cudaFree(f);
   for (auto &f : c->f_field) cudaFree(f);
   cudaFree(c->d_coef32);

@@ -56,6 +56,10 @@ struct FftPlan {
 // capacity (blocks) of each plane of the reduction partials array
 constexpr int kMaxBlocksReduce = 4096;
 
+// running statistics of mod_statistics (src/mod_statistics.hh:13): u, v, w,
+// u*u, v*v, w*w, u*v, u*w, v*w, p, p*p
+constexpr int kStatVars = 11;
+
 // Mixed form: Thomas systems whose packed x and y indices are both below
 // kLowModes (wavenumbers |m| < kLowModes/2, the Nyquist line of each axis
 // included) sweep in FP64; the others in FP32.
@@ -105,6 +109,10 @@ struct plc_ctx {
   cudaGraphExec_t graph = nullptr;
   int graph_kernels = 0;
   long long nstep = 0;
+  // statistics (plc_stat_init): running sums, nx*ny*nz doubles each
+  double *d_stat[plc::kStatVars] = {nullptr};
+  int stat_nts = 0, stat_nte = 0, stat_nspl = 0;
+  bool stat_ready = false;
   int last_nan_passed = 1;
   plc_value_index last_cfl{0, 1, 1, 1}, last_div{0, 1, 1, 1};
   std::string err;
