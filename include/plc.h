@@ -293,6 +293,11 @@ int plc_extract_region(plc_ctx *ctx, const int *region_ijk, int field, double *h
 /* ---- initial field (mod_initFlow.cc:47-102) on the context's u, v, w ---- */
 /* Followed by transform2CRF and the boundary update, as main.cc:73-82. */
 int plc_init_flow(plc_ctx *ctx);
+/* main.cc:77-82 for fields uploaded by the caller (inputData on restart):
+ * u -= u_crf on the interior with vel_force[0] shifted likewise
+ * (transform2CRF, mod_calcVel.cc:13-25), then the velocity and pressure
+ * boundary update.  Either form. */
+int plc_finish_input(plc_ctx *ctx);
 
 /* ---- fused time step: main.cc:116-154 on the context's fields ---- */
 /* Runs nsteps steps of the plain sequence RK1, RK2, RHS, Poisson, correction,
@@ -310,6 +315,9 @@ int plc_check(plc_ctx *ctx, int *nan_passed, plc_value_index *cfl_max,
               plc_value_index *div_max);
 /* Number of steps taken by plc_step so far. */
 int plc_step_count(plc_ctx *ctx, long long *count);
+/* Sets the step counter (the nt of the last completed step), so that the
+ * checks of a restarted run fall on the multiples of nt_check of nt. */
+int plc_set_step_count(plc_ctx *ctx, long long count);
 /* Number of kernel launches one plc_step step issues (graph nodes). */
 int plc_kernels_per_step(plc_ctx *ctx, int *count);
 /* plc_step(ctx, nsteps) bracketed by CUDA events on the context's stream;
@@ -339,6 +347,68 @@ int plc_mesh_by_func(int mesh_type, int stretch_func, double stretch_ratio, int 
 int plc_trid_tables(int nx, int ny, int nz, double lx, double ly,
                     const double *h_dzf_global, double *h_rpiv, double *h_a,
                     double *h_c);
+/* ---- data I/O: mod_dataIO (src/mod_dataIO.cc), outputMesh
+ * (src/mod_mesh.cc:127-147), mod_monitor files (src/mod_monitor.cc) and the
+ * time-marching driver (src/main.cc:114-222) ----
+ * HDF5 files are written and read without libhdf5 (superblock 2, compact root
+ * group, contiguous little-endian datasets), with the reference's datasets: a
+ * field file holds the [nz][ny][nx] f64 dataset "u", "v", "w" or "p" and a
+ * 1-element int dataset "nt"; a statistics file holds "<type>_stat" with
+ * "nts", "nte", "nspl" (type u v w u2 v2 w2 uv uw vw p p2, PLC_STAT_* order).
+ * Readers accept any file of that shape written by HDF5 1.10+ with the
+ * latest-format property (superblock 2 or 3, compact groups, contiguous data);
+ * others give PLC_ERR_IO. */
+/* The HDF5 subset on plain host arrays (no context, no GPU).
+ * plc_h5_write: nsets datasets in the root group; types[q] 0 = f64, 1 = i32;
+ * dims holds the ndims[q] dimensions of each dataset in turn (slowest first).
+ * plc_h5_read: dataset `name` converted to double into out (capacity
+ * elements; out may be NULL to query the shape); *ndim in: capacity of dims,
+ * out: the rank.  plc_h5_lookup3: the metadata checksum (Jenkins lookup3). */
+int plc_h5_write(const char *path, int nsets, const char *const *names, const int *types,
+                 const int *ndims, const long long *dims, const void *const *data);
+int plc_h5_read(const char *path, const char *name, double *out, size_t capacity,
+                long long *dims, int *ndim);
+unsigned int plc_h5_lookup3(const void *key, size_t length, unsigned int initval);
+/* Directory for the files written by plc_output_mesh / plc_output_init /
+ * plc_output_data / plc_run (default: the working directory). */
+int plc_set_output_dir(plc_ctx *ctx, const char *dir);
+/* outputField (mod_dataIO.cc:86-101) of one field (PLC_U..PLC_P) at path.
+ * u is written as outputData does (:141-147): u_crf added on the device,
+ * downloaded, subtracted again, so the file holds the lab-frame velocity. */
+int plc_write_field_h5(plc_ctx *ctx, const char *path, int field, int nt);
+/* inputField (mod_dataIO.cc:68-84): the dataset named after the field into
+ * the field's interior (halos kept), *nt = the file's "nt".  No frame shift:
+ * call plc_finish_input after reading u, v, w. */
+int plc_read_field_h5(plc_ctx *ctx, const char *path, int field, int *nt);
+/* A statistics file of statistic `which` (outputField / inputField with
+ * stat_info); the read restores nts/nte/nspl, *nte receives nte. */
+int plc_write_stat_h5(plc_ctx *ctx, const char *path, int which);
+int plc_read_stat_h5(plc_ctx *ctx, const char *path, int which, int *nte);
+/* outputMesh: mesh_<nx>-<ny>-<nz>.h5 (xc, yc, zc) and mesh_<nz:05>.out. */
+int plc_output_mesh(plc_ctx *ctx);
+/* Restart (main.cc:59-88): inputData (mod_dataIO.cc:104-128) from
+ * <fn_prefix_input_inst>_{u,v,w}.h5 with the timestamp checks, the frame
+ * shift and boundary update (plc_finish_input), inputStatData (:232-252)
+ * from <fn_prefix_input_stat>_<type>.h5 when nt_in + 1 > nt_init_stat + 1,
+ * and the step counter set to nt_in. */
+int plc_input_data(plc_ctx *ctx, int *nt_in);
+/* initMonitor (mod_monitor.cc:208-310): creates the monitor text files of
+ * the enabled monitors with their headers (truncating, as the reference's
+ * out|ate open does) and clips region_ijk to the domain. */
+int plc_output_init(plc_ctx *ctx);
+/* outputData (mod_dataIO.cc:130-230) after step nt: monitors every
+ * nt_out_moni, inst_<nt:08>_{u,v,w,p}.h5 every nt_out_inst, checkpoints
+ * save_{u,v,w}.h5 (save_<nt:08>_... unless overwrite_save) every nt_out_save,
+ * statistics files, automatic cleanup.  A period of 0 disables its output. */
+int plc_output_data(plc_ctx *ctx, int nt);
+/* freeMonitor: closes the monitor files. */
+int plc_output_free(plc_ctx *ctx);
+/* The main loop of main.cc:114-222 for nt = nt_start..nt_end: steps (graph
+ * replays between the steps that need host work), checks every nt_check,
+ * statistics started at nt_init_stat + 1, the screen line every nt_out_scrn
+ * (verbose != 0) and plc_output_data. */
+int plc_run(plc_ctx *ctx, int nt_start, int verbose);
+
 /* Pinned host memory for fast uploads/downloads. */
 int plc_host_alloc(size_t bytes, void **ptr);
 int plc_host_free(void *ptr);

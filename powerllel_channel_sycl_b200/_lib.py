@@ -117,6 +117,7 @@ _SIGS = {
     "plc_calc_max_cfl": [_vp, _dp, _dp, _dp, C.POINTER(PlcValueIndex)],
     "plc_calc_max_div": [_vp, _dp, _dp, _dp, C.POINTER(PlcValueIndex)],
     "plc_init_flow": [_vp],
+    "plc_finish_input": [_vp],
     "plc_stat_init": [_vp],
     "plc_stat_free": [_vp],
     "plc_calc_stat": [_vp, _int],
@@ -132,6 +133,22 @@ _SIGS = {
     "plc_last_check": [_vp, C.POINTER(_int), C.POINTER(PlcValueIndex), C.POINTER(PlcValueIndex)],
     "plc_check": [_vp, C.POINTER(_int), C.POINTER(PlcValueIndex), C.POINTER(PlcValueIndex)],
     "plc_step_count": [_vp, C.POINTER(C.c_longlong)],
+    "plc_set_step_count": [_vp, C.c_longlong],
+    "plc_h5_write": [C.c_char_p, _int, C.POINTER(C.c_char_p), C.POINTER(_int), C.POINTER(_int),
+                     C.POINTER(C.c_longlong), C.POINTER(_vp)],
+    "plc_h5_read": [C.c_char_p, C.c_char_p, _hp, C.c_size_t, C.POINTER(C.c_longlong),
+                    C.POINTER(_int)],
+    "plc_set_output_dir": [_vp, C.c_char_p],
+    "plc_write_field_h5": [_vp, C.c_char_p, _int, _int],
+    "plc_read_field_h5": [_vp, C.c_char_p, _int, C.POINTER(_int)],
+    "plc_write_stat_h5": [_vp, C.c_char_p, _int],
+    "plc_read_stat_h5": [_vp, C.c_char_p, _int, C.POINTER(_int)],
+    "plc_output_mesh": [_vp],
+    "plc_input_data": [_vp, C.POINTER(_int)],
+    "plc_output_init": [_vp],
+    "plc_output_data": [_vp, _int],
+    "plc_output_free": [_vp],
+    "plc_run": [_vp, _int, _int],
     "plc_kernels_per_step": [_vp, C.POINTER(_int)],
     "plc_get_stream": [_vp, C.POINTER(_vp)],
     "plc_step_timed": [_vp, _int, C.POINTER(_dbl)],
@@ -147,7 +164,7 @@ _SIGS = {
 def exported_symbols():
     """Names of the entry points this binding expects (all declared in plc.h)."""
     return sorted(list(_SIGS) + ["plc_last_error", "plc_step_kernel_name",
-                                 "plc_step_kernel_name_ctx"])
+                                 "plc_step_kernel_name_ctx", "plc_h5_lookup3"])
 
 
 def lib():
@@ -171,6 +188,8 @@ def lib():
         L.plc_step_kernel_name.restype = C.c_char_p
         L.plc_step_kernel_name_ctx.argtypes = [_vp, _int]
         L.plc_step_kernel_name_ctx.restype = C.c_char_p
+        L.plc_h5_lookup3.argtypes = [_vp, C.c_size_t, C.c_uint]
+        L.plc_h5_lookup3.restype = C.c_uint
         _lib = L
         return L
 

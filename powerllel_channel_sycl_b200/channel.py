@@ -30,6 +30,7 @@ Array arguments name a context field ("u", "v", "w", "u1", "v1", "w1", "p",
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Mapping
 
 import numpy as np
@@ -370,6 +371,68 @@ class Channel:
 
     def initFlow(self):
         self._check(lib().plc_init_flow(self._ctx))
+
+    def finish_input(self):
+        """transform2CRF and the boundary update after uploading u, v, w (main.cc:77-82)."""
+        self._check(lib().plc_finish_input(self._ctx))
+
+    @property
+    def step_count(self) -> int:
+        n = C.c_longlong()
+        self._check(lib().plc_step_count(self._ctx, C.byref(n)))
+        return n.value
+
+    @step_count.setter
+    def step_count(self, n: int):
+        self._check(lib().plc_set_step_count(self._ctx, int(n)))
+
+    # ---- data I/O (mod_dataIO, outputMesh, mod_monitor files, main loop) ----
+    def set_output_dir(self, path):
+        self._check(lib().plc_set_output_dir(self._ctx, os.fsencode(str(path))))
+
+    def outputField(self, path, field: str, nt: int):
+        """HDF5 file of one field (u in the lab frame, as outputData writes it)."""
+        self._check(lib().plc_write_field_h5(self._ctx, os.fsencode(str(path)), FIELDS[field], int(nt)))
+
+    def inputField(self, path, field: str) -> int:
+        """Reads a field file into the field's interior; returns its nt."""
+        nt = C.c_int()
+        self._check(lib().plc_read_field_h5(self._ctx, os.fsencode(str(path)), FIELDS[field],
+                                            C.byref(nt)))
+        return nt.value
+
+    def outputStatField(self, path, which):
+        q = self.STAT_NAMES.index(which) if isinstance(which, str) else int(which)
+        self._check(lib().plc_write_stat_h5(self._ctx, os.fsencode(str(path)), q))
+
+    def inputStatField(self, path, which) -> int:
+        """Reads a statistics file (sum and nts/nte/nspl); returns nte."""
+        q = self.STAT_NAMES.index(which) if isinstance(which, str) else int(which)
+        nte = C.c_int()
+        self._check(lib().plc_read_stat_h5(self._ctx, os.fsencode(str(path)), q, C.byref(nte)))
+        return nte.value
+
+    def outputMesh(self):
+        self._check(lib().plc_output_mesh(self._ctx))
+
+    def inputData(self) -> int:
+        """Restart from <fn_prefix_input_inst>_{u,v,w}.h5 (and statistics); returns nt_in."""
+        nt = C.c_int()
+        self._check(lib().plc_input_data(self._ctx, C.byref(nt)))
+        return nt.value
+
+    def initMonitor(self):
+        self._check(lib().plc_output_init(self._ctx))
+
+    def outputData(self, nt: int):
+        self._check(lib().plc_output_data(self._ctx, int(nt)))
+
+    def freeMonitor(self):
+        self._check(lib().plc_output_free(self._ctx))
+
+    def run(self, nt_start: int = 1, verbose: bool = False):
+        """The main loop of main.cc for nt_start..nt_end with checks, statistics and outputs."""
+        self._check(lib().plc_run(self._ctx, int(nt_start), 1 if verbose else 0))
 
     def step(self, nsteps: int = 1):
         self._check(lib().plc_step(self._ctx, int(nsteps)))

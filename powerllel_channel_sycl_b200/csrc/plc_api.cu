@@ -339,6 +339,17 @@ int init_fields(plc_ctx *c, const std::vector<double> &prof, bool is_mean, T *co
 }
 
 }  // namespace
+
+int shift_field(plc_ctx *c, int field, double delta) {
+  if (field < PLC_U || field > PLC_P) return set_error(c, PLC_ERR_ARG, "bad field");
+  if (c->mixed)
+    PLC_CUDA(c, launch_shift(c, c->f_field[field], delta, c->stream));
+  else
+    PLC_CUDA(c, launch_shift(c, c->d_field[field], delta, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
 }  // namespace plc
 
 using namespace plc;
@@ -513,6 +524,7 @@ int plc_destroy(plc_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_poisson(c);  // also releases the captured step
   plc_stat_free(c);
+  io_free(c);
   for (auto &f : c->d_field) cudaFree(f);
   for (auto &f : c->f_field) cudaFree(f);
   cudaFree(c->d_coef32);
@@ -978,6 +990,33 @@ int plc_init_flow(plc_ctx *c) {
   return PLC_OK;
 }
 
+// main.cc:77-82 after fields were uploaded (inputData on restart): u -= u_crf
+// with vel_force[0] shifted likewise, then the velocity and pressure boundary
+// update, in either form.
+int plc_finish_input(plc_ctx *c) {
+  PLC_CHECK_CTX(c);
+  const plc_params &P = c->prm;
+  if (P.u_crf != 0.0) {
+    if (int rc = shift_field(c, PLC_U, P.u_crf)) return rc;
+    c->prm.vel_force[0] -= P.u_crf;
+  }
+  if (c->mixed) {
+    PLC_CUDA(c, launch_bound_vel(c, P.u_crf, c->f_field[PLC_U], c->f_field[PLC_V],
+                                 c->f_field[PLC_W], c->stream));
+    PLC_CUDA(c, launch_bound_p(c, c->f_field[PLC_P], c->stream));
+  } else {
+    PLC_CUDA(c, launch_bound_vel(c, P.u_crf, c->d_field[PLC_U], c->d_field[PLC_V],
+                                 c->d_field[PLC_W], c->stream));
+    PLC_CUDA(c, launch_bound_p(c, c->d_field[PLC_P], c->stream));
+  }
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (c->graph) {  // the graph bakes vel_force in
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return PLC_OK;
+}
+
 // ---- fused time step ------------------------------------------------------
 // nsteps graph launches with the checks of main.cc:156-178 every nt_check
 // steps; the device error word is not read here.
@@ -1050,6 +1089,13 @@ int plc_step_count(plc_ctx *c, long long *count) {
   PLC_CHECK_CTX(c);
   PLC_REQ(c, count);
   *count = c->nstep;
+  return PLC_OK;
+}
+
+int plc_set_step_count(plc_ctx *c, long long count) {
+  PLC_CHECK_CTX(c);
+  if (count < 0) return set_error(c, PLC_ERR_ARG, "negative step count");
+  c->nstep = count;
   return PLC_OK;
 }
 

@@ -65,6 +65,9 @@ constexpr int kStatVars = 11;
 // included) sweep in FP64; the others in FP32.
 constexpr int kLowModes = 16;
 
+// output files and monitor state of the data-I/O entry points (plc_io.cc)
+struct IoState;
+
 }  // namespace plc
 
 struct plc_ctx {
@@ -113,6 +116,7 @@ struct plc_ctx {
   double *d_stat[plc::kStatVars] = {nullptr};
   int stat_nts = 0, stat_nte = 0, stat_nspl = 0;
   bool stat_ready = false;
+  plc::IoState *io = nullptr;  // plc_output_init / plc_set_output_dir
   int last_nan_passed = 1;
   plc_value_index last_cfl{0, 1, 1, 1}, last_div{0, 1, 1, 1};
   std::string err;
@@ -232,5 +236,10 @@ cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);
 // and keeps the fastest (overwrites the spectral array and p)
 cudaError_t fft_autotune(plc_ctx *c);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
+
+// var -= delta on the interior of the context's field (either form), synchronous
+int shift_field(plc_ctx *c, int field, double delta);
+// closes the monitor files and releases the I/O state (plc_io.cc)
+void io_free(plc_ctx *c);
 
 }  // namespace plc
