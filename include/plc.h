@@ -369,6 +369,12 @@ int plc_h5_write(const char *path, int nsets, const char *const *names, const in
 int plc_h5_read(const char *path, const char *name, double *out, size_t capacity,
                 long long *dims, int *ndim);
 unsigned int plc_h5_lookup3(const void *key, size_t length, unsigned int initval);
+/* inputMesh (src/mod_mesh.cc:78-93): nz spacings from a mesh.in text file
+ * into dzf_global[1..nz], with dzf_global[0] and [nz+1] copied from the
+ * neighbours (the dzf_global argument of plc_create when read_mesh = 1). */
+int plc_read_mesh_in(const char *path, int nz, double *dzf_global);
+/* Name of CUDA device `device` (the "Selected device" line of main.cc). */
+int plc_device_name(int device, char *buf, int len);
 /* Directory for the files written by plc_output_mesh / plc_output_init /
  * plc_output_data / plc_run (default: the working directory). */
 int plc_set_output_dir(plc_ctx *ctx, const char *dir);

@@ -138,6 +138,8 @@ _SIGS = {
                      C.POINTER(C.c_longlong), C.POINTER(_vp)],
     "plc_h5_read": [C.c_char_p, C.c_char_p, _hp, C.c_size_t, C.POINTER(C.c_longlong),
                     C.POINTER(_int)],
+    "plc_read_mesh_in": [C.c_char_p, _int, _hp],
+    "plc_device_name": [_int, C.c_char_p, _int],
     "plc_set_output_dir": [_vp, C.c_char_p],
     "plc_write_field_h5": [_vp, C.c_char_p, _int, _int],
     "plc_read_field_h5": [_vp, C.c_char_p, _int, C.POINTER(_int)],

@@ -442,6 +442,35 @@ int plc_h5_read(const char *path, const char *name, double *out, size_t capacity
   return PLC_OK;
 }
 
+int plc_read_mesh_in(const char *path, int nz, double *dzf_global) {
+  if (!path || !dzf_global || nz < 1) return set_error(nullptr, PLC_ERR_ARG, "bad argument");
+  // inputMesh (mod_mesh.cc:78-93): nz whitespace-separated spacings, the
+  // ghost entries copied from their neighbours
+  FILE *f = std::fopen(path, "r");
+  if (!f)
+    return set_error(nullptr, PLC_ERR_IO,
+                     std::string("PowerLLEL.ERROR.inputMesh: File ") + path + " doesn't exist!");
+  for (int k = 1; k <= nz; ++k)
+    if (std::fscanf(f, "%lf", &dzf_global[k]) != 1) {
+      std::fclose(f);
+      return set_error(nullptr, PLC_ERR_IO,
+                       fmt_str("PowerLLEL.ERROR.inputMesh: %s holds fewer than nz = %d values", path, nz));
+    }
+  std::fclose(f);
+  dzf_global[0] = dzf_global[1];
+  dzf_global[nz + 1] = dzf_global[nz];
+  return PLC_OK;
+}
+
+int plc_device_name(int device, char *buf, int len) {
+  if (!buf || len < 1) return set_error(nullptr, PLC_ERR_ARG, "bad argument");
+  cudaDeviceProp prop;
+  const cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return set_error(nullptr, PLC_ERR_CUDA, cudaGetErrorString(e));
+  std::snprintf(buf, (size_t)len, "%s", prop.name);
+  return PLC_OK;
+}
+
 int plc_set_output_dir(plc_ctx *c, const char *dir) {
   if (!c) return set_error(nullptr, PLC_ERR_ARG, "null context");
   io_of(c).dir = dir ? dir : "";
