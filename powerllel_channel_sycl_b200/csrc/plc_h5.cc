@@ -149,6 +149,15 @@ std::vector<uint8_t> root_header(const std::vector<Dataset> &sets,
 }
 
 // ---- reading ----------------------------------------------------------------
+// Object headers of version 1 (the library's default format) and 2, with
+// their continuation blocks; groups of Link messages (compact, version-2
+// superblocks) or of a symbol table (version-1 B-tree of symbol nodes over a
+// local heap, version-0/1 superblocks).
+struct Msg {
+  uint16_t type;
+  size_t at, size;
+};
+
 struct Reader {
   std::vector<uint8_t> f;
   std::string err;
@@ -156,34 +165,153 @@ struct Reader {
     err = m;
     return false;
   }
-  uint64_t le(size_t at, int n) const {
+  bool have(uint64_t at, uint64_t n) const { return at <= f.size() && n <= f.size() - at; }
+  uint64_t le(size_t at, int n) const {  // callers check have(at, n) first
     uint64_t x = 0;
     for (int i = 0; i < n; ++i) x |= uint64_t(f[at + i]) << (8 * i);
     return x;
   }
-  // messages of the version-2 object header at addr: (type, payload offset, size)
-  bool messages(uint64_t addr, std::vector<std::tuple<uint8_t, size_t, size_t>> &out) {
-    if (addr + 8 > f.size() || std::memcmp(&f[addr], "OHDR", 4) != 0)
-      return fail("not a version-2 object header");
-    if (f[addr + 4] != 2) return fail("object header version");
-    const uint8_t flags = f[addr + 5];
-    size_t at = addr + 6;
-    if (flags & 0x20) at += 16;  // times
-    if (flags & 0x10) at += 4;   // attribute phase change values
-    const int width = 1 << (flags & 3);
-    const uint64_t chunk = le(at, width);
-    at += width;
-    const size_t end = at + chunk;
-    if (end + 4 > f.size()) return fail("truncated object header");
-    if (lookup3(&f[addr], end - addr) != uint32_t(le(end, 4))) return fail("object header checksum");
-    const size_t mh = (flags & 0x04) ? 6 : 4;
+
+  // messages of a version-2 block: [at, end) holds messages with mh-byte headers
+  bool v2_block(size_t at, size_t end, size_t mh, std::vector<Msg> &out,
+                std::vector<std::pair<uint64_t, uint64_t>> &cont) {
     while (at + mh <= end) {
-      const uint8_t type = f[at];
+      const uint16_t type = f[at];
       const size_t size = le(at + 1, 2);
       at += mh;
-      if (at + size > end) return fail("message past the header");
-      out.emplace_back(type, at, size);
+      if (at + size > end) return fail("message past the object header");
+      if (type == 0x10) {
+        if (size < 16) return fail("bad continuation message");
+        cont.emplace_back(le(at, 8), le(at + 8, 8));
+      } else {
+        out.push_back({type, at, size});
+      }
       at += size;
+    }
+    return true;
+  }
+
+  bool messages(uint64_t addr, std::vector<Msg> &out) {
+    std::vector<std::pair<uint64_t, uint64_t>> cont;
+    if (have(addr, 16) && std::memcmp(&f[addr], "OHDR", 4) == 0) {
+      if (f[addr + 4] != 2) return fail("object header version");
+      const uint8_t flags = f[addr + 5];
+      size_t at = addr + 6;
+      if (flags & 0x20) at += 16;  // times
+      if (flags & 0x10) at += 4;   // attribute phase change values
+      const int width = 1 << (flags & 3);
+      if (!have(at, width)) return fail("truncated object header");
+      const uint64_t chunk = le(at, width);
+      at += width;
+      if (chunk > f.size() || !have(at, chunk + 4)) return fail("truncated object header");
+      const size_t end = at + chunk;
+      if (lookup3(&f[addr], end - addr) != uint32_t(le(end, 4))) return fail("object header checksum");
+      const size_t mh = (flags & 0x04) ? 6 : 4;
+      if (!v2_block(at, end, mh, out, cont)) return false;
+      for (size_t q = 0; q < cont.size(); ++q) {  // "OCHK" blocks, checksummed
+        const uint64_t b = cont[q].first, n = cont[q].second;
+        if (q > 64 || n < 8 || !have(b, n) || std::memcmp(&f[b], "OCHK", 4) != 0)
+          return fail("bad object header continuation block");
+        if (lookup3(&f[b], n - 4) != uint32_t(le(b + n - 4, 4)))
+          return fail("object header continuation checksum");
+        if (!v2_block(b + 4, b + n - 4, mh, out, cont)) return false;
+      }
+      return true;
+    }
+    // version 1: version, reserved, message count (2), reference count (4),
+    // header size (4), padding to 8 bytes; messages 8-byte aligned with
+    // type (2), size (2), flags (1), reserved (3)
+    if (!have(addr, 16) || f[addr] != 1) return fail("unknown object header");
+    cont.emplace_back(addr + 16, le(addr + 8, 4));
+    for (size_t q = 0; q < cont.size(); ++q) {
+      const uint64_t b = cont[q].first, n = cont[q].second;
+      if (q > 64 || !have(b, n)) return fail("bad object header block");
+      size_t at = b;
+      const size_t end = b + n;
+      while (at + 8 <= end) {
+        const uint16_t type = uint16_t(le(at, 2));
+        const size_t size = le(at + 2, 2);
+        at += 8;
+        if (at + size > end) return fail("message past the object header");
+        if (type == 0x10) {
+          if (size < 16) return fail("bad continuation message");
+          cont.emplace_back(le(at, 8), le(at + 8, 8));
+        } else {
+          out.push_back({type, at, size});
+        }
+        at += size;
+      }
+    }
+    return true;
+  }
+
+  // members of the group whose object header is at addr: name -> header address
+  bool members(uint64_t addr, std::vector<std::pair<std::string, uint64_t>> &out) {
+    std::vector<Msg> msgs;
+    if (!messages(addr, msgs)) return false;
+    for (const Msg &m : msgs) {
+      if (m.type == 0x06) {  // link
+        size_t at = m.at;
+        const size_t end = m.at + m.size;
+        if (m.size < 2 || f[at] != 1) return fail("link message version");
+        const uint8_t flags = f[at + 1];
+        at += 2;
+        uint8_t ltype = 0;
+        if (flags & 0x08) {
+          if (at >= end) return fail("bad link message");
+          ltype = f[at++];
+        }
+        if (flags & 0x04) at += 8;
+        if (flags & 0x10) at += 1;
+        const int lw = 1 << (flags & 3);
+        if (at + lw > end) return fail("bad link message");
+        const size_t nlen = le(at, lw);
+        at += lw;
+        if (at + nlen > end) return fail("bad link message");
+        std::string nm(reinterpret_cast<const char *>(&f[at]), nlen);
+        at += nlen;
+        if (ltype == 0) {
+          if (at + 8 > end) return fail("bad link message");
+          out.emplace_back(nm, le(at, 8));
+        }
+      } else if (m.type == 0x11) {  // symbol table: B-tree and local heap
+        if (m.size < 16) return fail("bad symbol table message");
+        if (!symbols(le(m.at, 8), le(m.at + 8, 8), out)) return false;
+      }
+    }
+    return true;
+  }
+
+  bool symbols(uint64_t btree, uint64_t heap, std::vector<std::pair<std::string, uint64_t>> &out) {
+    if (!have(heap, 32) || std::memcmp(&f[heap], "HEAP", 4) != 0) return fail("bad local heap");
+    const uint64_t seg_size = le(heap + 8, 8), seg = le(heap + 24, 8);
+    if (!have(seg, seg_size)) return fail("bad local heap data segment");
+    std::vector<uint64_t> nodes{btree};
+    for (size_t q = 0; q < nodes.size(); ++q) {
+      const uint64_t n = nodes[q];
+      if (q > 100000 || !have(n, 24) || std::memcmp(&f[n], "TREE", 4) != 0 || f[n + 4] != 0)
+        return fail("bad group B-tree node");
+      const int level = f[n + 5];
+      const size_t used = le(n + 6, 2);
+      // key 0 (8), child 0 (8), key 1, child 1, ..., key used
+      if (!have(n + 24, 16 * used + 8)) return fail("truncated group B-tree node");
+      for (size_t i = 0; i < used; ++i) {
+        const uint64_t child = le(n + 24 + 8 + 16 * i, 8);
+        if (level > 0) {
+          nodes.push_back(child);
+          continue;
+        }
+        if (!have(child, 8) || std::memcmp(&f[child], "SNOD", 4) != 0) return fail("bad symbol node");
+        const size_t nsym = le(child + 6, 2);
+        if (!have(child + 8, 40 * nsym)) return fail("truncated symbol node");
+        for (size_t e = 0; e < nsym; ++e) {
+          const size_t ent = child + 8 + 40 * e;
+          const uint64_t name_off = le(ent, 8);
+          if (name_off >= seg_size) return fail("symbol name outside the local heap");
+          const char *p = reinterpret_cast<const char *>(&f[seg + name_off]);
+          out.emplace_back(std::string(p, strnlen(p, seg_size - name_off)), le(ent + 8, 8));
+        }
+      }
     }
     return true;
   }
@@ -310,54 +438,61 @@ bool read_dataset(const std::string &path, const std::string &name, std::vector<
   };
   if (!got || r.f.size() < 48 || std::memcmp(r.f.data(), kSignature, 8) != 0)
     return fail("not an HDF5 file");
+  // superblock: the root group's object header
   const uint8_t ver = r.f[8];
-  if (ver != 2 && ver != 3) return fail("superblock version " + std::to_string(ver) + " not supported");
-  if (r.f[9] != 8 || r.f[10] != 8) return fail("offset/length sizes other than 8");
-  if (lookup3(r.f.data(), 44) != uint32_t(r.le(44, 4))) return fail("superblock checksum");
-  const uint64_t root = r.le(36, 8);
-  std::vector<std::tuple<uint8_t, size_t, size_t>> msgs;
-  if (!r.messages(root, msgs)) return fail(r.err);
-  uint64_t addr = kUndef;
-  for (auto &m : msgs) {
-    if (std::get<0>(m) != kMsgLink) continue;
-    size_t at = std::get<1>(m);
-    const uint8_t flags = r.f[at + 1];
-    at += 2;
-    uint8_t ltype = 0;
-    if (flags & 0x08) ltype = r.f[at++];
-    if (flags & 0x04) at += 8;
-    if (flags & 0x10) at += 1;
-    const int lw = 1 << (flags & 3);
-    const size_t nlen = r.le(at, lw);
-    at += lw;
-    const std::string nm(reinterpret_cast<const char *>(&r.f[at]), nlen);
-    at += nlen;
-    if (ltype == 0 && nm == name) addr = r.le(at, 8);
+  uint64_t root = kUndef;
+  if (ver == 2 || ver == 3) {
+    if (r.f[9] != 8 || r.f[10] != 8) return fail("offset/length sizes other than 8");
+    if (lookup3(r.f.data(), 44) != uint32_t(r.le(44, 4))) return fail("superblock checksum");
+    root = r.le(36, 8);
+  } else if (ver == 0 || ver == 1) {
+    if (r.f[13] != 8 || r.f[14] != 8) return fail("offset/length sizes other than 8");
+    // base, free-space, end-of-file and driver addresses, then the root
+    // group's symbol table entry (link name offset, object header address)
+    const size_t entry = ver == 0 ? 56 : 60;
+    if (!r.have(entry, 40)) return fail("truncated superblock");
+    if (r.le(entry - 32, 8) != 0) return fail("base address other than 0");
+    root = r.le(entry + 8, 8);
+  } else {
+    return fail("superblock version " + std::to_string(ver) + " not supported");
   }
+  std::vector<std::pair<std::string, uint64_t>> links;
+  if (!r.members(root, links)) return fail(r.err);
+  uint64_t addr = kUndef;
+  for (auto &l : links)
+    if (l.first == name) addr = l.second;
   if (addr == kUndef) return fail("no dataset '" + name + "' in the root group");
-  msgs.clear();
+  std::vector<Msg> msgs;
   if (!r.messages(addr, msgs)) return fail(r.err);
   int cls = -1;
   size_t esize = 0;
+  bool is_signed = true;
   uint64_t daddr = kUndef, dsize = 0;
+  bool have_space = false;
   dims.clear();
-  for (auto &m : msgs) {
-    const size_t at = std::get<1>(m);
-    switch (std::get<0>(m)) {
+  for (const Msg &m : msgs) {
+    const size_t at = m.at;
+    switch (m.type) {
       case kMsgDataspace: {
-        const int v = r.f[at], nd = r.f[at + 1], fl = r.f[at + 2];
+        if (m.size < 4) return fail("bad dataspace message");
+        const int v = r.f[at], nd = r.f[at + 1];
         const size_t d0 = (v == 1) ? at + 8 : at + 4;
-        (void)fl;
+        if (v == 2 && r.f[at + 3] == 2) return fail("null dataspace");
+        if (d0 + 8 * size_t(nd) > at + m.size) return fail("bad dataspace message");
         for (int i = 0; i < nd; ++i) dims.push_back(r.le(d0 + 8 * i, 8));
+        have_space = true;
         break;
       }
       case kMsgDatatype:
+        if (m.size < 8) return fail("bad datatype message");
         cls = r.f[at] & 0x0f;
         esize = r.le(at + 4, 4);
         if (r.f[at + 1] & 0x01) return fail("big-endian data not supported");
+        is_signed = (r.f[at + 1] & 0x08) != 0;
         break;
       case kMsgLayout:
-        if (r.f[at] != 3 || r.f[at + 1] != 1) return fail("only contiguous layouts are supported");
+        if (m.size < 18 || r.f[at] != 3 || r.f[at + 1] != 1)
+          return fail("only contiguous layouts are supported");
         daddr = r.le(at + 2, 8);
         dsize = r.le(at + 10, 8);
         break;
@@ -365,8 +500,18 @@ bool read_dataset(const std::string &path, const std::string &name, std::vector<
         break;
     }
   }
-  const uint64_t n = elements(dims);
-  if (daddr == kUndef || dsize != n * esize || daddr + dsize > r.f.size())
+  if (!have_space) return fail("dataset '" + name + "' has no dataspace");
+  uint64_t n = 1;
+  for (uint64_t d : dims) {
+    if (d != 0 && n > r.f.size() / d) return fail("dataset '" + name + "' larger than the file");
+    n *= d;
+  }
+  if (n == 0) {
+    out.clear();
+    return true;
+  }
+  if (daddr == kUndef) return fail("dataset '" + name + "' has no data written");
+  if (esize == 0 || esize > 8 || dsize != n * esize || !r.have(daddr, dsize))
     return fail("dataset '" + name + "' has no readable contiguous data");
   out.resize(n);
   const uint8_t *p = &r.f[daddr];
@@ -380,11 +525,11 @@ bool read_dataset(const std::string &path, const std::string &name, std::vector<
     } else if (cls == 0 && esize == 4) {
       int32_t x;
       std::memcpy(&x, p + 4 * i, 4);
-      out[i] = x;
+      out[i] = is_signed ? double(x) : double(uint32_t(x));
     } else if (cls == 0 && esize == 8) {
       int64_t x;
       std::memcpy(&x, p + 8 * i, 8);
-      out[i] = double(x);
+      out[i] = is_signed ? double(x) : double(uint64_t(x));
     } else {
       return fail("datatype not supported");
     }

@@ -206,3 +206,148 @@ def test_c_reader_optional_fields(tmp_path, times, order, v1):
     rc, back = read(p, "u")
     assert rc == 0, back
     assert np.array_equal(back, arr)
+
+
+# ---- the library's default format: superblock 0, symbol-table groups ---------
+UNDEF = 0xFFFFFFFFFFFFFFFF
+
+
+def _pad8(b):
+    return b + b"\0" * (-len(b) % 8)
+
+
+def _v1_msg(mtype, payload):
+    payload = _pad8(payload)
+    return struct.pack("<HHB3x", mtype, len(payload), 0) + payload
+
+
+def _v1_header(msgs_bytes, nmsgs):
+    return struct.pack("<BBHII4x", 1, 0, nmsgs, 1, len(msgs_bytes)) + msgs_bytes
+
+
+def _entry(name_off, addr, cache=0, scratch=b"\0" * 16):
+    return struct.pack("<QQI4x", name_off, addr, cache) + scratch
+
+
+def build_v0_file(path, sets, superblock=0, two_level=False):
+    """A file in the layout an HDF5 library writes with default properties:
+    superblock 0 (or 1), version-1 object headers, the root group as a symbol
+    table (local heap, version-1 B-tree, symbol nodes), dataspace version 1,
+    fill value version 2, and the layout message in a continuation block."""
+    buf = bytearray()
+
+    def alloc(n):
+        a = len(buf)
+        buf.extend(b"\0" * n)
+        return a
+
+    sb_len = (56 if superblock == 0 else 60) + 40
+    alloc(sb_len)
+    names = sorted(s[0] for s in sets)
+    # local heap: "" at 0, then each name, 8-byte aligned
+    heap_data = bytearray(b"\0" * 8)
+    offs = {}
+    for n in names:
+        offs[n] = len(heap_data)
+        heap_data += _pad8(n.encode() + b"\0")
+    heap_seg = alloc(len(heap_data))
+    buf[heap_seg:heap_seg + len(heap_data)] = heap_data
+    heap = alloc(32)
+    buf[heap:heap + 32] = b"HEAP" + bytes([0, 0, 0, 0]) + struct.pack("<QQQ", len(heap_data), UNDEF, heap_seg)
+    # datasets
+    hdr_addr = {}
+    for name, arr in sets:
+        arr = np.ascontiguousarray(arr)
+        data = alloc(arr.nbytes)
+        buf[data:data + arr.nbytes] = arr.tobytes()
+        ds = bytes([1, arr.ndim, 0, 0, 0, 0, 0, 0]) + b"".join(struct.pack("<Q", d) for d in arr.shape)
+        if arr.dtype == np.float64:
+            dt = bytes([0x11, 0x20, 63, 0]) + struct.pack("<I", 8) + struct.pack("<HHBBBBI", 0, 64, 52, 11, 0, 52, 1023)
+        else:
+            dt = bytes([0x10, 0x08, 0, 0]) + struct.pack("<I", 4) + struct.pack("<HH", 0, 32)
+        fill = bytes([2, 1, 2, 0])
+        lay = bytes([3, 1]) + struct.pack("<QQ", data, arr.nbytes)
+        cont_block = _v1_msg(0x08, lay)
+        cont = alloc(len(cont_block))
+        buf[cont:cont + len(cont_block)] = cont_block
+        msgs = (_v1_msg(0x01, ds) + _v1_msg(0x03, dt) + _v1_msg(0x05, fill)
+                + _v1_msg(0x10, struct.pack("<QQ", cont, len(cont_block))))
+        h = _v1_header(msgs, 5)
+        a = alloc(len(h))
+        buf[a:a + len(h)] = h
+        hdr_addr[name] = a
+    # symbol nodes (one per name in the two-level case) and B-tree nodes
+    def snod(group):
+        body = b"SNOD" + bytes([1, 0]) + struct.pack("<H", len(group))
+        body += b"".join(_entry(offs[n], hdr_addr[n]) for n in group)
+        body += b"\0" * (40 * (8 - len(group)))  # unused entries of a node of 2K = 8
+        a = alloc(len(body))
+        buf[a:a + len(body)] = body
+        return a
+
+    def tree(level, keys, children):
+        body = b"TREE" + bytes([0, level]) + struct.pack("<HQQ", len(children), UNDEF, UNDEF)
+        for k, c in zip(keys, children):
+            body += struct.pack("<QQ", k, c)
+        body += struct.pack("<Q", keys[-1])
+        a = alloc(len(body))
+        buf[a:a + len(body)] = body
+        return a
+
+    if two_level:
+        leaves = [tree(0, [0, offs[n]], [snod([n])]) for n in names]
+        root_tree = tree(1, [0] + [offs[n] for n in names], leaves)
+    else:
+        root_tree = tree(0, [0, offs[names[-1]]], [snod(names)])
+    rh = _v1_header(_v1_msg(0x11, struct.pack("<QQ", root_tree, heap)), 1)
+    root = alloc(len(rh))
+    buf[root:root + len(rh)] = rh
+    sb = SIGNATURE + bytes([superblock, 0, 0, 0, 0, 8, 8, 0]) + struct.pack("<HHI", 4, 16, 0)
+    if superblock == 1:
+        sb += struct.pack("<HH", 32, 0)
+    sb += struct.pack("<QQQQ", 0, UNDEF, len(buf), UNDEF)
+    sb += _entry(0, root, 1, struct.pack("<QQ", root_tree, heap))
+    assert len(sb) == sb_len
+    buf[0:sb_len] = sb
+    path.write_bytes(bytes(buf))
+
+
+@pytest.mark.parametrize("superblock,two_level", [(0, False), (1, False), (0, True)])
+def test_c_reader_default_library_format(tmp_path, superblock, two_level):
+    """A checkpoint in the format the reference's libhdf5 writes by default."""
+    u = np.random.default_rng(2).standard_normal((4, 3, 5))
+    p = tmp_path / "save_u.h5"
+    build_v0_file(p, [("nt", np.array([1234], np.int32)), ("u", u)], superblock, two_level)
+    rc, back = read(p, "u")
+    assert rc == 0, back
+    assert np.array_equal(back, u)
+    rc, back = read(p, "nt")
+    assert rc == 0 and back.tolist() == [1234.0]
+    rc, msg = read(p, "v")
+    assert rc == -6 and "no dataset 'v'" in msg
+
+
+@pytest.mark.parametrize("fmt", ["latest", "default"])
+def test_c_reader_survives_damaged_files(tmp_path, fmt):
+    """Truncated or corrupted files give PLC_ERR_IO (or, where the damage is
+    harmless, the data), never a crash or an out-of-file read."""
+    u = np.arange(24, dtype=np.float64).reshape(2, 3, 4)
+    p = tmp_path / "ok.h5"
+    if fmt == "latest":
+        write(p, [("nt", np.array([7], np.int32)), ("u", u)])
+    else:
+        build_v0_file(p, [("nt", np.array([7], np.int32)), ("u", u)])
+    good = p.read_bytes()
+    rng = np.random.default_rng(11)
+    q = tmp_path / "bad.h5"
+    cases = [good[:n] for n in rng.integers(0, len(good), 40)]
+    for _ in range(300):
+        b = bytearray(good)
+        for pos in rng.integers(0, len(good), rng.integers(1, 4)):
+            b[pos] = int(rng.integers(0, 256))
+        cases.append(bytes(b))
+    for data in cases:
+        q.write_bytes(data)
+        for name in ("u", "nt"):
+            rc, _ = read(q, name)
+            assert rc in (0, -6)
