@@ -9,7 +9,10 @@ CFL-controlled dt with CFL 0.5), FP64, seeded laminar + noise initial field
 generated on the device.  Every field (613 MB) is larger than the 126 MB L2,
 so no L2 flush is needed between steps.  The line's "mixed" object reports
 the mixed-precision form on the same workload (FP32 fields) with its
-speed-up over the FP64 form and its 10-step error against it.
+speed-up over the FP64 form and its 10-step error against it; its
+"ensemble" object a batch of 16 uneven channels (64x48x48 to 256x192x128,
+mixed form) stepped as one graph launch per ensemble step, split over the
+GPUs by the cost model when N > 1.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -382,6 +385,63 @@ def workload_config(args, wl):
             if wl["nx"] * wl["ny"] * wl["nz"] > 20_000_000 else "working set partly L2-resident"}
 
 
+def ensemble_members(seed=3, n=16):
+    """16 uneven channels: grids between 64x48x48 and 256x192x128 (2^a 3^b),
+    Re_tau ~ U[120, 400] (re = (Re_tau / 0.09)^(1/0.88) / 2), independent
+    seeds, mixed precision, CFL-controlled dt."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nx = int(rng.choice([64, 96, 128, 192, 256]))
+        ny = int(rng.choice([48, 64, 96, 128, 192]))
+        nz = int(rng.choice([48, 64, 96, 128]))
+        re_tau = float(rng.uniform(120.0, 400.0))
+        out.append(dict(nx=nx, ny=ny, nz=nz, lx=4 * math.pi, ly=2 * math.pi, lz=2.0,
+                        stretch_ratio=1.5, re=0.5 * (re_tau / 0.09) ** (1 / 0.88), dt=1e-4,
+                        cfl_target=0.5, re_tau=re_tau))
+    return out
+
+
+def run_ensemble(args, world, rank, local, pg):
+    """Batched ensemble: this rank's share of the 16 channels (placed by the
+    cost model) stepped as one graph launch per ensemble step."""
+    import torch
+    from powerllel_channel_sycl_b200 import Ensemble
+    from powerllel_channel_sycl_b200.ensemble import members_of_rank
+
+    specs = ensemble_members()
+    costs = [float(s["nx"] * s["ny"] * s["nz"]) for s in specs]
+    mine = members_of_rank(costs, rank, world)
+    prms = [channel_params(specs[i], args.nt_check, precision="mixed") for i in mine]
+    ens = Ensemble(prms, device=local)
+    ens.initFlow()
+    tune = ens.autotune(steps=5)
+    ens.step(args.warmup)
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    ms = ens.step_timed(args.steps)
+    torch.cuda.synchronize(local)
+    barrier(pg, local)
+    ms_max = max_over_ranks(ms, pg, local)
+    total_pts = sum(costs)
+    value = total_pts * args.steps / (ms_max / 1e3)
+    sched, groups, budgets = ens.schedule()
+    seq = tune.get("sequential")
+    mine_pts = sum(costs[i] for i in mine)
+    out = {
+        "value": value, "unit": "grid-pt*step/s", "ms_per_step": ms_max / args.steps,
+        "members": len(specs), "members_this_rank": len(mine), "points": int(total_pts),
+        "grids": [f"{s['nx']}x{s['ny']}x{s['nz']}" for s in specs],
+        "dtype": "f32 fields (mixed form)", "scaling": "strong",
+        "schedule": sched, "sm_budgets": budgets, "groups": groups,
+        "autotune_ms_per_step": tune,
+        "speedup_vs_sequential": (seq / (ms / args.steps)) if seq else None,
+        "sequential_value_this_rank": (mine_pts / (seq / 1e3)) if seq else None,
+    }
+    ens.close()
+    return out
+
+
 def run_ours(args, wl, rank, world, local, pg):
     import torch  # noqa: F401  (device init; the library owns its stream)
     from powerllel_channel_sycl_b200 import Channel
@@ -480,6 +540,10 @@ def run_ours(args, wl, rank, world, local, pg):
     if not args.no_mixed:
         line["mixed"] = run_mixed(args, wl, world, local, pg, ms_max)
         line["gpu_launches"] += args.steps * len(MIXED_BYTES_PER_POINT)
+    if not args.no_ensemble:
+        ens = run_ensemble(args, world, rank, local, pg)
+        line["ensemble"] = ens
+        line["gpu_launches"] += args.steps * ens["members_this_rank"] * len(MIXED_BYTES_PER_POINT)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, nsteps, threads = cpu_oracle_rate(wl, budget_s=args.cpu_budget, max_steps=1,
                                                 warmup=0)
@@ -503,6 +567,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision measurement")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the 16-channel ensemble measurement")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -415,6 +415,53 @@ int plc_output_free(plc_ctx *ctx);
  * (verbose != 0) and plc_output_data. */
 int plc_run(plc_ctx *ctx, int nt_start, int verbose);
 
+/* ---- SM budget of a context ----
+ * The persistent kernels of the step size their grids to the context's SM
+ * budget (default: all SMs of the device).  A smaller budget lets several
+ * contexts' steps run side by side; results do not depend on it.  Rebuilds
+ * the captured step. */
+int plc_set_sm_budget(plc_ctx *ctx, int sms);
+int plc_get_sm_budget(const plc_ctx *ctx, int *sms);
+
+/* ---- batched ensembles of independent channels (no reference counterpart) ----
+ * n member contexts with their own parameters (any grid, Re, dt, precision)
+ * on one device; one ensemble step is one CUDA graph launch whose branches
+ * are the members' fused steps.  Checks, CFL-controlled dt and error words
+ * stay per member (as plc_step); plc_ensemble_member gives a member's context
+ * for every other entry point (upload, download, statistics, I/O). */
+typedef struct plc_ensemble plc_ensemble;
+#define PLC_ENS_CONCURRENT 0   /* all members at once, full SM budgets */
+#define PLC_ENS_PROPORTIONAL 1 /* all at once, SMs shared in proportion to cost */
+#define PLC_ENS_TWO_GROUPS 2   /* two cost-balanced groups one after the other */
+#define PLC_ENS_SEQUENTIAL 3   /* one member after another */
+#define PLC_ENS_NUM_SCHEDULES 4
+/* dzf_globals: NULL, or n pointers (each NULL or nz+2 spacings, as plc_create). */
+int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_globals,
+                        int device, plc_ensemble **out);
+int plc_ensemble_destroy(plc_ensemble *ens);
+const char *plc_ensemble_last_error(const plc_ensemble *ens);
+int plc_ensemble_size(const plc_ensemble *ens, int *n);
+int plc_ensemble_member(plc_ensemble *ens, int i, plc_ctx **ctx);
+/* plc_init_flow on every member. */
+int plc_ensemble_init_flow(plc_ensemble *ens);
+/* nsteps ensemble steps; every member advances nsteps steps. */
+int plc_ensemble_step(plc_ensemble *ens, int nsteps);
+/* The same bracketed by CUDA events on the ensemble's stream: *ms = device time. */
+int plc_ensemble_step_timed(plc_ensemble *ens, int nsteps, double *ms);
+/* A schedule PLC_ENS_*: member groups and SM budgets from the cost model
+ * (grid points until plc_ensemble_autotune has measured each member). */
+int plc_ensemble_set_schedule(plc_ensemble *ens, int scheme);
+/* The schedule in use; groups and sm_budgets (n entries each) may be NULL. */
+int plc_ensemble_schedule(const plc_ensemble *ens, int *scheme, int *groups, int *sm_budgets);
+/* Autotuner: times each member alone (the cost model), then every schedule
+ * over `steps` ensemble steps, keeps the fastest and restores the members'
+ * u, v, w, p (step counters and dt are untouched).  ms_per_scheme
+ * (PLC_ENS_NUM_SCHEDULES entries, -1 = not applicable) may be NULL. */
+int plc_ensemble_autotune(plc_ensemble *ens, int steps, float *ms_per_scheme);
+/* Multi-GPU placement of members: longest-processing-time-first over the
+ * given costs; gpu_of[i] in [0, n_gpus).  Host only. */
+int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of);
+
 /* Pinned host memory for fast uploads/downloads. */
 int plc_host_alloc(size_t bytes, void **ptr);
 int plc_host_free(void *ptr);

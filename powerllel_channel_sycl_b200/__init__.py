@@ -6,6 +6,7 @@ module interface over that ABI (see :mod:`.channel`).
 """
 from ._lib import FIELDS, PlcError, PlcParams, lib  # noqa: F401
 from .channel import Channel, get_eigen_values, make_params, read_param_json  # noqa: F401
+from .ensemble import Ensemble, partition  # noqa: F401
 
-__all__ = ["Channel", "PlcError", "PlcParams", "make_params", "read_param_json",
-           "get_eigen_values", "lib", "FIELDS"]
+__all__ = ["Channel", "Ensemble", "PlcError", "PlcParams", "make_params", "read_param_json",
+           "get_eigen_values", "lib", "FIELDS", "partition"]

@@ -140,6 +140,19 @@ _SIGS = {
                     C.POINTER(_int)],
     "plc_read_mesh_in": [C.c_char_p, _int, _hp],
     "plc_device_name": [_int, C.c_char_p, _int],
+    "plc_set_sm_budget": [_vp, _int],
+    "plc_get_sm_budget": [_vp, C.POINTER(_int)],
+    "plc_ensemble_create": [_int, C.POINTER(PlcParams), C.POINTER(_vp), _int, C.POINTER(_vp)],
+    "plc_ensemble_destroy": [_vp],
+    "plc_ensemble_size": [_vp, C.POINTER(_int)],
+    "plc_ensemble_member": [_vp, _int, C.POINTER(_vp)],
+    "plc_ensemble_init_flow": [_vp],
+    "plc_ensemble_step": [_vp, _int],
+    "plc_ensemble_step_timed": [_vp, _int, C.POINTER(_dbl)],
+    "plc_ensemble_set_schedule": [_vp, _int],
+    "plc_ensemble_schedule": [_vp, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
+    "plc_ensemble_autotune": [_vp, _int, C.POINTER(C.c_float)],
+    "plc_ensemble_partition": [_int, C.POINTER(_dbl), _int, C.POINTER(_int)],
     "plc_set_output_dir": [_vp, C.c_char_p],
     "plc_write_field_h5": [_vp, C.c_char_p, _int, _int],
     "plc_read_field_h5": [_vp, C.c_char_p, _int, C.POINTER(_int)],
@@ -166,7 +179,8 @@ _SIGS = {
 def exported_symbols():
     """Names of the entry points this binding expects (all declared in plc.h)."""
     return sorted(list(_SIGS) + ["plc_last_error", "plc_step_kernel_name",
-                                 "plc_step_kernel_name_ctx", "plc_h5_lookup3"])
+                                 "plc_step_kernel_name_ctx", "plc_h5_lookup3",
+                                 "plc_ensemble_last_error"])
 
 
 def lib():
@@ -190,6 +204,8 @@ def lib():
         L.plc_step_kernel_name.restype = C.c_char_p
         L.plc_step_kernel_name_ctx.argtypes = [_vp, _int]
         L.plc_step_kernel_name_ctx.restype = C.c_char_p
+        L.plc_ensemble_last_error.argtypes = [_vp]
+        L.plc_ensemble_last_error.restype = C.c_char_p
         L.plc_h5_lookup3.argtypes = [_vp, C.c_size_t, C.c_uint]
         L.plc_h5_lookup3.restype = C.c_uint
         _lib = L

@@ -103,8 +103,23 @@ class Channel:
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
         self.mixed = params.precision == PRECISION["mixed"]
 
+    @classmethod
+    def _wrap(cls, ctx, params: PlcParams, owner):
+        """A view of a context owned elsewhere (an ensemble member)."""
+        self = cls.__new__(cls)
+        self.params = params
+        self._dzf = None
+        self._ctx = ctx
+        self._owner = owner  # keeps the owner alive; close() does not destroy
+        self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
+        self.mixed = params.precision == PRECISION["mixed"]
+        return self
+
     # -- lifetime ---------------------------------------------------------------
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._ctx = None
+            return
         if getattr(self, "_ctx", None):
             lib().plc_destroy(self._ctx)
             self._ctx = None
@@ -385,6 +400,16 @@ class Channel:
     @step_count.setter
     def step_count(self, n: int):
         self._check(lib().plc_set_step_count(self._ctx, int(n)))
+
+    @property
+    def sm_budget(self) -> int:
+        n = C.c_int()
+        self._check(lib().plc_get_sm_budget(self._ctx, C.byref(n)))
+        return n.value
+
+    @sm_budget.setter
+    def sm_budget(self, sms: int):
+        self._check(lib().plc_set_sm_budget(self._ctx, int(sms)))
 
     # ---- data I/O (mod_dataIO, outputMesh, mod_monitor files, main loop) ----
     def set_output_dir(self, path):

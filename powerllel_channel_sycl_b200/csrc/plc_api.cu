@@ -81,11 +81,8 @@ int upload_step_consts(plc_ctx *c, double dt) {
 
 void free_poisson(plc_ctx *c) {
   // the captured step holds the solver's tables and tile sizes
-  if (c->graph) {
-    cudaStreamSynchronize(c->stream);
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  if (c->graph) cudaStreamSynchronize(c->stream);
+  drop_graph(c);
   cudaFree(c->d_rpiv);
   cudaFree(c->d_ac);
   cudaFree(c->d_low);
@@ -340,6 +337,22 @@ int init_fields(plc_ctx *c, const std::vector<double> &prof, bool is_mean, T *co
 
 }  // namespace
 
+int capture_step(plc_ctx *c, cudaStream_t s) { return enqueue_step(c, s); }
+
+int step_graph(plc_ctx *c, cudaGraphExec_t *g) {
+  if (int rc = build_graph(c)) return rc;
+  *g = c->graph;
+  return PLC_OK;
+}
+
+void drop_graph(plc_ctx *c) {
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  ++c->graph_epoch;
+}
+
 int shift_field(plc_ctx *c, int field, double delta) {
   if (field < PLC_U || field > PLC_P) return set_error(c, PLC_ERR_ARG, "bad field");
   if (c->mixed)
@@ -508,6 +521,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   if ((e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) !=
       cudaSuccess)
     return fail(cuda_status(c, e, "cudaDeviceGetAttribute"));
+  c->device_sms = c->num_sms;
   if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
   if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
   // the fields hold zeros: time the transforms' tile sizes on them
@@ -805,10 +819,6 @@ int plc_free_poisson_solver(plc_ctx *c) {
   PLC_CHECK_CTX(c);
   PLC_CUDA(c, cudaStreamSynchronize(c->stream));
   free_poisson(c);
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
   return PLC_OK;
 }
 
@@ -983,10 +993,7 @@ int plc_init_flow(plc_ctx *c) {
                           : init_fields(c, prof, is_mean, c->d_field);
   if (rc != PLC_OK) return rc;
   // the graph bakes the forcing configuration in: rebuild it on the next step
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  drop_graph(c);
   return PLC_OK;
 }
 
@@ -1010,21 +1017,16 @@ int plc_finish_input(plc_ctx *c) {
     PLC_CUDA(c, launch_bound_p(c, c->d_field[PLC_P], c->stream));
   }
   PLC_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (c->graph) {  // the graph bakes vel_force in
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  drop_graph(c);  // the graph bakes vel_force in
   return PLC_OK;
 }
 
 // ---- fused time step ------------------------------------------------------
-// nsteps graph launches with the checks of main.cc:156-178 every nt_check
-// steps; the device error word is not read here.
-static int step_launches(plc_ctx *c, int nsteps) {
-  PLC_CHECK_CTX(c);
-  if (nsteps < 0) return set_error(c, PLC_ERR_ARG, "nsteps < 0");
-  PLC_NEED_POISSON(c);
-  if (int rc = build_graph(c)) return rc;
+}  // extern "C"
+
+namespace plc {
+
+int pre_steps(plc_ctx *c) {
   const plc_params &P = c->prm;
   if (P.cfl_target > 0.0 && c->nstep == 0) {
     int passed;
@@ -1033,49 +1035,77 @@ static int step_launches(plc_ctx *c, int nsteps) {
     if (c->h_check->cfl > 0.0)
       if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
   }
+  return PLC_OK;
+}
+
+bool step_needs_host(const plc_ctx *c) {
+  const plc_params &P = c->prm;
+  const long long n = c->nstep + 1;
+  if (P.cfl_target > 0.0 && n < P.nt_check && (n & (n - 1)) == 0) return true;
+  return P.nt_check > 0 && n % P.nt_check == 0;
+}
+
+int post_step(plc_ctx *c) {
+  const plc_params &P = c->prm;
+  ++c->nstep;
+  // Under CFL control the first steps also re-evaluate dt (steps 1, 2, 4,
+  // ... below nt_check), without the limit checks: the first forcing step
+  // moves the bulk velocity from that of the initial field (the reference's
+  // rescale divides by nz*ny, mod_initFlow.cc:92) to vel_force, which changes
+  // the CFL rate by up to nx/nz.
+  if (P.cfl_target > 0.0 && c->nstep < P.nt_check && (c->nstep & (c->nstep - 1)) == 0) {
+    if (int rc = run_check_fields(c, 2)) return rc;
+    if (c->h_check->cfl > 0.0)
+      if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+    return PLC_OK;
+  }
+  if (P.nt_check > 0 && c->nstep % P.nt_check == 0) {
+    // main.cc:156-178
+    int passed;
+    plc_value_index cm, dm;
+    if (int rc = plc_check(c, &passed, &cm, &dm)) return rc;
+    bool ok = passed != 0;
+    std::string msg;
+    if (!passed) msg += "PowerLLEL.ERROR.checkNaN: NaN has been detected in <u>!\n";
+    if (cm.value > P.cfl_limit || std::isnan(cm.value)) {
+      ok = false;
+      msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
+    }
+    // The mixed form's divergence is at FP32 rounding level: its limit is
+    // div_limit scaled by the ratio of the unit round-offs, 2^-24 / 2^-53.
+    const double div_limit = c->mixed ? P.div_limit * 536870912.0 : P.div_limit;
+    if (dm.value > div_limit || std::isnan(dm.value)) {
+      ok = false;
+      msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
+    }
+    if (!ok) {
+      char buf[256];
+      snprintf(buf, sizeof buf,
+               "PowerLLEL.ERROR: nt = %9lld, cfl_max = %10.3e at (%5d,%5d,%5d), div_max = %10.3e at (%5d,%5d,%5d)",
+               c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
+      return set_error(c, PLC_ERR_CHECK, msg + buf);
+    }
+    if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
+      if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+  }
+  return PLC_OK;
+}
+
+}  // namespace plc
+
+extern "C" {
+
+// nsteps graph launches with the checks of main.cc:156-178 every nt_check
+// steps; the device error word is not read here.
+static int step_launches(plc_ctx *c, int nsteps) {
+  PLC_CHECK_CTX(c);
+  if (nsteps < 0) return set_error(c, PLC_ERR_ARG, "nsteps < 0");
+  PLC_NEED_POISSON(c);
+  if (int rc = build_graph(c)) return rc;
+  if (int rc = pre_steps(c)) return rc;
   for (int s = 0; s < nsteps; ++s) {
     PLC_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
-    ++c->nstep;
-    // Under CFL control the first steps also re-evaluate dt (steps 1, 2, 4,
-    // ... below nt_check), without the limit checks: the first forcing step
-    // moves the bulk velocity from that of the initial field (the reference's
-    // rescale divides by nz*ny, mod_initFlow.cc:92) to vel_force, which changes
-    // the CFL rate by up to nx/nz.
-    if (P.cfl_target > 0.0 && c->nstep < P.nt_check && (c->nstep & (c->nstep - 1)) == 0) {
-      if (int rc = run_check_fields(c, 2)) return rc;
-      if (c->h_check->cfl > 0.0)
-        if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
-      continue;
-    }
-    if (P.nt_check > 0 && c->nstep % P.nt_check == 0) {
-      // main.cc:156-178
-      int passed;
-      plc_value_index cm, dm;
-      if (int rc = plc_check(c, &passed, &cm, &dm)) return rc;
-      bool ok = passed != 0;
-      std::string msg;
-      if (!passed) msg += "PowerLLEL.ERROR.checkNaN: NaN has been detected in <u>!\n";
-      if (cm.value > P.cfl_limit || std::isnan(cm.value)) {
-        ok = false;
-        msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
-      }
-      // The mixed form's divergence is at FP32 rounding level: its limit is
-      // div_limit scaled by the ratio of the unit round-offs, 2^-24 / 2^-53.
-      const double div_limit = c->mixed ? P.div_limit * 536870912.0 : P.div_limit;
-      if (dm.value > div_limit || std::isnan(dm.value)) {
-        ok = false;
-        msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
-      }
-      if (!ok) {
-        char buf[256];
-        snprintf(buf, sizeof buf,
-                 "PowerLLEL.ERROR: nt = %9lld, cfl_max = %10.3e at (%5d,%5d,%5d), div_max = %10.3e at (%5d,%5d,%5d)",
-                 c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
-        return set_error(c, PLC_ERR_CHECK, msg + buf);
-      }
-      if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
-        if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
-    }
+    if (int rc = post_step(c)) return rc;
   }
   return PLC_OK;
 }
@@ -1096,6 +1126,21 @@ int plc_set_step_count(plc_ctx *c, long long count) {
   PLC_CHECK_CTX(c);
   if (count < 0) return set_error(c, PLC_ERR_ARG, "negative step count");
   c->nstep = count;
+  return PLC_OK;
+}
+
+int plc_set_sm_budget(plc_ctx *c, int sms) {
+  PLC_CHECK_CTX(c);
+  if (sms < 1) return set_error(c, PLC_ERR_ARG, "SM budget < 1");
+  c->num_sms = sms < c->device_sms ? sms : c->device_sms;
+  if (c->poisson_ready) PLC_CUDA(c, fft_set_lines(c, c->fft_lines_xf, c->fft_lines_x, c->fft_lines_y));
+  drop_graph(c);
+  return PLC_OK;
+}
+
+int plc_get_sm_budget(const plc_ctx *c, int *sms) {
+  if (!c || !sms) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  *sms = c->num_sms;
   return PLC_OK;
 }
 

@@ -1,0 +1,439 @@
+// Batched ensembles of independent channels on one GPU.  No counterpart in
+// the reference: its main loop (src/main.cc:114-154) runs one channel.  Each
+// member is an ordinary context (its own parameters, fields, solver tables
+// and tuned FFT tiles); one ensemble step is ONE graph launch whose branches
+// are the members' fused steps, so small members that cannot fill 148 SMs
+// alone run side by side.  Members are scheduled in groups (the members of a
+// group run concurrently, groups one after another), and every member's
+// persistent kernels get an SM budget; an autotuner times candidate
+// schedules on the members' own fields and keeps the fastest.  Checks,
+// CFL-controlled dt and the device error word stay per member, as in
+// plc_step.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "plc_internal.h"
+
+struct plc_ensemble {
+  int device = 0;
+  std::vector<plc_ctx *> members;
+  cudaStream_t stream = nullptr;  // graph launches
+  cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<unsigned> epochs;  // member graph epochs the graph was captured at
+  std::vector<int> group;        // group of each member
+  int ngroups = 1;
+  int scheme = PLC_ENS_CONCURRENT;
+  std::vector<double> cost;  // measured ms per step of each member alone (0 = not measured)
+  std::string err;
+};
+
+namespace {
+
+std::string g_ens_err;
+
+int ens_error(plc_ensemble *e, int code, const std::string &msg) {
+  if (e) e->err = msg;
+  g_ens_err = msg;
+  return code;
+}
+
+int ens_cuda(plc_ensemble *e, cudaError_t r, const char *what) {
+  return ens_error(e, PLC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(r));
+}
+
+#define ENS_CUDA(e, call)                                   \
+  do {                                                      \
+    cudaError_t _r = (call);                                \
+    if (_r != cudaSuccess) return ens_cuda(e, _r, #call);   \
+  } while (0)
+
+// a member's failure, reported with the member's index and message
+int member_error(plc_ensemble *e, int m, int rc) {
+  return ens_error(e, rc, "member " + std::to_string(m) + ": " + plc_last_error(e->members[m]));
+}
+
+void drop(plc_ensemble *e) {
+  if (e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+}
+
+// Captures one ensemble step: per group, a fork from the ensemble stream to
+// the members' streams, each member's fused step, a join back.
+int build(plc_ensemble *e) {
+  const int n = (int)e->members.size();
+  bool stale = e->graph == nullptr;
+  for (int m = 0; m < n && !stale; ++m) stale = e->epochs[m] != e->members[m]->graph_epoch;
+  if (!stale) return PLC_OK;
+  drop(e);
+  for (int m = 0; m < n; ++m)
+    if (!e->members[m]->poisson_ready)
+      return ens_error(e, PLC_ERR_STATE, "member " + std::to_string(m) + ": Poisson solver not initialised");
+  cudaGraph_t g = nullptr;
+  ENS_CUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = PLC_OK;
+  cudaError_t r = cudaSuccess;
+  for (int grp = 0; grp < e->ngroups && rc == PLC_OK && r == cudaSuccess; ++grp) {
+    if ((r = cudaEventRecord(e->fork, e->stream)) != cudaSuccess) break;
+    for (int m = 0; m < n && rc == PLC_OK && r == cudaSuccess; ++m) {
+      if (e->group[m] != grp) continue;
+      plc_ctx *c = e->members[m];
+      if ((r = cudaStreamWaitEvent(c->stream, e->fork, 0)) != cudaSuccess) break;
+      if ((rc = plc::capture_step(c, c->stream)) != PLC_OK) {
+        rc = member_error(e, m, rc);
+        break;
+      }
+      r = cudaEventRecord(e->join[m], c->stream);
+    }
+    for (int m = 0; m < n && rc == PLC_OK && r == cudaSuccess; ++m)
+      if (e->group[m] == grp) r = cudaStreamWaitEvent(e->stream, e->join[m], 0);
+  }
+  const cudaError_t re = cudaStreamEndCapture(e->stream, &g);
+  if (rc != PLC_OK || r != cudaSuccess || re != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (rc != PLC_OK) return rc;
+    return ens_cuda(e, r != cudaSuccess ? r : re, "ensemble step capture");
+  }
+  r = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (r != cudaSuccess) return ens_cuda(e, r, "cudaGraphInstantiate");
+  for (int m = 0; m < n; ++m) e->epochs[m] = e->members[m]->graph_epoch;
+  return PLC_OK;
+}
+
+// orders the ensemble stream after all work queued on the members' streams
+int ens_after_members(plc_ensemble *e) {
+  for (size_t m = 0; m < e->members.size(); ++m) {
+    ENS_CUDA(e, cudaEventRecord(e->join[m], e->members[m]->stream));
+    ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
+  }
+  return PLC_OK;
+}
+
+// orders the members' streams after the work queued on the ensemble stream
+int members_after_ens(plc_ensemble *e) {
+  ENS_CUDA(e, cudaEventRecord(e->done, e->stream));
+  for (plc_ctx *c : e->members) ENS_CUDA(e, cudaStreamWaitEvent(c->stream, e->done, 0));
+  return PLC_OK;
+}
+
+int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
+  if (nsteps < 0) return ens_error(e, PLC_ERR_ARG, "nsteps < 0");
+  const int n = (int)e->members.size();
+  if (int rc = build(e)) return rc;
+  for (int m = 0; m < n; ++m)
+    if (int rc = plc::pre_steps(e->members[m])) return member_error(e, m, rc);
+  if (int rc = ens_after_members(e)) return rc;
+  if (ms) ENS_CUDA(e, cudaEventRecord(e->t0, e->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    bool host = false;
+    for (plc_ctx *c : e->members) host = host || plc::step_needs_host(c);
+    ENS_CUDA(e, cudaGraphLaunch(e->graph, e->stream));
+    if (host)
+      if (int rc = members_after_ens(e)) return rc;
+    for (int m = 0; m < n; ++m)
+      if (int rc = plc::post_step(e->members[m])) return member_error(e, m, rc);
+    // a member's host work (checks, a new dt) finished on its stream before
+    // post_step returned; the next launch is queued after it
+  }
+  if (ms) {
+    ENS_CUDA(e, cudaEventRecord(e->t1, e->stream));
+    ENS_CUDA(e, cudaEventSynchronize(e->t1));
+    float t = 0.f;
+    ENS_CUDA(e, cudaEventElapsedTime(&t, e->t0, e->t1));
+    *ms = t;
+  }
+  if (int rc = members_after_ens(e)) return rc;
+  // the device error word of each member (bounded waits that gave up)
+  for (int m = 0; m < n; ++m)
+    if (int rc = plc_sync(e->members[m])) return member_error(e, m, rc);
+  return PLC_OK;
+}
+
+// Device copies of the members' u, v, w, p (the state an autotuning run
+// advances), restored afterwards.
+struct Snapshot {
+  std::vector<void *> buf;
+  ~Snapshot() {
+    for (void *p : buf) cudaFree(p);
+  }
+};
+
+const int kStateFields[4] = {PLC_U, PLC_V, PLC_W, PLC_P};
+
+void *field_of(plc_ctx *c, int f) {
+  return c->mixed ? static_cast<void *>(c->f_field[f]) : static_cast<void *>(c->d_field[f]);
+}
+size_t field_bytes(const plc_ctx *c) { return c->nfield * (c->mixed ? sizeof(float) : sizeof(double)); }
+
+int snapshot(plc_ensemble *e, Snapshot &s, bool save) {
+  size_t q = 0;
+  for (plc_ctx *c : e->members)
+    for (int f : kStateFields) {
+      if (save) {
+        void *p = nullptr;
+        ENS_CUDA(e, cudaMalloc(&p, field_bytes(c)));
+        s.buf.push_back(p);
+        ENS_CUDA(e, cudaMemcpyAsync(p, field_of(c, f), field_bytes(c), cudaMemcpyDeviceToDevice, c->stream));
+      } else {
+        ENS_CUDA(e, cudaMemcpyAsync(field_of(c, f), s.buf[q++], field_bytes(c), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+      }
+    }
+  for (plc_ctx *c : e->members) ENS_CUDA(e, cudaStreamSynchronize(c->stream));
+  return PLC_OK;
+}
+
+// launches only (no checks, no step counting): the timing loop of the autotuner
+int time_launches(plc_ensemble *e, int steps, float *ms) {
+  if (int rc = build(e)) return rc;
+  if (int rc = ens_after_members(e)) return rc;
+  ENS_CUDA(e, cudaGraphLaunch(e->graph, e->stream));  // warm-up
+  ENS_CUDA(e, cudaEventRecord(e->t0, e->stream));
+  for (int s = 0; s < steps; ++s) ENS_CUDA(e, cudaGraphLaunch(e->graph, e->stream));
+  ENS_CUDA(e, cudaEventRecord(e->t1, e->stream));
+  ENS_CUDA(e, cudaEventSynchronize(e->t1));
+  ENS_CUDA(e, cudaEventElapsedTime(ms, e->t0, e->t1));
+  return members_after_ens(e);
+}
+
+// a member alone: its own captured step replayed on its stream (launches
+// only: no checks, no step counting)
+int time_member(plc_ensemble *e, int m, int steps, float *ms) {
+  plc_ctx *c = e->members[m];
+  cudaGraphExec_t g = nullptr;
+  if (int rc = plc::step_graph(c, &g)) return member_error(e, m, rc);
+  ENS_CUDA(e, cudaGraphLaunch(g, c->stream));  // warm-up
+  ENS_CUDA(e, cudaEventRecord(e->t0, c->stream));
+  for (int s = 0; s < steps; ++s) ENS_CUDA(e, cudaGraphLaunch(g, c->stream));
+  ENS_CUDA(e, cudaEventRecord(e->t1, c->stream));
+  ENS_CUDA(e, cudaEventSynchronize(e->t1));
+  float t = 0.f;
+  ENS_CUDA(e, cudaEventElapsedTime(&t, e->t0, e->t1));
+  *ms = t / steps;
+  return PLC_OK;
+}
+
+// Applies a schedule: SM budgets per member and the grouping.
+int apply_scheme(plc_ensemble *e, int scheme) {
+  const int n = (int)e->members.size();
+  const int sms = e->members[0]->device_sms;
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e->cost[a] > e->cost[b]; });
+  e->group.assign(n, 0);
+  e->ngroups = 1;
+  std::vector<int> budget(n, sms);
+  const double total = std::accumulate(e->cost.begin(), e->cost.end(), 0.0);
+  switch (scheme) {
+    case PLC_ENS_CONCURRENT:  // all members at once, full budgets
+      break;
+    case PLC_ENS_PROPORTIONAL:  // all at once, SMs shared in proportion to cost
+      for (int m = 0; m < n; ++m)
+        budget[m] = std::max(1, (int)std::lround(sms * (total > 0 ? e->cost[m] / total : 1.0 / n)));
+      break;
+    case PLC_ENS_TWO_GROUPS: {  // two cost-balanced groups (LPT), proportional within each
+      double load[2] = {0.0, 0.0};
+      for (int m : order) {
+        const int g = load[0] <= load[1] ? 0 : 1;
+        e->group[m] = g;
+        load[g] += e->cost[m];
+      }
+      e->ngroups = 2;
+      for (int m = 0; m < n; ++m) {
+        const double l = load[e->group[m]];
+        budget[m] = std::max(1, (int)std::lround(sms * (l > 0 ? e->cost[m] / l : 1.0)));
+      }
+      break;
+    }
+    case PLC_ENS_SEQUENTIAL:  // one member after another, full budgets
+      for (int q = 0; q < n; ++q) e->group[order[q]] = q;
+      e->ngroups = n;
+      break;
+    default:
+      return ens_error(e, PLC_ERR_ARG, "unknown ensemble schedule");
+  }
+  for (int m = 0; m < n; ++m)
+    if (int rc = plc_set_sm_budget(e->members[m], budget[m])) return member_error(e, m, rc);
+  e->scheme = scheme;
+  drop(e);
+  return PLC_OK;
+}
+
+}  // namespace
+
+using namespace plc;
+
+extern "C" {
+
+const char *plc_ensemble_last_error(const plc_ensemble *e) { return e ? e->err.c_str() : g_ens_err.c_str(); }
+
+int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_globals, int device,
+                        plc_ensemble **out) {
+  if (!out || !prms || n < 1) return ens_error(nullptr, PLC_ERR_ARG, "bad argument");
+  *out = nullptr;
+  plc_ensemble *e = new plc_ensemble;
+  e->device = device;
+  auto fail = [&](int rc) {
+    const std::string msg = e->err;
+    plc_ensemble_destroy(e);
+    return ens_error(nullptr, rc, msg);
+  };
+  for (int m = 0; m < n; ++m) {
+    plc_ctx *c = nullptr;
+    const int rc = plc_create(&prms[m], dzf_globals ? dzf_globals[m] : nullptr, device, &c);
+    if (rc != PLC_OK) {
+      e->err = "member " + std::to_string(m) + ": " + plc_last_error(nullptr);
+      return fail(rc);
+    }
+    e->members.push_back(c);
+  }
+  cudaError_t r;
+  if ((r = cudaSetDevice(device)) != cudaSuccess ||
+      (r = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (r = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (r = cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming)) != cudaSuccess ||
+      (r = cudaEventCreate(&e->t0)) != cudaSuccess || (r = cudaEventCreate(&e->t1)) != cudaSuccess) {
+    ens_cuda(e, r, "ensemble stream/events");
+    return fail(PLC_ERR_CUDA);
+  }
+  e->join.assign(n, nullptr);
+  for (auto &ev : e->join)
+    if ((r = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) {
+      ens_cuda(e, r, "ensemble events");
+      return fail(PLC_ERR_CUDA);
+    }
+  e->epochs.assign(n, ~0u);
+  e->group.assign(n, 0);
+  // cost model before measurement: grid points (FP32 fields move half the bytes)
+  e->cost.resize(n);
+  for (int m = 0; m < n; ++m) {
+    const plc_ctx *c = e->members[m];
+    e->cost[m] = double(c->nx) * c->ny * c->nz * (c->mixed ? 0.5 : 1.0);
+  }
+  *out = e;
+  return PLC_OK;
+}
+
+int plc_ensemble_destroy(plc_ensemble *e) {
+  if (!e) return PLC_OK;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  drop(e);
+  for (plc_ctx *c : e->members) plc_destroy(c);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {e->fork, e->done, e->t0, e->t1})
+    if (ev) cudaEventDestroy(ev);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return PLC_OK;
+}
+
+int plc_ensemble_size(const plc_ensemble *e, int *n) {
+  if (!e || !n) return ens_error(nullptr, PLC_ERR_ARG, "null argument");
+  *n = (int)e->members.size();
+  return PLC_OK;
+}
+
+int plc_ensemble_member(plc_ensemble *e, int i, plc_ctx **ctx) {
+  if (!e || !ctx) return ens_error(nullptr, PLC_ERR_ARG, "null argument");
+  if (i < 0 || i >= (int)e->members.size()) return ens_error(e, PLC_ERR_ARG, "member index out of range");
+  *ctx = e->members[i];
+  return PLC_OK;
+}
+
+int plc_ensemble_init_flow(plc_ensemble *e) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  for (size_t m = 0; m < e->members.size(); ++m)
+    if (int rc = plc_init_flow(e->members[m])) return member_error(e, (int)m, rc);
+  return PLC_OK;
+}
+
+int plc_ensemble_step(plc_ensemble *e, int nsteps) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  return ens_steps(e, nsteps, nullptr);
+}
+
+int plc_ensemble_step_timed(plc_ensemble *e, int nsteps, double *ms) {
+  if (!e || !ms) return ens_error(e, PLC_ERR_ARG, "null argument");
+  return ens_steps(e, nsteps, ms);
+}
+
+int plc_ensemble_set_schedule(plc_ensemble *e, int scheme) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  return apply_scheme(e, scheme);
+}
+
+int plc_ensemble_schedule(const plc_ensemble *e, int *scheme, int *groups, int *sm_budgets) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  if (scheme) *scheme = e->scheme;
+  if (groups)
+    for (size_t m = 0; m < e->members.size(); ++m) groups[m] = e->group[m];
+  if (sm_budgets)
+    for (size_t m = 0; m < e->members.size(); ++m) sm_budgets[m] = e->members[m]->num_sms;
+  return PLC_OK;
+}
+
+int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
+  if (!e || steps < 1) return ens_error(e, PLC_ERR_ARG, "bad argument");
+  const int n = (int)e->members.size();
+  Snapshot snap;
+  if (int rc = snapshot(e, snap, true)) return rc;
+  int rc = PLC_OK;
+  // 1. cost model: each member's step time alone, full budget
+  for (int m = 0; m < n && rc == PLC_OK; ++m) {
+    if ((rc = plc_set_sm_budget(e->members[m], e->members[m]->device_sms)) != PLC_OK) {
+      rc = member_error(e, m, rc);
+      break;
+    }
+    float t = 0.f;
+    if ((rc = time_member(e, m, steps, &t)) == PLC_OK) e->cost[m] = t;
+  }
+  // 2. every schedule on the ensemble graph; the fastest is kept
+  int best = PLC_ENS_CONCURRENT;
+  float best_t = -1.f;
+  for (int s = 0; s < PLC_ENS_NUM_SCHEDULES && rc == PLC_OK; ++s) {
+    if (s == PLC_ENS_TWO_GROUPS && n < 2) {
+      if (ms_per_scheme) ms_per_scheme[s] = -1.f;
+      continue;
+    }
+    float t = 0.f;
+    if ((rc = apply_scheme(e, s)) != PLC_OK || (rc = time_launches(e, steps, &t)) != PLC_OK) break;
+    t /= steps;
+    if (ms_per_scheme) ms_per_scheme[s] = t;
+    if (best_t < 0.f || t < best_t) {
+      best_t = t;
+      best = s;
+    }
+  }
+  if (rc == PLC_OK) rc = apply_scheme(e, best);
+  const int rc2 = snapshot(e, snap, false);
+  return rc != PLC_OK ? rc : rc2;
+}
+
+int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of) {
+  if (n < 0 || n_gpus < 1 || (n > 0 && (!cost || !gpu_of)))
+    return ens_error(nullptr, PLC_ERR_ARG, "bad argument");
+  // longest processing time first: the costliest member to the least loaded GPU
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<double> load(n_gpus, 0.0);
+  for (int m : order) {
+    const int g = int(std::min_element(load.begin(), load.end()) - load.begin());
+    gpu_of[m] = g;
+    load[g] += cost[m];
+  }
+  return PLC_OK;
+}
+
+}  // extern "C"

@@ -1025,9 +1025,7 @@ cudaError_t fft_setup_t(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max, i
 // Tile sizes (line pairs per tile) and persistent grid sizes of the
 // transforms, from the shared memory each needs and the occupancy it gets.
 cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max) {
-  int sms = 0;
-  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  if (e != cudaSuccess) return e;
+  const int sms = c->num_sms;  // the context's SM budget
   return c->mixed ? fft_setup_t<float>(c, smem_cap_per_block, dev_max, sms)
                   : fft_setup_t<double>(c, smem_cap_per_block, dev_max, sms);
 }
@@ -1186,10 +1184,9 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
 }  // namespace
 
 cudaError_t fft_autotune(plc_ctx *c) {
-  int sms = 0, dev_max = 0;
-  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  if (e == cudaSuccess)
-    e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const int sms = c->num_sms;
+  int dev_max = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if (e != cudaSuccess) return e;
   e = c->mixed ? fft_autotune_t<float>(c, c->f_field, (size_t)dev_max, sms)
                : fft_autotune_t<double>(c, c->d_field, (size_t)dev_max, sms);
@@ -1200,10 +1197,9 @@ cudaError_t fft_autotune(plc_ctx *c) {
 // Applies line counts chosen earlier (a re-initialised solver keeps the
 // context's tuning).
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y) {
-  int sms = 0, dev_max = 0;
-  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  if (e == cudaSuccess)
-    e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  const int sms = c->num_sms;
+  int dev_max = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
   if (e != cudaSuccess) return e;
   c->fft_lines_xf = lines_xf;
   c->fft_lines_x = lines_x;

@@ -103,13 +103,15 @@ struct plc_ctx {
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
   unsigned int *d_counter = nullptr;   // last-block counters
   int *d_err = nullptr;                // set by a kernel whose bounded wait gave up
-  int num_sms = 148;
+  int num_sms = 148;      // SM budget of the persistent grids (plc_set_sm_budget)
+  int device_sms = 148;   // SMs of the device
   plc::CheckResult *d_check = nullptr;
   plc::CheckResult *h_check = nullptr;  // pinned
   double *h_scal = nullptr;             // pinned scalars
   double dt_host = 0;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
+  unsigned graph_epoch = 0;  // bumped whenever a captured step becomes stale
   int graph_kernels = 0;
   long long nstep = 0;
   // statistics (plc_stat_init): running sums, nx*ny*nz doubles each
@@ -239,6 +241,20 @@ cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 // var -= delta on the interior of the context's field (either form), synchronous
 int shift_field(plc_ctx *c, int field, double delta);
+// the launches of one fused step on stream s (for capture into a caller's graph)
+int capture_step(plc_ctx *c, cudaStream_t s);
+// the context's captured step, built if needed
+int step_graph(plc_ctx *c, cudaGraphExec_t *g);
+// releases the context's captured step (it is rebuilt on the next step)
+void drop_graph(plc_ctx *c);
+// host work around graph-launched steps: before the first step (CFL-controlled
+// dt) and after each step (step counter, early dt re-evaluation, the checks
+// every nt_check steps); post_step expects the step's work to be ordered
+// before the context's stream
+int pre_steps(plc_ctx *c);
+int post_step(plc_ctx *c);
+// true when post_step will do host work after the next step
+bool step_needs_host(const plc_ctx *c);
 // closes the monitor files and releases the I/O state (plc_io.cc)
 void io_free(plc_ctx *c);
 
