@@ -481,12 +481,6 @@ class Channel:
         return bool(ok.value), _vi(c), _vi(d)
 
     @property
-    def step_count(self) -> int:
-        n = C.c_longlong()
-        self._check(lib().plc_step_count(self._ctx, C.byref(n)))
-        return n.value
-
-    @property
     def stream(self) -> int:
         """The context's cudaStream_t as an integer handle."""
         h = C.c_void_p()

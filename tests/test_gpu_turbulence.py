@@ -1,0 +1,117 @@
+"""The mixed form against FP64 in developed flow: the 256 x 192 x 128 channel
+(4pi x 2pi x 2, tanh 1.5, Re_b = 5600) spun up to turbulence, then 10 steps
+and 2000-step statistics of both forms from the same state.
+
+The reference's laminar + cell-noise recipe relaminarises at this size
+(Re_tau falls from 165 to 113 over 20000 steps), so the spin-up adds
+divergence-free streamwise vortices (three pairs across y, modulated twice
+along x) of amplitude 0.15 to the Poiseuille profile.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ = 256, 192, 128
+LX, LY, LZ = 4 * math.pi, 2 * math.pi, 2.0
+SPIN = 30000
+
+
+def params(precision, **kw):
+    from powerllel_channel_sycl_b200 import make_params
+    return make_params(nx=NX, ny=NY, nz=NZ, lx=LX, ly=LY, lz=LZ, mesh_type=1, stretch_func=0,
+                       stretch_ratio=1.5, re=2800.0, u_ref=1.0, l_ref=1.0, dt=2e-3, nt_check=100,
+                       cfl_limit=1.0, div_limit=1e-9, initial_field="poi", init_with_noise=1,
+                       noise_intensity=0.1, is_forced=[1, 0, 0], vel_force=[1.0, 0, 0],
+                       precision=precision, stat_which_var=[1] * 11, **kw)
+
+
+def add_vortices(ch, amp=0.15):
+    """v, w from a streamfunction psi(y, z) on the cell edges: the discrete
+    divergence of the perturbation is zero, and psi and its z-derivative
+    vanish at the walls."""
+    case = oracle.Case(NX, NY, NZ, lx=LX, ly=LY, lz=LZ, stretch_ratio=1.5)
+    dzf = case.dzf_global
+    zf = np.concatenate([[0.0], np.cumsum(dzf[1:NZ + 1])])  # top face of cell k
+    dy, dx = LY / NY, LX / NX
+    j = np.arange(NY + 2)
+    zeta = 2 * zf / LZ - 1
+    psi = amp * np.sin(2 * math.pi * 3 * j * dy / LY)[None, :] * ((1 - zeta ** 2) ** 2)[:, None]
+    psi[0, :] = 0.0
+    psi[NZ, :] = 0.0
+    fx = 1 + 0.5 * np.cos(2 * math.pi * 2 * np.arange(NX + 2) * dx / LX)
+    v, w = ch.download("v"), ch.download("w")
+    for k in range(1, NZ + 1):
+        v[k, 1:NY + 1, :] += ((psi[k, 1:NY + 1] - psi[k - 1, 1:NY + 1]) / dzf[k])[:, None] * fx
+    for k in range(1, NZ):
+        w[k, 1:NY + 1, :] += (-(psi[k, 1:NY + 1] - psi[k, 0:NY]) / dy)[:, None] * fx
+    ch.upload("v", v)
+    ch.upload("w", w)
+    ch.finish_input()
+
+
+@pytest.fixture(scope="module")
+def turbulent_state():
+    from powerllel_channel_sycl_b200 import Channel
+    ch = Channel(params("fp64"))
+    ch.initFlow()
+    add_vortices(ch)
+    ch.step(SPIN)
+    re_tau = ch.re_tau()
+    state = {q: ch.download(q) for q in "uvw"}
+    ch.close()
+    return re_tau, state
+
+
+def from_state(precision, state, **kw):
+    from powerllel_channel_sycl_b200 import Channel
+    ch = Channel(params(precision, **kw))
+    for q in "uvw":
+        ch.upload(q, state[q])
+    return ch
+
+
+def test_spun_up_flow_is_turbulent(turbulent_state):
+    re_tau, _ = turbulent_state
+    # laminar Poiseuille at Re_b = 5600 has Re_tau = sqrt(3 * 2800) = 91.7
+    assert re_tau > 140, re_tau
+
+
+def test_ten_step_error_in_turbulence(turbulent_state):
+    _, state = turbulent_state
+    a, b = from_state("fp64", state), from_state("mixed", state)
+    a.step(10)
+    b.step(10)
+    for q in "uvw":
+        x = a.download(q)[1:-1, 1:-1, 1:-1]
+        y = b.download(q)[1:-1, 1:-1, 1:-1]
+        err = np.linalg.norm(y - x) / np.linalg.norm(x)
+        assert err <= 1e-4, (q, err)
+    assert a.check()[2][0] < 1e-12
+    assert b.check()[2][0] < 1e-3
+
+
+def test_statistics_profiles_in_turbulence(turbulent_state):
+    """Mean and RMS profiles over 2000 steps (a sample every 10)."""
+    _, state = turbulent_state
+    prof = {}
+    for form in ("fp64", "mixed"):
+        ch = from_state(form, state, nt_init_stat=SPIN, sample_interval=10)
+        ch.step_count = SPIN
+        ch.initStat()
+        for k in range(1, 2001):
+            ch.step(1)
+            ch.calcStat(SPIN + k)
+        prof[form] = ch.stat_profiles()
+        ch.close()
+    a, b = prof["fp64"], prof["mixed"]
+    assert np.max(np.abs(b["u"] - a["u"])) / np.max(np.abs(a["u"])) <= 5e-3
+    rms = {f: np.sqrt(np.maximum(p["u2"] - p["u"] ** 2, 0)) for f, p in prof.items()}
+    assert np.max(np.abs(rms["mixed"] - rms["fp64"])) / np.max(rms["fp64"]) <= 5e-2
+    assert np.max(rms["fp64"]) > 0.05  # fluctuations of developed flow
