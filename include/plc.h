@@ -115,6 +115,7 @@ typedef struct plc_params {
   /* B200 build options (not in the reference's param.json) */
   int precision; /* PLC_FP64 (default) or PLC_MIXED */
   double cfl_target; /* > 0: dt = cfl_target / max CFL rate, evaluated every nt_check steps */
+  double init_vortex_amp; /* != 0: plc_init_flow adds divergence-free streamwise vortices */
 } plc_params;
 
 typedef struct plc_value_index {
@@ -275,6 +276,11 @@ int plc_stat_upload(plc_ctx *ctx, int which, const double *h_src, int nts, int n
  * are post-processed from the stat files). */
 int plc_stat_profiles(plc_ctx *ctx, double *h_prof);
 
+/* Instantaneous plane means of u + u_crf, h_prof[k-1] for k = 1..nz (no
+ * counterpart in the reference; the spin-up judge of the learned
+ * initialiser). */
+int plc_mean_profile(plc_ctx *ctx, double *h_prof);
+
 /* ---- mod_monitor (src/mod_monitor.cc:57-205) on the context's fields ---- */
 /* calcAndWriteForcing (:57-75): Mean of each forced component (u + u_crf), 0 else. */
 int plc_monitor_forcing(plc_ctx *ctx, double *vel_mean3);
@@ -290,8 +296,19 @@ int plc_monitor_skf(plc_ctx *ctx, int wall, double *u_tau, double *cf);
  * (centred along their own direction, u + u_crf) or p, into h_dst (x fastest). */
 int plc_extract_region(plc_ctx *ctx, const int *region_ijk, int field, double *h_dst);
 
+/* The solver's projection of the context's u, v, w onto divergence-free
+ * fields: p = div(u)/dt (calcRHS), the Poisson solve, correctVel and the
+ * boundary updates, without time integration.  Either form. */
+int plc_project(plc_ctx *ctx);
+
 /* ---- initial field (mod_initFlow.cc:47-102) on the context's u, v, w ---- */
-/* Followed by transform2CRF and the boundary update, as main.cc:73-82. */
+/* Followed by transform2CRF and the boundary update, as main.cc:73-82.
+ * With init_vortex_amp = A != 0 (no counterpart in the reference, whose
+ * laminar + noise field relaminarises on fine grids) the profile and noise
+ * are followed by streamwise vortices: v, w from the streamfunction
+ * psi = A sin(2 pi n_y y / ly) (1 - zeta^2)^2 (zeta = 2 z / lz - 1) on the
+ * cell edges, times 1 + cos(2 pi n_x x / lx) / 2, with n_y = 3 pairs per 2 pi
+ * of span and n_x = 2 per 4 pi of length; discretely divergence-free. */
 int plc_init_flow(plc_ctx *ctx);
 /* main.cc:77-82 for fields uploaded by the caller (inputData on restart):
  * u -= u_crf on the interior with vel_force[0] shifted likewise
@@ -461,6 +478,61 @@ int plc_ensemble_autotune(plc_ensemble *ens, int steps, float *ms_per_scheme);
 /* Multi-GPU placement of members: longest-processing-time-first over the
  * given costs; gpu_of[i] in [0, n_gpus).  Host only. */
 int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of);
+
+/* ---- learned initialiser (no reference counterpart) ----
+ * A conditional 3-D convolutional generator: Gaussian latent + Re_tau ->
+ * u, v, w at the cell centres of an nx x ny x nz grid (4 levels, each
+ * doubling the grid: nx, ny, nz divisible by 8), 3x3x3 convolutions periodic
+ * in x, y and zero-padded at the walls, FiLM conditioning on Re_tau per
+ * wall-normal plane, BF16 weights and activations with FP32 accumulation on
+ * the tensor cores, FP32 master weights and Adam.  Trained on statistics of
+ * DNS snapshots coarse-grained to its grid (PLC_GEN_NSTAT per plane: means of
+ * u, v, w; their variances; the u-w covariance; lagged covariances of u, v, w
+ * at 1, 2, 4, 8 cells along x and along y). */
+typedef struct plc_gen plc_gen;
+typedef struct plc_gen_config {
+  int nx, ny, nz;          /* output grid of the generator, divisible by 8 */
+  int channels[4];         /* per level, coarse to fine; multiples of 16, <= 128 */
+  int latent_channels;     /* multiple of 16 */
+  int batch;               /* samples per forward / training step */
+  unsigned long long seed; /* initial weights */
+} plc_gen_config;
+#define PLC_GEN_NSTAT 31
+int plc_gen_config_default(plc_gen_config *cfg);
+int plc_gen_create(const plc_gen_config *cfg, int device, plc_gen **out);
+int plc_gen_destroy(plc_gen *gen);
+const char *plc_gen_last_error(const plc_gen *gen);
+int plc_gen_num_params(const plc_gen *gen, long long *n);
+/* FP32 master parameters: the conv weights W[tap][co][ci] of every layer,
+ * then per layer the FiLM tables A0, A1, B0, B1 [z][co]. */
+int plc_gen_get_params(plc_gen *gen, float *h);
+int plc_gen_set_params(plc_gen *gen, const float *h);
+/* Training targets: n entries of (Re_tau, nz x PLC_GEN_NSTAT statistics). */
+int plc_gen_set_targets(plc_gen *gen, int n, const double *re_tau, const double *stats);
+/* The Gaussian latent of a seed ([batch][nz/8][ny/8][nx/8][latent] floats). */
+int plc_gen_latent(plc_gen *gen, unsigned long long seed, float *h);
+/* Forward pass for batch Re_tau values; h_out (batch*nz*ny*nx*3, u v w
+ * fastest) may be NULL.  plc_gen_output_stats: the statistics of the last
+ * output (batch*nz*PLC_GEN_NSTAT). */
+int plc_gen_forward(plc_gen *gen, const double *re_tau, unsigned long long latent_seed,
+                    float *h_out);
+int plc_gen_output_stats(plc_gen *gen, double *h_stats);
+/* Loss of one batch against targets target_idx (with their Re_tau) and, if
+ * h_grads != NULL, the gradient of every parameter. */
+int plc_gen_loss_grad(plc_gen *gen, const int *target_idx, const double *re_tau,
+                      unsigned long long latent_seed, double *loss, float *h_grads);
+/* One Adam step (lr) on the gradients of the last plc_gen_loss_grad. */
+int plc_gen_adam_step(plc_gen *gen, double lr);
+/* iters Adam steps (warm-up, cosine decay from lr) on random batches of the
+ * targets; h_loss (iters) may be NULL. */
+int plc_gen_train(plc_gen *gen, int iters, double lr, unsigned long long seed, double *h_loss);
+/* Statistics (nz x PLC_GEN_NSTAT) of a context's u + u_crf, v, w box-averaged
+ * to the generator's grid (the context's grid a multiple of it). */
+int plc_gen_stats_of(plc_gen *gen, plc_ctx *ctx, double *h_stats);
+/* Proposes u, v, w for Re_tau into the context (its nz a multiple of the
+ * generator's; interpolated onto the staggered grid, zero at the walls) and
+ * projects them with plc_project. */
+int plc_gen_propose(plc_gen *gen, plc_ctx *ctx, double re_tau, unsigned long long latent_seed);
 
 /* Pinned host memory for fast uploads/downloads. */
 int plc_host_alloc(size_t bytes, void **ptr);

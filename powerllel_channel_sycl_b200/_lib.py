@@ -56,6 +56,7 @@ class PlcParams(C.Structure):
         ("region_ijk", C.c_int * 6),
         ("precision", C.c_int),
         ("cfl_target", C.c_double),
+        ("init_vortex_amp", C.c_double),
     ]
 
 
@@ -140,6 +141,23 @@ _SIGS = {
                     C.POINTER(_int)],
     "plc_read_mesh_in": [C.c_char_p, _int, _hp],
     "plc_device_name": [_int, C.c_char_p, _int],
+    "plc_project": [_vp],
+    "plc_mean_profile": [_vp, _hp],
+    "plc_gen_config_default": [_vp],
+    "plc_gen_create": [_vp, _int, C.POINTER(_vp)],
+    "plc_gen_destroy": [_vp],
+    "plc_gen_num_params": [_vp, C.POINTER(C.c_longlong)],
+    "plc_gen_get_params": [_vp, _hp],
+    "plc_gen_set_params": [_vp, _hp],
+    "plc_gen_set_targets": [_vp, _int, _hp, _hp],
+    "plc_gen_latent": [_vp, C.c_ulonglong, _hp],
+    "plc_gen_forward": [_vp, _hp, C.c_ulonglong, _hp],
+    "plc_gen_output_stats": [_vp, _hp],
+    "plc_gen_loss_grad": [_vp, _hp, _hp, C.c_ulonglong, C.POINTER(_dbl), _hp],
+    "plc_gen_adam_step": [_vp, _dbl],
+    "plc_gen_train": [_vp, _int, _dbl, C.c_ulonglong, _hp],
+    "plc_gen_stats_of": [_vp, _vp, _hp],
+    "plc_gen_propose": [_vp, _vp, _dbl, C.c_ulonglong],
     "plc_set_sm_budget": [_vp, _int],
     "plc_get_sm_budget": [_vp, C.POINTER(_int)],
     "plc_ensemble_create": [_int, C.POINTER(PlcParams), C.POINTER(_vp), _int, C.POINTER(_vp)],
@@ -180,7 +198,7 @@ def exported_symbols():
     """Names of the entry points this binding expects (all declared in plc.h)."""
     return sorted(list(_SIGS) + ["plc_last_error", "plc_step_kernel_name",
                                  "plc_step_kernel_name_ctx", "plc_h5_lookup3",
-                                 "plc_ensemble_last_error"])
+                                 "plc_ensemble_last_error", "plc_gen_last_error"])
 
 
 def lib():
@@ -204,6 +222,8 @@ def lib():
         L.plc_step_kernel_name.restype = C.c_char_p
         L.plc_step_kernel_name_ctx.argtypes = [_vp, _int]
         L.plc_step_kernel_name_ctx.restype = C.c_char_p
+        L.plc_gen_last_error.argtypes = [_vp]
+        L.plc_gen_last_error.restype = C.c_char_p
         L.plc_ensemble_last_error.argtypes = [_vp]
         L.plc_ensemble_last_error.restype = C.c_char_p
         L.plc_h5_lookup3.argtypes = [_vp, C.c_size_t, C.c_uint]

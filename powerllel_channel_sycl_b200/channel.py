@@ -387,6 +387,16 @@ class Channel:
     def initFlow(self):
         self._check(lib().plc_init_flow(self._ctx))
 
+    def project(self):
+        """Makes u, v, w divergence-free with the solver's own projection."""
+        self._check(lib().plc_project(self._ctx))
+
+    def mean_profile(self) -> np.ndarray:
+        """Plane means of u + u_crf, k = 1..nz."""
+        out = np.empty(self.nz)
+        self._check(lib().plc_mean_profile(self._ctx, out.ctypes.data))
+        return out
+
     def finish_input(self):
         """transform2CRF and the boundary update after uploading u, v, w (main.cc:77-82)."""
         self._check(lib().plc_finish_input(self._ctx))

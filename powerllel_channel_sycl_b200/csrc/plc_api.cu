@@ -324,6 +324,16 @@ int init_fields(plc_ctx *c, const std::vector<double> &prof, bool is_mean, T *co
       PLC_CUDA(c, launch_scale(c, u, scratch, c->stream));
     }
   }
+  if (P.init_vortex_amp != 0.0) {
+    // face heights zf[0..nz] after the profile in the scratch
+    std::vector<double> zf(c->nz + 1, 0.0);
+    for (int k = 1; k <= c->nz; ++k) zf[k] = zf[k - 1] + c->h_dzf_global[k];
+    double *d_zf = scratch + prof.size();
+    PLC_CUDA(c, cudaMemcpyAsync(d_zf, zf.data(), zf.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+    PLC_CUDA(c, launch_add_vortices(c, v, w, d_zf, c->stream));
+    PLC_CUDA(c, cudaStreamSynchronize(c->stream));  // zf is a host temporary
+  }
   // transform2CRF (mod_calcVel.cc:13-25)
   if (P.u_crf != 0.0) {
     PLC_CUDA(c, launch_shift(c, u, P.u_crf, c->stream));
@@ -1026,6 +1036,30 @@ int plc_finish_input(plc_ctx *c) {
 
 namespace plc {
 
+// The solver's projection on the context's u, v, w (a proposed or uploaded
+// field): the velocity halos, p = div(u)/dt (calcRHS), the Poisson solve
+// with the pressure halos, u -= dt grad p (correctVel), the velocity halos
+// again.  Either form.
+template <class T>
+int project_t(plc_ctx *c, T *const *f) {
+  T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W], *p = f[PLC_P], *spec = f[PLC_SPEC];
+  cudaStream_t s = c->stream;
+  // the divergence reads the halos and the wall faces: impose them first
+  PLC_CUDA(c, launch_bound_vel(c, c->prm.u_crf, u, v, w, s));
+  if constexpr (std::is_same<T, double>::value)
+    PLC_CUDA(c, launch_fft_x_fwd(c, nullptr, u, v, w, spec, s));
+  else
+    PLC_CUDA(c, launch_fft_x_fwd(c, u, v, w, spec, s));
+  PLC_CUDA(c, launch_fft_y(c, spec, false, s));
+  PLC_CUDA(c, launch_trid(c, spec, s));
+  PLC_CUDA(c, launch_fft_y(c, spec, true, s));
+  PLC_CUDA(c, launch_fft_x_bwd(c, spec, p, true, s));
+  PLC_CUDA(c, launch_correct(c, false, p, u, v, w, s));
+  PLC_CUDA(c, launch_bound_vel(c, c->prm.u_crf, u, v, w, s));
+  PLC_CUDA(c, cudaStreamSynchronize(s));
+  return PLC_OK;
+}
+
 int pre_steps(plc_ctx *c) {
   const plc_params &P = c->prm;
   if (P.cfl_target > 0.0 && c->nstep == 0) {
@@ -1094,6 +1128,13 @@ int post_step(plc_ctx *c) {
 }  // namespace plc
 
 extern "C" {
+
+int plc_project(plc_ctx *c) {
+  PLC_CHECK_CTX(c);
+  PLC_NEED_POISSON(c);
+  return c->mixed ? project_t<float>(c, c->f_field) : project_t<double>(c, c->d_field);
+}
+
 
 // nsteps graph launches with the checks of main.cc:156-178 every nt_check
 // steps; the device error word is not read here.

@@ -430,6 +430,7 @@ int host_parse_param_json(const char *path, plc_params *prm, std::string &err) {
         }
       }
       rd(*b, "cfl_target", prm->cfl_target);
+      rd(*b, "init_vortex_amp", prm->init_vortex_amp);
     }
   }
   return PLC_OK;

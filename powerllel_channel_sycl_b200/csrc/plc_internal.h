@@ -231,6 +231,11 @@ cudaError_t launch_scale(const plc_ctx *c, double *var, const double *d_mult,
                          cudaStream_t s);
 cudaError_t launch_scale(const plc_ctx *c, float *var, const double *d_mult,
                          cudaStream_t s);
+// streamwise vortices of plc_init_flow (zf: nz+1 face heights, zf[0] = 0)
+cudaError_t launch_add_vortices(const plc_ctx *c, double *v, double *w, const double *d_zf,
+                                cudaStream_t s);
+cudaError_t launch_add_vortices(const plc_ctx *c, float *v, float *w, const double *d_zf,
+                                cudaStream_t s);
 size_t fft_smem_bytes(int n, int lines);
 cudaError_t fft_configure(size_t max_bytes);
 cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);

@@ -144,6 +144,27 @@ __global__ void k_extract_region(Geo g, const T *__restrict__ var, int dir, int3
   }
 }
 
+// Plane means of u + u_crf (instantaneous mean profile), one block per plane.
+template <class T>
+__global__ void __launch_bounds__(256) k_plane_mean(Geo g, const T *__restrict__ u, double u_crf,
+                                                    double *__restrict__ out) {
+  __shared__ double red[8];
+  const int k = blockIdx.x + 1;
+  double s = 0.0;
+  for (int t = threadIdx.x; t < g.nx * g.ny; t += blockDim.x) {
+    const int j = t / g.nx + 1, i = t % g.nx + 1;
+    s += double(u[g.at(i, j, k)]);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    out[k - 1] = tot / ((double)g.nx * g.ny) + u_crf;
+  }
+}
+
 StatSums stat_sums(const plc_ctx *c) {
   StatSums s;
   for (int q = 0; q < kStatVars; ++q) s.s[q] = c->d_stat[q];
@@ -298,6 +319,25 @@ int plc_stat_profiles(plc_ctx *c, double *h_prof) {
   if (e == cudaSuccess) e = ef;
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_status(c, e, "plc_stat_profiles");
+  return PLC_OK;
+}
+
+int plc_mean_profile(plc_ctx *c, double *h_prof) {
+  PLC_CHECK_CTX(c);
+  if (!h_prof) return set_error(c, PLC_ERR_ARG, "null destination");
+  double *d = nullptr;
+  PLC_CUDA(c, cudaMallocAsync(&d, c->nz * sizeof(double), c->stream));
+  if (c->mixed)
+    k_plane_mean<float><<<c->nz, 256, 0, c->stream>>>(c->geo(), c->f_field[PLC_U], c->prm.u_crf, d);
+  else
+    k_plane_mean<double><<<c->nz, 256, 0, c->stream>>>(c->geo(), c->d_field[PLC_U], c->prm.u_crf, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h_prof, d, c->nz * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  const cudaError_t ef = cudaFreeAsync(d, c->stream);
+  if (e == cudaSuccess) e = ef;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(c, e, "plc_mean_profile");
   return PLC_OK;
 }
 

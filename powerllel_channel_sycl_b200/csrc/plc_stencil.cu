@@ -531,19 +531,20 @@ __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, in
   }
 }
 
-// correctVel (mod_calcVel.cc:253-278), interior only.
+// correctVel (mod_calcVel.cc:253-278), interior only.  T = float: the
+// mixed form's plain correction (the projection of plc_project).
+template <class T>
 __global__ void __launch_bounds__(BX *BY) k_correct(Geo g, const StepConst *__restrict__ sc,
-                                                    const double *__restrict__ p, double *u,
-                                                    double *v, double *w) {
+                                                    const T *__restrict__ p, T *u, T *v, T *w) {
   const int i = blockIdx.x * BX + threadIdx.x + 1;
   const int j = blockIdx.y * BY + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   if (i > g.nx || j > g.ny) return;
   const long long c = g.at(i, j, k);
-  const double pc = p[c];
-  u[c] -= (p[c + 1] - pc) * sc->dtdxi;
-  v[c] -= (p[c + g.X] - pc) * sc->dtdyi;
-  w[c] -= (p[c + g.XY] - pc) * sc->dt * __ldg(g.dzc_inv + k);
+  const T pc = p[c];
+  u[c] -= (p[c + 1] - pc) * T(sc->dtdxi);
+  v[c] -= (p[c + g.X] - pc) * T(sc->dtdyi);
+  w[c] -= (p[c + g.XY] - pc) * T(sc->dt) * T(__ldg(g.dzc_inv + k));
 }
 
 // Fused correction of the step: correctVel, the halo images of every
@@ -831,6 +832,34 @@ __global__ void k_init_flow(Geo g, const double *__restrict__ prof, int with_noi
   w[c] = T(ww);
 }
 
+// Streamwise vortices added to v, w (plc_init_flow with init_vortex_amp):
+// psi(j, k) at the cell edge (y = j dy, z = zf[k]); v(j,k) = dpsi/dz and
+// w(j,k) = -dpsi/dy as differences over the cell, so that the discrete
+// divergence of the perturbation vanishes; psi and dpsi/dz are zero at the
+// walls.
+__device__ __forceinline__ double vortex_psi(double amp, double ky, double dy, const double *zf,
+                                             double lz, int j, int k) {
+  const double zeta = 2.0 * zf[k] / lz - 1.0;
+  const double e = 1.0 - zeta * zeta;
+  return amp * sin(ky * j * dy) * e * e;
+}
+
+template <class T>
+__global__ void k_add_vortices(Geo g, const double *__restrict__ zf, double amp, double kx,
+                               double ky, double dx, double dy, double lz, T *v, T *w) {
+  const int i = blockIdx.x * BX + threadIdx.x + 1;
+  const int j = blockIdx.y * BY + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  if (i > g.nx || j > g.ny) return;
+  const long long c = g.at(i, j, k);
+  const double fx = 1.0 + 0.5 * cos(kx * i * dx);
+  const double p = vortex_psi(amp, ky, dy, zf, lz, j, k);
+  const double pz = vortex_psi(amp, ky, dy, zf, lz, j, k - 1);
+  const double py = vortex_psi(amp, ky, dy, zf, lz, j - 1, k);
+  v[c] = T(double(v[c]) + (p - pz) * g.dzf_inv[k] * fx);
+  w[c] = T(double(w[c]) - (p - py) / dy * fx);
+}
+
 // ---------------------------------------------------------------------------
 // NaN / CFL / divergence check (mod_utils.cc:77-205).  what: bit 0 NaN of u
 // (halos included), bit 1 CFL, bit 2 divergence.  Max with the smallest
@@ -1103,14 +1132,15 @@ cudaError_t check_t(const plc_ctx *c, const T *u, const T *v, const T *w, int wh
 cudaError_t launch_correct(const plc_ctx *c, bool fused, const double *p, double *u, double *v,
                            double *w, cudaStream_t s) {
   if (fused) return correct_fused_t<double>(c, p, u, v, w, s);
-  k_correct<<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, p, u, v, w);
+  k_correct<double><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, p, u, v, w);
   return cudaGetLastError();
 }
-// mixed form: the fused correction of the step only
+// mixed form: the fused correction of the step, or the plain one
 cudaError_t launch_correct(const plc_ctx *c, bool fused, const float *p, float *u, float *v,
                            float *w, cudaStream_t s) {
-  if (!fused) return cudaErrorInvalidValue;
-  return correct_fused_t<float>(c, p, u, v, w, s);
+  if (fused) return correct_fused_t<float>(c, p, u, v, w, s);
+  k_correct<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, p, u, v, w);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_force_apply(const plc_ctx *c, bool fuse_bc, double *u, double *v, double *w,
@@ -1193,6 +1223,26 @@ cudaError_t launch_init_flow(const plc_ctx *c, float *u, float *v, float *w,
   k_init_flow<float><<<interior_grid(c), dim3(BX, BY), 0, s>>>(
       c->geo(), d_prof, c->prm.init_with_noise, c->prm.noise_intensity, u, v, w);
   return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t vortices_t(const plc_ctx *c, T *v, T *w, const double *d_zf, cudaStream_t s) {
+  const plc_params &P = c->prm;
+  const double pi = 3.14159265358979323846;
+  const double ny_pairs = fmax(1.0, nearbyint(3.0 * P.ly / (2.0 * pi)));
+  const double nx_mod = fmax(1.0, nearbyint(2.0 * P.lx / (4.0 * pi)));
+  k_add_vortices<T><<<interior_grid(c), dim3(BX, BY), 0, s>>>(
+      c->geo(), d_zf, P.init_vortex_amp, 2.0 * pi * nx_mod / P.lx, 2.0 * pi * ny_pairs / P.ly,
+      c->dx, c->dy, P.lz, v, w);
+  return cudaGetLastError();
+}
+cudaError_t launch_add_vortices(const plc_ctx *c, double *v, double *w, const double *d_zf,
+                                cudaStream_t s) {
+  return vortices_t(c, v, w, d_zf, s);
+}
+cudaError_t launch_add_vortices(const plc_ctx *c, float *v, float *w, const double *d_zf,
+                                cudaStream_t s) {
+  return vortices_t(c, v, w, d_zf, s);
 }
 
 }  // namespace plc

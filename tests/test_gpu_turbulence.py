@@ -56,12 +56,30 @@ def add_vortices(ch, amp=0.15):
     ch.finish_input()
 
 
+def test_device_vortices_match_host_construction():
+    """plc_init_flow's init_vortex_amp against the perturbation built here."""
+    from powerllel_channel_sycl_b200 import Channel
+    a = Channel(params("fp64"))
+    a.initFlow()
+    add_vortices(a)
+    b = Channel(params("fp64", init_vortex_amp=0.15))
+    b.initFlow()
+    for q in "uvw":
+        x, y = a.download(q), b.download(q)
+        assert np.max(np.abs(x - y)) < 1e-12, q
+    # without the cell noise the field is discretely divergence-free
+    c = Channel(params("fp64", init_vortex_amp=0.15))
+    c.params.init_with_noise = 0
+    c = Channel(c.params)
+    c.initFlow()
+    assert c.check()[2][0] < 1e-12
+
+
 @pytest.fixture(scope="module")
 def turbulent_state():
     from powerllel_channel_sycl_b200 import Channel
-    ch = Channel(params("fp64"))
+    ch = Channel(params("fp64", init_vortex_amp=0.15))
     ch.initFlow()
-    add_vortices(ch)
     ch.step(SPIN)
     re_tau = ch.re_tau()
     state = {q: ch.download(q) for q in "uvw"}
