@@ -5,8 +5,9 @@ No counterpart in the reference, whose initial fields are laminar profiles
 plus cell noise (mod_initFlow.cc).  ``Generator.propose`` writes a projected
 (divergence-free) developed-turbulence guess for a given Re_tau into a
 channel; ``spinup`` steps a channel until the stationarity criteria hold
-(Re_tau within 1 % and the mean profile within 1 % in L2 over a 2000-step
-window) and is the judge of both the generator and the laminar fallback.
+(Re_tau and the mean profile, averaged over a 2000-step window, within 1 %
+of the previous window's) and is the judge of both the generator and the
+laminar fallback.
 """
 from __future__ import annotations
 
@@ -169,13 +170,15 @@ def re_from_re_tau(re_tau: float) -> float:
 # ---- the spin-up judge -------------------------------------------------------
 def spinup(channel, max_steps: int, window: int = 2000, every: int = 100, tol: float = 0.01,
            min_re_tau: float = 0.0, callback=None) -> dict:
-    """Steps the channel until Re_tau (both walls) stays within tol of its
-    window mean and the plane-mean u profile within tol in relative L2 over
-    the last `window` steps, with Re_tau >= min_re_tau (the turbulent branch).
-    Returns the steps taken (None if max_steps passed first), the history and
-    the wall-clock time."""
+    """Steps the channel until it is statistically stationary: the means over
+    the last `window` steps of Re_tau (both walls, sampled every `every`
+    steps) and of the plane-mean u profile agree with those of the window
+    before within tol (relative; the profile in L2), with the mean Re_tau at
+    least min_re_tau (the turbulent branch; laminar flow also becomes
+    stationary).  Returns the step count at which that first held (None if
+    max_steps passed first), the history and the wall-clock time."""
+    per = window // every
     hist_n, hist_re, hist_u = [], [], []
-    need = window // every + 1
     t0 = time.perf_counter()
     n = 0
     stationary_at = None
@@ -187,14 +190,87 @@ def spinup(channel, max_steps: int, window: int = 2000, every: int = 100, tol: f
         hist_u.append(channel.mean_profile())
         if callback:
             callback(n, hist_re[-1])
-        if len(hist_re) >= need:
-            re = np.array(hist_re[-need:])
-            us = np.array(hist_u[-need:])
-            um = us.mean(axis=0)
-            ok_re = np.max(np.abs(re - re.mean())) <= tol * re.mean()
-            ok_u = np.max(np.linalg.norm(us - um, axis=1)) <= tol * np.linalg.norm(um)
-            if ok_re and ok_u and re.mean() >= min_re_tau:
+        if len(hist_re) >= 2 * per:
+            re_now = np.mean(hist_re[-per:])
+            re_before = np.mean(hist_re[-2 * per:-per])
+            u_now = np.mean(hist_u[-per:], axis=0)
+            u_before = np.mean(hist_u[-2 * per:-per], axis=0)
+            ok_re = abs(re_now - re_before) <= tol * re_now
+            ok_u = np.linalg.norm(u_now - u_before) <= tol * np.linalg.norm(u_now)
+            if ok_re and ok_u and re_now >= min_re_tau:
                 stationary_at = n
                 break
     return {"steps": stationary_at, "steps_run": n, "re_tau": np.array(hist_re),
             "n": np.array(hist_n), "wall_s": time.perf_counter() - t0}
+
+
+# ---- training data from the batched DNS ----------------------------------------
+def member_specs(n: int = 16, seed: int = 7, re_tau_range=(120.0, 400.0)) -> list:
+    """n channels of the 4pi x 2pi x 2 box (tanh 1.5) with Re_tau drawn
+    uniformly in re_tau_range; grids grow with Re_tau and are multiples of
+    the generator's 64 x 48 x 64."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        rt = float(rng.uniform(*re_tau_range))
+        if rt < 200:
+            nx, ny, nz = 128, 96, 64
+        elif rt < 300:
+            nx, ny, nz = 192, 144, 128
+        else:
+            nx, ny, nz = 256, 192, 128
+        out.append(dict(nx=nx, ny=ny, nz=nz, re_tau_target=rt, re=re_from_re_tau(rt)))
+    return out
+
+
+def channel_params_for(spec: dict, precision="mixed", cfl_target=0.4, nt_check=50,
+                       vortices=0.15, noise=0.1):
+    from .channel import make_params
+    return make_params(nx=spec["nx"], ny=spec["ny"], nz=spec["nz"], lx=4 * math.pi,
+                       ly=2 * math.pi, lz=2.0, mesh_type=1, stretch_func=0, stretch_ratio=1.5,
+                       re=spec["re"], u_ref=1.0, l_ref=1.0, dt=1e-3, nt_check=nt_check,
+                       cfl_limit=1.0, div_limit=1e-6, initial_field="poi", init_with_noise=1,
+                       noise_intensity=noise, is_forced=[1, 0, 0], vel_force=[1.0, 0.0, 0.0],
+                       precision=precision, cfl_target=cfl_target, init_vortex_amp=vortices)
+
+
+def collect(gen: Generator, specs: list, spin_steps: int, snap_every: int = 500,
+            n_snap: int = 10, device: int = 0, log=print) -> dict:
+    """Runs the members as one batched ensemble from laminar + noise +
+    vortices, then takes n_snap snapshots every snap_every steps: per member
+    the generator-grid statistics and Re_tau of each snapshot."""
+    from .ensemble import Ensemble
+    ens = Ensemble([channel_params_for(s) for s in specs], device=device)
+    ens.initFlow()
+    ens.autotune(steps=3)
+    t0 = time.perf_counter()
+    done = 0
+    while done < spin_steps:
+        k = min(5000, spin_steps - done)
+        ens.step(k)
+        done += k
+        if log:
+            log(f"spin-up {done}/{spin_steps} steps, Re_tau "
+                + " ".join(f"{m.re_tau():.0f}" for m in ens.members)
+                + f"  ({time.perf_counter() - t0:.0f} s)")
+    stats = np.zeros((len(specs), n_snap, gen.cfg.nz, NSTAT))
+    re_tau = np.zeros((len(specs), n_snap))
+    for q in range(n_snap):
+        ens.step(snap_every)
+        for i, m in enumerate(ens.members):
+            stats[i, q] = gen.stats_of(m)
+            re_tau[i, q] = m.re_tau()
+    ens.close()
+    return {"stats": stats, "re_tau": re_tau,
+            "re": np.array([s["re"] for s in specs]),
+            "grids": np.array([[s["nx"], s["ny"], s["nz"]] for s in specs]),
+            "spin_steps": spin_steps, "snap_every": snap_every,
+            "wall_s": time.perf_counter() - t0}
+
+
+def targets_from(data: dict, min_re_tau: float = 110.0):
+    """Per member: mean Re_tau and mean statistics over its snapshots, for the
+    members that stayed turbulent."""
+    re = data["re_tau"].mean(axis=1)
+    keep = re >= min_re_tau
+    return re[keep], data["stats"][keep].mean(axis=1)
