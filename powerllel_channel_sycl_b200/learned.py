@@ -274,3 +274,97 @@ def targets_from(data: dict, min_re_tau: float = 110.0):
     re = data["re_tau"].mean(axis=1)
     keep = re >= min_re_tau
     return re[keep], data["stats"][keep].mean(axis=1)
+
+
+# ---- the stored model --------------------------------------------------------
+import os as _os
+
+MODEL_DIR = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "models")
+WEIGHTS = _os.path.join(MODEL_DIR, "initialiser_weights.npz")
+TARGETS = _os.path.join(MODEL_DIR, "initialiser_targets.npz")
+
+
+def save_weights(gen: Generator, path: str = WEIGHTS):
+    """Parameters stored as BF16 (the precision the network computes in)."""
+    p = gen.params.astype(np.float32)
+    u = p.view(np.uint32).astype(np.uint64)
+    b = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    np.savez_compressed(path, params_bf16=b, **{k: np.asarray(v) for k, v in cfg_dict(gen.cfg).items()})
+
+
+def load_weights(path: str = WEIGHTS, device: int = 0, batch: int = 1) -> Generator:
+    d = np.load(path)
+    cfg = config(nx=int(d["nx"]), ny=int(d["ny"]), nz=int(d["nz"]),
+                 channels=[int(c) for c in d["channels"]],
+                 latent_channels=int(d["latent_channels"]), batch=batch)
+    g = Generator(cfg, device=device)
+    g.params = (d["params_bf16"].astype(np.uint32) << 16).view(np.float32)
+    return g
+
+
+def _main(argv=None):
+    """python -m powerllel_channel_sycl_b200.learned collect|train|evaluate"""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(prog="python -m powerllel_channel_sycl_b200.learned")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("collect", help="snapshot statistics from the batched DNS")
+    c.add_argument("--members", type=int, default=16)
+    c.add_argument("--spin", type=int, default=30000)
+    c.add_argument("--snapshots", type=int, default=10)
+    c.add_argument("--every", type=int, default=500)
+    c.add_argument("--out", default=TARGETS)
+    t = sub.add_parser("train", help="train the generator on collected targets")
+    t.add_argument("--targets", default=TARGETS)
+    t.add_argument("--iters", type=int, default=6000)
+    t.add_argument("--lr", type=float, default=2e-3)
+    t.add_argument("--out", default=WEIGHTS)
+    e = sub.add_parser("evaluate", help="steps to stationarity: generator vs fallbacks")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--re-tau", type=float, nargs="+", default=[180.0, 300.0, 395.0])
+    e.add_argument("--max-steps", type=int, default=60000)
+    e.add_argument("--json", default=None)
+    a = ap.parse_args(argv)
+    if a.cmd == "collect":
+        gen = Generator(config(batch=1))
+        data = collect(gen, member_specs(a.members), a.spin, a.every, a.snapshots)
+        re, st = targets_from(data)
+        np.savez_compressed(a.out, re_tau=re, stats=st, snapshot_re_tau=data["re_tau"],
+                            grids=data["grids"], re=data["re"], spin=a.spin)
+        print(f"{len(re)} targets, Re_tau {np.round(re, 1)} -> {a.out}")
+    elif a.cmd == "train":
+        d = np.load(a.targets)
+        gen = Generator(config(batch=4, seed=1))
+        gen.set_targets(d["re_tau"], d["stats"])
+        t0 = time.perf_counter()
+        hist = gen.train(a.iters, lr=a.lr, seed=1)
+        print(f"{a.iters} iterations in {time.perf_counter() - t0:.1f} s, loss "
+              f"{hist[:50].mean():.3g} -> {hist[-50:].mean():.3g}")
+        save_weights(gen, a.out)
+    else:
+        from .channel import Channel
+        gen = load_weights(a.weights)
+        res = {}
+        for rt in a.re_tau:
+            spec = dict(nx=256, ny=192, nz=128, re=re_from_re_tau(rt))
+            for method in ("generator", "vortices", "laminar_noise"):
+                ch = Channel(channel_params_for(spec, vortices=0.15 if method == "vortices" else 0.0))
+                ch.initFlow()
+                t0 = time.perf_counter()
+                if method == "generator":
+                    gen.propose(ch, rt, seed=1)
+                t_init = time.perf_counter() - t0
+                r = spinup(ch, a.max_steps, min_re_tau=0.75 * rt)
+                res[f"{rt:g}/{method}"] = {"steps": r["steps"], "steps_run": r["steps_run"],
+                                           "wall_s": r["wall_s"] + t_init,
+                                           "re_tau_end": float(r["re_tau"][-1])}
+                print(f"Re_tau {rt:g} {method:13s} stationary after {r['steps']} steps "
+                      f"({r['wall_s'] + t_init:.1f} s), Re_tau {r['re_tau'][-1]:.1f}", flush=True)
+                ch.close()
+        if a.json:
+            with open(a.json, "w") as f:
+                json.dump(res, f, indent=1)
+
+
+if __name__ == "__main__":
+    _main()
