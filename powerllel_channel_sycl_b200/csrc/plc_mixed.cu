@@ -102,7 +102,7 @@ struct Rhs3f {
   float u, v, w;
 };
 
-// (visc - conv) at one point; P(f, di, dj, dk) reads field f (0 u, 1 v, 2 w)
+// (visc - conv) at one point (the RK1 stage); P(f, di, dj, dk) reads field f (0 u, 1 v, 2 w)
 // at offset (di, dj, dk) from the point.
 template <bool CRF, class Acc>
 __device__ __forceinline__ Rhs3f momentum_rhs32(const RkConst &K, const Coef &z, const Acc &P) {
@@ -155,12 +155,97 @@ __device__ __forceinline__ Rhs3f momentum_rhs32(const RkConst &K, const Coef &z,
   return r;
 }
 
+// (visc - conv) of the momentum equations (mod_calcVel.cc:27-129) for the
+// two rows (j, j+1) of a thread at once, on Blackwell's packed FP32x2
+// arithmetic (FFMA2 / FADD2 / FMUL2: one instruction for both points).
+// P(f, di, dj, dk) gives field f (0 u, 1 v, 2 w) at offset (di, dj, dk) for
+// {row j, row j+1}.  Subtraction is a fused multiply-add by -1 (exact
+// product, one rounding); the z diffusion is vt*u(k+1) + vb*u(k-1) -
+// (vt+vb)*u(k).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
+
+struct Rhs3x2 {
+  float2 u, v, w;
+};
+
+template <bool CRF, class Acc2>
+__device__ __forceinline__ Rhs3x2 momentum_rhs32x2(const RkConst &K, const Coef &z, float vtb,
+                                                   float wtb, const Acc2 &P) {
+  const float2 qx = f2(K.qx), qy = f2(K.qy), rx = f2(K.rx), ry = f2(K.ry), m2 = f2(-2.f);
+  const float2 at = f2(z.at), bt = f2(z.bt), ab = f2(z.ab), bb = f2(z.bb);
+  const float2 u0 = P(0, 0, 0, 0), v0 = P(1, 0, 0, 0), w0 = P(2, 0, 0, 0);
+  Rhs3x2 r;
+  {
+    const float2 upx = P(0, 1, 0, 0), umx = P(0, -1, 0, 0), upy = P(0, 0, 1, 0),
+                 umy = P(0, 0, -1, 0), uzp = P(0, 0, 0, 1), uzm = P(0, 0, 0, -1);
+    const float2 ue = add2(u0, upx), uw = add2(umx, u0), un = add2(u0, upy), us = add2(umy, u0);
+    const float2 ut = fma2(u0, at, mul2(uzp, bt)), ub = fma2(u0, ab, mul2(uzm, bb));
+    const float2 vn = add2(v0, P(1, 1, 0, 0)), vs = add2(P(1, 0, -1, 0), P(1, 1, -1, 0));
+    const float2 wt = add2(w0, P(2, 1, 0, 0)), wb = add2(P(2, 0, 0, -1), P(2, 1, 0, -1));
+    float2 conv = mul2(qx, mul2(add2(ue, uw), sub2(ue, uw)));
+    conv = fma2(qy, sub2(mul2(un, vn), mul2(us, vs)), conv);
+    conv = fma2(f2(z.cz), sub2(mul2(ut, wt), mul2(ub, wb)), conv);
+    if (CRF) conv = fma2(f2(K.crf), sub2(ue, uw), conv);
+    const float2 zt = fma2(f2(z.vt), uzp, fma2(f2(z.vb), uzm, mul2(f2(-vtb), u0)));
+    const float2 visc = fma2(rx, fma2(u0, m2, add2(upx, umx)), fma2(ry, fma2(u0, m2, add2(upy, umy)), zt));
+    r.u = sub2(visc, conv);
+  }
+  {
+    const float2 vpx = P(1, 1, 0, 0), vmx = P(1, -1, 0, 0), vpy = P(1, 0, 1, 0),
+                 vmy = P(1, 0, -1, 0), vzp = P(1, 0, 0, 1), vzm = P(1, 0, 0, -1);
+    const float2 ve = add2(v0, vpx), vw = add2(vmx, v0), vn = add2(v0, vpy), vs = add2(vmy, v0);
+    const float2 vt = fma2(v0, at, mul2(vzp, bt)), vb = fma2(v0, ab, mul2(vzm, bb));
+    const float2 ue = add2(u0, P(0, 0, 1, 0)), uw = add2(P(0, -1, 0, 0), P(0, -1, 1, 0));
+    const float2 wt = add2(w0, P(2, 0, 1, 0)), wb = add2(P(2, 0, 0, -1), P(2, 0, 1, -1));
+    float2 conv = mul2(qx, sub2(mul2(ue, ve), mul2(uw, vw)));
+    conv = fma2(qy, mul2(add2(vn, vs), sub2(vn, vs)), conv);
+    conv = fma2(f2(z.cz), sub2(mul2(wt, vt), mul2(wb, vb)), conv);
+    if (CRF) conv = fma2(f2(K.crf), sub2(ve, vw), conv);
+    const float2 zt = fma2(f2(z.vt), vzp, fma2(f2(z.vb), vzm, mul2(f2(-vtb), v0)));
+    const float2 visc = fma2(rx, fma2(v0, m2, add2(vpx, vmx)), fma2(ry, fma2(v0, m2, add2(vpy, vmy)), zt));
+    r.v = sub2(visc, conv);
+  }
+  {
+    const float2 wpx = P(2, 1, 0, 0), wmx = P(2, -1, 0, 0), wpy = P(2, 0, 1, 0),
+                 wmy = P(2, 0, -1, 0), wzp = P(2, 0, 0, 1), wzm = P(2, 0, 0, -1);
+    const float2 we = add2(w0, wpx), ww = add2(wmx, w0), wn = add2(w0, wpy), ws = add2(wmy, w0);
+    const float2 wt = add2(w0, wzp), wb = add2(w0, wzm);
+    const float2 ue = fma2(u0, at, mul2(P(0, 0, 0, 1), bt));
+    const float2 uw = fma2(P(0, -1, 0, 0), at, mul2(P(0, -1, 0, 1), bt));
+    const float2 vn = fma2(v0, at, mul2(P(1, 0, 0, 1), bt));
+    const float2 vs = fma2(P(1, 0, -1, 0), at, mul2(P(1, 0, -1, 1), bt));
+    float2 conv = mul2(qx, sub2(mul2(ue, we), mul2(uw, ww)));
+    conv = fma2(qy, sub2(mul2(vn, wn), mul2(vs, ws)), conv);
+    conv = fma2(f2(z.cw), mul2(add2(wt, wb), sub2(wt, wb)), conv);
+    if (CRF) conv = fma2(f2(K.crf), sub2(we, ww), conv);
+    const float2 zt = fma2(f2(z.wt), wzp, fma2(f2(z.wb), wzm, mul2(f2(-wtb), w0)));
+    const float2 visc = fma2(rx, fma2(w0, m2, add2(wpx, wmx)), fma2(ry, fma2(w0, m2, add2(wpy, wmy)), zt));
+    r.w = sub2(visc, conv);
+  }
+  return r;
+}
+
 // Operand access from the three plane slots (k-1, k, k+1) of each field.
 struct SmemAcc32 {
   const float *base;
   int off[3];  // slot offset of planes k-1, k, k+1 plus the thread's point
   __device__ __forceinline__ float operator()(int f, int di, int dj, int dk) const {
     return base[f * NSLOT * SLOT + off[dk + 1] + di + dj * HX];
+  }
+};
+
+// Operand access from the three plane slots (k-1, k, k+1) of each field for
+// both rows of the thread: {row j, row j+1}
+struct SmemAcc32x2 {
+  const float *base;
+  int off[3];
+  __device__ __forceinline__ float2 operator()(int f, int di, int dj, int dk) const {
+    const float *q = base + f * NSLOT * SLOT + off[dk + 1] + di + dj * HX;
+    return make_float2(q[0], q[HX]);
   }
 };
 
@@ -195,7 +280,7 @@ struct BulkMean {
 // base values of each interior plane of its chunk (the interior rows of u, v,
 // w, with the operand planes and on the same barrier) into a second ring.
 template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *TY, 2)
+__global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
            const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap bu,
            const __grid_constant__ CUtensorMap bv, const __grid_constant__ CUtensorMap bw, Geo g,
@@ -290,36 +375,45 @@ __global__ void __launch_bounds__(RX *TY, 2)
     if (!ok_s[par]) break;  // the whole block leaves the loop together
     if (act_a) {
       const Coef z = zc[k - kb];
-      SmemAcc32 a;
-      a.base = slot;
-      a.off[0] = sm * SLOT + o;
-      a.off[1] = s0 * SLOT + o;
-      a.off[2] = sp * SLOT + o;
-      SmemAcc32 b = a;
-      b.off[0] += HX;
-      b.off[1] += HX;
-      b.off[2] += HX;
-      const Rhs3f ra = momentum_rhs32<CRF>(K, z, a);
-      const Rhs3f rb = momentum_rhs32<CRF>(K, z, b);
-      float va[3] = {a(0, 0, 0, 0), a(1, 0, 0, 0), a(2, 0, 0, 0)};
-      float vb[3] = {b(0, 0, 0, 0), b(1, 0, 0, 0), b(2, 0, 0, 0)};
-      const float fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
-      float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};  // RK2 base values
-      if (STAGE == 2) {
+      float va[3], vb[3];
+      if constexpr (STAGE == 2) {
+        // packed FP32x2: both rows per instruction (RK2 runs at 2 blocks per
+        // SM either way; its arithmetic chains are what the packing shortens)
+        SmemAcc32x2 a2;
+        a2.base = slot;
+        a2.off[0] = sm * SLOT + o;
+        a2.off[1] = s0 * SLOT + o;
+        a2.off[2] = sp * SLOT + o;
+        const Rhs3x2 r2 = momentum_rhs32x2<CRF>(K, z, z.vt + z.vb, z.wt + z.wb, a2);
+        const float2 q2[3] = {a2(0, 0, 0, 0), a2(1, 0, 0, 0), a2(2, 0, 0, 0)};
+        const float2 f2v[3] = {r2.u, r2.v, r2.w};
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          ba[d] = bslot[d * NSLOT * BPLANE + s0 * BPLANE + ob];
-          bb[d] = bslot[d * NSLOT * BPLANE + s0 * BPLANE + ob + HX];
+          const float *bs = bslot + d * NSLOT * BPLANE + s0 * BPLANE + ob;  // RK2 base values
+          const float2 x = mul2(add2(fma2(f2(dt), f2v[d], q2[d]), make_float2(bs[0], bs[HX])), f2(0.5f));
+          va[d] = x.x;
+          vb[d] = x.y;
         }
-      }
+      } else {
+        // scalar (fewer registers: RK1 keeps 3 blocks per SM)
+        SmemAcc32 a;
+        a.base = slot;
+        a.off[0] = sm * SLOT + o;
+        a.off[1] = s0 * SLOT + o;
+        a.off[2] = sp * SLOT + o;
+        SmemAcc32 b = a;
+        b.off[0] += HX;
+        b.off[1] += HX;
+        b.off[2] += HX;
+        const Rhs3f ra = momentum_rhs32<CRF>(K, z, a);
+        const Rhs3f rb = momentum_rhs32<CRF>(K, z, b);
+        const float fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
+        const float qa[3] = {a(0, 0, 0, 0), a(1, 0, 0, 0), a(2, 0, 0, 0)};
+        const float qb[3] = {b(0, 0, 0, 0), b(1, 0, 0, 0), b(2, 0, 0, 0)};
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        if (STAGE == 1) {
-          va[d] = fmaf(dt, fa[d], va[d]);
-          vb[d] = fmaf(dt, fb[d], vb[d]);
-        } else {
-          va[d] = (fmaf(dt, fa[d], va[d]) + ba[d]) * 0.5f;
-          vb[d] = (fmaf(dt, fb[d], vb[d]) + bb[d]) * 0.5f;
+        for (int d = 0; d < 3; ++d) {
+          va[d] = fmaf(dt, fa[d], qa[d]);
+          vb[d] = fmaf(dt, fb[d], qb[d]);
         }
       }
       if (kMean) {
