@@ -12,7 +12,9 @@ the mixed-precision form on the same workload (FP32 fields) with its
 speed-up over the FP64 form and its 10-step error against it; its
 "ensemble" object a batch of 16 uneven channels (64x48x48 to 256x192x128,
 mixed form) stepped as one graph launch per ensemble step, split over the
-GPUs by the cost model when N > 1.
+GPUs by the cost model when N > 1; its "spinup" object the steps and
+seconds to a stationary turbulent state at 256x192x128, Re_tau 180, from the
+learned initialiser against the laminar fallbacks (rank 0).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -442,6 +444,48 @@ def run_ensemble(args, world, rank, local, pg):
     return out
 
 
+def run_spinup(args, local):
+    """Spin-up to a stationary turbulent state at 256 x 192 x 128, Re_tau 180
+    (mixed form, CFL 0.4): from the learned initialiser's proposal, from the
+    laminar + noise + vortices fallback, and from the reference's laminar +
+    noise recipe (capped at 7x the generator's steps; it relaminarises)."""
+    from powerllel_channel_sycl_b200 import Channel
+    from powerllel_channel_sycl_b200 import learned as L
+    rt = 180.0
+    spec = dict(nx=256, ny=192, nz=128, re=L.re_from_re_tau(rt))
+    gen = L.load_weights(device=local)
+    out = {"re_tau": rt, "grid": "256x192x128", "precision": "mixed", "cfl": 0.4,
+           "criterion": "Re_tau and mean u profile over a 2000-step window within 1% of the "
+                        "previous window's, Re_tau >= 0.75 x target"}
+    runs = {}
+    for method in ("generator", "vortices", "laminar_noise"):
+        ch = Channel(L.channel_params_for(spec, vortices=0.15 if method == "vortices" else 0.0),
+                     device=local)
+        ch.initFlow()
+        t0 = time.perf_counter()
+        if method == "generator":
+            gen.propose(ch, rt, seed=1)
+        t_init = time.perf_counter() - t0
+        cap = 60000 if method != "laminar_noise" else 7 * max(runs["generator"]["steps"] or 0, 2000)
+        r = L.spinup(ch, cap, min_re_tau=0.75 * rt)
+        runs[method] = {"steps": r["steps"], "steps_run": r["steps_run"],
+                        "wall_s": r["wall_s"] + t_init, "re_tau_end": float(r["re_tau"][-1])}
+        ch.close()
+    gen.close()
+    out["runs"] = runs
+    g = runs["generator"]
+    if g["steps"]:
+        if runs["vortices"]["steps"]:
+            out["steps_ratio_vs_vortices"] = runs["vortices"]["steps"] / g["steps"]
+            out["wall_ratio_vs_vortices"] = runs["vortices"]["wall_s"] / g["wall_s"]
+        lam = runs["laminar_noise"]
+        # the laminar + noise run never became turbulent within its cap: a lower bound
+        out["steps_ratio_vs_laminar_noise_at_least"] = (
+            lam["steps_run"] / g["steps"] if lam["steps"] is None else lam["steps"] / g["steps"])
+        out["wall_ratio_vs_laminar_noise_at_least"] = lam["wall_s"] / g["wall_s"]
+    return out
+
+
 def run_ours(args, wl, rank, world, local, pg):
     import torch  # noqa: F401  (device init; the library owns its stream)
     from powerllel_channel_sycl_b200 import Channel
@@ -544,6 +588,8 @@ def run_ours(args, wl, rank, world, local, pg):
         ens = run_ensemble(args, world, rank, local, pg)
         line["ensemble"] = ens
         line["gpu_launches"] += args.steps * ens["members_this_rank"] * len(MIXED_BYTES_PER_POINT)
+    if rank == 0 and not args.no_spinup:
+        line["spinup"] = run_spinup(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, nsteps, threads = cpu_oracle_rate(wl, budget_s=args.cpu_budget, max_steps=1,
                                                 warmup=0)
@@ -569,6 +615,8 @@ def main():
                     help="skip the mixed-precision measurement")
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the 16-channel ensemble measurement")
+    ap.add_argument("--no-spinup", action="store_true",
+                    help="skip the learned-initialiser spin-up comparison")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -135,6 +135,10 @@ int plc_params_read_json(const char *path, plc_params *prm);
 int plc_params_check(const plc_params *prm);
 
 /* ---- context: owns the mesh, fields, Poisson state and CUDA stream ---- */
+/* The FFT tile sizes are timed per context at creation (plc_fft_tiles);
+ * the environment variables PLC_FFT_TILES (FP64 form) and PLC_FFT_TILES_F32
+ * (mixed form), "xf,x,y" line pairs per tile, pin them instead (a profiler
+ * distorts the event timings the autotuner compares). */
 /* initMesh (src/mod_mesh.cc:13-76) + allocVariables (mod_variables.cc:4-12)
  * + init_poisson_solver (mod_poisson_solver.cc:180-315).  dzf_global (nz+2
  * entries, k = 0..nz+1) may be NULL, in which case the mesh is generated

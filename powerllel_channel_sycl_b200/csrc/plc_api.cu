@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -535,7 +536,20 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   if (int rc = upload_step_consts(c, prm->dt)) return fail(rc);
   if (int rc = init_poisson(c, c->h_dzf_global.data())) return fail(rc);
   // the fields hold zeros: time the transforms' tile sizes on them
-  if ((e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
+  // PLC_FFT_TILES / PLC_FFT_TILES_F32 = "xf,x,y" (line pairs per tile of the
+  // forward x, backward x and y transforms) replace the timing of the FP64 /
+  // FP32 transforms: a profiler distorts the event times the autotuner
+  // compares, so a profiled run pins the tiles an unprofiled run chose.
+  bool pinned = false;
+  if (const char *env = getenv(c->mixed ? "PLC_FFT_TILES_F32" : "PLC_FFT_TILES")) {
+    int xf = 0, xb = 0, y = 0;
+    if (sscanf(env, "%d,%d,%d", &xf, &xb, &y) != 3 || xf < 1 || xb < 1 || y < 1 ||
+        (c->ny / 2) % xf || (c->ny / 2) % xb || (c->nx / 2) % y || (c->mixed && y % 2) ||
+        fft_set_lines(c, xf, xb, y) != cudaSuccess)
+      return fail(set_error(c, PLC_ERR_ARG, std::string("invalid FFT tiles in the environment: ") + env));
+    pinned = true;
+  }
+  if (!pinned && (e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
   c->tuned_lines[0] = c->fft_lines_xf;
   c->tuned_lines[1] = c->fft_lines_x;
   c->tuned_lines[2] = c->fft_lines_y;

@@ -276,3 +276,21 @@ def test_step_matches_module_sequence():
 def test_kernels_per_step():
     case, ch = make_pair(32, 24, 16)
     assert ch.kernels_per_step == 9
+
+
+def test_fft_tiles_pinned_by_environment(monkeypatch):
+    """PLC_FFT_TILES / PLC_FFT_TILES_F32 replace the tile autotuner."""
+    from powerllel_channel_sycl_b200 import Channel, PlcError
+    kw = case_kwargs(64, 48, 32)
+    monkeypatch.setenv("PLC_FFT_TILES", "2,1,4")
+    ch = Channel(channel_params(**kw))
+    assert ch.fft_tiles == {"x_fwd": 2, "x_bwd": 1, "y": 4}
+    monkeypatch.setenv("PLC_FFT_TILES", "5,1,1")  # 5 does not divide ny/2 = 24
+    with pytest.raises(PlcError):
+        Channel(channel_params(**kw))
+    monkeypatch.delenv("PLC_FFT_TILES")
+    prm = channel_params(**kw)
+    prm.precision = 1
+    monkeypatch.setenv("PLC_FFT_TILES_F32", "3,3,3")  # odd y tiles are refused in FP32
+    with pytest.raises(PlcError):
+        Channel(prm)
