@@ -603,18 +603,34 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
     const V *Z = fft_run_n<N, true>(A, B, nl, LS, P);
+    // rows j = j0 + 2l + 1 (a) and j + 1 (b) of plane k + 1; with FUSE_BC
+    // also their periodic images (x ends of each row, the y image row) and
+    // the zero-gradient ghost plane (updateBoundP): row-level decisions, so
+    // an interior element costs one store and one compare
+    const int kk = k + 1;
+    const int kimg = !FUSE_BC ? -1 : (kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1));
     for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
       const int l = e / n, t = e - l * n;
       const V z = Z[l * LS + padi<V>(t)];
-      const T a = scale * z.x, b = scale * z.y;
-      const int i = t + 1, ja = j0 + 2 * l + 1, kk = k + 1;
-      if (FUSE_BC) {
-        store_with_halo(p, g, i, ja, kk, a, BC_ZEROGRAD, T(0));
-        store_with_halo(p, g, i, ja + 1, kk, b, BC_ZEROGRAD, T(0));
-      } else {
-        const long long ca = g.at(i, ja, kk);
-        p[ca] = a;
-        p[ca + g.X] = b;
+      const T ab[2] = {scale * z.x, scale * z.y};
+      const int i = t + 1;
+      const int iimg = !FUSE_BC ? -1 : (i == g.nx ? 0 : (i == 1 ? g.nx + 1 : -1));
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = j0 + 2 * l + 1 + h;
+        const int jimg = !FUSE_BC ? -1 : (j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1));
+        const T v = ab[h];
+        auto row = [&](int jj, int kq) {
+          T *r = p + (long long)jj * g.X + (long long)kq * g.XY;
+          r[i] = v;
+          if (iimg >= 0) r[iimg] = v;
+        };
+        row(j, kk);
+        if (jimg >= 0) row(jimg, kk);
+        if (kimg >= 0) {
+          row(j, kimg);
+          if (jimg >= 0) row(jimg, kimg);
+        }
       }
     }
   }
