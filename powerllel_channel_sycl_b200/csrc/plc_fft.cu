@@ -106,6 +106,22 @@ template <class V>
 __device__ __forceinline__ V csub(V a, V b) {
   return mk<V>(a.x - b.x, a.y - b.y);
 }
+// FP32 complex arithmetic on Blackwell's packed FP32x2 instructions (FADD2,
+// FMUL2, FFMA2): a complex add or subtract is one instruction, a complex
+// product two, instead of two and four scalar ones.  The FFT butterflies are
+// mostly these operations; FP64 keeps the scalar forms above.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);  // exact product, one rounding
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);  // (ax bx, ax by)
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  const float2 t = __fmul2_rn(a, make_float2(b.x, b.x));      // (ax bx, ay bx)
+  return __ffma2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y), t);
+}
 // multiply by -i (forward) or +i (inverse)
 template <bool INV, class V>
 __device__ __forceinline__ V rot90(V a) {
