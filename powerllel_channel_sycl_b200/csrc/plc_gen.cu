@@ -491,6 +491,7 @@ struct plc_gen {
   float sc_mean = 1.f, sc_var = 1.f;
   long long adam_t = 0;
   float *coarse = nullptr;              // [Z][Y][X][16], plc_gen_stats_of
+  int *derr = nullptr;                  // device error word of the tcgen05 kernels
   std::string err;
 };
 
@@ -530,32 +531,99 @@ void gen_free(plc_gen *gn) {
                   (void *)gn->bufA, (void *)gn->bufB, (void *)gn->dbf, (void *)gn->r,
                   (void *)gn->tidx, (void *)gn->coef, (void *)gn->means, (void *)gn->loss,
                   (void *)gn->stats, (void *)gn->targets, (void *)gn->target_re,
-                  (void *)gn->coarse})
+                  (void *)gn->coarse, (void *)gn->derr})
     cudaFree(q);
   if (gn->stream) cudaStreamDestroy(gn->stream);
 }
 
+// forward convolution and input gradient: the tcgen05 kernel, 128 voxels x
+// all output channels per block
+template <int N>
+cudaError_t conv_tc(plc_gen *gn, Shape s, const bf16 *x, const bf16 *w, float *y, int ci) {
+  const unsigned gx = (unsigned)((s.voxels() + kTcM - 1) / kTcM);
+  k_conv3d_tc<N><<<gx, 128, tc_smem_bytes<N>(), gn->stream>>>(s, x, w, y, ci, gn->derr);
+  return cudaGetLastError();
+}
+
 int conv(plc_gen *gn, Shape s, const bf16 *x, const bf16 *w, float *y, int ci, int co) {
-  const unsigned gx = (unsigned)((s.voxels() + kConvBM - 1) / kConvBM);
-  if (co % 32 == 0)
-    k_conv3d<32><<<dim3(gx, co / 32), 128, 0, gn->stream>>>(s, x, w, y, ci, co);
-  else
-    k_conv3d<16><<<dim3(gx, co / 16), 128, 0, gn->stream>>>(s, x, w, y, ci, co);
-  GEN_CUDA(gn, cudaGetLastError());
+  cudaError_t e;
+  switch (co) {
+    case 16: e = conv_tc<16>(gn, s, x, w, y, ci); break;
+    case 32: e = conv_tc<32>(gn, s, x, w, y, ci); break;
+    case 48: e = conv_tc<48>(gn, s, x, w, y, ci); break;
+    case 64: e = conv_tc<64>(gn, s, x, w, y, ci); break;
+    case 80: e = conv_tc<80>(gn, s, x, w, y, ci); break;
+    case 96: e = conv_tc<96>(gn, s, x, w, y, ci); break;
+    case 112: e = conv_tc<112>(gn, s, x, w, y, ci); break;
+    case 128: e = conv_tc<128>(gn, s, x, w, y, ci); break;
+    default: return gen_error(gn, PLC_ERR_ARG, "convolution channels must be a multiple of 16 <= 128");
+  }
+  GEN_CUDA(gn, e);
   return PLC_OK;
 }
 
-int wgrad(plc_gen *gn, Shape s, const bf16 *dy, const bf16 *x, float *dw, int ci, int co) {
+cudaError_t conv_configure() {
+  cudaError_t e = cudaSuccess;
+  auto one = [&](auto kern, size_t bytes) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  };
+  one(k_conv3d_tc<16>, tc_smem_bytes<16>());
+  one(k_conv3d_tc<32>, tc_smem_bytes<32>());
+  one(k_conv3d_tc<48>, tc_smem_bytes<48>());
+  one(k_conv3d_tc<64>, tc_smem_bytes<64>());
+  one(k_conv3d_tc<80>, tc_smem_bytes<80>());
+  one(k_conv3d_tc<96>, tc_smem_bytes<96>());
+  one(k_conv3d_tc<112>, tc_smem_bytes<112>());
+  one(k_conv3d_tc<128>, tc_smem_bytes<128>());
+  one(k_conv3d_wgrad_tc<16>, tc_smem_bytes<16, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<32>, tc_smem_bytes<32, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<48>, tc_smem_bytes<48, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<64>, tc_smem_bytes<64, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<80>, tc_smem_bytes<80, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<96>, tc_smem_bytes<96, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<112>, tc_smem_bytes<112, kWgG, kWgNB>());
+  one(k_conv3d_wgrad_tc<128>, tc_smem_bytes<128, kWgG, kWgNB>());
+  return e;
+}
+
+// the device error word of the tcgen05 kernels (a bounded wait that gave up)
+int check_device_error(plc_gen *gn) {
+  int flag = 0;
+  GEN_CUDA(gn, cudaMemcpyAsync(&flag, gn->derr, sizeof(int), cudaMemcpyDeviceToHost, gn->stream));
+  GEN_CUDA(gn, cudaStreamSynchronize(gn->stream));
+  if (flag) return gen_error(gn, PLC_ERR_CUDA, "a tensor-core convolution's bounded wait timed out");
+  return PLC_OK;
+}
+
+template <int N>
+cudaError_t wgrad_tc(plc_gen *gn, Shape s, const bf16 *dy, const bf16 *x, float *dw, int co) {
   const long long M = s.voxels();
-  // about 4 waves of blocks over the 27 taps and channel tiles
-  const int tiles = ((co + 63) / 64) * ((ci + 63) / 64);
-  long long splits = std::max(1ll, std::min((long long)(148 * 8) / (27 * tiles) + 1, M / 64));
+  // about 8 blocks per SM over the 27 taps, at least 16 voxels each
+  long long splits = std::max(1ll, std::min((long long)(148 * 8) / 27 + 1, (M + 15) / 16));
   long long chunk = (M + splits - 1) / splits;
   chunk = (chunk + 15) / 16 * 16;
   splits = (M + chunk - 1) / chunk;
-  k_conv3d_wgrad<<<dim3((unsigned)splits, tiles, 27), 128, 0, gn->stream>>>(s, dy, x, dw, ci, co,
-                                                                          chunk);
-  GEN_CUDA(gn, cudaGetLastError());
+  k_conv3d_wgrad_tc<N><<<dim3((unsigned)splits, 1, 27), 128, tc_smem_bytes<N, kWgG, kWgNB>(), gn->stream>>>(
+      s, dy, x, dw, co, chunk, gn->derr);
+  return cudaGetLastError();
+}
+
+// weight gradient on the tensor cores: M = co (zero-padded to 128), N = ci
+int wgrad(plc_gen *gn, Shape s, const bf16 *dy, const bf16 *x, float *dw, int ci, int co) {
+  if (co > 128 || co % 16) return gen_error(gn, PLC_ERR_ARG, "weight gradient: co must be a multiple of 16 <= 128");
+  cudaError_t e;
+  switch (ci) {
+    case 16: e = wgrad_tc<16>(gn, s, dy, x, dw, co); break;
+    case 32: e = wgrad_tc<32>(gn, s, dy, x, dw, co); break;
+    case 48: e = wgrad_tc<48>(gn, s, dy, x, dw, co); break;
+    case 64: e = wgrad_tc<64>(gn, s, dy, x, dw, co); break;
+    case 80: e = wgrad_tc<80>(gn, s, dy, x, dw, co); break;
+    case 96: e = wgrad_tc<96>(gn, s, dy, x, dw, co); break;
+    case 112: e = wgrad_tc<112>(gn, s, dy, x, dw, co); break;
+    case 128: e = wgrad_tc<128>(gn, s, dy, x, dw, co); break;
+    default: return gen_error(gn, PLC_ERR_ARG, "weight gradient: ci must be a multiple of 16 <= 128");
+  }
+  GEN_CUDA(gn, e);
   return PLC_OK;
 }
 
@@ -742,6 +810,10 @@ int plc_gen_create(const plc_gen_config *cfg, int device, plc_gen **out) {
     const int sh = kLevels - 1 - l;
     gn->lv[l] = Shape{C.batch, C.nz >> sh, C.ny >> sh, C.nx >> sh};
   }
+  if (gn->lv[kLevels - 1].voxels() * 128 >= (1ll << 31)) {  // 32-bit voxel and element indices
+    gn->err = "generator grid x batch too large";
+    return fail(PLC_ERR_SIZE);
+  }
   // layers and parameter layout
   long long off = 0;
   auto add = [&](int ci, int co, int level, bool act) {
@@ -800,7 +872,9 @@ int plc_gen_create(const plc_gen_config *cfg, int device, plc_gen **out) {
       (e = dalloc(&gn->r, C.batch)) || (e = dalloc(&gn->tidx, C.batch)) ||
       (e = dalloc(&gn->coef, bzn * PLC_GEN_NSTAT)) || (e = dalloc(&gn->means, bzn * 3)) ||
       (e = dalloc(&gn->stats, bzn * PLC_GEN_NSTAT)) ||
-      (e = dalloc(&gn->coarse, (long long)top.Z * top.Y * top.X * kOutC))) {
+      (e = dalloc(&gn->coarse, (long long)top.Z * top.Y * top.X * kOutC)) ||
+      (e = dalloc(&gn->derr, 1)) || (e = cudaMemset(gn->derr, 0, sizeof(int))) ||
+      (e = conv_configure())) {
     gn->err = std::string("generator allocation: ") + cudaGetErrorString(e);
     return fail(PLC_ERR_NOMEM);
   }
@@ -911,6 +985,7 @@ int plc_gen_forward(plc_gen *gn, const double *re_tau, unsigned long long latent
   if (!gn || !re_tau) return gen_error(gn, PLC_ERR_ARG, "null argument");
   if (int rc = upload_r(gn, re_tau)) return rc;
   if (int rc = forward(gn, latent_seed)) return rc;
+  if (int rc = check_device_error(gn)) return rc;
   if (h_out) {
     const Shape s = gn->lv[kLevels - 1];
     std::vector<float> o(s.voxels() * kOutC);
@@ -955,6 +1030,7 @@ int plc_gen_loss_grad(plc_gen *gn, const int *target_idx, const double *re_tau,
   GEN_CUDA(gn, cudaMemsetAsync(gn->g, 0, gn->nparams * sizeof(float), gn->stream));
   if (int rc = forward(gn, latent_seed)) return rc;
   if (int rc = backward(gn, gn->loss)) return rc;
+  if (int rc = check_device_error(gn)) return rc;
   GEN_CUDA(gn, cudaMemcpyAsync(loss, gn->loss, sizeof(double), cudaMemcpyDeviceToHost, gn->stream));
   if (h_grads)
     GEN_CUDA(gn, cudaMemcpyAsync(h_grads, gn->g, gn->nparams * sizeof(float), cudaMemcpyDeviceToHost,
@@ -986,6 +1062,7 @@ int plc_gen_train(plc_gen *gn, int iters, double lr, unsigned long long seed, do
     if (int rc = backward(gn, gn->loss + it)) return rc;
     if (int rc = adam_step(gn, (float)(lr * f))) return rc;
   }
+  if (int rc = check_device_error(gn)) return rc;
   if (h_loss)
     GEN_CUDA(gn, cudaMemcpyAsync(h_loss, gn->loss, iters * sizeof(double), cudaMemcpyDeviceToHost,
                                  gn->stream));
@@ -1034,6 +1111,7 @@ int plc_gen_propose(plc_gen *gn, plc_ctx *c, double re_tau, unsigned long long l
   std::vector<double> re(gn->cfg.batch, re_tau);
   if (int rc = upload_r(gn, re.data())) return rc;
   if (int rc = forward(gn, latent_seed)) return rc;
+  if (int rc = check_device_error(gn)) return rc;
   std::vector<int> lo, hi;
   std::vector<double> wt;
   z_map(c, top.Z, lo, hi, wt);
