@@ -505,6 +505,8 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     e = cudaMemset(ptr, 0, n * esize);
     if (e != cudaSuccess) return fail(cuda_status(c, e, "cudaMemset field"));
   }
+  if (!c->mixed && (e = rk_tma_configure()) != cudaSuccess)
+    return fail(cuda_status(c, e, "rk_tma_configure"));
   if (c->mixed) {
     if ((e = rk32_configure()) != cudaSuccess) return fail(cuda_status(c, e, "rk32_configure"));
     // one partial per block of the fused RK2

@@ -174,6 +174,7 @@ cudaError_t launch_to_f64(const plc_ctx *c, const float *src, double *dst, long 
                           int pitch, cudaStream_t s);
 // shared-memory limit of the FP32 RK kernels on the current device
 cudaError_t rk32_configure();
+cudaError_t rk_tma_configure();
 // blocks of the FP32 RK grid
 long long rk32_blocks(const plc_ctx *c);
 // per-plane coefficient rows of the FP32 RK kernels, rk32_coef_floats() per plane

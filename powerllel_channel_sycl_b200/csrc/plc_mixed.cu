@@ -60,6 +60,9 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
                "r"(bytes)
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -251,7 +254,7 @@ struct SmemAcc32x2 {
 
 size_t rk32_smem_bytes(int stage) {
   return (size_t)3 * NSLOT * SLOT * 4 + (stage == 2 ? (size_t)3 * NSLOT * BPLANE * 4 : 0) +
-         (size_t)(KCHUNK + 2) * NCOEF * 4 + NSLOT * 8 + 128;
+         (size_t)(KCHUNK + 2) * NCOEF * 4 + 2 * NSLOT * 8 + 128;
 }
 
 // Bulk mean of the forced components, summed by the mixed form's fused RK2
@@ -273,12 +276,15 @@ struct BulkMean {
 //
 // A block of 32 x 8 threads owns a 32 x 16 tile of interior columns; each
 // thread computes the two rows j, j+1 of its column pair (the operands the two
-// points share are read from shared memory once).  Plane k+3 is copied into
-// the slot of plane k-3 while plane k is computed: that slot was last read in
-// iteration k-2, which every thread finished before it reached the barrier of
-// iteration k-1, so one barrier per plane orders the ring.  RK2 also brings the
-// base values of each interior plane of its chunk (the interior rows of u, v,
-// w, with the operand planes and on the same barrier) into a second ring.
+// points share are read from shared memory once).  The ring has no block-wide
+// barrier: every slot has a "full" mbarrier (the copy's transaction bytes) that
+// each thread waits on before it reads the plane, and an "empty" mbarrier on
+// which each warp arrives once it has read the plane for the last time (at the
+// end of iteration p+1 for plane p).  Thread 0 copies plane k+3 into the slot
+// of plane k+3-NSLOT = k-3 after that slot's empty barrier completed, so warps
+// drift apart by up to two planes without stalling the others.  RK2 also
+// brings the base values of each interior plane of its chunk (the interior
+// rows of u, v, w, on the same full barrier) into a second ring.
 template <int STAGE, bool FUSE, bool CRF>
 __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
@@ -293,8 +299,8 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
   float *bslot = slot + 3 * NSLOT * SLOT;  // RK2 base ring (3 * NSLOT * BPLANE)
   Coef *zc = reinterpret_cast<Coef *>(bslot + (STAGE == 2 ? 3 * NSLOT * BPLANE : 0));
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
-  __shared__ int ok_s[2];  // by iteration parity: a fast thread 0 cannot overwrite a flag
-                           // that a slow thread has still to read
+  unsigned long long *empty = bar + NSLOT;
+  constexpr unsigned kWarps = RX * TY / 32;
 
   constexpr bool kMean = (STAGE == 2 && FUSE);
   float msum[3] = {0.f, 0.f, 0.f};  // kMean: the thread's dz-weighted sums
@@ -321,19 +327,24 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
       tma_load_plane(bslot + 2 * NSLOT * BPLANE + s * BPLANE, &bw, x0, y0 + 1, p, &bar[s]);
     }
   };
-  auto wait_plane = [&](int p) -> bool {  // thread 0 only
+  // bounded waits for plane p's copy to land (full) or to be read by every
+  // warp for the last time (empty)
+  auto wait_on = [&](unsigned long long *b, int p, long long limit) -> bool {
     const int rel = p - (kb - 1);
-    const int s = rel % NSLOT;
     const unsigned parity = (unsigned)((rel / NSLOT) & 1);
-    for (long long it = 0; it < kWaitLimit; ++it)
-      if (mbar_try_wait(&bar[s], parity)) return true;
+    for (long long it = 0; it < limit; ++it)
+      if (mbar_try_wait(&b[rel % NSLOT], parity)) return true;
     return false;
   };
 
+  int issued = min(kb + 2, plast);  // thread 0: the last plane copied
   if (tid == 0) {
-    for (int s = 0; s < NSLOT; ++s) mbar_init(&bar[s], 1);
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&bar[s], 1);
+      mbar_init(&empty[s], kWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (int p = kb - 1; p <= min(kb + 2, plast); ++p) issue(p);
+    for (int p = kb - 1; p <= issued; ++p) issue(p);
   }
   // coefficient rows of the block's planes (and, for the bulk mean, dzf/lz)
   __shared__ float zl[KCHUNK];
@@ -347,32 +358,26 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
   long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
   const int ob = (2 * ty) * HX + (tx + 1);  // point a in a base slot
   const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
+  const bool xy_edge = (ha.dx | ha.dy | hb.dx | hb.dy) != 0;  // images in x or y
   const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
   int sm = 0, s0 = 1, sp = 2;                  // slots of planes k-1, k, k+1
   for (int k = kb; k <= ke; ++k) {
-    const int par = (k - kb) & 1;
-    if (tid == 0) {
-      bool ok = true;
-      if (k + 3 <= plast) {
+    bool ok = true;
+    if (tid == 0 && k + 3 <= plast) {
+      // the slot of plane k+3 last held plane k+3-NSLOT
+      if (k + 3 - NSLOT >= kb - 1) ok = wait_on(empty, k + 3 - NSLOT, kWaitLimit);
+      if (ok) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(k + 3);
-      }
-      if (k == kb) ok = wait_plane(kb - 1) && wait_plane(kb);
-      ok = ok && wait_plane(k + 1);
-      ok_s[par] = ok ? 1 : 0;
-      if (!ok) {
-        atomicExch(err, 1);
-        // give the copies still in flight a bounded chance to land before
-        // the block leaves
-        for (int p = k + 2; p <= min(k + 3, plast); ++p) {
-          const int rel = p - (kb - 1);
-          for (int it = 0; it < (1 << 20); ++it)
-            if (mbar_try_wait(&bar[rel % NSLOT], (unsigned)((rel / NSLOT) & 1))) break;
-        }
+        issued = k + 3;
       }
     }
-    __syncthreads();
-    if (!ok_s[par]) break;  // the whole block leaves the loop together
+    if (ok && k == kb) ok = wait_on(bar, kb - 1, kWaitLimit) && wait_on(bar, kb, kWaitLimit);
+    ok = ok && wait_on(bar, k + 1, kWaitLimit);
+    if (!ok) {
+      atomicExch(err, 1);
+      break;  // the other threads' waits run out as well
+    }
     if (act_a) {
       const Coef z = zc[k - kb];
       float va[3], vb[3];
@@ -427,7 +432,7 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
             msum[d] = fmaf(x, dzl, msum[d]);
           }
       }
-      if (FUSE) {
+      if (FUSE && (xy_edge || k == 1 || k == g.nz)) {
         store_point(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
         store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
         store_point(ow, g, ha, c, k, va[2], BC_FACE, 0.f);
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
           store_point(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.f);
           store_point(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.f);
         }
-      } else {
+      } else {  // no image or ghost to write
         ou[c] = va[0];
         ov[c] = va[1];
         ow[c] = va[2];
@@ -448,10 +453,18 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
       }
     }
 
+    // this warp is done with plane k-1 (slot sm)
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(&empty[sm]);
     sm = s0;
     s0 = sp;
     sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
     c += XY;
+  }
+  if (tid == 0) {
+    // no copy may still be writing into shared memory when the block leaves
+    // (after an error; on the normal path every copy has been waited for)
+    for (int p = max(kb - 1, issued - NSLOT + 1); p <= issued; ++p) wait_on(bar, p, 1 << 20);
   }
   if constexpr (kMean) {
     __shared__ float red[RX * TY / 32][3];

@@ -50,19 +50,32 @@ struct GlobalAcc {
   }
 };
 
+// Wall-normal metric factors of plane k used by the momentum right-hand
+// side: dzf(k-1..k+1), 1/dzf(k..k+1), 1/dzc(k-1..k).
+struct alignas(16) ZMetric {
+  double dzf_m, dzf_0, dzf_p, dzfi_0, dzfi_p, dzci_m, dzci_0, pad;
+};
+__device__ __forceinline__ ZMetric zmetric(const Geo &g, int k) {
+  return ZMetric{__ldg(g.dzf + k - 1),     __ldg(g.dzf + k),         __ldg(g.dzf + k + 1),
+                 __ldg(g.dzf_inv + k),     __ldg(g.dzf_inv + k + 1), __ldg(g.dzc_inv + k - 1),
+                 __ldg(g.dzc_inv + k),     0.0};
+}
+
 // (visc - conv) of the three momentum components at (i,j,k),
 // mod_calcVel.cc:61-125 (the same expression for RK1 and RK2).  Acc gives the
-// operand values at offsets (di,dj,dk) from the point.
-template <class Acc>
-__device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const Acc &a, int k) {
+// operand values at offsets (di,dj,dk) from the point.  CRF = false drops the
+// convecting-frame terms conv + 0.5*u_crf*(qe - qw)/dx, which add an exact
+// zero when u_crf = 0.
+template <bool CRF = true, class Acc>
+__device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const Acc &a,
+                                             const ZMetric &z) {
   const double _dx_inv = g.dx_inv, _dy_inv = g.dy_inv, _re_inv = g.re_inv;
 #define U(di, dj, dk) a.U(di, dj, dk)
 #define V(di, dj, dk) a.V(di, dj, dk)
 #define W(di, dj, dk) a.W(di, dj, dk)
-  const double dzf_m = __ldg(g.dzf + k - 1), dzf_0 = __ldg(g.dzf + k),
-               dzf_p = __ldg(g.dzf + k + 1);
-  const double dzfi_0 = __ldg(g.dzf_inv + k), dzfi_p = __ldg(g.dzf_inv + k + 1);
-  const double dzci_m = __ldg(g.dzc_inv + k - 1), dzci_0 = __ldg(g.dzc_inv + k);
+  const double dzf_m = z.dzf_m, dzf_0 = z.dzf_0, dzf_p = z.dzf_p;
+  const double dzfi_0 = z.dzfi_0, dzfi_p = z.dzfi_p;
+  const double dzci_m = z.dzci_m, dzci_0 = z.dzci_0;
   double uw, ue, us, un, ub, ut;
   double ww, we, ws, wn, wb, wt;
   double vw, ve, vs, vn, vb, vt;
@@ -92,7 +105,7 @@ __device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const A
     dqb = (u000 - u00m) * dzci_m;
     conv = 0.25 * ((ue * ue - uw * uw) * _dx_inv + (un * vn - us * vs) * _dy_inv +
                    (ut * wt - ub * wb) * dzfi_0);
-    conv = conv + 0.5 * u_crf * (ue - uw) * _dx_inv;
+    if (CRF) conv = conv + 0.5 * u_crf * (ue - uw) * _dx_inv;
     visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzfi_0) * _re_inv;
     r.u = visc - conv;
   }
@@ -118,7 +131,7 @@ __device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const A
     dqb = (v000 - v00m) * dzci_m;
     conv = 0.25 * ((ue * ve - uw * vw) * _dx_inv + (vn * vn - vs * vs) * _dy_inv +
                    (wt * vt - wb * vb) * dzfi_0);
-    conv = conv + 0.5 * u_crf * (ve - vw) * _dx_inv;
+    if (CRF) conv = conv + 0.5 * u_crf * (ve - vw) * _dx_inv;
     visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzfi_0) * _re_inv;
     r.v = visc - conv;
   }
@@ -144,7 +157,7 @@ __device__ __forceinline__ Rhs3 momentum_rhs(const Geo &g, double u_crf, const A
     dqb = (w000 - w00m) * dzfi_0;
     conv = 0.25 * ((ue * we - uw * ww) * _dx_inv + (vn * wn - vs * ws) * _dy_inv +
                    (wt * wt - wb * wb) * dzci_0);
-    conv = conv + 0.5 * u_crf * (we - ww) * _dx_inv;
+    if (CRF) conv = conv + 0.5 * u_crf * (we - ww) * _dx_inv;
     visc = ((dqe - dqw) * _dx_inv + (dqn - dqs) * _dy_inv + (dqt - dqb) * dzci_0) * _re_inv;
     r.w = visc - conv;
   }
@@ -168,7 +181,7 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
   if (i > g.nx || j > g.ny) return;
   const double dt = sc->dt;
   const long long c = g.at(i, j, k);
-  const Rhs3 r = momentum_rhs(g, u_crf, GlobalAcc{qu, qv, qw, c, g.X, g.XY}, k);
+  const Rhs3 r = momentum_rhs(g, u_crf, GlobalAcc{qu, qv, qw, c, g.X, g.XY}, zmetric(g, k));
   double nu, nv, nw;
   if (STAGE == 1) {
     nu = qu[c] + dt * r.u;
@@ -195,19 +208,23 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
 //
 // A block owns a 32 x 8 tile of interior (i, j) columns and a chunk of z
 // planes.  For each operand field the (32+2) x (8+2) halo tile of every plane
-// is brought into a 5-slot shared-memory ring by one 3-D bulk tensor copy
-// (cp.async.bulk.tensor, completion on an mbarrier), two planes ahead of the
-// plane being computed, so every operand value crosses HBM once per block and
-// the copies overlap the arithmetic.  Thread 0 issues the copies and waits on
-// the barriers (bounded: on a timeout it raises *err and the whole block
-// leaves together); the expression trees are those of momentum_rhs, so the
-// results are bit-identical to the global-load kernel above.
+// is brought into a 6-slot shared-memory ring by one 3-D bulk tensor copy
+// (cp.async.bulk.tensor, completion on a "full" mbarrier), two planes ahead of
+// the plane being computed, so every operand value crosses HBM once per block
+// and the copies overlap the arithmetic.  There is no block-wide barrier in the
+// march: every thread waits on the full barrier of the plane it is about to
+// read, each warp arrives on the slot's "empty" mbarrier when it has read the
+// plane for the last time, and thread 0 refills a slot once its empty barrier
+// completed.  Every wait is bounded (a timeout raises *err and the thread
+// leaves the march; the others' waits run out in turn).  The expression trees
+// are those of momentum_rhs, so the results are bit-identical to the
+// global-load kernel above.
 // ---------------------------------------------------------------------------
 constexpr int RX = 32, RY = 8;                  // interior tile
 constexpr int HX = RX + 2, HY = RY + 2;         // halo tile (34 x 10)
 constexpr int PLANE = HX * HY;                  // doubles per field-plane
 constexpr int SLOT = ((PLANE * 8 + 127) / 128) * 128 / 8;  // doubles, 128-B aligned
-constexpr int NSLOT = 5;
+constexpr int NSLOT = 6;
 constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 8u;  // three fields per plane
 constexpr long long kWaitLimit = 1ll << 22;            // try_wait polls before giving up
 
@@ -221,6 +238,9 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes)
                : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
   unsigned ok;
@@ -259,9 +279,12 @@ struct SmemAcc {
   }
 };
 
-size_t rk_tma_smem_bytes() { return (size_t)3 * NSLOT * SLOT * 8 + NSLOT * 8 + 128; }
+constexpr int KCHUNK_TMA = 32;  // planes per block (at most)
+size_t rk_tma_smem_bytes() {
+  return (size_t)3 * NSLOT * SLOT * 8 + KCHUNK_TMA * sizeof(ZMetric) + 2 * NSLOT * 8 + 128;
+}
 
-template <int STAGE, bool FUSE>
+template <int STAGE, bool FUSE, bool CRF>
 __global__ void __launch_bounds__(RX *RY, 3)
     k_rk_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
              const __grid_constant__ CUtensorMap mw, Geo g, const StepConst *__restrict__ sc,
@@ -270,8 +293,10 @@ __global__ void __launch_bounds__(RX *RY, 3)
   double *base = reinterpret_cast<double *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
   double *slot_u = base, *slot_v = base + NSLOT * SLOT, *slot_w = base + 2 * NSLOT * SLOT;
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(base + 3 * NSLOT * SLOT);
-  __shared__ int ok_s;
+  ZMetric *zrow = reinterpret_cast<ZMetric *>(base + 3 * NSLOT * SLOT);  // planes kb..ke
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(zrow + KCHUNK_TMA);
+  unsigned long long *empty = bar + NSLOT;
+  constexpr unsigned kWarps = RX * RY / 32;
 
   const int tid = threadIdx.x;
   const int tx = tid & (RX - 1), ty = tid / RX;
@@ -290,20 +315,28 @@ __global__ void __launch_bounds__(RX *RY, 3)
     tma_load_plane(slot_v + s * SLOT, &mv, x0, y0, p, &bar[s]);
     tma_load_plane(slot_w + s * SLOT, &mw, x0, y0, p, &bar[s]);
   };
-  auto wait_plane = [&](int p) -> bool {  // thread 0 only
+  // bounded waits for plane p's copy to land (full) or to be read by every
+  // warp for the last time (empty)
+  auto wait_on = [&](unsigned long long *b, int p, long long limit) -> bool {
     const int rel = p - (kb - 1);
-    const int s = rel % NSLOT;
     const unsigned parity = (unsigned)((rel / NSLOT) & 1);
-    for (long long it = 0; it < kWaitLimit; ++it)
-      if (mbar_try_wait(&bar[s], parity)) return true;
+    for (long long it = 0; it < limit; ++it)
+      if (mbar_try_wait(&b[rel % NSLOT], parity)) return true;
     return false;
   };
 
+  int issued = min(kb + 2, plast);  // thread 0: the last plane copied
   if (tid == 0) {
-    for (int s = 0; s < NSLOT; ++s) mbar_init(&bar[s], 1);
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&bar[s], 1);
+      mbar_init(&empty[s], kWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (int p = kb - 1; p <= min(kb + 2, plast); ++p) issue(p);
+    for (int p = kb - 1; p <= issued; ++p) issue(p);
   }
+  // metric factors of the block's planes, read once (a plane's row is four
+  // 16-byte shared loads, the same for every thread)
+  for (int k = kb + tid; k <= ke; k += blockDim.x) zrow[k - kb] = zmetric(g, k);
   __syncthreads();
 
   const double dt = sc->dt;
@@ -316,31 +349,25 @@ __global__ void __launch_bounds__(RX *RY, 3)
     bw = ow[c];
   }
   const HaloCol hc = halo_col(g, i, j);
+  const bool xy_edge = (hc.dx | hc.dy) != 0;  // the column has periodic images
   const int o = (ty + 1) * HX + (tx + 1);
   for (int k = kb; k <= ke; ++k) {
-    __syncthreads();  // every thread is done with plane k-2's slot
-    if (tid == 0) {
-      bool ok = true;
-      if (k + 3 <= plast) {
+    bool ok = true;
+    if (tid == 0 && k + 3 <= plast) {
+      // the slot of plane k+3 last held plane k+3-NSLOT
+      if (k + 3 - NSLOT >= kb - 1) ok = wait_on(empty, k + 3 - NSLOT, kWaitLimit);
+      if (ok) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(k + 3);
-      }
-      if (k == kb) ok = wait_plane(kb - 1) && wait_plane(kb);
-      ok = ok && wait_plane(k + 1);
-      ok_s = ok ? 1 : 0;
-      if (!ok) {
-        atomicExch(err, 1);
-        // give the copies still in flight a bounded chance to land before
-        // the block leaves
-        for (int p = k + 2; p <= min(k + 3, plast); ++p) {
-          const int rel = p - (kb - 1);
-          for (int it = 0; it < (1 << 20); ++it)
-            if (mbar_try_wait(&bar[rel % NSLOT], (unsigned)((rel / NSLOT) & 1))) break;
-        }
+        issued = k + 3;
       }
     }
-    __syncthreads();
-    if (!ok_s) return;  // the whole block leaves together
+    if (ok && k == kb) ok = wait_on(bar, kb - 1, kWaitLimit) && wait_on(bar, kb, kWaitLimit);
+    ok = ok && wait_on(bar, k + 1, kWaitLimit);
+    if (!ok) {
+      atomicExch(err, 1);
+      break;  // the other threads' waits run out as well
+    }
     double nbu = 0.0, nbv = 0.0, nbw = 0.0;
     if (STAGE == 2 && active && k < ke) {
       nbu = ou[c + XY];
@@ -355,7 +382,7 @@ __global__ void __launch_bounds__(RX *RY, 3)
       a.off[0] = rm * SLOT + o;
       a.off[1] = r0 * SLOT + o;
       a.off[2] = rp * SLOT + o;
-      const Rhs3 r = momentum_rhs(g, u_crf, a, k);
+      const Rhs3 r = momentum_rhs<CRF>(g, u_crf, a, zrow[k - kb]);
       const double qu = a.U(0, 0, 0), qv = a.V(0, 0, 0), qw = a.W(0, 0, 0);
       double nu, nv, nw;
       if (STAGE == 1) {
@@ -367,20 +394,28 @@ __global__ void __launch_bounds__(RX *RY, 3)
         nv = (qv + dt * r.v + bv) * 0.5;
         nw = (qw + dt * r.w + bw) * 0.5;
       }
-      if (FUSE) {
+      if (FUSE && (xy_edge || k == 1 || k == g.nz)) {
         store_point(ou, g, hc, c, k, nu, BC_CENTRED, 0.0 - u_crf);
         store_point(ov, g, hc, c, k, nv, BC_CENTRED, 0.0);
         store_point(ow, g, hc, c, k, nw, BC_FACE, 0.0);
-      } else {
+      } else {  // no image or ghost to write
         ou[c] = nu;
         ov[c] = nv;
         ow[c] = nw;
       }
     }
+    // this warp is done with plane k-1
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(&empty[(k - kb) % NSLOT]);
     bu = nbu;
     bv = nbv;
     bw = nbw;
     c += XY;
+  }
+  if (tid == 0) {
+    // no copy may still be writing into shared memory when the block leaves
+    // (after an error; on the normal path every copy has been waited for)
+    for (int p = max(kb - 1, issued - NSLOT + 1); p <= issued; ++p) wait_on(bar, p, 1 << 20);
   }
 }
 
@@ -1035,14 +1070,39 @@ template <int STAGE, bool FUSE>
 cudaError_t launch_rk_tma(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
                           const CUtensorMap &mw, double u_crf, double *ou, double *ov, double *ow,
                           cudaStream_t s) {
-  const int kchunk = c->nz < 32 ? c->nz : 32;
+  const int kchunk = c->nz < KCHUNK_TMA ? c->nz : KCHUNK_TMA;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
-  k_rk_tma<STAGE, FUSE><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
-      mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
+  if (u_crf != 0.0)
+    k_rk_tma<STAGE, FUSE, true><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
+        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
+  else
+    k_rk_tma<STAGE, FUSE, false><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
+        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
   return cudaGetLastError();
 }
 
 }  // namespace
+
+// Raises the dynamic shared-memory limit of the FP64 RK kernels (~51 KB) on
+// the current device.
+cudaError_t rk_tma_configure() {
+  const int bytes = (int)rk_tma_smem_bytes();
+  cudaError_t e = cudaSuccess;
+#define PLC_RK_ATTR(S, F, C)                                                                \
+  if (e == cudaSuccess)                                                                     \
+    e = cudaFuncSetAttribute(k_rk_tma<S, F, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                             bytes);
+  PLC_RK_ATTR(1, true, true)
+  PLC_RK_ATTR(1, true, false)
+  PLC_RK_ATTR(1, false, true)
+  PLC_RK_ATTR(1, false, false)
+  PLC_RK_ATTR(2, true, true)
+  PLC_RK_ATTR(2, true, false)
+  PLC_RK_ATTR(2, false, true)
+  PLC_RK_ATTR(2, false, false)
+#undef PLC_RK_ATTR
+  return e;
+}
 
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const double *qu,
                       const double *qv, const double *qw, double *ou, double *ov, double *ow,
