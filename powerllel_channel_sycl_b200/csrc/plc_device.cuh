@@ -48,6 +48,25 @@ static __device__ __forceinline__ void store_with_halo(T *q, const Geo &g, int i
 // writing many planes of the column pays for the image rules once.  The
 // offsets are within one plane (at most ny*pitch elements), so 32 bits hold
 // them.
+// Division by a divisor that is fixed for a kernel's lifetime, by one
+// multiply-high, an add and a shift: q = (umulhi(e, mul) + e) >> shr with
+// shr = ceil(log2 d) and mul = floor(2^32 (2^shr - d) / d) + 1 (the
+// round-up multiplier method of Granlund and Montgomery, "Division by
+// invariant integers using multiplication", 1994).  Exact for 1 <= d < 2^31
+// and 0 <= e < 2^31.  A runtime integer division costs about twenty
+// instructions; the index loops of the transforms divide once per element.
+struct FastDiv {
+  unsigned mul, shr;
+  __host__ __device__ explicit FastDiv(unsigned d) {
+    shr = 0;
+    while ((1u << shr) < d) ++shr;
+    mul = (unsigned)(((1ull << 32) * ((1ull << shr) - d)) / d + 1);
+  }
+  __device__ __forceinline__ int div(int e) const {
+    return (int)((__umulhi((unsigned)e, mul) + (unsigned)e) >> shr);
+  }
+};
+
 struct HaloCol {
   int dx, dy;
 };

@@ -531,14 +531,14 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 // Copies `rows` rows of `len` elements (len a multiple of 16 bytes, 16-byte
 // aligned rows) from src (row stride `stride` elements) to dst (row stride
-// `len`).
+// `len`); fcpr divides by the chunks per row, len / (16 / sizeof(T)).
 template <class T>
 __device__ __forceinline__ void stage_rows(T *dst, const T *src, int rows, int len,
-                                           long long stride) {
+                                           long long stride, const FastDiv &fcpr) {
   constexpr int per = 16 / sizeof(T);  // elements per 16-byte chunk
   const int cpr = len / per;           // chunks per row
   for (int e = threadIdx.x; e < rows * cpr; e += blockDim.x) {
-    const int r = e / cpr, ch = e - r * cpr;
+    const int r = fcpr.div(e), ch = e - r * cpr;
     cp_async16(dst + r * len + per * ch, src + r * stride + per * ch);
   }
 }
@@ -556,9 +556,10 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>:
   T *S = reinterpret_cast<T *>(B + nl * LS);  // R halo'd rows
   const int tiles_y = g.ny / R;
   const int ntiles = tiles_y * g.nz;
+  const FastDiv fcpr(X / (16 / sizeof(T)));
   auto issue = [&](int tile) {
     const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;  // 0-based
-    stage_rows(S, p + g.at(0, j0 + 1, k + 1), R, X, X);
+    stage_rows(S, p + g.at(0, j0 + 1, k + 1), R, X, X, fcpr);
     cp_async_commit();
   };
   int tile = blockIdx.x;
@@ -600,9 +601,10 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
   const int tiles_y = g.ny / R;
   const int ntiles = tiles_y * g.nz;
   const T scale = T(nf);
+  const FastDiv fcpr(n / (16 / sizeof(T)));
   auto issue = [&](int tile) {
     const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
-    stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n);
+    stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n, fcpr);
     cp_async_commit();
   };
   int tile = blockIdx.x;
@@ -635,6 +637,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
       using T16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
       constexpr int VW = 16 / sizeof(T);
       const int X = g.X, nq = X / VW;
+      const FastDiv fnq(nq);
       // line l: rows a, b at 2*l*X
       T *O = reinterpret_cast<T *>(
           (reinterpret_cast<unsigned long long>(Z == A ? B : A) + 15ull) & ~15ull);
@@ -661,7 +664,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
       __syncthreads();
       const int kimg = kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1);
       for (int e = threadIdx.x; e < 2 * nl * nq; e += blockDim.x) {
-        const int r = e / nq, q = e - r * nq;  // r = 2l + h
+        const int r = fnq.div(e), q = e - r * nq;  // r = 2l + h
         const T16 val = reinterpret_cast<const T16 *>(O + r * X)[q];
         const int j = j0 + r + 1;
         const int jimg = j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1);
@@ -722,9 +725,10 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
   T *S = reinterpret_cast<T *>(B + nl * LS);  // n rows of TX elements
   const int tiles_x = nx / TX;
   const int ntiles = tiles_x * nz;
+  const FastDiv fcpr(TX / (16 / sizeof(T))), fnl(nl);
   auto issue = [&](int tile) {
     const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
-    stage_rows(S, var + (long long)k * nx * ny + i0, n, TX, nx);
+    stage_rows(S, var + (long long)k * nx * ny + i0, n, TX, nx, fcpr);
     cp_async_commit();
   };
   int tile = blockIdx.x;
@@ -739,7 +743,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
       // columns 2l, 2l+1 of row t form element t of line l: one vector
       // load and store per pair
       for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
-        const int t = e / nl, l = e - t * nl;
+        const int t = fnl.div(e), l = e - t * nl;
         A[l * LS + padi<V>(t)] = reinterpret_cast<const V *>(S + t * TX)[l];
       }
     } else {
@@ -747,7 +751,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
       // the staged rows are adjacent (a stride of 2*TX elements between
       // threads would put every lane in one bank)
       for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
-        const int m = e / nl, l = e - m * nl;
+        const int m = fnl.div(e), l = e - m * nl;
         pack_pair(A + l * LS, n, m, S + 2 * l, S + 2 * l + 1, TX);
       }
     }
@@ -756,7 +760,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
     const V *Z = fft_run_n<N, INV>(A, B, nl, LS, P);
     if (!INV) {
       for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
-        const int m = e / nl, l = e - m * nl;
+        const int m = fnl.div(e), l = e - m * nl;
         V a, b;
         unpack_four(Z + l * LS, n, m, a, b);
         const int q0 = (m == 0) ? 0 : 2 * m;
@@ -766,7 +770,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
       }
     } else {
       for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
-        const int t = e / nl, l = e - t * nl;
+        const int t = fnl.div(e), l = e - t * nl;
         reinterpret_cast<V *>(plane + (long long)t * nx)[l] = Z[l * LS + padi<V>(t)];
       }
     }
@@ -979,9 +983,14 @@ size_t fft_bytes(int n, int lines) {
 size_t fft_smem_bytes(int n, int lines) { return fft_bytes<double>(n, lines); }
 
 namespace {
+// halo'd row length of a field: nx + 2, padded to 16 bytes in FP32
+template <class T>
+size_t x_pitch(int nx) {
+  return sizeof(T) == 4 ? (size_t)((nx + 2 + 3) / 4) * 4 : (size_t)nx + 2;
+}
 template <class T>
 size_t smem_x_fwd(int nx, int nl) {
-  return fft_bytes<T>(nx, nl) + (size_t)2 * nl * (nx + 2) * sizeof(T);
+  return fft_bytes<T>(nx, nl) + (size_t)2 * nl * x_pitch<T>(nx) * sizeof(T);
 }
 template <class T>
 size_t smem_x_bwd(int nx, int nl) {

@@ -532,18 +532,6 @@ __device__ bool grid_sum_last(DD (&v)[NV], double *partials, unsigned int *count
   return threadIdx.x == 0;
 }
 
-__device__ __forceinline__ void interior_coords(const Geo &g, long long t, int &i, int &j,
-                                                int &k) {
-  const long long nxy = (long long)g.nx * g.ny;
-  k = (int)(t / nxy);
-  const long long r = t - (long long)k * nxy;
-  j = (int)(r / g.nx);
-  i = (int)(r - (long long)j * g.nx);
-  ++i;
-  ++j;
-  ++k;
-}
-
 // Mean (mod_utils.cc:30-51): sum(var*dzflzi) / nxg / nyg -> sc->mean[comp]
 // (products and sums in FP64 also for an FP32 field)
 template <class T>
@@ -551,13 +539,15 @@ __global__ void __launch_bounds__(256) k_mean(Geo g, StepConst *sc, int comp, in
                                               const T *__restrict__ var, double *partials,
                                               unsigned int *counter) {
   __shared__ double smem[2 * 32];
-  const long long n = (long long)g.nx * g.ny * g.nz;
   DD s[1] = {{0.0, 0.0}};
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (long long)gridDim.x * blockDim.x) {
-    int i, j, k;
-    interior_coords(g, t, i, j, k);
-    dd_add(s[0], double(var[g.at(i, j, k)]) * __ldg(g.dzflzi + k));
+  // interior rows over the blocks, their x points over the threads (the
+  // double-double sum does not depend on the order)
+  const int nrows = g.ny * g.nz;
+  for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+    const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
+    const double wz = __ldg(g.dzflzi + k);
+    for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x)
+      dd_add(s[0], double(var[g.at(i, j, k)]) * wz);
   }
   block_sum<1>(s, smem);
   if (grid_sum_last<1>(s, partials, counter, gridDim.x, blockIdx.x, smem)) {
@@ -954,23 +944,25 @@ __global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restr
       if (isnan(u[t])) nan_found = 1;
   }
   if (what & 6) {
-    const long long n = (long long)g.nx * g.ny * g.nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-      int i, j, k;
-      interior_coords(g, t, i, j, k);
-      const long long c = g.at(i, j, k);
+    // interior rows (j, k) over the blocks, the x points of a row over the
+    // threads: one division per row instead of two per point
+    const int nrows = g.ny * g.nz;
+    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+      const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
       const double dzfi = __ldg(g.dzf_inv + k);
-      const double uc = u[c], um = u[c - 1], vc = v[c], vm = v[c - g.X], wc = w[c],
-                   wm = w[c - g.XY];
-      if (what & 2) {
-        const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
-                         fabs((wc + wm) * 0.5) * dzfi;
-        max_combine(cfl, r, c);
-      }
-      if (what & 4) {
-        const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
-        max_combine(div, d, c);
+      for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+        const long long c = g.at(i, j, k);
+        const double uc = u[c], um = u[c - 1], vc = v[c], vm = v[c - g.X], wc = w[c],
+                     wm = w[c - g.XY];
+        if (what & 2) {
+          const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
+                           fabs((wc + wm) * 0.5) * dzfi;
+          max_combine(cfl, r, c);
+        }
+        if (what & 4) {
+          const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
+          max_combine(div, d, c);
+        }
       }
     }
   }
