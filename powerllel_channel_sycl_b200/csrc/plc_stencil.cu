@@ -220,8 +220,8 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
 // are those of momentum_rhs, so the results are bit-identical to the
 // global-load kernel above.
 // ---------------------------------------------------------------------------
-constexpr int RX = 32, RY = 8;                  // interior tile
-constexpr int HX = RX + 2, HY = RY + 2;         // halo tile (34 x 10)
+constexpr int RX = 32, TY = 8, RY = 2 * TY;    // interior tile 32 x 16: two rows per thread
+constexpr int HX = RX + 2, HY = RY + 2;         // halo tile (34 x 18)
 constexpr int PLANE = HX * HY;                  // doubles per field-plane
 constexpr int SLOT = ((PLANE * 8 + 127) / 128) * 128 / 8;  // doubles, 128-B aligned
 constexpr int NSLOT = 6;
@@ -285,7 +285,7 @@ size_t rk_tma_smem_bytes() {
 }
 
 template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *RY, 3)
+__global__ void __launch_bounds__(RX *TY, 2)
     k_rk_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
              const __grid_constant__ CUtensorMap mw, Geo g, const StepConst *__restrict__ sc,
              double u_crf, double *ou, double *ov, double *ow, int kchunk, int *err) {
@@ -296,13 +296,16 @@ __global__ void __launch_bounds__(RX *RY, 3)
   ZMetric *zrow = reinterpret_cast<ZMetric *>(base + 3 * NSLOT * SLOT);  // planes kb..ke
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(zrow + KCHUNK_TMA);
   unsigned long long *empty = bar + NSLOT;
-  constexpr unsigned kWarps = RX * RY / 32;
+  constexpr unsigned kWarps = RX * TY / 32;
 
   const int tid = threadIdx.x;
   const int tx = tid & (RX - 1), ty = tid / RX;
   const int x0 = blockIdx.x * RX, y0 = blockIdx.y * RY;  // halo'd coords of the tile corner
-  const int i = x0 + tx + 1, j = y0 + ty + 1;
-  const bool active = (i <= g.nx) && (j <= g.ny);
+  // rows ja and jb = ja + 1 of column i; the second row shares the first's
+  // north-face terms as its south-face terms
+  const int i = x0 + tx + 1, ja = y0 + 2 * ty + 1, jb = ja + 1;
+  const bool act_a = (i <= g.nx) && (ja <= g.ny);
+  const bool act_b = act_a && (jb <= g.ny);
   const int kb = blockIdx.z * kchunk + 1;
   const int ke = min(kb + kchunk - 1, g.nz);
   const int plast = ke + 1;  // last plane to bring in
@@ -340,17 +343,24 @@ __global__ void __launch_bounds__(RX *RY, 3)
   __syncthreads();
 
   const double dt = sc->dt;
-  const long long XY = g.XY;
-  long long c = g.at(active ? i : 1, active ? j : 1, kb);
-  double bu = 0.0, bv = 0.0, bw = 0.0;  // RK2 base values (u, v, w) of plane k
-  if (STAGE == 2 && active) {
-    bu = ou[c];
-    bv = ov[c];
-    bw = ow[c];
+  const long long X = g.X, XY = g.XY;
+  long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
+  // RK2 base values (u, v, w) of plane k at points a and b
+  double ba[3] = {0.0, 0.0, 0.0}, bb[3] = {0.0, 0.0, 0.0};
+  if (STAGE == 2 && act_a) {
+    ba[0] = ou[c];
+    ba[1] = ov[c];
+    ba[2] = ow[c];
+    if (act_b) {
+      bb[0] = ou[c + X];
+      bb[1] = ov[c + X];
+      bb[2] = ow[c + X];
+    }
   }
-  const HaloCol hc = halo_col(g, i, j);
-  const bool xy_edge = (hc.dx | hc.dy) != 0;  // the column has periodic images
-  const int o = (ty + 1) * HX + (tx + 1);
+  const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
+  const bool xy_edge = (ha.dx | ha.dy | hb.dx | hb.dy) != 0;  // images in x or y
+  const int o = (2 * ty + 1) * HX + (tx + 1);                 // point a in a slot
+  int sm = 0, s0 = 1, sp = 2;                                 // slots of planes k-1, k, k+1
   for (int k = kb; k <= ke; ++k) {
     bool ok = true;
     if (tid == 0 && k + 3 <= plast) {
@@ -368,48 +378,75 @@ __global__ void __launch_bounds__(RX *RY, 3)
       atomicExch(err, 1);
       break;  // the other threads' waits run out as well
     }
-    double nbu = 0.0, nbv = 0.0, nbw = 0.0;
-    if (STAGE == 2 && active && k < ke) {
-      nbu = ou[c + XY];
-      nbv = ov[c + XY];
-      nbw = ow[c + XY];
+    double na[3] = {0.0, 0.0, 0.0}, nb[3] = {0.0, 0.0, 0.0};  // base values of plane k+1
+    if (STAGE == 2 && act_a && k < ke) {
+      na[0] = ou[c + XY];
+      na[1] = ov[c + XY];
+      na[2] = ow[c + XY];
+      if (act_b) {
+        nb[0] = ou[c + X + XY];
+        nb[1] = ov[c + X + XY];
+        nb[2] = ow[c + X + XY];
+      }
     }
-    if (active) {
-      const int rm = (k - 1 - (kb - 1)) % NSLOT, r0 = (k - (kb - 1)) % NSLOT,
-                rp = (k + 1 - (kb - 1)) % NSLOT;
+    if (act_a) {
       SmemAcc a;
       a.base = slot_u;
-      a.off[0] = rm * SLOT + o;
-      a.off[1] = r0 * SLOT + o;
-      a.off[2] = rp * SLOT + o;
-      const Rhs3 r = momentum_rhs<CRF>(g, u_crf, a, zrow[k - kb]);
-      const double qu = a.U(0, 0, 0), qv = a.V(0, 0, 0), qw = a.W(0, 0, 0);
-      double nu, nv, nw;
-      if (STAGE == 1) {
-        nu = qu + dt * r.u;
-        nv = qv + dt * r.v;
-        nw = qw + dt * r.w;
-      } else {
-        nu = (qu + dt * r.u + bu) * 0.5;
-        nv = (qv + dt * r.v + bv) * 0.5;
-        nw = (qw + dt * r.w + bw) * 0.5;
+      a.off[0] = sm * SLOT + o;
+      a.off[1] = s0 * SLOT + o;
+      a.off[2] = sp * SLOT + o;
+      SmemAcc b = a;
+      b.off[0] += HX;
+      b.off[1] += HX;
+      b.off[2] += HX;
+      const ZMetric zm = zrow[k - kb];
+      const Rhs3 ra = momentum_rhs<CRF>(g, u_crf, a, zm);
+      const Rhs3 rb = momentum_rhs<CRF>(g, u_crf, b, zm);
+      const double fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
+      const double qa[3] = {a.U(0, 0, 0), a.V(0, 0, 0), a.W(0, 0, 0)};
+      const double qb[3] = {b.U(0, 0, 0), b.V(0, 0, 0), b.W(0, 0, 0)};
+      double va[3], vb[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (STAGE == 1) {
+          va[d] = qa[d] + dt * fa[d];
+          vb[d] = qb[d] + dt * fb[d];
+        } else {
+          va[d] = (qa[d] + dt * fa[d] + ba[d]) * 0.5;
+          vb[d] = (qb[d] + dt * fb[d] + bb[d]) * 0.5;
+        }
       }
       if (FUSE && (xy_edge || k == 1 || k == g.nz)) {
-        store_point(ou, g, hc, c, k, nu, BC_CENTRED, 0.0 - u_crf);
-        store_point(ov, g, hc, c, k, nv, BC_CENTRED, 0.0);
-        store_point(ow, g, hc, c, k, nw, BC_FACE, 0.0);
+        store_point(ou, g, ha, c, k, va[0], BC_CENTRED, 0.0 - u_crf);
+        store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.0);
+        store_point(ow, g, ha, c, k, va[2], BC_FACE, 0.0);
+        if (act_b) {
+          store_point(ou, g, hb, c + X, k, vb[0], BC_CENTRED, 0.0 - u_crf);
+          store_point(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.0);
+          store_point(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.0);
+        }
       } else {  // no image or ghost to write
-        ou[c] = nu;
-        ov[c] = nv;
-        ow[c] = nw;
+        ou[c] = va[0];
+        ov[c] = va[1];
+        ow[c] = va[2];
+        if (act_b) {
+          ou[c + X] = vb[0];
+          ov[c + X] = vb[1];
+          ow[c + X] = vb[2];
+        }
       }
     }
-    // this warp is done with plane k-1
+    // this warp is done with plane k-1 (slot sm)
     __syncwarp();
-    if ((tid & 31) == 0) mbar_arrive(&empty[(k - kb) % NSLOT]);
-    bu = nbu;
-    bv = nbv;
-    bw = nbw;
+    if ((tid & 31) == 0) mbar_arrive(&empty[sm]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ba[d] = na[d];
+      bb[d] = nb[d];
+    }
+    sm = s0;
+    s0 = sp;
+    sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
     c += XY;
   }
   if (tid == 0) {
@@ -1065,10 +1102,10 @@ cudaError_t launch_rk_tma(const plc_ctx *c, const CUtensorMap &mu, const CUtenso
   const int kchunk = c->nz < KCHUNK_TMA ? c->nz : KCHUNK_TMA;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   if (u_crf != 0.0)
-    k_rk_tma<STAGE, FUSE, true><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
+    k_rk_tma<STAGE, FUSE, true><<<grid, RX * TY, rk_tma_smem_bytes(), s>>>(
         mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
   else
-    k_rk_tma<STAGE, FUSE, false><<<grid, RX * RY, rk_tma_smem_bytes(), s>>>(
+    k_rk_tma<STAGE, FUSE, false><<<grid, RX * TY, rk_tma_smem_bytes(), s>>>(
         mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
   return cudaGetLastError();
 }
