@@ -224,6 +224,83 @@ struct Dft<3, INV> {
   }
 };
 
+// 24-point DFT as three 8-point DFTs of the interleaved subsequences
+// x[3m + r], the twiddles W24^(r k), and eight 3-point DFTs across r:
+// X[k + 8q] = sum_r W3^(r q) W24^(r k) Y_r[k] (Cooley-Tukey with n = 3m + r,
+// k' = k + 8q).  The twiddles W24^j = cos(15 j deg) -+ i sin(15 j deg) that are
+// not trivial are applied by complex multiplication; j = 6 is a rotation by
+// 90 degrees and j = 3 a scaled sum and difference.
+template <bool INV>
+struct Dft<24, INV> {
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[24]) {
+    using S = ScalarOf<V>;
+    // cos and sin of 15 j degrees, j = 0 .. 14
+    const S c[15] = {S(1),
+                     S(0.96592582628906828675),
+                     S(0.86602540378443864676),
+                     S(0.70710678118654752440),
+                     S(0.5),
+                     S(0.25881904510252076235),
+                     S(0),
+                     S(-0.25881904510252076235),
+                     S(-0.5),
+                     S(-0.70710678118654752440),
+                     S(-0.86602540378443864676),
+                     S(-0.96592582628906828675),
+                     S(-1),
+                     S(-0.96592582628906828675),
+                     S(-0.86602540378443864676)};
+    const S sn[15] = {S(0),
+                      S(0.25881904510252076235),
+                      S(0.5),
+                      S(0.70710678118654752440),
+                      S(0.86602540378443864676),
+                      S(0.96592582628906828675),
+                      S(1),
+                      S(0.96592582628906828675),
+                      S(0.86602540378443864676),
+                      S(0.70710678118654752440),
+                      S(0.5),
+                      S(0.25881904510252076235),
+                      S(0),
+                      S(-0.25881904510252076235),
+                      S(-0.5)};
+    V y[3][8];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+      for (int m = 0; m < 8; ++m) y[r][m] = v[3 * m + r];
+      Dft<8, INV>::run(y[r]);
+    }
+#pragma unroll
+    for (int r = 1; r < 3; ++r)
+#pragma unroll
+      for (int k = 1; k < 8; ++k) {
+        const int j = r * k;
+        const V x = y[r][k];
+        if (j == 6) {
+          y[r][k] = rot90<INV>(x);
+        } else if (j == 3) {  // W24^3 = (1 -+ i)/sqrt(2)
+          const S h = c[3];
+          y[r][k] = INV ? mk<V>(h * (x.x - x.y), h * (x.x + x.y))
+                        : mk<V>(h * (x.x + x.y), h * (x.y - x.x));
+        } else {
+          const V w = mk<V>(c[j], -sn[j]);  // W24^j, forward sign
+          y[r][k] = INV ? cmulc(x, w) : cmul(x, w);
+        }
+      }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      V t[3] = {y[0][k], y[1][k], y[2][k]};
+      Dft<3, INV>::run(t);
+      v[k] = t[0];
+      v[k + 8] = t[1];
+      v[k + 16] = t[2];
+    }
+  }
+};
+
 // One Stockham pass of radix R over nl lines of length n (line stride LS).
 template <int R, bool INV, class V>
 __device__ __forceinline__ void fft_pass(const V *__restrict__ src, V *__restrict__ dst, int nl,
@@ -298,12 +375,24 @@ __host__ __device__ constexpr int count3(int n) {
   }
   return b;
 }
+// In FP32 (W24 = true), lengths 3 * 2^a with 3 <= a <= 7 (24 .. 384) take two
+// passes: radix 2^(a-3) and then 24 (one pass for 24 itself).  FP64 keeps the
+// 16 / 8 / 3 passes: its 24 complex values of a radix-24 butterfly need about
+// 156 registers, which halves the resident blocks.
+__host__ __device__ constexpr bool plan_has24(int n) {
+  const int a = count2(n);
+  return (n >> a) == 3 && a >= 3 && a <= 7;
+}
+template <bool W24>
 __host__ __device__ constexpr int plan_npass(int n) {
   const int a = count2(n), b = count3(n >> a);
+  if (W24 && plan_has24(n)) return a == 3 ? 1 : 2;
   return a / 4 + (a % 4 != 0 ? 1 : 0) + b;
 }
+template <bool W24>
 __host__ __device__ constexpr int plan_radix(int n, int p) {
   const int a = count2(n);
+  if (W24 && plan_has24(n)) return (a == 3 || p == 1) ? 24 : (1 << (a - 3));
   if (p < a / 4) return 16;
   p -= a / 4;
   if (a % 4 != 0) {
@@ -370,8 +459,9 @@ __device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restr
 
 template <int N, int NS, int P, bool INV, class V>
 __device__ __forceinline__ void passes_t(V *&A, V *&B, int nl, const V *__restrict__ tw) {
-  if constexpr (P < plan_npass(N)) {
-    constexpr int R = plan_radix(N, P);
+  constexpr bool W24 = sizeof(ScalarOf<V>) == 4;
+  if constexpr (P < plan_npass<W24>(N)) {
+    constexpr int R = plan_radix<W24>(N, P);
     fft_pass_t<R, INV, N, NS>(A, B, nl, tw);
     __syncthreads();
     V *t = A;
