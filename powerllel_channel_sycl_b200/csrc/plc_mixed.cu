@@ -42,9 +42,6 @@ constexpr int PLANE = HX * HY;          // floats per field-plane
 constexpr int SLOT = ((PLANE * 4 + 127) / 128) * 128 / 4;  // floats, 128-B aligned
 constexpr int NSLOT = 6;
 constexpr unsigned PLANE_TX_BYTES = 3u * PLANE * 4u;
-// RK2 base values (u, v, w of plane k): the interior rows of the tile, 36 x 16
-constexpr int BPLANE = HX * RY;         // 576 floats = 2304 bytes, a multiple of 128
-constexpr unsigned BASE_TX_BYTES = 3u * BPLANE * 4u;
 constexpr long long kWaitLimit = 1ll << 22;  // try_wait polls before giving up
 constexpr int KCHUNK = 32;
 constexpr int NCOEF = 12;               // per-plane coefficient row (10 used), 3 float4
@@ -158,80 +155,6 @@ __device__ __forceinline__ Rhs3f momentum_rhs32(const RkConst &K, const Coef &z,
   return r;
 }
 
-// (visc - conv) of the momentum equations (mod_calcVel.cc:27-129) for the
-// two rows (j, j+1) of a thread at once, on Blackwell's packed FP32x2
-// arithmetic (FFMA2 / FADD2 / FMUL2: one instruction for both points).
-// P(f, di, dj, dk) gives field f (0 u, 1 v, 2 w) at offset (di, dj, dk) for
-// {row j, row j+1}.  Subtraction is a fused multiply-add by -1 (exact
-// product, one rounding); the z diffusion is vt*u(k+1) + vb*u(k-1) -
-// (vt+vb)*u(k).
-__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
-
-struct Rhs3x2 {
-  float2 u, v, w;
-};
-
-template <bool CRF, class Acc2>
-__device__ __forceinline__ Rhs3x2 momentum_rhs32x2(const RkConst &K, const Coef &z, float vtb,
-                                                   float wtb, const Acc2 &P) {
-  const float2 qx = f2(K.qx), qy = f2(K.qy), rx = f2(K.rx), ry = f2(K.ry), m2 = f2(-2.f);
-  const float2 at = f2(z.at), bt = f2(z.bt), ab = f2(z.ab), bb = f2(z.bb);
-  const float2 u0 = P(0, 0, 0, 0), v0 = P(1, 0, 0, 0), w0 = P(2, 0, 0, 0);
-  Rhs3x2 r;
-  {
-    const float2 upx = P(0, 1, 0, 0), umx = P(0, -1, 0, 0), upy = P(0, 0, 1, 0),
-                 umy = P(0, 0, -1, 0), uzp = P(0, 0, 0, 1), uzm = P(0, 0, 0, -1);
-    const float2 ue = add2(u0, upx), uw = add2(umx, u0), un = add2(u0, upy), us = add2(umy, u0);
-    const float2 ut = fma2(u0, at, mul2(uzp, bt)), ub = fma2(u0, ab, mul2(uzm, bb));
-    const float2 vn = add2(v0, P(1, 1, 0, 0)), vs = add2(P(1, 0, -1, 0), P(1, 1, -1, 0));
-    const float2 wt = add2(w0, P(2, 1, 0, 0)), wb = add2(P(2, 0, 0, -1), P(2, 1, 0, -1));
-    float2 conv = mul2(qx, mul2(add2(ue, uw), sub2(ue, uw)));
-    conv = fma2(qy, sub2(mul2(un, vn), mul2(us, vs)), conv);
-    conv = fma2(f2(z.cz), sub2(mul2(ut, wt), mul2(ub, wb)), conv);
-    if (CRF) conv = fma2(f2(K.crf), sub2(ue, uw), conv);
-    const float2 zt = fma2(f2(z.vt), uzp, fma2(f2(z.vb), uzm, mul2(f2(-vtb), u0)));
-    const float2 visc = fma2(rx, fma2(u0, m2, add2(upx, umx)), fma2(ry, fma2(u0, m2, add2(upy, umy)), zt));
-    r.u = sub2(visc, conv);
-  }
-  {
-    const float2 vpx = P(1, 1, 0, 0), vmx = P(1, -1, 0, 0), vpy = P(1, 0, 1, 0),
-                 vmy = P(1, 0, -1, 0), vzp = P(1, 0, 0, 1), vzm = P(1, 0, 0, -1);
-    const float2 ve = add2(v0, vpx), vw = add2(vmx, v0), vn = add2(v0, vpy), vs = add2(vmy, v0);
-    const float2 vt = fma2(v0, at, mul2(vzp, bt)), vb = fma2(v0, ab, mul2(vzm, bb));
-    const float2 ue = add2(u0, P(0, 0, 1, 0)), uw = add2(P(0, -1, 0, 0), P(0, -1, 1, 0));
-    const float2 wt = add2(w0, P(2, 0, 1, 0)), wb = add2(P(2, 0, 0, -1), P(2, 0, 1, -1));
-    float2 conv = mul2(qx, sub2(mul2(ue, ve), mul2(uw, vw)));
-    conv = fma2(qy, mul2(add2(vn, vs), sub2(vn, vs)), conv);
-    conv = fma2(f2(z.cz), sub2(mul2(wt, vt), mul2(wb, vb)), conv);
-    if (CRF) conv = fma2(f2(K.crf), sub2(ve, vw), conv);
-    const float2 zt = fma2(f2(z.vt), vzp, fma2(f2(z.vb), vzm, mul2(f2(-vtb), v0)));
-    const float2 visc = fma2(rx, fma2(v0, m2, add2(vpx, vmx)), fma2(ry, fma2(v0, m2, add2(vpy, vmy)), zt));
-    r.v = sub2(visc, conv);
-  }
-  {
-    const float2 wpx = P(2, 1, 0, 0), wmx = P(2, -1, 0, 0), wpy = P(2, 0, 1, 0),
-                 wmy = P(2, 0, -1, 0), wzp = P(2, 0, 0, 1), wzm = P(2, 0, 0, -1);
-    const float2 we = add2(w0, wpx), ww = add2(wmx, w0), wn = add2(w0, wpy), ws = add2(wmy, w0);
-    const float2 wt = add2(w0, wzp), wb = add2(w0, wzm);
-    const float2 ue = fma2(u0, at, mul2(P(0, 0, 0, 1), bt));
-    const float2 uw = fma2(P(0, -1, 0, 0), at, mul2(P(0, -1, 0, 1), bt));
-    const float2 vn = fma2(v0, at, mul2(P(1, 0, 0, 1), bt));
-    const float2 vs = fma2(P(1, 0, -1, 0), at, mul2(P(1, 0, -1, 1), bt));
-    float2 conv = mul2(qx, sub2(mul2(ue, we), mul2(uw, ww)));
-    conv = fma2(qy, sub2(mul2(vn, wn), mul2(vs, ws)), conv);
-    conv = fma2(f2(z.cw), mul2(add2(wt, wb), sub2(wt, wb)), conv);
-    if (CRF) conv = fma2(f2(K.crf), sub2(we, ww), conv);
-    const float2 zt = fma2(f2(z.wt), wzp, fma2(f2(z.wb), wzm, mul2(f2(-wtb), w0)));
-    const float2 visc = fma2(rx, fma2(w0, m2, add2(wpx, wmx)), fma2(ry, fma2(w0, m2, add2(wpy, wmy)), zt));
-    r.w = sub2(visc, conv);
-  }
-  return r;
-}
-
 // Operand access from the three plane slots (k-1, k, k+1) of each field.
 struct SmemAcc32 {
   const float *base;
@@ -241,20 +164,8 @@ struct SmemAcc32 {
   }
 };
 
-// Operand access from the three plane slots (k-1, k, k+1) of each field for
-// both rows of the thread: {row j, row j+1}
-struct SmemAcc32x2 {
-  const float *base;
-  int off[3];
-  __device__ __forceinline__ float2 operator()(int f, int di, int dj, int dk) const {
-    const float *q = base + f * NSLOT * SLOT + off[dk + 1] + di + dj * HX;
-    return make_float2(q[0], q[HX]);
-  }
-};
-
-size_t rk32_smem_bytes(int stage) {
-  return (size_t)3 * NSLOT * SLOT * 4 + (stage == 2 ? (size_t)3 * NSLOT * BPLANE * 4 : 0) +
-         (size_t)(KCHUNK + 2) * NCOEF * 4 + 2 * NSLOT * 8 + 128;
+size_t rk32_smem_bytes() {
+  return (size_t)3 * NSLOT * SLOT * 4 + (size_t)(KCHUNK + 2) * NCOEF * 4 + 2 * NSLOT * 8 + 128;
 }
 
 // Bulk mean of the forced components, summed by the mixed form's fused RK2
@@ -282,22 +193,19 @@ struct BulkMean {
 // which each warp arrives once it has read the plane for the last time (at the
 // end of iteration p+1 for plane p).  Thread 0 copies plane k+3 into the slot
 // of plane k+3-NSLOT = k-3 after that slot's empty barrier completed, so warps
-// drift apart by up to two planes without stalling the others.  RK2 also
-// brings the base values of each interior plane of its chunk (the interior
-// rows of u, v, w, on the same full barrier) into a second ring.
+// drift apart by up to two planes without stalling the others.  RK2 reads the
+// base values o of its two points one plane ahead from global memory.  Both
+// stages run at 3 blocks per SM (80 registers, 50 KB of shared memory).
 template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
+__global__ void __launch_bounds__(RX *TY, 3)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
-           const __grid_constant__ CUtensorMap mw, const __grid_constant__ CUtensorMap bu,
-           const __grid_constant__ CUtensorMap bv, const __grid_constant__ CUtensorMap bw, Geo g,
-           RkConst K,
+           const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
            float *ou, float *ov, float *ow, int kchunk, int *err, BulkMean bm) {
   extern __shared__ unsigned char smem_raw[];
   float *slot = reinterpret_cast<float *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
-  float *bslot = slot + 3 * NSLOT * SLOT;  // RK2 base ring (3 * NSLOT * BPLANE)
-  Coef *zc = reinterpret_cast<Coef *>(bslot + (STAGE == 2 ? 3 * NSLOT * BPLANE : 0));
+  Coef *zc = reinterpret_cast<Coef *>(slot + 3 * NSLOT * SLOT);
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
   unsigned long long *empty = bar + NSLOT;
   constexpr unsigned kWarps = RX * TY / 32;
@@ -316,16 +224,10 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
 
   auto issue = [&](int p) {  // thread 0 only
     const int s = (p - (kb - 1)) % NSLOT;
-    const bool base = (STAGE == 2) && p >= kb && p <= ke;
-    mbar_expect_tx(&bar[s], PLANE_TX_BYTES + (base ? BASE_TX_BYTES : 0u));
+    mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
     tma_load_plane(slot + s * SLOT, &mu, x0, y0, p, &bar[s]);
     tma_load_plane(slot + NSLOT * SLOT + s * SLOT, &mv, x0, y0, p, &bar[s]);
     tma_load_plane(slot + 2 * NSLOT * SLOT + s * SLOT, &mw, x0, y0, p, &bar[s]);
-    if (base) {
-      tma_load_plane(bslot + s * BPLANE, &bu, x0, y0 + 1, p, &bar[s]);
-      tma_load_plane(bslot + NSLOT * BPLANE + s * BPLANE, &bv, x0, y0 + 1, p, &bar[s]);
-      tma_load_plane(bslot + 2 * NSLOT * BPLANE + s * BPLANE, &bw, x0, y0 + 1, p, &bar[s]);
-    }
   };
   // bounded waits for plane p's copy to land (full) or to be read by every
   // warp for the last time (empty)
@@ -356,7 +258,18 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
   const float dt = float(sc->dt);
   const long long X = g.X, XY = g.XY;
   long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
-  const int ob = (2 * ty) * HX + (tx + 1);  // point a in a base slot
+  // RK2 base values (u, v, w) of plane k at rows a and b, read a plane ahead
+  float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};
+  if (STAGE == 2 && act_a) {
+    ba[0] = ou[c];
+    ba[1] = ov[c];
+    ba[2] = ow[c];
+    if (act_b) {
+      bb[0] = ou[c + X];
+      bb[1] = ov[c + X];
+      bb[2] = ow[c + X];
+    }
+  }
   const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
   const bool xy_edge = (ha.dx | ha.dy | hb.dx | hb.dy) != 0;  // images in x or y
   const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
@@ -378,29 +291,22 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
       atomicExch(err, 1);
       break;  // the other threads' waits run out as well
     }
+    float na[3] = {0.f, 0.f, 0.f}, nb[3] = {0.f, 0.f, 0.f};  // base values of plane k+1
+    if (STAGE == 2 && act_a && k < ke) {
+      na[0] = ou[c + XY];
+      na[1] = ov[c + XY];
+      na[2] = ow[c + XY];
+      if (act_b) {
+        nb[0] = ou[c + X + XY];
+        nb[1] = ov[c + X + XY];
+        nb[2] = ow[c + X + XY];
+      }
+    }
     if (act_a) {
       const Coef z = zc[k - kb];
       float va[3], vb[3];
-      if constexpr (STAGE == 2) {
-        // packed FP32x2: both rows per instruction (RK2 runs at 2 blocks per
-        // SM either way; its arithmetic chains are what the packing shortens)
-        SmemAcc32x2 a2;
-        a2.base = slot;
-        a2.off[0] = sm * SLOT + o;
-        a2.off[1] = s0 * SLOT + o;
-        a2.off[2] = sp * SLOT + o;
-        const Rhs3x2 r2 = momentum_rhs32x2<CRF>(K, z, z.vt + z.vb, z.wt + z.wb, a2);
-        const float2 q2[3] = {a2(0, 0, 0, 0), a2(1, 0, 0, 0), a2(2, 0, 0, 0)};
-        const float2 f2v[3] = {r2.u, r2.v, r2.w};
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float *bs = bslot + d * NSLOT * BPLANE + s0 * BPLANE + ob;  // RK2 base values
-          const float2 x = mul2(add2(fma2(f2(dt), f2v[d], q2[d]), make_float2(bs[0], bs[HX])), f2(0.5f));
-          va[d] = x.x;
-          vb[d] = x.y;
-        }
-      } else {
-        // scalar (fewer registers: RK1 keeps 3 blocks per SM)
+      {
+        // two rows in scalar FP32 (80 registers: 3 blocks per SM)
         SmemAcc32 a;
         a.base = slot;
         a.off[0] = sm * SLOT + o;
@@ -419,6 +325,10 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
         for (int d = 0; d < 3; ++d) {
           va[d] = fmaf(dt, fa[d], qa[d]);
           vb[d] = fmaf(dt, fb[d], qb[d]);
+          if (STAGE == 2) {
+            va[d] = (va[d] + ba[d]) * 0.5f;
+            vb[d] = (vb[d] + bb[d]) * 0.5f;
+          }
         }
       }
       if (kMean) {
@@ -456,6 +366,11 @@ __global__ void __launch_bounds__(RX *TY, STAGE == 1 ? 3 : 2)
     // this warp is done with plane k-1 (slot sm)
     __syncwarp();
     if ((tid & 31) == 0) mbar_arrive(&empty[sm]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ba[d] = na[d];
+      bb[d] = nb[d];
+    }
     sm = s0;
     s0 = sp;
     sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
@@ -522,12 +437,12 @@ __global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkM
 // Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 18
 // tile of one plane.  The pitch is a multiple of 4 (16 bytes) and the tile's x
 // origin 32*bx is 128-byte aligned.
-bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g, int box_rows = HY) {
+bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g) {
   auto enc = tensor_map_encoder();
   if (!enc || (reinterpret_cast<unsigned long long>(ptr) & 15ull) || (g.X & 3)) return false;
   cuuint64_t dims[3] = {(cuuint64_t)g.X, (cuuint64_t)g.Y, (cuuint64_t)(g.nz + 2)};
   cuuint64_t strides[2] = {(cuuint64_t)g.X * 4ull, (cuuint64_t)g.XY * 4ull};
-  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)box_rows, 1u};
+  cuuint32_t box[3] = {(cuuint32_t)HX, (cuuint32_t)HY, 1u};
   cuuint32_t estr[3] = {1u, 1u, 1u};
   const CUresult r =
       enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(ptr), dims, strides, box,
@@ -537,9 +452,9 @@ bool field_tensor_map32(CUtensorMap *m, const float *ptr, const Geo &g, int box_
 }
 
 template <int STAGE, bool FUSE, bool CRF>
-cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[6], const RkConst &K,
+cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[3], const RkConst &K,
                           float bc_u, float *ou, float *ov, float *ow, cudaStream_t s) {
-  const size_t smem = rk32_smem_bytes(STAGE);
+  const size_t smem = rk32_smem_bytes();
   const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   BulkMean bm;
@@ -549,7 +464,7 @@ cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[6], const RkC
   }
   bm.partials = c->d_mean_partials;
   k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
-      m[0], m[1], m[2], m[3], m[4], m[5], c->geo(), K,
+      m[0], m[1], m[2], c->geo(), K,
       reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err,
       bm);
   if constexpr (STAGE == 2 && FUSE) {
@@ -601,7 +516,7 @@ long long rk32_blocks(const plc_ctx *c) {
 // Raises the dynamic shared-memory limit of the FP32 RK kernels (up to ~90 KB)
 // on the current device.
 cudaError_t rk32_configure() {
-  const int bytes = (int)rk32_smem_bytes(2);
+  const int bytes = (int)rk32_smem_bytes();
   cudaError_t e = cudaSuccess;
 #define PLC_RK32_ATTR(S, F, C)                                                            \
   if (e == cudaSuccess)                                                                   \
@@ -623,18 +538,11 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
                       const float *qv, const float *qw, float *ou, float *ov, float *ow,
                       cudaStream_t s) {
   const Geo g = c->geo();
-  // operand tiles (36 x 18) of q, and for RK2 the base tiles (36 x 16) of o
-  CUtensorMap m[6];
+  // operand tiles (36 x 18) of q
+  CUtensorMap m[3];
   if (!field_tensor_map32(&m[0], qu, g) || !field_tensor_map32(&m[1], qv, g) ||
       !field_tensor_map32(&m[2], qw, g))
     return cudaErrorInvalidValue;  // FP32 fields are allocated 16-byte aligned and padded
-  if (stage == 2) {
-    if (!field_tensor_map32(&m[3], ou, g, RY) || !field_tensor_map32(&m[4], ov, g, RY) ||
-        !field_tensor_map32(&m[5], ow, g, RY))
-      return cudaErrorInvalidValue;
-  } else {
-    m[3] = m[4] = m[5] = m[0];  // not read by RK1
-  }
   RkConst K;
   K.qx = float(0.25 * c->dx_inv);
   K.qy = float(0.25 * c->dy_inv);
