@@ -195,9 +195,10 @@ struct BulkMean {
 // of plane k+3-NSLOT = k-3 after that slot's empty barrier completed, so warps
 // drift apart by up to two planes without stalling the others.  RK2 reads the
 // base values o of its two points one plane ahead from global memory.  Both
-// stages run at 3 blocks per SM (80 registers, 50 KB of shared memory).
+// stages run at 4 blocks per SM (64 registers, 50 KB of shared memory; RK1
+// measured 0.56 ms at 4 blocks against 0.59 ms at 3, 768 x 384 x 256).
 template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *TY, 3)
+__global__ void __launch_bounds__(RX *TY, 4)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
            const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
