@@ -954,25 +954,100 @@ __device__ __forceinline__ void thomas_sweep(int nz, const Sys &sys) {
   }
 }
 
-// A system solved in place in the spectral array, with data, pivots and
-// coefficients of type S.
-template <class S>
-struct InPlaceSys {
-  S *q;
-  long long plane;
-  const S *rp;
-  long long PS;
-  const S *ca, *cc;
-  __device__ __forceinline__ S rhs(int k) const { return q[(long long)k * plane]; }
-  __device__ __forceinline__ S piv(int k) const { return __ldg(rp + (long long)k * PS); }
-  __device__ __forceinline__ S a(int k) const { return __ldg(ca + k); }
-  __device__ __forceinline__ S c(int k) const { return __ldg(cc + k); }
-  __device__ __forceinline__ void fwd_put(int k, S x) const {
-    if (k > 0) q[(long long)k * plane] = x;  // the k = 0 value is the right-hand side
+// The same sweep for a system solved in place in the spectral array (data,
+// pivots and coefficients of type A), with the addresses walked by pointer
+// increments (one 64-bit add an access instead of a 64-bit multiply-add):
+// q = right-hand side and solution (plane stride `plane`), rp = reciprocal
+// pivots (stride PS), ca / cc = the 1-D sub- and super-diagonal.  Same
+// operations in the same order as thomas_sweep.
+template <class A, int PF>
+__device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long long plane,
+                                               const A *__restrict__ rp, long long PS,
+                                               const A *__restrict__ ca,
+                                               const A *__restrict__ cc) {
+  A prev = q[0];
+  const A *lq = q + plane;  // next right-hand side to load (k = 1)
+  const A *lr = rp;         // next pivot to load (k - 1 = 0)
+  A *wq = q + plane;        // next forward value to store (k = 1)
+  {
+    A xn[PF], rn[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (1 + s < nz) {
+        xn[s] = *lq;
+        lq += plane;
+        rn[s] = __ldg(lr);
+        lr += PS;
+      }
+    for (int k = 1; k < nz; k += PF) {
+      A x[PF], r[PF];
+#pragma unroll
+      for (int s = 0; s < PF; ++s) {
+        x[s] = xn[s];
+        r[s] = rn[s];
+      }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k + PF + s < nz) {
+          xn[s] = *lq;
+          lq += plane;
+          rn[s] = __ldg(lr);
+          lr += PS;
+        }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k + s < nz) {
+          A cur = x[s];
+          cur -= (__ldg(ca + k + s) * r[s]) * prev;
+          *wq = cur;
+          wq += plane;
+          prev = cur;
+        }
+    }
   }
-  __device__ __forceinline__ S fwd_get(int k) const { return q[(long long)k * plane]; }
-  __device__ __forceinline__ void out(int k, S x) const { q[(long long)k * plane] = x; }
-};
+  // lr is at pivot nz-1, wq one plane past the last forward value
+  prev *= __ldg(lr);
+  wq -= plane;
+  *wq = prev;
+  {
+    const A *bq = wq - plane;  // next forward value to load (k = nz - 2)
+    const A *br = lr - PS;     // its pivot
+    A *bw = wq - plane;        // next solution value to store
+    A xn[PF], rn[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (nz - 2 - s >= 0) {
+        xn[s] = *bq;
+        bq -= plane;
+        rn[s] = __ldg(br);
+        br -= PS;
+      }
+    for (int k = nz - 2; k >= 0; k -= PF) {
+      A x[PF], r[PF];
+#pragma unroll
+      for (int s = 0; s < PF; ++s) {
+        x[s] = xn[s];
+        r[s] = rn[s];
+      }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k - PF - s >= 0) {
+          xn[s] = *bq;
+          bq -= plane;
+          rn[s] = __ldg(br);
+          br -= PS;
+        }
+#pragma unroll
+      for (int s = 0; s < PF; ++s)
+        if (k - s >= 0) {
+          const A cur = (x[s] - __ldg(cc + k - s) * prev) * r[s];
+          *bw = cur;
+          bw -= plane;
+          prev = cur;
+        }
+    }
+  }
+}
 
 // A low-wavenumber system of the mixed form: FP32 right-hand side and
 // solution, FP64 pivots and arithmetic, forward values in the FP64 buffer
@@ -1019,7 +1094,7 @@ __global__ void __launch_bounds__(128) k_trid(int nx, int ny, int nz,
   long long pv;
   trid_index(t, nx, ny, i, j, pv);
   const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
-  thomas_sweep<double, 8>(nz, InPlaceSys<double>{var + t, plane, rpiv + pv, PS, a, c});
+  thomas_inplace<double, 8>(nz, var + t, plane, rpiv + pv, PS, a, c);
 }
 
 // Mixed form: systems whose packed x and y indices are both below kLowModes
@@ -1044,7 +1119,7 @@ __global__ void __launch_bounds__(128) k_trid_mixed(
     thomas_sweep<double, 8>(
         nz, LowSys{var + t, plane, low + j * kLowModes + i, LP, rpiv + pv, PS, a, c});
   } else {
-    thomas_sweep<float, 16>(nz, InPlaceSys<float>{var + t, plane, rpiv32 + pv, PS, a32, c32});
+    thomas_inplace<float, 16>(nz, var + t, plane, rpiv32 + pv, PS, a32, c32);
   }
 }
 
