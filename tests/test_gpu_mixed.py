@@ -145,3 +145,32 @@ def test_profile_step_mixed():
     ms = ch.profile_step(2)
     assert len(ms) == 8 and all(t > 0 for t in ms.values())
     assert "correct+force+bound(u)" in ms
+
+
+# line lengths of every FP32 transform plan: 3*2^a (two passes ending in a
+# radix-24 butterfly, or one for 24), 2^a, and the 16/16/3 plan of 768
+@pytest.mark.parametrize("nx,ny,nz", [(48, 32, 8), (96, 32, 8), (192, 32, 8), (384, 32, 8),
+                                      (768, 16, 4), (32, 24, 8), (32, 48, 8), (32, 96, 8),
+                                      (32, 192, 8), (16, 384, 8), (64, 256, 4)])
+def test_fp32_transform_plans_project_like_fp64(nx, ny, nz):
+    """The projection of one random field in both forms: the mixed form's
+    velocity is divergence-free to FP32 rounding and within 1e-4 of the FP64
+    form's, for transforms of every FP32 plan in x and in y."""
+    from powerllel_channel_sycl_b200 import Channel
+    rng = np.random.default_rng(nx * 1000 + ny)
+    out = []
+    for precision in (0, 1):
+        prm = channel_params(**case_kwargs(nx, ny, nz))
+        prm.precision = precision
+        ch = Channel(prm)
+        if precision == 0:
+            fields = {q: rng.normal(size=ch.shape) for q in "uvw"}
+        for q in "uvw":
+            ch.upload(q, fields[q])
+        ch.project()
+        out.append(({q: interior(ch.download(q)) for q in "uvw"}, ch.check()[2][0]))
+        ch.close()
+    (ref, _), (mix, div) = out
+    assert div < DIV_TOL, div
+    for q in "uvw":
+        assert rel_l2(mix[q], ref[q]) < VEL_TOL, (q, rel_l2(mix[q], ref[q]))
