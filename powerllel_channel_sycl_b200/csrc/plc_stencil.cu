@@ -1182,8 +1182,8 @@ cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cuda
   if (nb > items) nb = items;
   if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
   if (c->mixed) {
-    // the mixed form's forward x transform has reduced the forcing already
-    constexpr int KZF = 4;
+    // the mixed form's fused RK2 stage has reduced the forcing already
+    constexpr int KZF = 8;  // 8 planes a thread: 0.418 ms against 0.437 for 4 (FP32, 768x384x256)
     dim3 grid((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, (c->nz + KZF - 1) / KZF);
     k_correct_forced<T, KZF><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, c->prm.u_crf, p, u,
                                                           v, w);
