@@ -170,6 +170,13 @@ int plc_download(plc_ctx *ctx, int field, double *h_dst);
 /* Current time step (device-resident; changes under CFL control). */
 int plc_get_dt(plc_ctx *ctx, double *dt);
 int plc_set_dt(plc_ctx *ctx, double dt);
+/* The bulk forcing of the last step, as the step computed it on the device:
+ * mean3 = the plane-weighted mean of each forced velocity component before
+ * the forcing (0 for unforced ones; the `Mean` of forceVel,
+ * mod_calcVel.cc:280-301), force3 (may be NULL) = vel_force - mean3, the
+ * uniform shift the step applied.  A 48-byte device-to-host read: the
+ * per-step result a caller can fetch without a reduction. */
+int plc_step_forcing(plc_ctx *ctx, double *mean3, double *force3);
 
 /* ---- mod_calcVel (src/mod_calcVel.hh:6-14) ---- */
 /* transform2CRF (mod_calcVel.cc:13-25); vel_force is updated in place on the host. */

@@ -94,6 +94,7 @@ _SIGS = {
     "plc_upload": [_vp, _int, _hp],
     "plc_download": [_vp, _int, _hp],
     "plc_get_dt": [_vp, C.POINTER(_dbl)],
+    "plc_step_forcing": [_vp, _hp, _hp],
     "plc_set_dt": [_vp, _dbl],
     "plc_transform2crf": [_vp, _dbl, _dp, C.POINTER(_dbl)],
     "plc_time_int_vel_rk1": [_vp, _dbl, _dp, _dp, _dp, _dp, _dp, _dp],

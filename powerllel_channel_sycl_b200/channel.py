@@ -209,6 +209,15 @@ class Channel:
     def dt(self, value: float):
         self._check(lib().plc_set_dt(self._ctx, float(value)))
 
+    def step_forcing(self):
+        """(mean, force) of the last step's bulk forcing, 3 each: the mean of
+        each forced component before the forcing and vel_force - mean (a
+        48-byte read of what the step computed on the device)."""
+        mean = np.zeros(3)
+        force = np.zeros(3)
+        self._check(lib().plc_step_forcing(self._ctx, mean.ctypes.data, force.ctypes.data))
+        return mean, force
+
     # -- mod_calcVel --------------------------------------------------------------
     def transform2CRF(self, vel_crf: float, vel="u", vel_force: float = 0.0) -> float:
         vf = C.c_double(vel_force)

@@ -706,6 +706,22 @@ int plc_get_dt(plc_ctx *c, double *dt) {
   return PLC_OK;
 }
 
+int plc_step_forcing(plc_ctx *c, double *mean3, double *force3) {
+  PLC_CHECK_CTX(c);
+  PLC_REQ(c, mean3);
+  // force[3] and mean[3] are adjacent in the device struct
+  static_assert(offsetof(StepConst, mean) == offsetof(StepConst, force) + 3 * sizeof(double),
+                "force and mean adjacent");
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_scal, reinterpret_cast<char *>(c->d_sc) + offsetof(StepConst, force),
+                              6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int d = 0; d < 3; ++d) {
+    mean3[d] = c->h_scal[3 + d];
+    if (force3) force3[d] = c->h_scal[d];
+  }
+  return PLC_OK;
+}
+
 int plc_set_dt(plc_ctx *c, double dt) {
   PLC_CHECK_CTX(c);
   if (!(dt > 0.0)) return set_error(c, PLC_ERR_ARG, "dt must be positive");

@@ -273,6 +273,40 @@ def test_step_matches_module_sequence():
     assert rel_l2(demean(a.download("p")), demean(b.download("p"))) < 1e-12
 
 
+def test_step_forcing_read():
+    """plc_step_forcing returns the forcing the fused step applied: forceVel's
+    value in the reference's call sequence, mean + force = vel_force, and the
+    mixed form's within FP32 rounding of the FP64 form's."""
+    from powerllel_channel_sycl_b200 import Channel
+    kwargs = case_kwargs(48, 32, 16)
+    a = Channel(channel_params(**kwargs))
+    b = Channel(channel_params(**kwargs))
+    prm = channel_params(**kwargs)
+    prm.precision = 1
+    m32 = Channel(prm)
+    for ch in (a, b, m32):
+        ch.initFlow()
+    for _ in range(3):
+        a.step(1)
+        m32.step(1)
+        b.timeIntVelRK1()
+        b.updateBoundVel(None, "u1", "v1", "w1")
+        b.timeIntVelRK2()
+        b.updateBoundVel()
+        b.calcRHS()
+        b.execute_poisson_solver()
+        b.updateBoundP()
+        b.correctVel()
+        f_ref = b.forceVel()
+        b.updateBoundVel()
+        mean, force = a.step_forcing()
+        assert abs(force[0] - f_ref[0]) <= 1e-12 * max(1.0, abs(f_ref[0])), (force, f_ref)
+        assert mean[0] + force[0] == pytest.approx(kwargs["vel_force"][0], abs=1e-14)
+        assert mean[1] == mean[2] == 0.0 and force[1] == force[2] == 0.0
+        mean32, force32 = m32.step_forcing()
+        assert abs(mean32[0] - mean[0]) < 1e-5 * abs(mean[0]), (mean32, mean)
+
+
 def test_kernels_per_step():
     case, ch = make_pair(32, 24, 16)
     assert ch.kernels_per_step == 9
