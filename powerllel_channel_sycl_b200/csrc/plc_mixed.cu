@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(RX *TY, 4)
       const Coef z = zc[k - kb];
       float va[3], vb[3];
       {
-        // two rows in scalar FP32 (80 registers: 3 blocks per SM)
+        // two rows in scalar FP32
         SmemAcc32 a;
         a.base = slot;
         a.off[0] = sm * SLOT + o;

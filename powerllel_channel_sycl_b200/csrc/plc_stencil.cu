@@ -206,12 +206,13 @@ __global__ void __launch_bounds__(BX *BY) k_rk(Geo g, const StepConst *__restric
 // ---------------------------------------------------------------------------
 // RK stages as z-marching kernels fed by TMA.
 //
-// A block owns a 32 x 8 tile of interior (i, j) columns and a chunk of z
-// planes.  For each operand field the (32+2) x (8+2) halo tile of every plane
-// is brought into a 6-slot shared-memory ring by one 3-D bulk tensor copy
-// (cp.async.bulk.tensor, completion on a "full" mbarrier), two planes ahead of
-// the plane being computed, so every operand value crosses HBM once per block
-// and the copies overlap the arithmetic.  There is no block-wide barrier in the
+// A block of 32 x 8 threads owns a 32 x 16 tile of interior (i, j) columns --
+// each thread two rows of one column -- and a chunk of z planes.  For each
+// operand field the (32+2) x (16+2) halo tile of every plane is brought into a
+// 6-slot shared-memory ring by one 3-D bulk tensor copy (cp.async.bulk.tensor,
+// completion on a "full" mbarrier), three planes ahead of the plane being
+// computed, so every operand value crosses HBM once per block and the copies
+// overlap the arithmetic.  There is no block-wide barrier in the
 // march: every thread waits on the full barrier of the plane it is about to
 // read, each warp arrives on the slot's "empty" mbarrier when it has read the
 // plane for the last time, and thread 0 refills a slot once its empty barrier
@@ -1078,7 +1079,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 namespace {
 
-// Tensor map of one halo'd field: dims (X, Y, Z), box = one 34 x 10 halo tile
+// Tensor map of one halo'd field: dims (X, Y, Z), box = one 34 x 18 halo tile
 // of one plane.  Base and strides are multiples of 16 bytes (X is even); the
 // tile's x origin 32*bx is even, i.e. 16-byte aligned.
 bool field_tensor_map(CUtensorMap *m, const double *ptr, const Geo &g) {
