@@ -502,10 +502,14 @@ __device__ __forceinline__ void unpack_four(const V *Z, int n, int m, V &a, V &b
 }
 
 // Builds Z_m and Z_{n-m} (0 <= m <= n/2) of the pair whose packed spectra are
-// ra[] (real sequence a) and rb[] (real sequence b), read with stride `st`.
+// those of the real sequences a and b (Z = A + iB), reading them with vector
+// loads.  Rows: the packed spectra of a and b lie in rows ra and rb, (Re, Im)
+// of mode m adjacent at 2m (x lines: one load gives Re and Im).  Columns: a
+// and b are adjacent columns, element k of both at ab[k*st] (y lines: one
+// load gives a and b).
 template <class V>
-__device__ __forceinline__ void pack_pair(V *Z, int n, int m, const ScalarOf<V> *ra,
-                                          const ScalarOf<V> *rb, int st) {
+__device__ __forceinline__ void pack_pair_rows(V *Z, int n, int m, const ScalarOf<V> *ra,
+                                               const ScalarOf<V> *rb) {
   using S = ScalarOf<V>;
   S reA, imA, reB, imB;
   if (m == 0) {
@@ -513,14 +517,63 @@ __device__ __forceinline__ void pack_pair(V *Z, int n, int m, const ScalarOf<V> 
     reB = rb[0];
     imA = imB = S(0);
   } else if (m == (n >> 1)) {
-    reA = ra[st];
-    reB = rb[st];
+    reA = ra[1];
+    reB = rb[1];
     imA = imB = S(0);
   } else {
-    reA = ra[(2 * m) * st];
-    imA = ra[(2 * m + 1) * st];
-    reB = rb[(2 * m) * st];
-    imB = rb[(2 * m + 1) * st];
+    const V a = reinterpret_cast<const V *>(ra)[m], b = reinterpret_cast<const V *>(rb)[m];
+    reA = a.x;
+    imA = a.y;
+    reB = b.x;
+    imB = b.y;
+  }
+  Z[padi<V>(m)] = mk<V>(reA - imB, imA + reB);
+  if (m != 0 && m != (n >> 1)) Z[padi<V>(n - m)] = mk<V>(reA + imB, reB - imA);
+}
+// The column form with scalar loads: element k of a at ab[k * st], of b at
+// ab[k * st + 1].
+template <class V>
+__device__ __forceinline__ void pack_pair_cols_scalar(V *Z, int n, int m,
+                                                      const ScalarOf<V> *ab, int st) {
+  using S = ScalarOf<V>;
+  S reA, imA, reB, imB;
+  if (m == 0) {
+    reA = ab[0];
+    reB = ab[1];
+    imA = imB = S(0);
+  } else if (m == (n >> 1)) {
+    reA = ab[st];
+    reB = ab[st + 1];
+    imA = imB = S(0);
+  } else {
+    reA = ab[(2 * m) * st];
+    reB = ab[(2 * m) * st + 1];
+    imA = ab[(2 * m + 1) * st];
+    imB = ab[(2 * m + 1) * st + 1];
+  }
+  Z[padi<V>(m)] = mk<V>(reA - imB, imA + reB);
+  if (m != 0 && m != (n >> 1)) Z[padi<V>(n - m)] = mk<V>(reA + imB, reB - imA);
+}
+template <class V>
+__device__ __forceinline__ void pack_pair_cols(V *Z, int n, int m, const V *ab, int st) {
+  using S = ScalarOf<V>;
+  S reA, imA, reB, imB;
+  if (m == 0) {
+    const V r = ab[0];
+    reA = r.x;
+    reB = r.y;
+    imA = imB = S(0);
+  } else if (m == (n >> 1)) {
+    const V r = ab[st];
+    reA = r.x;
+    reB = r.y;
+    imA = imB = S(0);
+  } else {
+    const V re = ab[(2 * m) * st], im = ab[(2 * m + 1) * st];
+    reA = re.x;
+    reB = re.y;
+    imA = im.x;
+    imB = im.y;
   }
   Z[padi<V>(m)] = mk<V>(reA - imB, imA + reB);
   if (m != 0 && m != (n >> 1)) Z[padi<V>(n - m)] = mk<V>(reA + imB, reB - imA);
@@ -706,7 +759,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
     __syncthreads();
     for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
       const int l = e / (half + 1), m = e - l * (half + 1);
-      pack_pair(A + l * LS, n, m, S + (2 * l) * n, S + (2 * l + 1) * n, 1);
+      pack_pair_rows(A + l * LS, n, m, S + (2 * l) * n, S + (2 * l + 1) * n);
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
@@ -842,7 +895,10 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
       // threads would put every lane in one bank)
       for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
         const int m = fnl.div(e), l = e - m * nl;
-        pack_pair(A + l * LS, n, m, S + 2 * l, S + 2 * l + 1, TX);
+        if constexpr (sizeof(T) == 4)
+          pack_pair_cols(A + l * LS, n, m, reinterpret_cast<const V *>(S) + l, nl);
+        else  // FP64: scalar loads (16-byte ones measured 3% slower)
+          pack_pair_cols_scalar(A + l * LS, n, m, S + 2 * l, TX);
       }
     }
     __syncthreads();
