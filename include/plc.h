@@ -164,6 +164,12 @@ int plc_field_ptr_f32(plc_ctx *ctx, int field, float **d_ptr, size_t *count, int
  * feasible size on the device (the choice changes speed, never results).
  * No counterpart in the reference. */
 int plc_fft_tiles(const plc_ctx *ctx, int *lines_xf, int *lines_x, int *lines_y);
+/* The radix plan family of the x and y transforms, timed per context with the
+ * tiles where a length has two (0: radix 16, one 8/4/2, then 3s; 1: for
+ * lengths 3 * 2^a with 3 <= a <= 7, two passes ending in a radix-24
+ * butterfly).  PLC_FFT_PLANS (FP64) and PLC_FFT_PLANS_F32 (mixed), "x,y",
+ * pin them. */
+int plc_fft_plans(const plc_ctx *ctx, int *plan_x, int *plan_y);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

@@ -542,6 +542,20 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   // forward x, backward x and y transforms) replace the timing of the FP64 /
   // FP32 transforms: a profiler distorts the event times the autotuner
   // compares, so a profiled run pins the tiles an unprofiled run chose.
+  // PLC_FFT_PLANS / PLC_FFT_PLANS_F32 = "x,y" pin the radix plan families of
+  // the x and y transforms (0 or 1; 1 only for lengths that have it) the same
+  // way; the tiles are then timed under the pinned families.
+  if (const char *env = getenv(c->mixed ? "PLC_FFT_PLANS_F32" : "PLC_FFT_PLANS")) {
+    int px = -1, py = -1;
+    if (sscanf(env, "%d,%d", &px, &py) != 2 || px < 0 || px > 1 || py < 0 || py > 1 ||
+        (px == 1 && !fft_has_two_plans(c->nx)) || (py == 1 && !fft_has_two_plans(c->ny)))
+      return fail(set_error(c, PLC_ERR_ARG, std::string("invalid FFT plans in the environment: ") + env));
+    c->fft_plan_x = px;
+    c->fft_plan_y = py;
+    c->fft_plans_pinned = true;
+    if ((e = fft_set_lines(c, c->fft_lines_xf, c->fft_lines_x, c->fft_lines_y)) != cudaSuccess)
+      return fail(cuda_status(c, e, "fft_set_lines"));
+  }
   bool pinned = false;
   if (const char *env = getenv(c->mixed ? "PLC_FFT_TILES_F32" : "PLC_FFT_TILES")) {
     int xf = 0, xb = 0, y = 0;
@@ -632,6 +646,13 @@ static void ref_shape(const plc_ctx *c, int field, long long *rows, int *len) {
     *rows = (long long)(c->ny + 2) * (c->nz + 2);
     *len = c->nx + 2;
   }
+}
+
+int plc_fft_plans(const plc_ctx *c, int *plan_x, int *plan_y) {
+  if (!c) return set_error(nullptr, PLC_ERR_ARG, "null context");
+  if (plan_x) *plan_x = c->fft_plan_x;
+  if (plan_y) *plan_y = c->fft_plan_y;
+  return PLC_OK;
 }
 
 int plc_fft_tiles(const plc_ctx *c, int *lines_xf, int *lines_x, int *lines_y) {

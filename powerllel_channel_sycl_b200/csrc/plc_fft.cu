@@ -375,9 +375,12 @@ __host__ __device__ constexpr int count3(int n) {
   }
   return b;
 }
-// In FP32 (W24 = true), lengths 3 * 2^a with 3 <= a <= 7 (24 .. 384) take two
-// passes: radix 2^(a-3) and then 24 (one pass for 24 itself).  FP64 keeps the
-// 16 / 8 / 3 passes: its 24 complex values of a radix-24 butterfly need about
+// Two plan families.  Family 0: 16s, then one 8/4/2, then 3s.  Family 1 (W24),
+// for lengths 3 * 2^a with 3 <= a <= 7 (24 .. 384): two passes, radix 2^(a-3)
+// and then 24 (one pass for 24 itself).  Each context's autotuner times both
+// families where a length has two (with the tile sizes) and keeps the faster
+// per direction: in FP32 the radix-24 family wins for the y lines of the
+// 768 x 384 x 256 case; in FP64 its 24 complex values per butterfly need about
 // 156 registers, which halves the resident blocks.
 __host__ __device__ constexpr bool plan_has24(int n) {
   const int a = count2(n);
@@ -457,9 +460,9 @@ __device__ __forceinline__ void fft_pass_t(const V *__restrict__ src, V *__restr
   }
 }
 
-template <int N, int NS, int P, bool INV, class V>
+template <int N, int NS, int P, bool INV, int PL, class V>
 __device__ __forceinline__ void passes_t(V *&A, V *&B, int nl, const V *__restrict__ tw) {
-  constexpr bool W24 = sizeof(ScalarOf<V>) == 4;
+  constexpr bool W24 = PL == 1;
   if constexpr (P < plan_npass<W24>(N)) {
     constexpr int R = plan_radix<W24>(N, P);
     fft_pass_t<R, INV, N, NS>(A, B, nl, tw);
@@ -467,15 +470,16 @@ __device__ __forceinline__ void passes_t(V *&A, V *&B, int nl, const V *__restri
     V *t = A;
     A = B;
     B = t;
-    passes_t<N, NS * R, P + 1, INV>(A, B, nl, tw);
+    passes_t<N, NS * R, P + 1, INV, PL>(A, B, nl, tw);
   }
 }
 
-// Complex FFT of nl lines held in A (compile-time plan for N > 0).
-template <int N, bool INV, class V>
+// Complex FFT of nl lines held in A (compile-time plan of family PL for
+// N > 0).
+template <int N, bool INV, int PL, class V>
 __device__ __forceinline__ V *fft_run_n(V *A, V *B, int nl, int LS, const FftDev<V> &P) {
   if constexpr (N > 0) {
-    passes_t<N, 1, 0, INV>(A, B, nl, P.tw);
+    passes_t<N, 1, 0, INV, PL>(A, B, nl, P.tw);
     return A;
   } else {
     return fft_run<INV>(A, B, nl, LS, P);
@@ -603,7 +607,7 @@ __device__ __forceinline__ float div_dt(const float *__restrict__ u, const float
 // Forward x transform fused with calcRHS, one tile per block: rows
 // (j0+2l, j0+2l+1) of plane k are div(u)/dt evaluated from global memory while
 // loading (many resident blocks hide the load latency), then transformed.
-template <class T, int N, bool FUSED>
+template <class T, int N, bool FUSED, int PL>
 __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx<T>::V> P, int nl,
                                                        const StepConst *__restrict__ sc,
                                                        const T *__restrict__ p,
@@ -640,7 +644,7 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx
     A[l * LS + padi<V>(t)] = mk<V>(a, b);
   }
   __syncthreads();
-  const V *Z = fft_run_n<N, false>(A, B, nl, LS, P);
+  const V *Z = fft_run_n<N, false, PL>(A, B, nl, LS, P);
   const int half = n >> 1;
   for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
     const int l = e / half, m = e - l * half;
@@ -688,7 +692,7 @@ __device__ __forceinline__ void stage_rows(T *dst, const T *src, int rows, int l
 
 // Forward x transform (persistent): rows (j0+2l, j0+2l+1) of p at plane k ->
 // packed spectra.  The halo'd rows are staged whole (16-byte aligned).
-template <class T, int N>
+template <class T, int N, int PL>
 __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>::V> P, int nl,
                                                    const T *__restrict__ p, T *__restrict__ var) {
   using V = typename Cx<T>::V;
@@ -717,7 +721,7 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>:
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const V *Z = fft_run_n<N, false>(A, B, nl, LS, P);
+    const V *Z = fft_run_n<N, false, PL>(A, B, nl, LS, P);
     const int half = n >> 1;
     for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
       const int l = e / half, m = e - l * half;
@@ -732,7 +736,7 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>:
 
 // Backward x transform: packed spectra -> p interior scaled by nf; with
 // FUSE_BC the pressure halos are written as well (updateBoundP).
-template <class T, int N, bool FUSE_BC>
+template <class T, int N, bool FUSE_BC, int PL>
 __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>::V> P, int nl,
                                                    double nf, const T *__restrict__ var, T *p) {
   using V = typename Cx<T>::V;
@@ -763,7 +767,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    V *Z = fft_run_n<N, true>(A, B, nl, LS, P);
+    V *Z = fft_run_n<N, true, PL>(A, B, nl, LS, P);
     // rows j = j0 + 2l + 1 (a) and j + 1 (b) of plane k + 1
     const int kk = k + 1;
     // FP32 with the pressure halos (updateBoundP) and rows shorter than a
@@ -856,7 +860,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
 
 // y transform in place on the spectral array: tile = columns i0..i0+2nl-1 of
 // plane k (TX = 2nl x-contiguous elements per row, row stride nx).
-template <class T, int N, bool INV>
+template <class T, int N, bool INV, int PL>
 __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
                                                FftDev<typename Cx<T>::V> P, int nl,
                                                T *__restrict__ var) {
@@ -903,7 +907,7 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
-    const V *Z = fft_run_n<N, INV>(A, B, nl, LS, P);
+    const V *Z = fft_run_n<N, INV, PL>(A, B, nl, LS, P);
     if (!INV) {
       for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
         const int m = fnl.div(e), l = e - m * nl;
@@ -1265,6 +1269,25 @@ cudaError_t with_size(int n, F &&f) {
 }
 constexpr int kPlanSizes[] = {0, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768};
 
+// The plan family of a transform of length N: 1 (radix 24) only where the
+// length has that family, 0 otherwise.
+template <int N, class F>
+cudaError_t with_plan(int plan, F &&f) {
+  if constexpr (N > 0 && plan_has24(N)) {
+    if (plan == 1) return f(std::integral_constant<int, 1>{});
+  }
+  return f(std::integral_constant<int, 0>{});
+}
+bool fft_has_two_plans(int n) {
+  bool two = false;
+  with_size(n, [&](auto NC) -> cudaError_t {
+    constexpr int N = decltype(NC)::value;
+    two = N > 0 && plan_has24(N);
+    return cudaSuccess;
+  });
+  return two;
+}
+
 // Raises the dynamic shared-memory limit of every FFT kernel (once per process).
 cudaError_t fft_configure(size_t max_bytes) {
   for (int n : kPlanSizes) {
@@ -1281,18 +1304,28 @@ cudaError_t fft_configure(size_t max_bytes) {
                              (int)(max_bytes - fa.sharedSizeBytes));                      \
     if (r != cudaSuccess) return r;                                                       \
   }
-      PLC_SMEM((k_fft_x_fwd<double, N>));
-      PLC_SMEM((k_fft_x_fwd_div<double, N, true>));
-      PLC_SMEM((k_fft_x_bwd<double, N, true>));
-      PLC_SMEM((k_fft_x_bwd<double, N, false>));
-      PLC_SMEM((k_fft_y<double, N, true>));
-      PLC_SMEM((k_fft_y<double, N, false>));
-      PLC_SMEM((k_fft_x_fwd<float, N>));
-      PLC_SMEM((k_fft_x_fwd_div<float, N, true>));
-      PLC_SMEM((k_fft_x_bwd<float, N, true>));
-      PLC_SMEM((k_fft_x_bwd<float, N, false>));
-      PLC_SMEM((k_fft_y<float, N, true>));
-      PLC_SMEM((k_fft_y<float, N, false>));
+      auto conf = [&](auto PC) -> cudaError_t {
+        constexpr int PL = decltype(PC)::value;
+        PLC_SMEM((k_fft_x_fwd<double, N, PL>));
+        PLC_SMEM((k_fft_x_fwd_div<double, N, true, PL>));
+        PLC_SMEM((k_fft_x_bwd<double, N, true, PL>));
+        PLC_SMEM((k_fft_x_bwd<double, N, false, PL>));
+        PLC_SMEM((k_fft_y<double, N, true, PL>));
+        PLC_SMEM((k_fft_y<double, N, false, PL>));
+        PLC_SMEM((k_fft_x_fwd<float, N, PL>));
+        PLC_SMEM((k_fft_x_fwd_div<float, N, true, PL>));
+        PLC_SMEM((k_fft_x_bwd<float, N, true, PL>));
+        PLC_SMEM((k_fft_x_bwd<float, N, false, PL>));
+        PLC_SMEM((k_fft_y<float, N, true, PL>));
+        PLC_SMEM((k_fft_y<float, N, false, PL>));
+        return cudaSuccess;
+      };
+      r = conf(std::integral_constant<int, 0>{});
+      if (r != cudaSuccess) return r;
+      if constexpr (N > 0 && plan_has24(N)) {
+        r = conf(std::integral_constant<int, 1>{});
+        if (r != cudaSuccess) return r;
+      }
 #undef PLC_SMEM
       return cudaSuccess;
     });
@@ -1315,15 +1348,21 @@ cudaError_t fft_grids_t(plc_ctx *c, size_t dev_max, int sms) {
   const long long tiles_y = (long long)(nx / (2 * c->fft_lines_y)) * nz;
   cudaError_t e = with_size(nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    c->grid_xf = persistent_grid(k_fft_x_fwd<T, N>, 128, need[0], sms, tiles_x);
-    c->grid_xb = persistent_grid(k_fft_x_bwd<T, N, true>, 128, need[2], sms, tiles_x);
-    return cudaSuccess;
+    return with_plan<N>(c->fft_plan_x, [&](auto PC) -> cudaError_t {
+      constexpr int PL = decltype(PC)::value;
+      c->grid_xf = persistent_grid(k_fft_x_fwd<T, N, PL>, 128, need[0], sms, tiles_x);
+      c->grid_xb = persistent_grid(k_fft_x_bwd<T, N, true, PL>, 128, need[2], sms, tiles_x);
+      return cudaSuccess;
+    });
   });
   if (e != cudaSuccess) return e;
   return with_size(ny, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    c->grid_y = persistent_grid(k_fft_y<T, N, false>, 256, need[3], sms, tiles_y);
-    return cudaSuccess;
+    return with_plan<N>(c->fft_plan_y, [&](auto PC) -> cudaError_t {
+      constexpr int PL = decltype(PC)::value;
+      c->grid_y = persistent_grid(k_fft_y<T, N, false, PL>, 256, need[3], sms, tiles_y);
+      return cudaSuccess;
+    });
   });
 }
 
@@ -1356,17 +1395,20 @@ cudaError_t fft_x_fwd_t(const plc_ctx *c, const T *p, const T *u, const T *v, co
                         cudaStream_t s) {
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    if (p) {
-      const int nl = c->fft_lines_x;
-      k_fft_x_fwd<T, N><<<c->grid_xf, 128, smem_x_fwd<T>(c->nx, nl), s>>>(
-          c->geo(), dev_plan<T>(c->plan_x), nl, p, var);
-    } else {
-      const int nl = c->fft_lines_xf;
-      dim3 grid(c->ny / (2 * nl), c->nz);
-      k_fft_x_fwd_div<T, N, true><<<grid, 256, fft_bytes<T>(c->nx, nl), s>>>(
-          c->geo(), dev_plan<T>(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
-    }
-    return cudaGetLastError();
+    return with_plan<N>(c->fft_plan_x, [&](auto PC) -> cudaError_t {
+      constexpr int PL = decltype(PC)::value;
+      if (p) {
+        const int nl = c->fft_lines_x;
+        k_fft_x_fwd<T, N, PL><<<c->grid_xf, 128, smem_x_fwd<T>(c->nx, nl), s>>>(
+            c->geo(), dev_plan<T>(c->plan_x), nl, p, var);
+      } else {
+        const int nl = c->fft_lines_xf;
+        dim3 grid(c->ny / (2 * nl), c->nz);
+        k_fft_x_fwd_div<T, N, true, PL><<<grid, 256, fft_bytes<T>(c->nx, nl), s>>>(
+            c->geo(), dev_plan<T>(c->plan_x), nl, c->d_sc, nullptr, u, v, w, var);
+      }
+      return cudaGetLastError();
+    });
   });
 }
 
@@ -1377,13 +1419,16 @@ cudaError_t fft_x_bwd_t(const plc_ctx *c, const T *var, T *p, bool fuse_bc, cuda
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    if (fuse_bc)
-      k_fft_x_bwd<T, N, true><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan<T>(c->plan_x), nl,
-                                                           nf, var, p);
-    else
-      k_fft_x_bwd<T, N, false><<<c->grid_xb, 128, sm, s>>>(c->geo(), dev_plan<T>(c->plan_x), nl,
-                                                            nf, var, p);
-    return cudaGetLastError();
+    return with_plan<N>(c->fft_plan_x, [&](auto PC) -> cudaError_t {
+      constexpr int PL = decltype(PC)::value;
+      if (fuse_bc)
+        k_fft_x_bwd<T, N, true, PL><<<c->grid_xb, 128, sm, s>>>(
+            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p);
+      else
+        k_fft_x_bwd<T, N, false, PL><<<c->grid_xb, 128, sm, s>>>(
+            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p);
+      return cudaGetLastError();
+    });
   });
 }
 
@@ -1393,13 +1438,16 @@ cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
   const size_t sm = smem_y<T>(c->ny, nl);
   return with_size(c->ny, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    if (inverse)
-      k_fft_y<T, N, true><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz, dev_plan<T>(c->plan_y),
-                                                      nl, var);
-    else
-      k_fft_y<T, N, false><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
-                                                       dev_plan<T>(c->plan_y), nl, var);
-    return cudaGetLastError();
+    return with_plan<N>(c->fft_plan_y, [&](auto PC) -> cudaError_t {
+      constexpr int PL = decltype(PC)::value;
+      if (inverse)
+        k_fft_y<T, N, true, PL><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
+                                                            dev_plan<T>(c->plan_y), nl, var);
+      else
+        k_fft_y<T, N, false, PL><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
+                                                             dev_plan<T>(c->plan_y), nl, var);
+      return cudaGetLastError();
+    });
   });
 }
 
@@ -1463,40 +1511,54 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
     return best;
   };
   // tunes one line count *field over the divisors of `pairs` (multiples of
-  // `step`); `fits` says whether a value fits the device
-  auto tune = [&](int *field, int pairs, int step, auto fits, auto launch) {
-    int best_d = *field;
+  // `step`) and, when `plan` is given and the length has two plan families
+  // (`two`), the family *plan with it; `fits` says whether a value fits the
+  // device
+  auto tune = [&](int *field, int *plan, bool two, int pairs, int step, auto fits,
+                  auto launch) {
+    int best_d = *field, best_p = plan ? *plan : 0;
     float best_t = -1.f;
-    for (int d = step; d <= pairs && d <= 16; d += step) {
-      if (pairs % d || !fits(d)) continue;
-      *field = d;
-      if (fft_grids_t<T>(c, dev_max, sms) != cudaSuccess) continue;
-      const float t = time_of(launch);
-      if (t >= 0.f && (best_t < 0.f || t < best_t)) {
-        best_t = t;
-        best_d = d;
+    const int p0 = (plan && two && !c->fft_plans_pinned) ? 0 : (plan ? *plan : 0);
+    const int p1 = (plan && two && !c->fft_plans_pinned) ? 1 : p0;
+    for (int pl = p0; pl <= p1; ++pl) {
+      if (plan) *plan = pl;
+      for (int d = step; d <= pairs && d <= 16; d += step) {
+        if (pairs % d || !fits(d)) continue;
+        *field = d;
+        if (fft_grids_t<T>(c, dev_max, sms) != cudaSuccess) continue;
+        const float t = time_of(launch);
+        if (t >= 0.f && (best_t < 0.f || t < best_t)) {
+          best_t = t;
+          best_d = d;
+          best_p = pl;
+        }
       }
     }
     *field = best_d;
+    if (plan) *plan = best_p;
     cudaGetLastError();  // a candidate that failed to launch leaves no error behind
   };
   T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W], *p = f[PLC_P], *spec = f[PLC_SPEC];
-  tune(&c->fft_lines_xf, ny / 2, 1, [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
+  // y: tile and plan family timed on a forward and an inverse transform
+  tune(&c->fft_lines_y, &c->fft_plan_y, fft_has_two_plans(ny), nx / 2, sizeof(T) == 4 ? 2 : 1,
+       [&](int d) { return smem_y<T>(ny, d) <= dev_max; },
+       [&]() -> cudaError_t {
+         cudaError_t r = launch_fft_y(c, spec, false, s);
+         return r == cudaSuccess ? launch_fft_y(c, spec, true, s) : r;
+       });
+  // x: the plan family (shared by both x transforms) with the backward tile,
+  // then the forward tile under that family
+  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), ny / 2, 1,
+       [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
+       [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
+  tune(&c->fft_lines_xf, nullptr, false, ny / 2, 1,
+       [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t {
          if constexpr (sizeof(T) == 8)
            return launch_fft_x_fwd(c, nullptr, u, v, w, spec, s);
          else
            return launch_fft_x_fwd(c, u, v, w, spec, s);
        });
-  tune(&c->fft_lines_y, nx / 2, sizeof(T) == 4 ? 2 : 1,
-       [&](int d) { return smem_y<T>(ny, d) <= dev_max; },
-       [&]() -> cudaError_t {
-         cudaError_t r = launch_fft_y(c, spec, false, s);
-         return r == cudaSuccess ? launch_fft_y(c, spec, true, s) : r;
-       });
-  tune(&c->fft_lines_x, ny / 2, 1,
-       [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
-       [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return fft_grids_t<T>(c, dev_max, sms);

@@ -98,6 +98,11 @@ struct plc_ctx {
   int fft_lines_x = 1, fft_lines_xf = 1, fft_lines_y = 1;  // line pairs per tile
   int grid_xf = 1, grid_xb = 1, grid_y = 1;                 // persistent grids
   int tuned_lines[3] = {0, 0, 0};  // autotuned (xf, x, y) line pairs, 0 = not tuned
+  // radix plan family of the x and y transforms (0: 16/8/4/2/3 passes; 1: two
+  // passes ending in radix 24, lengths 24 .. 384 with one factor 3); autotuned
+  // with the tiles unless the environment pins them
+  int fft_plan_x = 0, fft_plan_y = 0;
+  bool fft_plans_pinned = false;
   // scalars and scratch
   plc::StepConst *d_sc = nullptr;
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce
@@ -243,6 +248,8 @@ cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);
 // times the feasible tile sizes of each transform on the context's buffers
 // and keeps the fastest (overwrites the spectral array and p)
 cudaError_t fft_autotune(plc_ctx *c);
+// whether a line length has the radix-24 plan family as well
+bool fft_has_two_plans(int n);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 // var -= delta on the interior of the context's field (either form), synchronous

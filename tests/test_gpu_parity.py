@@ -318,7 +318,8 @@ def test_fft_tiles_pinned_by_environment(monkeypatch):
     kw = case_kwargs(64, 48, 32)
     monkeypatch.setenv("PLC_FFT_TILES", "2,1,4")
     ch = Channel(channel_params(**kw))
-    assert ch.fft_tiles == {"x_fwd": 2, "x_bwd": 1, "y": 4}
+    t = ch.fft_tiles
+    assert (t["x_fwd"], t["x_bwd"], t["y"]) == (2, 1, 4)
     monkeypatch.setenv("PLC_FFT_TILES", "5,1,1")  # 5 does not divide ny/2 = 24
     with pytest.raises(PlcError):
         Channel(channel_params(**kw))
@@ -328,3 +329,39 @@ def test_fft_tiles_pinned_by_environment(monkeypatch):
     monkeypatch.setenv("PLC_FFT_TILES_F32", "3,3,3")  # odd y tiles are refused in FP32
     with pytest.raises(PlcError):
         Channel(prm)
+
+
+@pytest.mark.parametrize("plans", ["0,0", "0,1", "1,0", "1,1"])
+def test_fft_plan_families_pinned_by_environment(monkeypatch, plans):
+    """PLC_FFT_PLANS / PLC_FFT_PLANS_F32 pin the radix plan families: the
+    Poisson solve of every family matches the oracle in FP64, and the mixed
+    form's projection is divergence-free with every family; a family a length
+    does not have is refused."""
+    from powerllel_channel_sycl_b200 import Channel, PlcError
+    px, py = (int(x) for x in plans.split(","))
+    nx, ny, nz = 96, 48, 8  # 96 = 4 x 24 and 48 = 2 x 24: both families in x and y
+    monkeypatch.setenv("PLC_FFT_PLANS", plans)
+    case, ch = make_pair(nx, ny, nz)
+    t = ch.fft_tiles
+    assert (t["plan_x"], t["plan_y"]) == (px, py)
+    u, v, w = bc_fields(case, 9)
+    p = case.zeros()
+    case.calc_rhs(u, v, w, p)
+    ch.upload("p", p)
+    case.poisson(p)
+    ch.execute_poisson_solver()
+    assert rel_l2(demean(ch.download("p")), demean(p)) < 1e-12
+    monkeypatch.setenv("PLC_FFT_PLANS_F32", plans)
+    prm = channel_params(**case_kwargs(nx, ny, nz))
+    prm.precision = 1
+    m = Channel(prm)
+    t = m.fft_tiles
+    assert (t["plan_x"], t["plan_y"]) == (px, py)
+    rng = np.random.default_rng(3)
+    for q in "uvw":
+        m.upload(q, rng.normal(size=m.shape))
+    m.project()
+    assert m.check()[2][0] < 1e-3
+    monkeypatch.setenv("PLC_FFT_PLANS", "1,1")
+    with pytest.raises(PlcError):  # 64 = 2^6 has no radix-24 family
+        make_pair(64, 48, 8)
