@@ -1020,11 +1020,31 @@ __device__ __forceinline__ void thomas_sweep(int nz, const Sys &sys) {
 // q = right-hand side and solution (plane stride `plane`), rp = reciprocal
 // pivots (stride PS), ca / cc = the 1-D sub- and super-diagonal.  Same
 // operations in the same order as thomas_sweep.
+// L2 priorities of the sweep's traffic: the right-hand side and the forward
+// values are read for the last time (evict first); the forward values are
+// stored to be read back by the back substitution (evict last).
+__device__ __forceinline__ double ld_last_use(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_last_use(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ unsigned long long l2_keep_policy() {
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void st_keep(double *p, double v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_keep(float *p, float v, unsigned long long pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol)
+               : "memory");
+}
+
 template <class A, int PF>
 __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long long plane,
                                                const A *__restrict__ rp, long long PS,
                                                const A *__restrict__ ca,
                                                const A *__restrict__ cc) {
+  const unsigned long long keep = l2_keep_policy();
   A prev = q[0];
   const A *lq = q + plane;  // next right-hand side to load (k = 1)
   const A *lr = rp;         // next pivot to load (k - 1 = 0)
@@ -1034,7 +1054,7 @@ __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long l
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (1 + s < nz) {
-        xn[s] = *lq;
+        xn[s] = ld_last_use(lq);
         lq += plane;
         rn[s] = __ldg(lr);
         lr += PS;
@@ -1049,7 +1069,7 @@ __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long l
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (k + PF + s < nz) {
-          xn[s] = *lq;
+          xn[s] = ld_last_use(lq);
           lq += plane;
           rn[s] = __ldg(lr);
           lr += PS;
@@ -1059,7 +1079,7 @@ __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long l
         if (k + s < nz) {
           A cur = x[s];
           cur -= (__ldg(ca + k + s) * r[s]) * prev;
-          *wq = cur;
+          st_keep(wq, cur, keep);
           wq += plane;
           prev = cur;
         }
@@ -1077,7 +1097,7 @@ __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long l
 #pragma unroll
     for (int s = 0; s < PF; ++s)
       if (nz - 2 - s >= 0) {
-        xn[s] = *bq;
+        xn[s] = ld_last_use(bq);
         bq -= plane;
         rn[s] = __ldg(br);
         br -= PS;
@@ -1092,7 +1112,7 @@ __device__ __forceinline__ void thomas_inplace(int nz, A *__restrict__ q, long l
 #pragma unroll
       for (int s = 0; s < PF; ++s)
         if (k - PF - s >= 0) {
-          xn[s] = *bq;
+          xn[s] = ld_last_use(bq);
           bq -= plane;
           rn[s] = __ldg(br);
           br -= PS;
