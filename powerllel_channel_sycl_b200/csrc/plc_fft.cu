@@ -738,7 +738,8 @@ __global__ void __launch_bounds__(128) k_fft_x_fwd(Geo g, FftDev<typename Cx<T>:
 // FUSE_BC the pressure halos are written as well (updateBoundP).
 template <class T, int N, bool FUSE_BC, int PL>
 __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>::V> P, int nl,
-                                                   double nf, const T *__restrict__ var, T *p) {
+                                                   double nf, const T *__restrict__ var, T *p,
+                                                   int rev) {
   using V = typename Cx<T>::V;
   extern __shared__ __align__(16) unsigned char fft_smem[];
   V *smem = reinterpret_cast<V *>(fft_smem);
@@ -750,7 +751,8 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
   const T scale = T(nf);
   const FastDiv fcpr(n / (16 / sizeof(T)));
   auto issue = [&](int tile) {
-    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
+    const int tt = rev ? ntiles - 1 - tile : tile;  // plane order
+    const int j0 = (tt % tiles_y) * R, k = tt / tiles_y;
     stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n, fcpr);
     cp_async_commit();
   };
@@ -758,7 +760,8 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
   if (tile < ntiles) issue(tile);
   const int half = n >> 1;
   for (; tile < ntiles; tile += gridDim.x) {
-    const int j0 = (tile % tiles_y) * R, k = tile / tiles_y;
+    const int tt = rev ? ntiles - 1 - tile : tile;
+    const int j0 = (tt % tiles_y) * R, k = tt / tiles_y;
     cp_async_wait_all();
     __syncthreads();
     for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
@@ -863,7 +866,7 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
 template <class T, int N, bool INV, int PL>
 __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
                                                FftDev<typename Cx<T>::V> P, int nl,
-                                               T *__restrict__ var) {
+                                               T *__restrict__ var, int rev) {
   using V = typename Cx<T>::V;
   extern __shared__ __align__(16) unsigned char fft_smem[];
   V *smem = reinterpret_cast<V *>(fft_smem);
@@ -874,7 +877,8 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
   const int ntiles = tiles_x * nz;
   const FastDiv fcpr(TX / (16 / sizeof(T))), fnl(nl);
   auto issue = [&](int tile) {
-    const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
+    const int tt = rev ? ntiles - 1 - tile : tile;  // plane order
+    const int i0 = (tt % tiles_x) * TX, k = tt / tiles_x;
     stage_rows(S, var + (long long)k * nx * ny + i0, n, TX, nx, fcpr);
     cp_async_commit();
   };
@@ -882,7 +886,8 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
   if (tile < ntiles) issue(tile);
   const int half = n >> 1;
   for (; tile < ntiles; tile += gridDim.x) {
-    const int i0 = (tile % tiles_x) * TX, k = tile / tiles_x;
+    const int tt = rev ? ntiles - 1 - tile : tile;
+    const int i0 = (tt % tiles_x) * TX, k = tt / tiles_x;
     T *plane = var + (long long)k * nx * ny + i0;
     cp_async_wait_all();
     __syncthreads();
@@ -1443,10 +1448,10 @@ cudaError_t fft_x_bwd_t(const plc_ctx *c, const T *var, T *p, bool fuse_bc, cuda
       constexpr int PL = decltype(PC)::value;
       if (fuse_bc)
         k_fft_x_bwd<T, N, true, PL><<<c->grid_xb, 128, sm, s>>>(
-            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p);
+            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p, c->order[SK_XB]);
       else
         k_fft_x_bwd<T, N, false, PL><<<c->grid_xb, 128, sm, s>>>(
-            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p);
+            c->geo(), dev_plan<T>(c->plan_x), nl, nf, var, p, c->order[SK_XB]);
       return cudaGetLastError();
     });
   });
@@ -1462,10 +1467,12 @@ cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
       constexpr int PL = decltype(PC)::value;
       if (inverse)
         k_fft_y<T, N, true, PL><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
-                                                            dev_plan<T>(c->plan_y), nl, var);
+                                                            dev_plan<T>(c->plan_y), nl, var,
+                                                            c->order[SK_YB]);
       else
         k_fft_y<T, N, false, PL><<<c->grid_y, 256, sm, s>>>(c->nx, c->ny, c->nz,
-                                                             dev_plan<T>(c->plan_y), nl, var);
+                                                             dev_plan<T>(c->plan_y), nl, var,
+                                                             c->order[SK_YF]);
       return cudaGetLastError();
     });
   });

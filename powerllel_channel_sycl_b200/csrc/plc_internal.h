@@ -10,9 +10,13 @@
 
 namespace plc {
 
+// indices into plc_ctx::order: the step kernels whose plane order is a choice
+enum StepKernel { SK_RK2, SK_YF, SK_YB, SK_XB, SK_ORDERS };
+
 // ---------------------------------------------------------------------------
 // Geometry passed by value to every kernel.
 // ---------------------------------------------------------------------------
+
 struct Geo {
   int nx, ny, nz;
   int X, Y;           // halo'd x and y lengths (nx+2, ny+2)
@@ -103,6 +107,10 @@ struct plc_ctx {
   // with the tiles unless the environment pins them
   int fft_plan_x = 0, fft_plan_y = 0;
   bool fft_plans_pinned = false;
+  // Plane order of the step kernels (0: low planes first, 1: high planes
+  // first), set per form at creation from measurements; only the speed
+  // depends on it.
+  unsigned char order[plc::SK_ORDERS] = {0, 0, 0, 0};
   // scalars and scratch
   plc::StepConst *d_sc = nullptr;
   double *d_partials = nullptr;        // 8 * kMaxBlocksReduce

@@ -289,7 +289,7 @@ template <int STAGE, bool FUSE, bool CRF>
 __global__ void __launch_bounds__(RX *TY, 2)
     k_rk_tma(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
              const __grid_constant__ CUtensorMap mw, Geo g, const StepConst *__restrict__ sc,
-             double u_crf, double *ou, double *ov, double *ow, int kchunk, int *err) {
+             double u_crf, double *ou, double *ov, double *ow, int kchunk, int *err, int rev) {
   extern __shared__ unsigned char smem_raw[];
   double *base = reinterpret_cast<double *>(
       (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(RX *TY, 2)
   const int i = x0 + tx + 1, ja = y0 + 2 * ty + 1, jb = ja + 1;
   const bool act_a = (i <= g.nx) && (ja <= g.ny);
   const bool act_b = act_a && (jb <= g.ny);
-  const int kb = blockIdx.z * kchunk + 1;
+  const int zc = rev ? (int)gridDim.z - 1 - (int)blockIdx.z : (int)blockIdx.z;  // plane order
+  const int kb = zc * kchunk + 1;
   const int ke = min(kb + kchunk - 1, g.nz);
   const int plast = ke + 1;  // last plane to bring in
 
@@ -719,7 +720,7 @@ __global__ void __launch_bounds__(256, 2) k_correct_fused(Geo g, StepConst *sc, 
 }
 
 // The mixed form's fused correction: correctVel (mod_calcVel.cc:272-274) plus
-// the forcing sc->force[d] that its forward x transform has already reduced
+// the forcing sc->force[d] that its fused RK2 stage has already reduced
 // (0 for unforced components), written with the halo images and wall ghosts.
 // No reduction, so a plain grid: each thread takes KZ planes of one column
 // (p(k+1) of a plane is p(k) of the next) with all loads issued first.
@@ -1104,10 +1105,12 @@ cudaError_t launch_rk_tma(const plc_ctx *c, const CUtensorMap &mu, const CUtenso
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   if (u_crf != 0.0)
     k_rk_tma<STAGE, FUSE, true><<<grid, RX * TY, rk_tma_smem_bytes(), s>>>(
-        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
+        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err,
+        STAGE == 2 ? c->order[SK_RK2] : 0);
   else
     k_rk_tma<STAGE, FUSE, false><<<grid, RX * TY, rk_tma_smem_bytes(), s>>>(
-        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err);
+        mu, mv, mw, c->geo(), c->d_sc, u_crf, ou, ov, ow, kchunk, c->d_err,
+        STAGE == 2 ? c->order[SK_RK2] : 0);
   return cudaGetLastError();
 }
 
