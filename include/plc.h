@@ -566,11 +566,14 @@ int plc_host_free(void *ptr);
  * entries) and d_mean (one double), all device memory, and a cudaStream_t
  * (NULL = default stream); the result is written to d_mean on that stream.
  * Nothing is allocated: the partial sums live in a static 128 KiB array of
- * the library (one double-double per z plane), held by every GPU that loads
- * the library until exit, so nz is limited to 8192 (PLC_ERR_SIZE beyond).
- * All calls share that array: calls that overlap on the GPU race.  The first
- * call on a device looks up the array's address (once per device); make it
- * before any stream capture.  Errors: plc_last_error(NULL). */
+ * the library (8192 double-double block sums, at least one per z plane),
+ * held by every GPU that loads the library until exit, so nz is limited to
+ * 8192 (PLC_ERR_SIZE beyond).  All calls share that array: calls that
+ * overlap on the GPU race.  A call outside stream capture looks up the
+ * array's address in the current CUDA context and remembers it; a call
+ * during capture uses the remembered address, so make one call outside
+ * capture first in each context (again after cudaDeviceReset).
+ * Errors: plc_last_error(NULL). */
 int plc_mean_noalloc(const double *d_var, const double *d_dzflzi, int nx, int ny,
                      int nz, int nx_global, int ny_global, double *d_mean,
                      void *stream);

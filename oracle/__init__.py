@@ -94,6 +94,8 @@ def lib():
             "orc_init_flow": (None, [G, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                      C.c_double, _dp, _dp, _dp, _dp]),
             "orc_step": (None, [G, vp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
+            "orc_run_cfl": (None, [G, vp, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp, _dp,
+                                   _dp, _dp, _dp, _dp]),
             "orc_calc_stat_sample": (None, [G, C.c_double, _dp, _dp, _dp, _dp,
                                             C.POINTER(C.c_void_p)]),
             "orc_wall_tau": (C.c_double, [G, C.c_int, C.c_double, _dp, C.c_double]),
@@ -289,6 +291,14 @@ class Case:
 
     def step(self, u, v, w, u1, v1, w1, p, nsteps=1):
         lib().orc_step(self.gp, self.ps, nsteps, u, v, w, u1, v1, w1, p)
+
+    def run_cfl(self, u, v, w, u1, v1, w1, p, nsteps, nt_check, cfl_target):
+        """nsteps of main.cc's loop with the CFL-controlled dt; returns the dt
+        of every step followed by the dt the next step would use."""
+        dts = np.zeros(nsteps + 1)
+        lib().orc_run_cfl(self.gp, self.ps, nsteps, nt_check, cfl_target, u, v, w, u1, v1, w1,
+                          p, dts)
+        return dts
 
 
 def set_threads(n: int) -> None:

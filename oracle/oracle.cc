@@ -1,8 +1,8 @@
 // CPU oracle for the PowerLLEL_Channel DNS time step -- TEST INFRASTRUCTURE.
 //
 // Plain FP64 restatement of the reference's hot path; see oracle.h for the
-// layout conventions and the parity status ("parity unpinned": the reference
-// ships no golden vectors and cannot be built here).  Compiled with
+// layout conventions and the parity status (pinned to the reference's own
+// modules compiled for the CPU, except for oneMKL's DFT).  Compiled with
 // -ffp-contract=off so that every expression is evaluated exactly in the
 // order written, which follows the reference expression by expression.
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
@@ -943,6 +943,52 @@ void orc_init_flow(const orc_grid *g, int initial_field, double u0,
 // ---------------------------------------------------------------------------
 // main.cc:116-154
 // ---------------------------------------------------------------------------
+// The CFL rate max(|u_c|/dx + |v_c|/dy + |w_c|/dzf) of calcMaxCFL
+// (mod_utils.cc:108-150) before its multiplication by dt: each point's value
+// is the reference's expression, and the maximum does not depend on the
+// order, so threads split the planes.
+static double cfl_rate(const orc_grid *g, const double *u, const double *v, const double *w) {
+  const Idx I = make_idx(g);
+  double best = 0.0;
+#pragma omp parallel for reduction(max : best)
+  for (int k = 1; k <= g->nz; ++k)
+    for (int j = 1; j <= g->ny; ++j)
+      for (int i = 1; i <= g->nx; ++i) {
+        const double cfl_tmp = fabs((u[I(i, j, k)] + u[I(i - 1, j, k)]) * 0.5) * g->dx_inv +
+                               fabs((v[I(i, j, k)] + v[I(i, j - 1, k)]) * 0.5) * g->dy_inv +
+                               fabs((w[I(i, j, k)] + w[I(i, j, k - 1)]) * 0.5) * g->dzf_inv[k];
+        if (cfl_tmp > best) best = cfl_tmp;
+      }
+  return best;
+}
+
+void orc_run_cfl(const orc_grid *g0, orc_poisson *ps, int nsteps, int nt_check,
+                 double cfl_target, double *u, double *v, double *w, double *u1,
+                 double *v1, double *w1, double *p, double *dt_used) {
+  // The time step of the main loop (main.cc:114-178) under a CFL target:
+  // dt = cfl_target / rate, where rate * dt is calcMaxCFL's value
+  // (mod_utils.cc:122-144), evaluated before the first step, after steps
+  // 1, 2, 4, 8, ... below nt_check (the first forcing step moves the bulk
+  // velocity from the initial field's rescaled value to vel_force), and
+  // after every nt_check-th step, where main.cc:156-178 runs its checks.
+  orc_grid g = *g0;
+  auto retune = [&]() {
+    const double rate = cfl_rate(&g, u, v, w);
+    if (rate > 0.0) g.dt = cfl_target / rate;
+  };
+  if (cfl_target > 0.0) retune();
+  for (int s = 1; s <= nsteps; ++s) {
+    if (dt_used) dt_used[s - 1] = g.dt;
+    orc_step(&g, ps, 1, u, v, w, u1, v1, w1, p);
+    if (cfl_target <= 0.0) continue;
+    if (s < nt_check && (s & (s - 1)) == 0)
+      retune();
+    else if (nt_check > 0 && s % nt_check == 0)
+      retune();
+  }
+  if (dt_used) dt_used[nsteps] = g.dt;
+}
+
 void orc_step(const orc_grid *g, orc_poisson *ps, int nsteps, double *u,
               double *v, double *w, double *u1, double *v1, double *w1,
               double *p) {

@@ -9,12 +9,23 @@
  * __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker;
  * the product library never links or calls it.
  *
- * PARITY STATUS: parity unpinned.  The reference ships no tests, golden
- * vectors or fixtures, and it cannot be built here (SYCL compiler, oneMKL,
- * oneDPL, MPI and HDF5 are absent).  The restatement is checked instead
- * against independent mathematics: its real FFT against numpy.fft, its
- * tridiagonal solve against a banded LU solve, and manufactured-solution /
- * divergence / bulk-flux invariants (tests/test_oracle_*.py).
+ * PARITY STATUS: pinned to the reference's own code, except for the DFT.
+ * The reference ships no tests, golden vectors or fixtures, and its build
+ * needs a SYCL compiler, oneMKL, oneDPL, MPI and HDF5, none of which is
+ * here.  Its time-step modules are instead compiled unmodified from its
+ * sources against host stand-ins for those libraries (oracle/reference_cpu,
+ * output oracle/_ref), and tests/test_reference_pin.py checks every
+ * function below against the reference's own: mesh, boundary updates, RK1,
+ * RK2, calcRHS, correctVel, transform2CRF, CFL/divergence maxima, the
+ * Thomas sweep and the initial v, w bit-identical; the bulk mean within the
+ * error bound of a sum in any order; the transforms to 1e-14 and ten full
+ * steps to 1e-12.  The one stage whose arithmetic is not the reference's
+ * own is oneMKL's DFT (closed source, absent): both the stand-in and this
+ * oracle compute the documented transform, checked against numpy.fft.  The
+ * noise generator of the initial field follows the C++ standard's minstd
+ * engine; oneDPL's exact stream is not available to compare.  Independent
+ * checks remain as well: numpy/scipy golden values and manufactured-solution
+ * / divergence / bulk-flux invariants (tests/test_oracle_*.py).
  *
  * Array layout (same as the reference's _Array3D with one halo cell on each
  * side, src/mod_type.hh:81-306): a field of interior size nx*ny*nz is stored
@@ -128,6 +139,14 @@ void orc_init_flow(const orc_grid *g, int initial_field, double u0,
 void orc_step(const orc_grid *g, orc_poisson *ps, int nsteps, double *u,
               double *v, double *w, double *u1, double *v1, double *w1,
               double *p);
+/* nsteps of the main loop with a CFL-controlled dt (cfl_target > 0): dt =
+ * cfl_target / (calcMaxCFL's value / dt) before step 1, after steps 1, 2, 4,
+ * ... below nt_check and after every nt_check-th step.  dt_used (nsteps+1
+ * entries, or NULL) receives the dt of each step and, last, the dt the next
+ * step would use.  With cfl_target <= 0 dt stays g->dt. */
+void orc_run_cfl(const orc_grid *g, orc_poisson *ps, int nsteps, int nt_check,
+                 double cfl_target, double *u, double *v, double *w, double *u1,
+                 double *v1, double *w1, double *p, double *dt_used);
 
 /* ---- mod_statistics (src/mod_statistics.cc:30-106) ---- */
 /* One sample of calcStat: adds to the enabled running sums (sums[q] != NULL,

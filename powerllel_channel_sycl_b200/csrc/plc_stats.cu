@@ -76,8 +76,10 @@ __global__ void __launch_bounds__(256) k_stat_profiles(int nx, int ny, int nz, S
   }
 }
 
-// Error-free double-double accumulation (Knuth TwoSum): the rounded total is
-// independent of the order of the terms.
+// Double-double accumulation (Knuth TwoSum): each addition's rounding error is
+// carried in the low word, so the rounded total is nearly independent of the
+// order of the terms (the low words' own sums still round, which can move the
+// total by an ulp on ill-conditioned data).
 __device__ __forceinline__ void dd_acc(double &hi, double &lo, double x) {
   const double s = hi + x;
   const double bb = s - hi;

@@ -365,3 +365,18 @@ def test_fft_plan_families_pinned_by_environment(monkeypatch, plans):
     monkeypatch.setenv("PLC_FFT_PLANS", "1,1")
     with pytest.raises(PlcError):  # 64 = 2^6 has no radix-24 family
         make_pair(64, 48, 8)
+
+
+@pytest.mark.parametrize("vel_crf", [0.0, 0.35])
+def test_transform2crf(vel_crf):
+    """transform2CRF (mod_calcVel.cc:13-25): vel -= vel_crf on the interior
+    only (halos untouched) and vel_force -= vel_crf, bit-identical to the
+    oracle; a zero vel_crf leaves both as they are."""
+    case, ch = make_pair(32, 24, 16)
+    (u,) = random_fields(case, 11, n=1)
+    ch.upload("u", u)
+    vf_ref = oracle.C.c_double(1.25)
+    oracle.lib().orc_transform2crf(case.gp, vel_crf, u, oracle.C.byref(vf_ref))
+    vf = ch.transform2CRF(vel_crf, "u", 1.25)
+    assert vf == vf_ref.value == 1.25 - vel_crf
+    np.testing.assert_array_equal(ch.download("u"), u)

@@ -151,3 +151,30 @@ def test_pressure_roundoff_floor():
     floor_u = rel_l2(b[0], a[0])
     assert 1e-13 < floor_p < 3e-12
     assert floor_u < 1e-15
+
+
+def test_run_cfl_schedule():
+    """orc_run_cfl: without a CFL target it is the fixed-dt loop; with one, dt
+    is re-evaluated before step 1, after steps 1, 2, 4, 8 (below nt_check) and
+    after every nt_check-th step, each time to cfl_target / rate, where
+    rate * dt is calcMaxCFL's value."""
+    case = oracle.Case(32, 24, 16)
+    fields = case.init_flow("poi", noise_intensity=0.1)
+    a = [f.copy() for f in fields] + [case.zeros() for _ in range(4)]
+    b = [f.copy() for f in fields] + [case.zeros() for _ in range(4)]
+    case.step(*a, nsteps=3)
+    dts = case.run_cfl(*b, nsteps=3, nt_check=10, cfl_target=0.0)
+    assert dts.tolist() == [case.dt] * 4
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    c = [f.copy() for f in fields] + [case.zeros() for _ in range(4)]
+    rate0 = case.max_cfl(*c[:3])[0] / case.dt
+    dts = case.run_cfl(*c, nsteps=12, nt_check=6, cfl_target=0.4)
+    assert dts[0] == 0.4 / rate0
+    # re-evaluated after steps 1, 2, 4 (below nt_check = 6) and 6, 12
+    changes = [s for s in range(1, 13) if dts[s] != dts[s - 1]]
+    assert set(changes) <= {1, 2, 4, 6, 12}, changes
+    assert dts[3] == dts[2] and dts[5] == dts[4] and dts[7:12].tolist() == [dts[6]] * 5
+    # the dt after the last step puts the final field at the target CFL
+    rate = case.max_cfl(*c[:3])[0] / case.dt
+    assert dts[12] == 0.4 / rate
