@@ -164,12 +164,18 @@ int plc_field_ptr_f32(plc_ctx *ctx, int field, float **d_ptr, size_t *count, int
  * feasible size on the device (the choice changes speed, never results).
  * No counterpart in the reference. */
 int plc_fft_tiles(const plc_ctx *ctx, int *lines_xf, int *lines_x, int *lines_y);
-/* The radix plan family of the x and y transforms, timed per context with the
- * tiles where a length has two (0: radix 16, one 8/4/2, then 3s; 1: for
- * lengths 3 * 2^a with 3 <= a <= 7, two passes ending in a radix-24
- * butterfly).  PLC_FFT_PLANS (FP64) and PLC_FFT_PLANS_F32 (mixed), "x,y",
- * pin them. */
+/* The plan family of the (backward) x and the y transforms, timed per
+ * context with the tiles where a length has more than one (0: radix 16, one
+ * 8/4/2, then 3s; 1: for lengths 3 * 2^a with 3 <= a <= 7, two passes
+ * ending in a radix-24 butterfly; 2: warp-line kernels, groups of four
+ * warps transforming their own lines with no block barrier, for lengths
+ * 32, 48, 64, 96, 128, 192, 256, 384, 512, 768).  PLC_FFT_PLANS (FP64) and
+ * PLC_FFT_PLANS_F32 (mixed), "x,y", pin them (x for both x transforms).
+ * No counterpart in the reference. */
 int plc_fft_plans(const plc_ctx *ctx, int *plan_x, int *plan_y);
+/* The family of the forward x transform (fused with calcRHS in the step),
+ * timed separately from the backward one.  No counterpart in the reference. */
+int plc_fft_plan_x_fwd(const plc_ctx *ctx, int *plan);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

@@ -92,6 +92,7 @@ _SIGS = {
     "plc_field_ptr_f32": [_vp, _int, C.POINTER(_vp), C.POINTER(C.c_size_t), C.POINTER(_int)],
     "plc_fft_tiles": [_vp, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int)],
     "plc_fft_plans": [_vp, C.POINTER(_int), C.POINTER(_int)],
+    "plc_fft_plan_x_fwd": [_vp, C.POINTER(_int)],
     "plc_upload": [_vp, _int, _hp],
     "plc_download": [_vp, _int, _hp],
     "plc_get_dt": [_vp, C.POINTER(_dbl)],

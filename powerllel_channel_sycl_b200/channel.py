@@ -159,14 +159,16 @@ class Channel:
 
     @property
     def fft_tiles(self):
-        """Line pairs per tile (x forward, x backward, y) and the radix plan
-        families of the x and y transforms chosen by the autotuner."""
+        """Line pairs per tile (x forward, x backward, y) and the plan
+        families of the backward x, the y and the forward x transforms chosen
+        by the autotuner."""
         a, b, c = C.c_int(), C.c_int(), C.c_int()
         self._check(lib().plc_fft_tiles(self._ctx, C.byref(a), C.byref(b), C.byref(c)))
-        px, py = C.c_int(), C.c_int()
+        px, py, pxf = C.c_int(), C.c_int(), C.c_int()
         self._check(lib().plc_fft_plans(self._ctx, C.byref(px), C.byref(py)))
+        self._check(lib().plc_fft_plan_x_fwd(self._ctx, C.byref(pxf)))
         return {"x_fwd": a.value, "x_bwd": b.value, "y": c.value, "plan_x": px.value,
-                "plan_y": py.value}
+                "plan_y": py.value, "plan_x_fwd": pxf.value}
 
     def ptr_f32(self, f):
         """(device pointer, element count, row pitch) of an FP32 field of a mixed context."""

@@ -552,15 +552,19 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     const unsigned char fp32[SK_ORDERS] = {0, 1, 0, 1};
     for (int q = 0; q < SK_ORDERS; ++q) c->order[q] = c->mixed ? fp32[q] : fp64[q];
   }
-  // PLC_FFT_PLANS / PLC_FFT_PLANS_F32 = "x,y" pin the radix plan families of
-  // the x and y transforms (0 or 1; 1 only for lengths that have it) the same
-  // way; the tiles are then timed under the pinned families.
+  // PLC_FFT_PLANS / PLC_FFT_PLANS_F32 = "x,y" pin the plan families of the x
+  // and y transforms (0: radix 16/8/4/2/3 passes, 1: two passes ending in
+  // radix 24, 2: warp-line kernels; 1 and 2 only for lengths that have them)
+  // the same way; the tiles are then timed under the pinned families.
   if (const char *env = getenv(c->mixed ? "PLC_FFT_PLANS_F32" : "PLC_FFT_PLANS")) {
     int px = -1, py = -1;
-    if (sscanf(env, "%d,%d", &px, &py) != 2 || px < 0 || px > 1 || py < 0 || py > 1 ||
-        (px == 1 && !fft_has_two_plans(c->nx)) || (py == 1 && !fft_has_two_plans(c->ny)))
+    if (sscanf(env, "%d,%d", &px, &py) != 2 || px < 0 || px > 2 || py < 0 || py > 2 ||
+        (px == 1 && !fft_has_two_plans(c->nx)) || (py == 1 && !fft_has_two_plans(c->ny)) ||
+        (px == 2 && !fft_has_warp_plan(c->nx, c->ny)) ||
+        (py == 2 && !fft_has_warp_plan(c->ny, c->nx)))
       return fail(set_error(c, PLC_ERR_ARG, std::string("invalid FFT plans in the environment: ") + env));
     c->fft_plan_x = px;
+    c->fft_plan_xf = px;
     c->fft_plan_y = py;
     c->fft_plans_pinned = true;
     if ((e = fft_set_lines(c, c->fft_lines_xf, c->fft_lines_x, c->fft_lines_y)) != cudaSuccess)
@@ -662,6 +666,12 @@ int plc_fft_plans(const plc_ctx *c, int *plan_x, int *plan_y) {
   if (!c) return set_error(nullptr, PLC_ERR_ARG, "null context");
   if (plan_x) *plan_x = c->fft_plan_x;
   if (plan_y) *plan_y = c->fft_plan_y;
+  return PLC_OK;
+}
+
+int plc_fft_plan_x_fwd(const plc_ctx *c, int *plan) {
+  if (!c || !plan) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  *plan = c->fft_plan_xf >= 0 ? c->fft_plan_xf : c->fft_plan_x;
   return PLC_OK;
 }
 

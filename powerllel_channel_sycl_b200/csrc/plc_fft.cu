@@ -933,6 +933,400 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
 }
 
 // ---------------------------------------------------------------------------
+// Warp-line transforms (plan family 2).  A warp owns L complex lines (2L
+// real lines) and transforms them with no block barrier: the first radix
+// pass loads its inputs straight from global memory into registers (a
+// Stockham pass of radix R reads the elements j + r N/R of a line, which are
+// consecutive over the lanes), the passes in between exchange through the
+// warp's own shared-memory lines under __syncwarp, and the last pass of an
+// inverse transform stores its outputs (the elements j + r N/R again)
+// straight to global memory; a forward transform separates the two real
+// spectra from the warp's shared memory after its last pass.  The plans
+// below give every lane the same number of butterflies in every pass, so
+// each lane holds L N / 32 complex values throughout.
+// ---------------------------------------------------------------------------
+
+// Prime-factor (Good-Thomas) 6- and 12-point DFTs: N = 3 N2 with N2 = 2 or 4
+// coprime to 3; x[(N2 n1 + 3 n2) mod N] -> 3-point DFTs over n1, then
+// N2-point DFTs over n2, with no twiddles; the output of (k1, k2) is
+// X[(N2 c k1 + 3 d k2) mod N], c = N2^-1 mod 3, d = 3^-1 mod N2
+// (W_N^(n k) = W_3^(n1 k1) W_N2^(n2 k2) for these index maps).
+template <bool INV>
+struct Dft<6, INV> {
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[6]) {
+    // n = (2 n1 + 3 n2) mod 6, k = (4 k1 + 3 k2) mod 6
+    V a[3] = {v[0], v[2], v[4]};
+    V b[3] = {v[3], v[5], v[1]};
+    Dft<3, INV>::run(a);
+    Dft<3, INV>::run(b);
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      V t[2] = {a[k1], b[k1]};
+      Dft<2, INV>::run(t);
+      v[(4 * k1) % 6] = t[0];
+      v[(4 * k1 + 3) % 6] = t[1];
+    }
+  }
+};
+
+template <bool INV>
+struct Dft<12, INV> {
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[12]) {
+    // n = (4 n1 + 3 n2) mod 12, k = (4 k1 + 9 k2) mod 12
+    V y[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+      for (int n1 = 0; n1 < 3; ++n1) y[n2][n1] = v[(4 * n1 + 3 * n2) % 12];
+      Dft<3, INV>::run(y[n2]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+      V t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      Dft<4, INV>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[(4 * k1 + 9 * k2) % 12] = t[k2];
+    }
+  }
+};
+
+// Lines per group and radices of the warp-line plans (0: no plan).  A group
+// of G warps owns L complex lines; the passes need not give every lane the
+// same number of butterflies (the lanes past the last one idle).
+__host__ __device__ constexpr int wp_base_lines(int n) {
+  return (n == 768 || n == 512)               ? 1
+         : (n == 384 || n == 256 || n == 192) ? 2
+         : (n == 128 || n == 96 || n == 64)   ? 4
+         : (n == 48 || n == 32)               ? 8
+                                              : 0;
+}
+// warps per line group: four, so that a lane holds a quarter of L N / 32
+// values and the registers leave room for more resident warps
+__host__ __device__ constexpr int wp_group(int n) { return wp_base_lines(n) > 0 ? 4 : 0; }
+// lines per group: the y transforms of FP32 take twice the lines, so that a
+// warp's row segments span whole 32-byte sectors
+__host__ __device__ constexpr int wp_lines(int n, bool f32_y) {
+  return wp_base_lines(n) * (f32_y ? 2 : 1);
+}
+// Radices of the plans; with L lines per group of 128 lanes, the passes
+// give the lanes equal shares where L N / R allows (the first pass of a
+// length-768 line idles half of them, its later passes a quarter).
+__host__ __device__ constexpr int wp_npass(int n, int L) {
+  return L == 0 ? 0
+         : (n == 768 || n == 512 || n == 384 || n == 192 || n == 96) ? 3
+         : (n == 256 || n == 128 || n == 64 || n == 48 || n == 32)   ? 2
+                                                                     : 0;
+}
+__host__ __device__ constexpr int wp_radix(int n, int L, int p) {
+  return n == 768   ? (p == 0 ? 12 : 8)                    // 12 8 8
+         : n == 512 ? 8                                     // 8 8 8
+         : n == 384 ? (p == 0 ? 12 : (p == 1 ? 8 : 4))     // 12 8 4
+         : n == 256 ? 16                                    // 16 16
+         : n == 192 ? (p == 0 ? 12 : 4)                     // 12 4 4
+         : n == 128 ? (p == 0 ? 8 : 16)                     // 8 16
+         : n == 96  ? (p == 0 ? 12 : (p == 1 ? 4 : 2))      // 12 4 2
+         : n == 64  ? 8                                     // 8 8
+         : n == 48  ? (p == 0 ? 12 : 4)                     // 12 4
+         : n == 32  ? (p == 0 ? 8 : 4)                      // 8 4
+                    : 0;
+}
+__host__ __device__ constexpr bool wp_radix_ok(int r) {
+  return r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 12 || r == 16;
+}
+
+// Butterfly b of a pass (L lines of NB butterflies): line l, butterfly j.
+// LFAST puts the lines of a butterfly on adjacent lanes (the y lines, whose
+// lines are adjacent columns), otherwise a line's butterflies are.
+template <int L, int NB, bool LFAST>
+__device__ __forceinline__ void wp_bfly(int b, int &l, int &j) {
+  if constexpr (L == 1) {
+    l = 0;
+    j = b;
+  } else if constexpr (LFAST) {
+    l = b % L;
+    j = b / L;
+  } else {
+    l = b / NB;
+    j = b - l * NB;
+  }
+}
+
+// Barrier of one line group (G warps): __syncwarp for one warp, else the
+// named barrier 1 + grp over its 32 G threads.
+template <int G>
+__device__ __forceinline__ void wp_sync(int grp) {
+  if constexpr (G == 1)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(32 * G) : "memory");
+}
+
+// One Stockham pass of radix R (NS = product of the earlier radices) over the
+// group's L lines; gl is the thread's index in its group.  GIN: inputs from
+// ld(l, e) instead of the shared lines; GOUT (last pass): outputs to
+// st(l, e, z) instead of the shared lines.
+template <int R, bool INV, int N, int L, int G, int NS, bool GIN, bool GOUT, bool LFAST, class V,
+          class Ld, class St>
+__device__ __forceinline__ void wp_pass(V *buf, const V *__restrict__ tw, int gl, int grp,
+                                        const Ld &ld, const St &st) {
+  constexpr int NB = N / R, TOT = L * NB, GT = 32 * G, T = (TOT + GT - 1) / GT;
+  constexpr int LS = line_stride<V>(N), tws = N / (NS * R);
+  constexpr bool FULL = TOT % GT == 0;
+  constexpr bool LF = (GIN || GOUT) && LFAST;
+  V v[T][R];
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int b = gl + GT * t;
+    if (FULL || b < TOT) {
+      int l, j;
+      wp_bfly<L, NB, LF>(b, l, j);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if constexpr (GIN)
+          v[t][r] = ld(l, j + r * NB);
+        else
+          v[t][r] = buf[l * LS + padi<V>(j + r * NB)];
+      }
+    }
+  }
+  if constexpr (!GIN) wp_sync<G>(grp);  // all reads of the lines precede the writes
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int b = gl + GT * t;
+    if (FULL || b < TOT) {
+      int l, j;
+      wp_bfly<L, NB, LF>(b, l, j);
+      const int jm = NS == 1 ? 0 : j % NS;
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const V w = __ldg(tw + r * jm * tws);
+          v[t][r] = INV ? cmulc(v[t][r], w) : cmul(v[t][r], w);
+        }
+      }
+      Dft<R, INV>::run(v[t]);
+      if constexpr (GOUT) {
+        // NS * R = N: output r of butterfly j is element j + r N/R
+#pragma unroll
+        for (int r = 0; r < R; ++r) st(l, j + r * NB, v[t][r]);
+      } else {
+        const int base = (j / NS) * NS * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[l * LS + padi<V>(base + r * NS)] = v[t][r];
+      }
+    }
+  }
+  if constexpr (!GOUT) wp_sync<G>(grp);
+}
+
+// The passes of the plan; GIN_FIRST: the first pass loads through ld (else
+// the lines are already in the shared buffer, natural order); GOUT_LAST:
+// the last pass stores through st (else to the shared buffer).
+template <int N, int L, int G, int P, int NS, bool INV, bool GIN_FIRST, bool GOUT_LAST,
+          bool LFAST, class V, class Ld, class St>
+__device__ __forceinline__ void wp_passes(V *buf, const V *__restrict__ tw, int gl, int grp,
+                                          const Ld &ld, const St &st) {
+  static_assert(wp_npass(N, L) > 0, "a plan for this length");
+  if constexpr (P < wp_npass(N, L)) {
+    constexpr int R = wp_radix(N, L, P);
+    static_assert(wp_radix_ok(R), "radix of the plan");
+    constexpr bool last = P + 1 == wp_npass(N, L);
+    wp_pass<R, INV, N, L, G, NS, P == 0 && GIN_FIRST, last && GOUT_LAST, LFAST>(buf, tw, gl, grp,
+                                                                                ld, st);
+    wp_passes<N, L, G, P + 1, NS * R, INV, GIN_FIRST, GOUT_LAST, LFAST>(buf, tw, gl, grp, ld, st);
+  }
+}
+
+// line groups per block for a group count along the line-pair axis: the
+// largest of 8/G, 4/G, 2/G, 1 that divides it
+inline int wp_groups_per_block(int groups, int G) {
+  for (int w : {8, 4, 2, 1})
+    if (w % G == 0 && groups % (w / G) == 0) return w / G;
+  return 1;
+}
+
+// y transform in place: group grp of block (bx, k) owns the column pairs
+// c0 .. c0 + 2L - 1, c0 = (bx GPB + grp) 2L, of plane k.
+template <class T, int N, bool INV>
+__global__ void __launch_bounds__(256) k_wfft_y(int nx, int ny, int nz,
+                                                const typename Cx<T>::V *__restrict__ tw,
+                                                T *__restrict__ var, int rev) {
+  using V = typename Cx<T>::V;
+  using S = T;
+  constexpr int G = wp_group(N), L = wp_lines(N, sizeof(T) == 4), LS = line_stride<V>(N);
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  const int gl = threadIdx.x % (32 * G), grp = threadIdx.x / (32 * G);
+  const int GPB = blockDim.x / (32 * G);
+  V *buf = reinterpret_cast<V *>(fft_smem) + grp * L * LS;
+  const int c0 = (blockIdx.x * GPB + grp) * 2 * L;
+  const int k = rev ? nz - 1 - (int)blockIdx.y : (int)blockIdx.y;
+  T *plane = var + (long long)k * nx * ny + c0;
+  auto nost = [](int, int, V) {};
+  if (!INV) {
+    // rows e of the column pair (2l, 2l+1) as one complex line a + i b
+    auto ld = [&](int l, int e) -> V {
+      return *reinterpret_cast<const V *>(plane + (long long)e * nx + 2 * l);
+    };
+    wp_passes<N, L, G, 0, 1, false, true, false, true>(buf, tw, gl, grp, ld, nost);
+    // separate the spectra: row q0 gets (A, B) real parts of mode m, q0 + 1
+    // the imaginary parts (mod_fft.cc:144-151, packed order)
+#pragma unroll 4
+    for (int b = gl; b < L * H; b += 32 * G) {
+      const int l = b % L, m = b / L;
+      V a, bb;
+      unpack_four(buf + l * LS, N, m, a, bb);
+      const int q0 = m == 0 ? 0 : 2 * m;
+      *reinterpret_cast<V *>(plane + (long long)q0 * nx + 2 * l) = mk<V>(a.x, bb.x);
+      *reinterpret_cast<V *>(plane + (long long)(q0 + 1) * nx + 2 * l) = mk<V>(a.y, bb.y);
+    }
+  } else {
+    // Z_e of the pair from the packed spectra of columns 2l, 2l+1
+    auto ld = [&](int l, int e) -> V {
+      const int m = e <= H ? e : N - e;
+      const T *col = plane + 2 * l;
+      S reA, reB, imA = S(0), imB = S(0);
+      if (m == 0 || m == H) {
+        const V r = *reinterpret_cast<const V *>(col + (m == 0 ? 0 : nx));
+        reA = r.x;
+        reB = r.y;
+      } else {
+        const V re = *reinterpret_cast<const V *>(col + (long long)(2 * m) * nx);
+        const V im = *reinterpret_cast<const V *>(col + (long long)(2 * m + 1) * nx);
+        reA = re.x;
+        reB = re.y;
+        imA = im.x;
+        imB = im.y;
+      }
+      return e <= H ? mk<V>(reA - imB, imA + reB) : mk<V>(reA + imB, reB - imA);
+    };
+    auto st = [&](int l, int e, V z) {
+      *reinterpret_cast<V *>(plane + (long long)e * nx + 2 * l) = z;
+    };
+    wp_passes<N, L, G, 0, 1, true, true, true, true>(buf, tw, gl, grp, ld, st);
+  }
+}
+
+// Forward x transform: group grp of block (bx, k) owns rows j0 .. j0 + 2L - 1,
+// j0 = (bx GPB + grp) 2L (0-based), of plane k, lines (j0 + 2l, j0 + 2l + 1);
+// FUSED evaluates div(u)/dt while loading (calcRHS), else reads p.
+template <class T, int N, bool FUSED>
+__global__ void __launch_bounds__(256) k_wfft_x_fwd(Geo g, const typename Cx<T>::V *__restrict__ tw,
+                                                    const StepConst *__restrict__ sc,
+                                                    const T *__restrict__ p,
+                                                    const T *__restrict__ u,
+                                                    const T *__restrict__ v,
+                                                    const T *__restrict__ w,
+                                                    T *__restrict__ var) {
+  using V = typename Cx<T>::V;
+  constexpr int G = wp_group(N), L = wp_lines(N, false), LS = line_stride<V>(N), H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  const int gl = threadIdx.x % (32 * G), grp = threadIdx.x / (32 * G);
+  const int GPB = blockDim.x / (32 * G);
+  V *buf = reinterpret_cast<V *>(fft_smem) + grp * L * LS;
+  const int j0 = (blockIdx.x * GPB + grp) * 2 * L;
+  const int k = blockIdx.y;
+  T dti = 0, dtidxi = 0, dtidyi = 0, dzfi = 0;
+  if (FUSED) {
+    dti = T(sc->dti);
+    dtidxi = T(sc->dtidxi);
+    dtidyi = T(sc->dtidyi);
+    dzfi = T(__ldg(g.dzf_inv + k + 1));
+  }
+  const long long c00 = g.at(1, j0 + 1, k + 1);
+  auto ld = [&](int l, int e) -> V {
+    const long long ca = c00 + e + 2LL * l * g.X, cb = ca + g.X;
+    if (FUSED)
+      return mk<V>(div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi),
+                   div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi));
+    else
+      return mk<V>(p[ca], p[cb]);
+  };
+  auto nost = [](int, int, V) {};
+  // div(u)/dt (or p) of the group's 2L rows into the shared lines, spread
+  // evenly over the group's lanes (each value costs six loads), then the
+  // passes from shared memory
+#pragma unroll 4
+  for (int b = gl; b < L * N; b += 32 * G) {
+    const int l = b / N, e = b - l * N;
+    buf[l * LS + padi<V>(e)] = ld(l, e);
+  }
+  wp_sync<G>(grp);
+  wp_passes<N, L, G, 0, 1, false, false, false, false>(buf, tw, gl, grp, ld, nost);
+#pragma unroll 4
+  for (int b = gl; b < L * H; b += 32 * G) {
+    const int l = b / H, m = b - l * H;
+    V a, bb;
+    unpack_four(buf + l * LS, N, m, a, bb);
+    const long long row = (long long)k * g.ny + j0 + 2 * l;
+    reinterpret_cast<V *>(var + row * N)[m] = a;
+    reinterpret_cast<V *>(var + (row + 1) * N)[m] = bb;
+  }
+}
+
+// Backward x transform: packed spectra -> p interior scaled by nf; with
+// FUSE_BC also the pressure halos (updateBoundP).
+template <class T, int N, bool FUSE_BC>
+__global__ void __launch_bounds__(256) k_wfft_x_bwd(Geo g, const typename Cx<T>::V *__restrict__ tw,
+                                                    double nf, const T *__restrict__ var, T *p,
+                                                    int rev) {
+  using V = typename Cx<T>::V;
+  using S = T;
+  constexpr int G = wp_group(N), L = wp_lines(N, false), LS = line_stride<V>(N), H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  const int gl = threadIdx.x % (32 * G), grp = threadIdx.x / (32 * G);
+  const int GPB = blockDim.x / (32 * G);
+  V *buf = reinterpret_cast<V *>(fft_smem) + grp * L * LS;
+  const int j0 = (blockIdx.x * GPB + grp) * 2 * L;
+  const int k = rev ? g.nz - 1 - (int)blockIdx.y : (int)blockIdx.y;
+  const T scale = T(nf);
+  const T *rows = var + ((long long)k * g.ny + j0) * N;
+  auto ld = [&](int l, int e) -> V {
+    const int m = e <= H ? e : N - e;
+    const T *ra = rows + (long long)(2 * l) * N, *rb = ra + N;
+    S reA, reB, imA = S(0), imB = S(0);
+    if (m == 0 || m == H) {
+      reA = ra[m == 0 ? 0 : 1];
+      reB = rb[m == 0 ? 0 : 1];
+    } else {
+      const V a = reinterpret_cast<const V *>(ra)[m], b = reinterpret_cast<const V *>(rb)[m];
+      reA = a.x;
+      imA = a.y;
+      reB = b.x;
+      imB = b.y;
+    }
+    return e <= H ? mk<V>(reA - imB, imA + reB) : mk<V>(reA + imB, reB - imA);
+  };
+  const int kk = k + 1;
+  const int kimg = !FUSE_BC ? -1 : (kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1));
+  auto st = [&](int l, int e, V z) {
+    const T ab[2] = {scale * z.x, scale * z.y};
+    const int i = e + 1;
+    const int iimg = !FUSE_BC ? -1 : (i == g.nx ? 0 : (i == 1 ? g.nx + 1 : -1));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = j0 + 2 * l + 1 + h;
+      const int jimg = !FUSE_BC ? -1 : (j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1));
+      const T val = ab[h];
+      auto row = [&](int jj, int kq) {
+        T *r = p + (long long)jj * g.X + (long long)kq * g.XY;
+        r[i] = val;
+        if (iimg >= 0) r[iimg] = val;
+      };
+      row(j, kk);
+      if (jimg >= 0) row(jimg, kk);
+      if (kimg >= 0) {
+        row(j, kimg);
+        if (jimg >= 0) row(jimg, kimg);
+      }
+    }
+  };
+  wp_passes<N, L, G, 0, 1, true, true, true, false>(buf, tw, gl, grp, ld, st);
+}
+
+// ---------------------------------------------------------------------------
 // Thomas sweep per (i,j) system with the reciprocal pivot table
 // rpiv[(k*(ny/2+1) + my)*(nx/2+1) + mx]; the reference's divisions by b
 // become multiplications by 1/b (mod_poisson_solver.cc:334-354).
@@ -1303,6 +1697,13 @@ cudaError_t with_plan(int plan, F &&f) {
   }
   return f(std::integral_constant<int, 0>{});
 }
+// A warp-line plan (family 2) exists for length n and a line-pair axis of
+// `pairs_axis` real lines (ny for the x transforms, nx for the y transforms).
+bool fft_has_warp_plan(int n, int lines_axis) {
+  // the larger line count (FP32 y transforms) must divide as well
+  const int L = wp_lines(n, true);
+  return L > 0 && lines_axis % (2 * L) == 0;
+}
 bool fft_has_two_plans(int n) {
   bool two = false;
   with_size(n, [&](auto NC) -> cudaError_t {
@@ -1345,6 +1746,20 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_fft_y<float, N, false, PL>));
         return cudaSuccess;
       };
+      if constexpr (N > 0 && wp_base_lines(N) > 0) {
+        PLC_SMEM((k_wfft_y<double, N, false>));
+        PLC_SMEM((k_wfft_y<double, N, true>));
+        PLC_SMEM((k_wfft_x_fwd<double, N, true>));
+        PLC_SMEM((k_wfft_x_fwd<double, N, false>));
+        PLC_SMEM((k_wfft_x_bwd<double, N, true>));
+        PLC_SMEM((k_wfft_x_bwd<double, N, false>));
+        PLC_SMEM((k_wfft_y<float, N, false>));
+        PLC_SMEM((k_wfft_y<float, N, true>));
+        PLC_SMEM((k_wfft_x_fwd<float, N, true>));
+        PLC_SMEM((k_wfft_x_fwd<float, N, false>));
+        PLC_SMEM((k_wfft_x_bwd<float, N, true>));
+        PLC_SMEM((k_wfft_x_bwd<float, N, false>));
+      }
       r = conf(std::integral_constant<int, 0>{});
       if (r != cudaSuccess) return r;
       if constexpr (N > 0 && plan_has24(N)) {
@@ -1415,12 +1830,47 @@ cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max) {
 }
 
 namespace {
+// Warp-line launch geometry: blocks of GPB line groups (G warps each) over
+// the `groups` line groups of one plane, grid (groups / GPB, nz); shared
+// memory GPB L line strides.
+template <class T, int N, bool YDIR>
+struct WpLaunch {
+  dim3 grid, block;
+  size_t smem;
+  WpLaunch(int lines_axis, int nz) {
+    using V = typename Cx<T>::V;
+    constexpr int G = wp_group(N), L = wp_lines(N, YDIR && sizeof(T) == 4);
+    const int groups = lines_axis / (2 * L);
+    const int gpb = wp_groups_per_block(groups, G);
+    grid = dim3(groups / gpb, nz);
+    block = dim3(32 * G * gpb);
+    smem = (size_t)gpb * L * line_stride<V>(N) * sizeof(V);
+  }
+};
+
 template <class T>
 cudaError_t fft_x_fwd_t(const plc_ctx *c, const T *p, const T *u, const T *v, const T *w, T *var,
                         cudaStream_t s) {
+  // the forward transform's own family (the backward one's when not set);
+  // the shared-memory families take the backward one's radix family
+  const int pf = c->fft_plan_xf >= 0 ? c->fft_plan_xf : c->fft_plan_x;
+  const int pfam = pf == 2 ? (c->fft_plan_x == 2 ? 0 : c->fft_plan_x) : pf;
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
-    return with_plan<N>(c->fft_plan_x, [&](auto PC) -> cudaError_t {
+    if constexpr (N > 0 && wp_base_lines(N) > 0) {
+      if (pf == 2) {
+        const WpLaunch<T, N, false> lc(c->ny, c->nz);
+        const auto tw = dev_plan<T>(c->plan_x).tw;
+        if (p)
+          k_wfft_x_fwd<T, N, false><<<lc.grid, lc.block, lc.smem, s>>>(
+              c->geo(), tw, c->d_sc, p, nullptr, nullptr, nullptr, var);
+        else
+          k_wfft_x_fwd<T, N, true><<<lc.grid, lc.block, lc.smem, s>>>(c->geo(), tw, c->d_sc,
+                                                                       nullptr, u, v, w, var);
+        return cudaGetLastError();
+      }
+    }
+    return with_plan<N>(pfam, [&](auto PC) -> cudaError_t {
       constexpr int PL = decltype(PC)::value;
       if (p) {
         const int nl = c->fft_lines_x;
@@ -1444,6 +1894,19 @@ cudaError_t fft_x_bwd_t(const plc_ctx *c, const T *var, T *p, bool fuse_bc, cuda
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0 && wp_base_lines(N) > 0) {
+      if (c->fft_plan_x == 2) {
+        const WpLaunch<T, N, false> lc(c->ny, c->nz);
+        const auto tw = dev_plan<T>(c->plan_x).tw;
+        if (fuse_bc)
+          k_wfft_x_bwd<T, N, true><<<lc.grid, lc.block, lc.smem, s>>>(c->geo(), tw, nf, var, p,
+                                                                       c->order[SK_XB]);
+        else
+          k_wfft_x_bwd<T, N, false><<<lc.grid, lc.block, lc.smem, s>>>(c->geo(), tw, nf, var, p,
+                                                                        c->order[SK_XB]);
+        return cudaGetLastError();
+      }
+    }
     return with_plan<N>(c->fft_plan_x, [&](auto PC) -> cudaError_t {
       constexpr int PL = decltype(PC)::value;
       if (fuse_bc)
@@ -1463,6 +1926,19 @@ cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
   const size_t sm = smem_y<T>(c->ny, nl);
   return with_size(c->ny, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0 && wp_base_lines(N) > 0) {
+      if (c->fft_plan_y == 2) {
+        const WpLaunch<T, N, true> lc(c->nx, c->nz);
+        const auto tw = dev_plan<T>(c->plan_y).tw;
+        if (inverse)
+          k_wfft_y<T, N, true><<<lc.grid, lc.block, lc.smem, s>>>(c->nx, c->ny, c->nz, tw, var,
+                                                                   c->order[SK_YB]);
+        else
+          k_wfft_y<T, N, false><<<lc.grid, lc.block, lc.smem, s>>>(c->nx, c->ny, c->nz, tw, var,
+                                                                    c->order[SK_YF]);
+        return cudaGetLastError();
+      }
+    }
     return with_plan<N>(c->fft_plan_y, [&](auto PC) -> cudaError_t {
       constexpr int PL = decltype(PC)::value;
       if (inverse)
@@ -1541,14 +2017,25 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
   // `step`) and, when `plan` is given and the length has two plan families
   // (`two`), the family *plan with it; `fits` says whether a value fits the
   // device
-  auto tune = [&](int *field, int *plan, bool two, int pairs, int step, auto fits,
+  auto tune = [&](int *field, int *plan, bool two, bool warp, int pairs, int step, auto fits,
                   auto launch) {
     int best_d = *field, best_p = plan ? *plan : 0;
     float best_t = -1.f;
-    const int p0 = (plan && two && !c->fft_plans_pinned) ? 0 : (plan ? *plan : 0);
-    const int p1 = (plan && two && !c->fft_plans_pinned) ? 1 : p0;
+    const bool free_plan = plan && !c->fft_plans_pinned;
+    const int p0 = free_plan ? 0 : (plan ? *plan : 0);
+    const int p1 = free_plan ? (warp ? 2 : (two ? 1 : 0)) : p0;
     for (int pl = p0; pl <= p1; ++pl) {
+      if (pl == 1 && !two) continue;
       if (plan) *plan = pl;
+      if (pl == 2) {
+        // the warp-line kernels have no tile size of their own
+        const float t = time_of(launch);
+        if (t >= 0.f && (best_t < 0.f || t < best_t)) {
+          best_t = t;
+          best_p = pl;
+        }
+        continue;
+      }
       for (int d = step; d <= pairs && d <= 16; d += step) {
         if (pairs % d || !fits(d)) continue;
         *field = d;
@@ -1567,7 +2054,8 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
   };
   T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W], *p = f[PLC_P], *spec = f[PLC_SPEC];
   // y: tile and plan family timed on a forward and an inverse transform
-  tune(&c->fft_lines_y, &c->fft_plan_y, fft_has_two_plans(ny), nx / 2, sizeof(T) == 4 ? 2 : 1,
+  tune(&c->fft_lines_y, &c->fft_plan_y, fft_has_two_plans(ny), fft_has_warp_plan(ny, nx), nx / 2,
+       sizeof(T) == 4 ? 2 : 1,
        [&](int d) { return smem_y<T>(ny, d) <= dev_max; },
        [&]() -> cudaError_t {
          cudaError_t r = launch_fft_y(c, spec, false, s);
@@ -1575,10 +2063,13 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
        });
   // x: the plan family (shared by both x transforms) with the backward tile,
   // then the forward tile under that family
-  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), ny / 2, 1,
+  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), ny / 2,
+       1,
        [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
-  tune(&c->fft_lines_xf, nullptr, false, ny / 2, 1,
+  if (c->fft_plans_pinned) c->fft_plan_xf = c->fft_plan_x;
+  tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny),
+       ny / 2, 1,
        [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t {
          if constexpr (sizeof(T) == 8)

@@ -106,6 +106,8 @@ struct plc_ctx {
   // passes ending in radix 24, lengths 24 .. 384 with one factor 3); autotuned
   // with the tiles unless the environment pins them
   int fft_plan_x = 0, fft_plan_y = 0;
+  // family of the forward x transform (-1: that of the backward one)
+  int fft_plan_xf = -1;
   bool fft_plans_pinned = false;
   // Plane order of the step kernels (0: low planes first, 1: high planes
   // first), set per form at creation from measurements; only the speed
@@ -258,6 +260,8 @@ cudaError_t fft_setup(plc_ctx *c, size_t smem_cap_per_block, size_t dev_max);
 cudaError_t fft_autotune(plc_ctx *c);
 // whether a line length has the radix-24 plan family as well
 bool fft_has_two_plans(int n);
+// a warp-line plan (family 2) for length n with `lines_axis` real lines
+bool fft_has_warp_plan(int n, int lines_axis);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 // var -= delta on the interior of the context's field (either form), synchronous
