@@ -160,6 +160,7 @@ int init_poisson(plc_ctx *c, const double *dzf_global) {
   // the limit is a per-kernel attribute shared by all contexts: raise it to the
   // device maximum so that no context can lower it under another one
   PLC_CUDA(c, fft_configure((size_t)dev_max));
+  c->trid_smem_max = (size_t)dev_max;
   if (fft_setup(c, 76 * 1024, (size_t)dev_max) != cudaSuccess)
     return set_error(c, PLC_ERR_SIZE, "FFT line too long for shared memory");
   c->poisson_ready = true;
@@ -569,6 +570,14 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     c->fft_plans_pinned = true;
     if ((e = fft_set_lines(c, c->fft_lines_xf, c->fft_lines_x, c->fft_lines_y)) != cudaSuccess)
       return fail(cuda_status(c, e, "fft_set_lines"));
+  }
+  // PLC_TRID = "tile" / "stream" pins the Thomas sweep (columns on chip or
+  // streamed through HBM) instead of timing both
+  if (const char *env = getenv("PLC_TRID")) {
+    if (strcmp(env, "tile") != 0 && strcmp(env, "stream") != 0)
+      return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_TRID: ") + env));
+    c->trid_tile = strcmp(env, "tile") == 0;
+    c->trid_pinned = true;
   }
   bool pinned = false;
   if (const char *env = getenv(c->mixed ? "PLC_FFT_TILES_F32" : "PLC_FFT_TILES")) {

@@ -1604,6 +1604,249 @@ __global__ void __launch_bounds__(128) k_trid_mixed(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Thomas sweep with the right-hand side held on chip.  A block of 32 threads
+// owns 32 consecutive systems (packed x indices i0 .. i0+31 of one packed y
+// row j) and copies their whole columns -- nz rows of 32 elements, one
+// 16-byte-aligned segment per plane -- into shared memory with bulk copies
+// (cp.async.bulk, no multicast), in eight chunks of planes each signalling
+// its own mbarrier.  The forward elimination starts on the first chunk while
+// the others land, keeps the forward values in place in shared memory, and
+// the back substitution writes the solution to global memory once: the
+// spectral array is read once and written once (the forward values no
+// longer round-trip through HBM).  Same operations in the same order as
+// thomas_inplace.  Every wait is bounded: on a timeout the block records
+// the error word and leaves.
+// ---------------------------------------------------------------------------
+constexpr int kTridChunks = 8;
+constexpr long long kTridWaitLimit = 1ll << 22;
+
+__device__ __forceinline__ unsigned trid_smem_addr(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void trid_bulk_load(void *dst, const void *src, unsigned bytes,
+                                               unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(trid_smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(trid_smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool trid_try_wait(unsigned long long *bar) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(trid_smem_addr(bar))
+      : "memory");
+  return ok != 0;
+}
+
+size_t trid_tile_smem(int nz, size_t elem) { return (size_t)nz * 32 * elem + 8 * kTridChunks + 16; }
+
+// The block's columns: systems t = blockIdx.x * 32 + lane (nx % 32 == 0, so
+// one packed y row j); xs[k * 32 + lane] holds row k of the lane's system.
+template <class A>
+__device__ __forceinline__ void trid_tile_load(A *xs, unsigned long long *bar, const A *col,
+                                               long long plane, int nz, int cp) {
+  const int lane = threadIdx.x;
+  if (lane == 0) {
+    for (int ch = 0; ch < kTridChunks; ++ch) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(trid_smem_addr(bar + ch)));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int ch = 0; ch < kTridChunks; ++ch) {
+      const int k0 = ch * cp, k1 = min(nz, k0 + cp);
+      const unsigned bytes = (unsigned)(k1 > k0 ? k1 - k0 : 0) * 32u * (unsigned)sizeof(A);
+      // the chunk's expected bytes (an empty chunk completes at once)
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                       trid_smem_addr(bar + ch)),
+                   "r"(bytes)
+                   : "memory");
+    }
+  }
+  __syncwarp();
+  for (int k = lane; k < nz; k += 32)
+    trid_bulk_load(xs + k * 32, col + k * plane, 32u * (unsigned)sizeof(A), bar + k / cp);
+}
+
+// Before the block exits: every chunk has landed (returns at once when the
+// sweep waited for them all; bounded when a wait gave up, so that no copy
+// into this block's shared memory is still in flight when it leaves).
+__device__ __forceinline__ void trid_drain(unsigned long long *bar, int *err) {
+  for (int ch = 0; ch < kTridChunks; ++ch) {
+    bool done = false;
+    for (long long it = 0; it < kTridWaitLimit && !done; ++it) done = trid_try_wait(bar + ch);
+    if (!done) atomicOr(err, 4);
+  }
+}
+
+__device__ __forceinline__ bool trid_wait_chunk(unsigned long long *bar, int ch, int *err) {
+  for (long long it = 0; it < kTridWaitLimit; ++it)
+    if (trid_try_wait(bar + ch)) return true;
+  atomicOr(err, 4);
+  return false;
+}
+
+// The sweep of one lane's system: xs column (stride 32), pivots rp (stride
+// PS), 1-D coefficients ca, cc; solution stored to q (plane stride).
+template <class A>
+__device__ __forceinline__ void trid_tile_sweep(A *xs, int nz, int cp,
+                                                unsigned long long *bar, const A *__restrict__ rp,
+                                                long long PS, const A *__restrict__ ca,
+                                                const A *__restrict__ cc, A *q, long long plane,
+                                                int *err, bool &ok) {
+  const int lane = threadIdx.x;
+  constexpr int PF = 8;
+  if (!trid_wait_chunk(bar, 0, err)) {
+    ok = false;
+    return;
+  }
+  A prev = xs[lane];
+  // forward elimination, pivots of PF planes loaded one batch ahead
+  A rn[PF];
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < nz - 1) rn[s] = __ldg(rp + (long long)s * PS);
+  int next_chunk = 1;
+  for (int k = 1; k < nz; k += PF) {
+    A r[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s) r[s] = rn[s];
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (k + PF + s - 1 <= nz - 2) rn[s] = __ldg(rp + (long long)(k + PF + s - 1) * PS);
+#pragma unroll
+    for (int s = 0; s < PF; ++s) {
+      const int kk = k + s;
+      if (kk < nz) {
+        while (next_chunk < kTridChunks && kk >= next_chunk * cp) {
+          if (!trid_wait_chunk(bar, next_chunk, err)) {
+            ok = false;
+            return;
+          }
+          ++next_chunk;
+        }
+        A cur = xs[kk * 32 + lane];
+        cur -= (__ldg(ca + kk) * r[s]) * prev;
+        xs[kk * 32 + lane] = cur;
+        prev = cur;
+      }
+    }
+  }
+  prev *= __ldg(rp + (long long)(nz - 1) * PS);
+  q[(long long)(nz - 1) * plane] = prev;
+  // back substitution
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (nz - 2 - s >= 0) rn[s] = __ldg(rp + (long long)(nz - 2 - s) * PS);
+  for (int k = nz - 2; k >= 0; k -= PF) {
+    A r[PF];
+#pragma unroll
+    for (int s = 0; s < PF; ++s) r[s] = rn[s];
+#pragma unroll
+    for (int s = 0; s < PF; ++s)
+      if (k - PF - s >= 0) rn[s] = __ldg(rp + (long long)(k - PF - s) * PS);
+#pragma unroll
+    for (int s = 0; s < PF; ++s) {
+      const int kk = k - s;
+      if (kk >= 0) {
+        const A cur = (xs[kk * 32 + lane] - __ldg(cc + kk) * prev) * r[s];
+        q[(long long)kk * plane] = cur;
+        prev = cur;
+      }
+    }
+  }
+}
+
+// FP64: the reference's solve with the columns on chip.
+__global__ void __launch_bounds__(32) k_trid_tile(int nx, int ny, int nz,
+                                                  const double *__restrict__ rpiv,
+                                                  const double *__restrict__ a,
+                                                  const double *__restrict__ c,
+                                                  double *__restrict__ var, int *err) {
+  extern __shared__ __align__(128) unsigned char trid_smem[];
+  double *xs = reinterpret_cast<double *>(trid_smem);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(xs + (size_t)nz * 32);
+  const int lane = threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  const long long t0 = (long long)blockIdx.x * 32;
+  const int cp = (nz + kTridChunks - 1) / kTridChunks;
+  trid_tile_load(xs, bar, var + t0, plane, nz, cp);
+  int i, j;
+  long long pv;
+  trid_index((int)(t0 + lane), nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  bool ok = true;
+  trid_tile_sweep<double>(xs, nz, cp, bar, rpiv + pv, PS, a, c, var + t0 + lane, plane, err, ok);
+  __syncwarp();
+  if (lane == 0) trid_drain(bar, err);
+}
+
+// A low-wavenumber system of the mixed form whose right-hand side is the
+// on-chip FP32 column xs (stride 32): FP64 pivots, arithmetic and forward
+// values (in lq), solution stored to q.
+struct LowSysSmem {
+  const float *xs;
+  float *q;
+  long long plane;
+  double *lq;
+  long long LP;
+  const double *rp;
+  long long PS;
+  const double *ca, *cc;
+  __device__ __forceinline__ double rhs(int k) const { return double(xs[k * 32]); }
+  __device__ __forceinline__ double piv(int k) const { return __ldg(rp + (long long)k * PS); }
+  __device__ __forceinline__ double a(int k) const { return __ldg(ca + k); }
+  __device__ __forceinline__ double c(int k) const { return __ldg(cc + k); }
+  __device__ __forceinline__ void fwd_put(int k, double x) const { lq[k * LP] = x; }
+  __device__ __forceinline__ double fwd_get(int k) const { return lq[k * LP]; }
+  __device__ __forceinline__ void out(int k, double x) const {
+    q[(long long)k * plane] = float(x);
+  }
+};
+
+// Mixed form: the FP32 systems sweep on chip as above; the systems of the
+// lowest wavenumbers (packed x and y indices below kLowModes) sweep in FP64
+// with their forward values in `low`, reading their right-hand side from
+// the same on-chip column.
+__global__ void __launch_bounds__(32) k_trid_mixed_tile(
+    int nx, int ny, int nz, const float *__restrict__ rpiv32, const float *__restrict__ a32,
+    const float *__restrict__ c32, const double *__restrict__ rpiv,
+    const double *__restrict__ a, const double *__restrict__ c, float *__restrict__ var,
+    double *__restrict__ low, int *err) {
+  extern __shared__ __align__(128) unsigned char trid_smem[];
+  float *xs = reinterpret_cast<float *>(trid_smem);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(
+      trid_smem + ((size_t)nz * 32 * sizeof(float) + 15) / 16 * 16);
+  const int lane = threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  const long long t0 = (long long)blockIdx.x * 32;
+  const int cp = (nz + kTridChunks - 1) / kTridChunks;
+  trid_tile_load(xs, bar, var + t0, plane, nz, cp);
+  int i, j;
+  long long pv;
+  trid_index((int)(t0 + lane), nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  bool ok = true;
+  if (i < kLowModes && j < kLowModes) {
+    // every chunk must have landed before the FP64 sweep reads the column
+    for (int ch = 0; ch < kTridChunks && ok; ++ch) ok = trid_wait_chunk(bar, ch, err);
+    if (ok) {
+      constexpr long long LP = (long long)kLowModes * kLowModes;
+      thomas_sweep<double, 8>(nz, LowSysSmem{xs + lane, var + t0 + lane, plane,
+                                             low + j * kLowModes + i, LP, rpiv + pv, PS, a, c});
+    }
+  } else {
+    trid_tile_sweep<float>(xs, nz, cp, bar, rpiv32 + pv, PS, a32, c32, var + t0 + lane, plane,
+                           err, ok);
+  }
+  __syncwarp();
+  if (lane == 0) trid_drain(bar, err);
+}
+
 template <class T>
 FftDev<typename Cx<T>::V> dev_plan(const FftPlan &p) {
   FftDev<typename Cx<T>::V> d;
@@ -1759,6 +2002,10 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_wfft_x_fwd<float, N, false>));
         PLC_SMEM((k_wfft_x_bwd<float, N, true>));
         PLC_SMEM((k_wfft_x_bwd<float, N, false>));
+      }
+      if constexpr (N == 0) {
+        PLC_SMEM(k_trid_tile);
+        PLC_SMEM(k_trid_mixed_tile);
       }
       r = conf(std::integral_constant<int, 0>{});
       if (r != cudaSuccess) return r;
@@ -2077,6 +2324,17 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
          else
            return launch_fft_x_fwd(c, u, v, w, spec, s);
        });
+  // the Thomas sweep: on chip or streaming, timed on the spectral array (the
+  // choice changes speed, never results)
+  if (c->nx % 32 == 0 && !c->trid_pinned) {
+    float t_tile = -1.f, t_stream = -1.f;
+    c->trid_tile = true;
+    t_tile = time_of([&]() -> cudaError_t { return launch_trid(c, spec, s); });
+    c->trid_tile = false;
+    t_stream = time_of([&]() -> cudaError_t { return launch_trid(c, spec, s); });
+    c->trid_tile = t_tile >= 0.f && (t_stream < 0.f || t_tile <= t_stream);
+    cudaGetLastError();
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return fft_grids_t<T>(c, dev_max, sms);
@@ -2108,8 +2366,18 @@ cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y) {
                   : fft_grids_t<double>(c, (size_t)dev_max, sms);
 }
 
+// The on-chip sweep needs whole 32-system rows (nx a multiple of 32) and its
+// columns within the device's shared memory; else the streaming sweep runs.
+static bool trid_tile_ok(const plc_ctx *c, size_t elem) {
+  return c->trid_tile && c->nx % 32 == 0 && trid_tile_smem(c->nz, elem) <= c->trid_smem_max;
+}
 cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
   const long long plane = (long long)c->nx * c->ny;
+  if (trid_tile_ok(c, sizeof(double))) {
+    k_trid_tile<<<(unsigned)(plane / 32), 32, trid_tile_smem(c->nz, sizeof(double)), s>>>(
+        c->nx, c->ny, c->nz, c->d_rpiv, c->d_ac, c->d_ac + c->nz, var, c->d_err);
+    return cudaGetLastError();
+  }
   const int bs = 128;
   k_trid<<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(c->nx, c->ny, c->nz, c->d_rpiv,
                                                           c->d_ac, c->d_ac + c->nz, var);
@@ -2117,6 +2385,12 @@ cudaError_t launch_trid(const plc_ctx *c, double *var, cudaStream_t s) {
 }
 cudaError_t launch_trid(const plc_ctx *c, float *var, cudaStream_t s) {
   const long long plane = (long long)c->nx * c->ny;
+  if (trid_tile_ok(c, sizeof(float))) {
+    k_trid_mixed_tile<<<(unsigned)(plane / 32), 32, trid_tile_smem(c->nz, sizeof(float)), s>>>(
+        c->nx, c->ny, c->nz, c->d_rpiv32, c->d_ac32, c->d_ac32 + c->nz, c->d_rpiv, c->d_ac,
+        c->d_ac + c->nz, var, c->d_low, c->d_err);
+    return cudaGetLastError();
+  }
   const int bs = 128;
   k_trid_mixed<<<(unsigned)((plane + bs - 1) / bs), bs, 0, s>>>(
       c->nx, c->ny, c->nz, c->d_rpiv32, c->d_ac32, c->d_ac32 + c->nz, c->d_rpiv, c->d_ac,

@@ -108,6 +108,11 @@ struct plc_ctx {
   int fft_plan_x = 0, fft_plan_y = 0;
   // family of the forward x transform (-1: that of the backward one)
   int fft_plan_xf = -1;
+  // Thomas sweep with the columns on chip (else the streaming sweep), chosen
+  // by the autotuner; the device's shared-memory limit per block
+  bool trid_tile = true;
+  bool trid_pinned = false;  // PLC_TRID = "tile" or "stream"
+  size_t trid_smem_max = 0;
   bool fft_plans_pinned = false;
   // Plane order of the step kernels (0: low planes first, 1: high planes
   // first), set per form at creation from measurements; only the speed
