@@ -229,7 +229,7 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
     ok, cfl, div = ch.check()
-    tiles = ch.fft_tiles
+    tiles = dict(ch.fft_tiles, rk_kchunk=ch.rk_kchunk)
     prof_steps = max(2, min(5, args.steps))
     prof = ch.profile_step(prof_steps)
     total = sum(prof.values())
@@ -534,7 +534,7 @@ def run_ours(args, wl, rank, world, local, pg):
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
     ok, cfl, div = ch.check()  # NaN / CFL / divergence of the state after the timed steps
-    tiles = ch.fft_tiles
+    tiles = dict(ch.fft_tiles, rk_kchunk=ch.rk_kchunk)
 
     # per-kernel device times of the same fused kernels (plain launches with
     # CUDA events between them on the library's stream)

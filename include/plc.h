@@ -176,6 +176,12 @@ int plc_fft_plans(const plc_ctx *ctx, int *plan_x, int *plan_y);
 /* The family of the forward x transform (fused with calcRHS in the step),
  * timed separately from the backward one.  No counterpart in the reference. */
 int plc_fft_plan_x_fwd(const plc_ctx *ctx, int *plan);
+/* z planes per block of the two RK stages, timed per context at creation
+ * among 8, 16, 24 and 32 (at most nz) on both fused stages; PLC_RK_KCHUNK
+ * pins it.  The choice changes speed; results only in the mixed form, whose
+ * RK2 sums the bulk mean per block in FP32 (by FP32 rounding).  No
+ * counterpart in the reference. */
+int plc_rk_kchunk(const plc_ctx *ctx, int *kchunk);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

@@ -170,6 +170,13 @@ class Channel:
         return {"x_fwd": a.value, "x_bwd": b.value, "y": c.value, "plan_x": px.value,
                 "plan_y": py.value, "plan_x_fwd": pxf.value}
 
+    @property
+    def rk_kchunk(self) -> int:
+        """z planes per block of the RK stages chosen by the autotuner."""
+        k = C.c_int()
+        self._check(lib().plc_rk_kchunk(self._ctx, C.byref(k)))
+        return k.value
+
     def ptr_f32(self, f):
         """(device pointer, element count, row pitch) of an FP32 field of a mixed context."""
         fid = FIELDS[f] if isinstance(f, str) else int(f)

@@ -215,6 +215,72 @@ int run_check_fields(plc_ctx *c, int what) {
   return run_check(c, what, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W]);
 }
 
+// Autotuner of the RK stages' z planes per block: each candidate of
+// kRkChunks (at most nz) timed on both fused stages over the context's own
+// fields (best of three after a warm-up launch); the chunk changes which
+// blocks compute which planes: no result of the FP64 form, and in the mixed
+// form only the FP32 rounding of the per-block bulk-mean sums.  Run at
+// creation, before
+// the fields hold data to keep (the stages overwrite u1..w1 and u..w).
+cudaError_t rk_autotune(plc_ctx *c) {
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  cudaStream_t s = c->stream;
+  const double u_crf = c->prm.u_crf;
+  auto launch = [&]() -> cudaError_t {
+    cudaError_t r;
+    if (c->mixed) {
+      float *const *f = c->f_field;
+      r = launch_rk(c, 1, true, u_crf, f[PLC_U], f[PLC_V], f[PLC_W], f[PLC_U1], f[PLC_V1],
+                    f[PLC_W1], s);
+      if (r == cudaSuccess)
+        r = launch_rk(c, 2, true, u_crf, f[PLC_U1], f[PLC_V1], f[PLC_W1], f[PLC_U], f[PLC_V],
+                      f[PLC_W], s);
+    } else {
+      double *const *f = c->d_field;
+      r = launch_rk(c, 1, true, u_crf, f[PLC_U], f[PLC_V], f[PLC_W], f[PLC_U1], f[PLC_V1],
+                    f[PLC_W1], s);
+      if (r == cudaSuccess)
+        r = launch_rk(c, 2, true, u_crf, f[PLC_U1], f[PLC_V1], f[PLC_W1], f[PLC_U], f[PLC_V],
+                      f[PLC_W], s);
+    }
+    return r;
+  };
+  int best_k = 0, last = -1;
+  float best_t = -1.f;
+  for (int k : kRkChunks) {
+    c->rk_kchunk = k;
+    const int eff = rk_chunk(c, 32);
+    if (eff == last) continue;  // the same chunk once clamped to nz
+    last = eff;
+    if ((e = launch()) != cudaSuccess) break;
+    float best = -1.f;
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+      if ((e = cudaEventRecord(e0, s)) != cudaSuccess || (e = launch()) != cudaSuccess ||
+          (e = cudaEventRecord(e1, s)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess)
+        break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best < 0.f || ms < best) best = ms;
+    }
+    if (e != cudaSuccess) break;
+    if (best_t < 0.f || best < best_t) {
+      best_t = best;
+      best_k = k;
+    }
+  }
+  c->rk_kchunk = best_k;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e;
+}
+
 const char *const kStepKernelNames[] = {
     "rk1+bound(u1)", "rk2+bound(u)", "calcRHS+fft_x_fwd", "fft_y_fwd", "trid_z",
     "fft_y_bwd",     "fft_x_bwd+bound(p)", "correct+mean", "force+bound(u)"};
@@ -589,6 +655,16 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     pinned = true;
   }
   if (!pinned && (e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
+  // PLC_RK_KCHUNK pins the RK stages' z planes per block instead of timing
+  // the candidates
+  if (const char *env = getenv("PLC_RK_KCHUNK")) {
+    const int k = atoi(env);
+    if (k < 1 || k > 32)
+      return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_RK_KCHUNK: ") + env));
+    c->rk_kchunk = k;
+  } else if ((e = rk_autotune(c)) != cudaSuccess) {
+    return fail(cuda_status(c, e, "rk_autotune"));
+  }
   c->tuned_lines[0] = c->fft_lines_xf;
   c->tuned_lines[1] = c->fft_lines_x;
   c->tuned_lines[2] = c->fft_lines_y;
@@ -675,6 +751,12 @@ int plc_fft_plans(const plc_ctx *c, int *plan_x, int *plan_y) {
   if (!c) return set_error(nullptr, PLC_ERR_ARG, "null context");
   if (plan_x) *plan_x = c->fft_plan_x;
   if (plan_y) *plan_y = c->fft_plan_y;
+  return PLC_OK;
+}
+
+int plc_rk_kchunk(const plc_ctx *c, int *kchunk) {
+  if (!c || !kchunk) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  *kchunk = rk_chunk(c, 32);
   return PLC_OK;
 }
 

@@ -3,7 +3,11 @@
 // member is an ordinary context (its own parameters, fields, solver tables
 // and tuned FFT tiles); one ensemble step is ONE graph launch whose branches
 // are the members' fused steps, so small members that cannot fill 148 SMs
-// alone run side by side.  Members are scheduled in groups (the members of a
+// alone run side by side.  Between two steps that need the host (checks, a
+// new CFL-controlled dt) the members need not meet: one launch of a second
+// graph runs K steps, each branch a member's K steps in a row, so members
+// that finish early leave the GPU to the others instead of waiting for the
+// largest at every step.  Members are scheduled in groups (the members of a
 // group run concurrently, groups one after another), and every member's
 // persistent kernels get an SM budget; an autotuner times candidate
 // schedules on the members' own fields and keeps the fastest.  Checks,
@@ -26,7 +30,10 @@ struct plc_ensemble {
   cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t graph = nullptr;
-  std::vector<unsigned> epochs;  // member graph epochs the graph was captured at
+  cudaGraphExec_t graph_k = nullptr;  // K steps per branch
+  int k_steps = 0;
+  std::vector<unsigned> epochs;    // member graph epochs the graph was captured at
+  std::vector<unsigned> epochs_k;  // ... and the K-step graph
   std::vector<int> group;        // group of each member
   int ngroups = 1;
   int scheme = PLC_ENS_CONCURRENT;
@@ -64,16 +71,24 @@ void drop(plc_ensemble *e) {
     cudaGraphExecDestroy(e->graph);
     e->graph = nullptr;
   }
+  if (e->graph_k) {
+    cudaGraphExecDestroy(e->graph_k);
+    e->graph_k = nullptr;
+  }
 }
 
-// Captures one ensemble step: per group, a fork from the ensemble stream to
-// the members' streams, each member's fused step, a join back.
-int build(plc_ensemble *e) {
+// Captures `steps` ensemble steps into *out: per group, a fork from the
+// ensemble stream to the members' streams, each member's fused steps in a
+// row, a join back.
+int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsigned> &epochs) {
   const int n = (int)e->members.size();
-  bool stale = e->graph == nullptr;
-  for (int m = 0; m < n && !stale; ++m) stale = e->epochs[m] != e->members[m]->graph_epoch;
+  bool stale = *out == nullptr;
+  for (int m = 0; m < n && !stale; ++m) stale = epochs[m] != e->members[m]->graph_epoch;
   if (!stale) return PLC_OK;
-  drop(e);
+  if (*out) {
+    cudaGraphExecDestroy(*out);
+    *out = nullptr;
+  }
   for (int m = 0; m < n; ++m)
     if (!e->members[m]->poisson_ready)
       return ens_error(e, PLC_ERR_STATE, "member " + std::to_string(m) + ": Poisson solver not initialised");
@@ -87,10 +102,9 @@ int build(plc_ensemble *e) {
       if (e->group[m] != grp) continue;
       plc_ctx *c = e->members[m];
       if ((r = cudaStreamWaitEvent(c->stream, e->fork, 0)) != cudaSuccess) break;
-      if ((rc = plc::capture_step(c, c->stream)) != PLC_OK) {
-        rc = member_error(e, m, rc);
-        break;
-      }
+      for (int q = 0; q < steps && rc == PLC_OK; ++q)
+        if ((rc = plc::capture_step(c, c->stream)) != PLC_OK) rc = member_error(e, m, rc);
+      if (rc != PLC_OK) break;
       r = cudaEventRecord(e->join[m], c->stream);
     }
     for (int m = 0; m < n && rc == PLC_OK && r == cudaSuccess; ++m)
@@ -103,11 +117,41 @@ int build(plc_ensemble *e) {
     if (rc != PLC_OK) return rc;
     return ens_cuda(e, r != cudaSuccess ? r : re, "ensemble step capture");
   }
-  r = cudaGraphInstantiate(&e->graph, g, 0);
+  r = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (r != cudaSuccess) return ens_cuda(e, r, "cudaGraphInstantiate");
-  for (int m = 0; m < n; ++m) e->epochs[m] = e->members[m]->graph_epoch;
+  for (int m = 0; m < n; ++m) epochs[m] = e->members[m]->graph_epoch;
   return PLC_OK;
+}
+
+int build(plc_ensemble *e) { return capture(e, 1, &e->graph, e->epochs); }
+
+// K of the multi-step graph: the members' common check period when they
+// share one (a block then ends on a check step), else 8.
+int k_of(const plc_ensemble *e) {
+  int k = e->members[0]->prm.nt_check;
+  for (const plc_ctx *c : e->members)
+    if (c->prm.nt_check != k) k = 0;
+  return k > 1 ? k : 8;
+}
+
+// Steps, at most `limit`, until (and including) the next step that needs the
+// host for any member: 1 when the next step itself does.
+int steps_to_host(const plc_ensemble *e, int limit) {
+  int best = limit;
+  for (const plc_ctx *c : e->members) {
+    const plc_params &P = c->prm;
+    for (int j = 1; j < best; ++j) {
+      const long long n = c->nstep + j;
+      const bool host = (P.cfl_target > 0.0 && n < P.nt_check && (n & (n - 1)) == 0) ||
+                        (P.nt_check > 0 && n % P.nt_check == 0);
+      if (host) {
+        best = j;
+        break;
+      }
+    }
+  }
+  return best;
 }
 
 // orders the ensemble stream after all work queued on the members' streams
@@ -130,20 +174,36 @@ int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
   if (nsteps < 0) return ens_error(e, PLC_ERR_ARG, "nsteps < 0");
   const int n = (int)e->members.size();
   if (int rc = build(e)) return rc;
+  const int K = k_of(e);
+  if (K != e->k_steps && e->graph_k) {
+    cudaGraphExecDestroy(e->graph_k);
+    e->graph_k = nullptr;
+  }
+  e->k_steps = K;
+  if (int rc = capture(e, K, &e->graph_k, e->epochs_k)) return rc;
   for (int m = 0; m < n; ++m)
     if (int rc = plc::pre_steps(e->members[m])) return member_error(e, m, rc);
   if (int rc = ens_after_members(e)) return rc;
   if (ms) ENS_CUDA(e, cudaEventRecord(e->t0, e->stream));
-  for (int s = 0; s < nsteps; ++s) {
+  for (int s = 0; s < nsteps;) {
+    // K steps in one launch when none before the block's last needs the host
+    const bool block = nsteps - s >= K && steps_to_host(e, K) == K;
+    const int q = block ? K : 1;
     bool host = false;
-    for (plc_ctx *c : e->members) host = host || plc::step_needs_host(c);
-    ENS_CUDA(e, cudaGraphLaunch(e->graph, e->stream));
+    for (plc_ctx *c : e->members) {
+      c->nstep += q - 1;  // the last step of the launch decides
+      host = host || plc::step_needs_host(c);
+      c->nstep -= q - 1;
+    }
+    ENS_CUDA(e, cudaGraphLaunch(block ? e->graph_k : e->graph, e->stream));
     if (host)
       if (int rc = members_after_ens(e)) return rc;
-    for (int m = 0; m < n; ++m)
-      if (int rc = plc::post_step(e->members[m])) return member_error(e, m, rc);
+    for (int r = 0; r < q; ++r)
+      for (int m = 0; m < n; ++m)
+        if (int rc = plc::post_step(e->members[m])) return member_error(e, m, rc);
     // a member's host work (checks, a new dt) finished on its stream before
     // post_step returned; the next launch is queued after it
+    s += q;
   }
   if (ms) {
     ENS_CUDA(e, cudaEventRecord(e->t1, e->stream));
@@ -313,6 +373,7 @@ int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_
       return fail(PLC_ERR_CUDA);
     }
   e->epochs.assign(n, ~0u);
+  e->epochs_k.assign(n, ~0u);
   e->group.assign(n, 0);
   // cost model before measurement: grid points (FP32 fields move half the bytes)
   e->cost.resize(n);

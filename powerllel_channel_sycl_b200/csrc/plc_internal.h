@@ -112,6 +112,9 @@ struct plc_ctx {
   // by the autotuner; the device's shared-memory limit per block
   bool trid_tile = true;
   bool trid_pinned = false;  // PLC_TRID = "tile" or "stream"
+  // z planes per block of the RK stages (0: the kernels' maximum), chosen by
+  // the autotuner among kRkChunks; PLC_RK_KCHUNK pins it
+  int rk_kchunk = 0;
   size_t trid_smem_max = 0;
   bool fft_plans_pinned = false;
   // Plane order of the step kernels (0: low planes first, 1: high planes
@@ -179,6 +182,9 @@ bool host_fft_factor(int n, int *radix, int *npass);
 int host_parse_param_json(const char *path, plc_params *prm, std::string &err);
 
 // kernel launchers (return cudaError_t of the launch) ---------------------------
+// RK z-chunk candidates and the chunk a launch uses (at most kmax and nz)
+constexpr int kRkChunks[4] = {8, 16, 24, 32};
+inline int rk_chunk(const plc_ctx *c, int kmax);
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf,
                       const double *qu, const double *qv, const double *qw,
                       double *ou, double *ov, double *ow, cudaStream_t s);
@@ -287,5 +293,11 @@ int post_step(plc_ctx *c);
 bool step_needs_host(const plc_ctx *c);
 // closes the monitor files and releases the I/O state (plc_io.cc)
 void io_free(plc_ctx *c);
+
+inline int rk_chunk(const plc_ctx *c, int kmax) {
+  int k = c->rk_kchunk > 0 ? c->rk_kchunk : kmax;
+  if (k > kmax) k = kmax;
+  return k < c->nz ? k : c->nz;
+}
 
 }  // namespace plc

@@ -456,7 +456,7 @@ template <int STAGE, bool FUSE, bool CRF>
 cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[3], const RkConst &K,
                           float bc_u, float *ou, float *ov, float *ow, cudaStream_t s) {
   const size_t smem = rk32_smem_bytes();
-  const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
+  const int kchunk = rk_chunk(c, KCHUNK);
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   BulkMean bm;
   for (int d = 0; d < 3; ++d) {
@@ -507,9 +507,10 @@ unsigned convert_blocks(const plc_ctx *c, long long n) {
 
 }  // namespace
 
-// Blocks of the FP32 RK grid (the number of bulk-mean partials).
+// Blocks of the FP32 RK grid at the smallest z chunk the autotuner may
+// choose (the capacity of the bulk-mean partials).
 long long rk32_blocks(const plc_ctx *c) {
-  const int kchunk = c->nz < KCHUNK ? c->nz : KCHUNK;
+  const int kchunk = c->nz < kRkChunks[0] ? c->nz : kRkChunks[0];
   return (long long)((c->nx + RX - 1) / RX) * ((c->ny + RY - 1) / RY) *
          ((c->nz + kchunk - 1) / kchunk);
 }

@@ -1101,7 +1101,7 @@ template <int STAGE, bool FUSE>
 cudaError_t launch_rk_tma(const plc_ctx *c, const CUtensorMap &mu, const CUtensorMap &mv,
                           const CUtensorMap &mw, double u_crf, double *ou, double *ov, double *ow,
                           cudaStream_t s) {
-  const int kchunk = c->nz < KCHUNK_TMA ? c->nz : KCHUNK_TMA;
+  const int kchunk = rk_chunk(c, KCHUNK_TMA);
   dim3 grid((c->nx + RX - 1) / RX, (c->ny + RY - 1) / RY, (c->nz + kchunk - 1) / kchunk);
   if (u_crf != 0.0)
     k_rk_tma<STAGE, FUSE, true><<<grid, RX * TY, rk_tma_smem_bytes(), s>>>(

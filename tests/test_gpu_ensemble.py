@@ -1,6 +1,7 @@
-"""Batched ensembles on one GPU: every schedule gives each member exactly the
-fields it gets stepping alone; the autotuner restores the state it advances;
-checks stay per member."""
+"""Batched ensembles on one GPU: every schedule, and the launches of several
+steps per member branch between host events, give each member exactly the
+fields it gets stepping alone; the autotuner restores the state it
+advances; checks stay per member."""
 from __future__ import annotations
 
 import numpy as np
@@ -34,8 +35,19 @@ def standalone(spec, nsteps, **extra):
     return {q: ch.download(q) for q in "uvwp"}
 
 
+@pytest.fixture(scope="module", autouse=True)
+def pinned_fft_families():
+    """The transform families pinned for the whole module: the autotuner of
+    each context may pick different families (whose results differ by
+    rounding) for a member and for the same channel alone."""
+    with pytest.MonkeyPatch.context() as mp:
+        mp.setenv("PLC_FFT_PLANS", "0,0")
+        mp.setenv("PLC_FFT_PLANS_F32", "0,0")
+        yield
+
+
 @pytest.fixture(scope="module")
-def alone():
+def alone(pinned_fft_families):
     return [standalone(s, 6, nt_check=3, cfl_limit=10.0, div_limit=1e-8) for s in MEMBERS]
 
 
