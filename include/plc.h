@@ -170,15 +170,16 @@ int plc_fft_tiles(const plc_ctx *ctx, int *lines_xf, int *lines_x, int *lines_y)
  * ending in a radix-24 butterfly; 2: warp-line kernels, groups of four
  * warps transforming their own lines with no block barrier, for lengths
  * 32, 48, 64, 96, 128, 192, 256, 384, 512, 768).  PLC_FFT_PLANS (FP64) and
- * PLC_FFT_PLANS_F32 (mixed), "x,y", pin them (x for both x transforms).
- * No counterpart in the reference. */
+ * PLC_FFT_PLANS_F32 (mixed), "x,y" or "x,y,xf", pin them (x for both x
+ * transforms unless xf gives the forward one's).  No counterpart in the
+ * reference. */
 int plc_fft_plans(const plc_ctx *ctx, int *plan_x, int *plan_y);
 /* The family of the forward x transform (fused with calcRHS in the step),
  * timed separately from the backward one.  No counterpart in the reference. */
 int plc_fft_plan_x_fwd(const plc_ctx *ctx, int *plan);
 /* z planes per block of the two RK stages, timed per context at creation
  * among 8, 16, 24 and 32 (at most nz) on both fused stages; PLC_RK_KCHUNK
- * pins it.  The choice changes speed; results only in the mixed form, whose
+ * (FP64 form) and PLC_RK_KCHUNK_F32 (mixed form) pin it.  The choice changes speed; results only in the mixed form, whose
  * RK2 sums the bulk mean per block in FP32 (by FP32 rounding).  No
  * counterpart in the reference. */
 int plc_rk_kchunk(const plc_ctx *ctx, int *kchunk);

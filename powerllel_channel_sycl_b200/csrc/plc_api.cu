@@ -623,15 +623,22 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   // and y transforms (0: radix 16/8/4/2/3 passes, 1: two passes ending in
   // radix 24, 2: warp-line kernels; 1 and 2 only for lengths that have them)
   // the same way; the tiles are then timed under the pinned families.
+  // A third value pins the forward x transform's family apart from the
+  // backward one's ("x,y,xf").
   if (const char *env = getenv(c->mixed ? "PLC_FFT_PLANS_F32" : "PLC_FFT_PLANS")) {
-    int px = -1, py = -1;
-    if (sscanf(env, "%d,%d", &px, &py) != 2 || px < 0 || px > 2 || py < 0 || py > 2 ||
-        (px == 1 && !fft_has_two_plans(c->nx)) || (py == 1 && !fft_has_two_plans(c->ny)) ||
-        (px == 2 && !fft_has_warp_plan(c->nx, c->ny)) ||
+    int px = -1, py = -1, pxf = -1;
+    const int nread = sscanf(env, "%d,%d,%d", &px, &py, &pxf);
+    if (nread == 2) pxf = px;
+    auto valid_x = [&](int q) {
+      return q >= 0 && q <= 2 && (q != 1 || fft_has_two_plans(c->nx)) &&
+             (q != 2 || fft_has_warp_plan(c->nx, c->ny));
+    };
+    if (nread < 2 || !valid_x(px) || !valid_x(pxf) || py < 0 || py > 2 ||
+        (py == 1 && !fft_has_two_plans(c->ny)) ||
         (py == 2 && !fft_has_warp_plan(c->ny, c->nx)))
       return fail(set_error(c, PLC_ERR_ARG, std::string("invalid FFT plans in the environment: ") + env));
     c->fft_plan_x = px;
-    c->fft_plan_xf = px;
+    c->fft_plan_xf = pxf;
     c->fft_plan_y = py;
     c->fft_plans_pinned = true;
     if ((e = fft_set_lines(c, c->fft_lines_xf, c->fft_lines_x, c->fft_lines_y)) != cudaSuccess)
@@ -657,7 +664,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   if (!pinned && (e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
   // PLC_RK_KCHUNK pins the RK stages' z planes per block instead of timing
   // the candidates
-  if (const char *env = getenv("PLC_RK_KCHUNK")) {
+  if (const char *env = getenv(c->mixed ? "PLC_RK_KCHUNK_F32" : "PLC_RK_KCHUNK")) {
     const int k = atoi(env);
     if (k < 1 || k > 32)
       return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_RK_KCHUNK: ") + env));

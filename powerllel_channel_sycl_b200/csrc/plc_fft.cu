@@ -2314,7 +2314,6 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
        1,
        [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
-  if (c->fft_plans_pinned) c->fft_plan_xf = c->fft_plan_x;
   tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny),
        ny / 2, 1,
        [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },

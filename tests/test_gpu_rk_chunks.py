@@ -1,5 +1,5 @@
 """The RK stages' z planes per block (autotuned among 8, 16, 24, 32; pinned
-by PLC_RK_KCHUNK) change which blocks compute which planes: three fused
+by PLC_RK_KCHUNK / PLC_RK_KCHUNK_F32) change which blocks compute which planes: three fused
 steps of the FP64 form are bit-identical under every chunk, including one
 that does not divide nz.  The mixed form's fused RK2 also sums the bulk
 mean per block in FP32, so the chunk moves the forcing by FP32 rounding:
@@ -17,10 +17,11 @@ def run(monkeypatch, kchunk, precision, nx=64, ny=48, nz=40):
     from powerllel_channel_sycl_b200 import Channel
     monkeypatch.setenv("PLC_FFT_PLANS", "0,0")
     monkeypatch.setenv("PLC_FFT_PLANS_F32", "0,0")
+    var = "PLC_RK_KCHUNK_F32" if precision else "PLC_RK_KCHUNK"
     if kchunk is None:
-        monkeypatch.delenv("PLC_RK_KCHUNK", raising=False)
+        monkeypatch.delenv(var, raising=False)
     else:
-        monkeypatch.setenv("PLC_RK_KCHUNK", str(kchunk))
+        monkeypatch.setenv(var, str(kchunk))
     prm = channel_params(**case_kwargs(nx, ny, nz))
     prm.precision = precision
     ch = Channel(prm)
