@@ -473,7 +473,8 @@ int plc_get_sm_budget(const plc_ctx *ctx, int *sms);
 /* ---- batched ensembles of independent channels (no reference counterpart) ----
  * n member contexts with their own parameters (any grid, Re, dt, precision)
  * on one device; one ensemble step is one CUDA graph launch whose branches
- * are the members' fused steps.  Checks, CFL-controlled dt and error words
+ * are the members' fused steps, or (PLC_ENS_BATCHED) whose nodes are the
+ * step's stages, each one launch over a work list of (member, tile) items.  Checks, CFL-controlled dt and error words
  * stay per member (as plc_step); plc_ensemble_member gives a member's context
  * for every other entry point (upload, download, statistics, I/O). */
 typedef struct plc_ensemble plc_ensemble;
@@ -481,7 +482,10 @@ typedef struct plc_ensemble plc_ensemble;
 #define PLC_ENS_PROPORTIONAL 1 /* all at once, SMs shared in proportion to cost */
 #define PLC_ENS_TWO_GROUPS 2   /* two cost-balanced groups one after the other */
 #define PLC_ENS_SEQUENTIAL 3   /* one member after another */
-#define PLC_ENS_NUM_SCHEDULES 4
+#define PLC_ENS_BATCHED 4      /* each stage of the mixed-form members' step as one launch
+                                  over all of them (per line length for the transforms);
+                                  FP64 members as concurrent branches */
+#define PLC_ENS_NUM_SCHEDULES 5
 /* dzf_globals: NULL, or n pointers (each NULL or nz+2 spacings, as plc_create). */
 int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_globals,
                         int device, plc_ensemble **out);
@@ -500,11 +504,22 @@ int plc_ensemble_step_timed(plc_ensemble *ens, int nsteps, double *ms);
 int plc_ensemble_set_schedule(plc_ensemble *ens, int scheme);
 /* The schedule in use; groups and sm_budgets (n entries each) may be NULL. */
 int plc_ensemble_schedule(const plc_ensemble *ens, int *scheme, int *groups, int *sm_budgets);
-/* Autotuner: times each member alone (the cost model), then every schedule
- * over `steps` ensemble steps, keeps the fastest and restores the members'
- * u, v, w, p (step counters and dt are untouched).  ms_per_scheme
+/* Autotuner: times each member alone (the cost model), the plan families,
+ * tiles and RK z chunk of the batched schedule's launches (per line-length
+ * group, on the mixed-form members), then every schedule over `steps`
+ * ensemble steps, keeps the fastest and restores the members' u, v, w, p
+ * (step counters and dt are untouched).  ms_per_scheme
  * (PLC_ENS_NUM_SCHEDULES entries, -1 = not applicable) may be NULL. */
 int plc_ensemble_autotune(plc_ensemble *ens, int steps, float *ms_per_scheme);
+/* The batched schedule's tuned choices: the chains of mixed-form members
+ * stepped concurrently (1 or 2, cost-balanced), the RK stages' z planes per
+ * block (0: each member's own), the resident blocks per SM of their
+ * kernels, and the line-length groups tuned for the forward x, backward x
+ * and y transforms (3 entries; any pointer may be NULL). */
+int plc_ensemble_batch_choice(const plc_ensemble *ens, int *chains, int *rk_kchunk,
+                              int *rk_blocks_per_sm, int *fft_groups);
+/* Sets the batched schedule's chains (1 or 2) instead of the autotuner. */
+int plc_ensemble_set_batch_chains(plc_ensemble *ens, int chains);
 /* Multi-GPU placement of members: longest-processing-time-first over the
  * given costs; gpu_of[i] in [0, n_gpus).  Host only. */
 int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of);

@@ -80,6 +80,23 @@ int upload_step_consts(plc_ctx *c, double dt) {
   return PLC_OK;
 }
 
+// The same without waiting for the copy (after a check that synchronised the
+// stream): the values are staged in pinned scalars 16..21, which only this
+// function writes, and the next upload comes after the next check's
+// synchronisation.
+int upload_step_consts_async(plc_ctx *c, double dt) {
+  double *st = c->h_scal + 16;
+  st[0] = dt;
+  st[1] = 1.0 / dt;
+  st[2] = st[1] * c->dx_inv;
+  st[3] = st[1] * c->dy_inv;
+  st[4] = dt * c->dx_inv;
+  st[5] = dt * c->dy_inv;
+  PLC_CUDA(c, cudaMemcpyAsync(c->d_sc, st, 6 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->dt_host = dt;
+  return PLC_OK;
+}
+
 void free_poisson(plc_ctx *c) {
   // the captured step holds the solver's tables and tile sizes
   if (c->graph) cudaStreamSynchronize(c->stream);
@@ -595,7 +612,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
       (e = cudaMemset(c->d_counter, 0, 8 * sizeof(unsigned int))) != cudaSuccess ||
       (e = cudaMalloc(&c->d_check, sizeof(CheckResult))) != cudaSuccess ||
       (e = cudaMallocHost(&c->h_check, sizeof(CheckResult))) != cudaSuccess ||
-      (e = cudaMallocHost(&c->h_scal, 16 * sizeof(double))) != cudaSuccess)
+      (e = cudaMallocHost(&c->h_scal, 32 * sizeof(double))) != cudaSuccess)
     return fail(cuda_status(c, e, "scratch allocation"));
   c->d_err = reinterpret_cast<int *>(c->d_counter + 4);  // zeroed with the counters
   if ((e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) !=
@@ -669,6 +686,7 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     if (k < 1 || k > 32)
       return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_RK_KCHUNK: ") + env));
     c->rk_kchunk = k;
+    c->rk_pinned = true;
   } else if ((e = rk_autotune(c)) != cudaSuccess) {
     return fail(cuda_status(c, e, "rk_autotune"));
   }
@@ -1250,50 +1268,80 @@ bool step_needs_host(const plc_ctx *c) {
   return P.nt_check > 0 && n % P.nt_check == 0;
 }
 
-int post_step(plc_ctx *c) {
+// post_step in two halves: post_step_begin queues the step's checks (when
+// the step needs them) on the context's stream and their result's copy to
+// the host; post_step_end waits for them and acts on the result.  Several
+// contexts (an ensemble's members) thus share one wait.
+int post_step_begin(plc_ctx *c) {
   const plc_params &P = c->prm;
   ++c->nstep;
+  c->pending_check = 0;
   // Under CFL control the first steps also re-evaluate dt (steps 1, 2, 4,
   // ... below nt_check), without the limit checks: the first forcing step
   // moves the bulk velocity from that of the initial field (the reference's
   // rescale divides by nz*ny, mod_initFlow.cc:92) to vel_force, which changes
   // the CFL rate by up to nx/nz.
-  if (P.cfl_target > 0.0 && c->nstep < P.nt_check && (c->nstep & (c->nstep - 1)) == 0) {
-    if (int rc = run_check_fields(c, 2)) return rc;
+  if (P.cfl_target > 0.0 && c->nstep < P.nt_check && (c->nstep & (c->nstep - 1)) == 0)
+    c->pending_check = 2;
+  else if (P.nt_check > 0 && c->nstep % P.nt_check == 0)
+    c->pending_check = 7;  // main.cc:156-178
+  if (!c->pending_check) return PLC_OK;
+  if (c->mixed)
+    PLC_CUDA(c, launch_check(c, c->f_field[PLC_U], c->f_field[PLC_V], c->f_field[PLC_W],
+                             c->pending_check, c->stream));
+  else
+    PLC_CUDA(c, launch_check(c, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W],
+                             c->pending_check, c->stream));
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_check, c->d_check, sizeof(CheckResult), cudaMemcpyDeviceToHost,
+                              c->stream));
+  return PLC_OK;
+}
+
+int post_step_end(plc_ctx *c) {
+  const plc_params &P = c->prm;
+  const int what = c->pending_check;
+  c->pending_check = 0;
+  if (!what) return PLC_OK;
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (what == 2) {
     if (c->h_check->cfl > 0.0)
-      if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+      if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl)) return rc;
     return PLC_OK;
   }
-  if (P.nt_check > 0 && c->nstep % P.nt_check == 0) {
-    // main.cc:156-178
-    int passed;
-    plc_value_index cm, dm;
-    if (int rc = plc_check(c, &passed, &cm, &dm)) return rc;
-    bool ok = passed != 0;
-    std::string msg;
-    if (!passed) msg += "PowerLLEL.ERROR.checkNaN: NaN has been detected in <u>!\n";
-    if (cm.value > P.cfl_limit || std::isnan(cm.value)) {
-      ok = false;
-      msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
-    }
-    // The mixed form's divergence is at FP32 rounding level: its limit is
-    // div_limit scaled by the ratio of the unit round-offs, 2^-24 / 2^-53.
-    const double div_limit = c->mixed ? P.div_limit * 536870912.0 : P.div_limit;
-    if (dm.value > div_limit || std::isnan(dm.value)) {
-      ok = false;
-      msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
-    }
-    if (!ok) {
-      char buf[256];
-      snprintf(buf, sizeof buf,
-               "PowerLLEL.ERROR: nt = %9lld, cfl_max = %10.3e at (%5d,%5d,%5d), div_max = %10.3e at (%5d,%5d,%5d)",
-               c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
-      return set_error(c, PLC_ERR_CHECK, msg + buf);
-    }
-    if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
-      if (int rc = upload_step_consts(c, P.cfl_target / c->h_check->cfl)) return rc;
+  c->last_nan_passed = c->h_check->nan_found ? 0 : 1;
+  to_ijk(c, c->h_check->cfl_idx, &c->last_cfl, c->h_check->cfl * c->dt_host);
+  to_ijk(c, c->h_check->div_idx, &c->last_div, c->h_check->div);
+  const int passed = c->last_nan_passed;
+  const plc_value_index cm = c->last_cfl, dm = c->last_div;
+  bool ok = passed != 0;
+  std::string msg;
+  if (!passed) msg += "PowerLLEL.ERROR.checkNaN: NaN has been detected in <u>!\n";
+  if (cm.value > P.cfl_limit || std::isnan(cm.value)) {
+    ok = false;
+    msg += "PowerLLEL.ERROR.checkCFL: Maximum CFL number exceeds the threshold specified by the user!\n";
   }
+  // The mixed form's divergence is at FP32 rounding level: its limit is
+  // div_limit scaled by the ratio of the unit round-offs, 2^-24 / 2^-53.
+  const double div_limit = c->mixed ? P.div_limit * 536870912.0 : P.div_limit;
+  if (dm.value > div_limit || std::isnan(dm.value)) {
+    ok = false;
+    msg += "PowerLLEL.ERROR.checkDiv: Maximum divergence exceeds the threshold specified by the user!\n";
+  }
+  if (!ok) {
+    char buf[256];
+    snprintf(buf, sizeof buf,
+             "PowerLLEL.ERROR: nt = %9lld, cfl_max = %10.3e at (%5d,%5d,%5d), div_max = %10.3e at (%5d,%5d,%5d)",
+             c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
+    return set_error(c, PLC_ERR_CHECK, msg + buf);
+  }
+  if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
+    if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl)) return rc;
   return PLC_OK;
+}
+
+int post_step(plc_ctx *c) {
+  if (int rc = post_step_begin(c)) return rc;
+  return post_step_end(c);
 }
 
 }  // namespace plc

@@ -119,4 +119,30 @@ static __device__ __forceinline__ void store_point(T *q, const Geo &g, const Hal
   if ((h.dx | h.dy) != 0 || k == 1 || k == g.nz) store_images(q, g, h, c, k, v, kind, bc);
 }
 
+// Block coordinates of a kernel body that runs as one block of a batched
+// launch over several channels of an ensemble: the block's place in its
+// channel's share of the grid.
+struct VBlk {
+  int x_, y_, z_, gx_, gy_, gz_;
+  __device__ __forceinline__ int x() const { return x_; }
+  __device__ __forceinline__ int y() const { return y_; }
+  __device__ __forceinline__ int z() const { return z_; }
+  __device__ __forceinline__ int gx() const { return gx_; }
+  __device__ __forceinline__ int gy() const { return gy_; }
+  __device__ __forceinline__ int gz() const { return gz_; }
+  // block b (linear, x fastest) of a grid gx x gy x gz
+  static __device__ __forceinline__ VBlk of(int b, int gx, int gy, int gz) {
+    const int t = b / gx;
+    return VBlk{b - t * gx, t % gy, t / gy, gx, gy, gz};
+  }
+};
+
+// The channel of block b in a batched launch: start[m] <= b < start[m + 1]
+// (start in the launch's parameters, n channels).
+static __device__ __forceinline__ int batch_member(const int *start, int n, int b) {
+  int m = 0;
+  while (m + 1 < n && b >= start[m + 1]) ++m;
+  return m;
+}
+
 }  // namespace plc

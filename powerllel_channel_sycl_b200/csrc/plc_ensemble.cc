@@ -9,10 +9,15 @@
 // that finish early leave the GPU to the others instead of waiting for the
 // largest at every step.  Members are scheduled in groups (the members of a
 // group run concurrently, groups one after another), and every member's
-// persistent kernels get an SM budget; an autotuner times candidate
-// schedules on the members' own fields and keeps the fastest.  Checks,
-// CFL-controlled dt and the device error word stay per member, as in
-// plc_step.
+// persistent kernels get an SM budget.  The batched schedule instead walks
+// the step stage by stage: each stage of the mixed-form members is ONE
+// launch over a work list of (member, tile) items -- its blocks fill the
+// device with tiles of all the members, so small members no longer run at
+// the latency of their own short kernels -- and the transforms take one
+// launch per line length (their plans are compiled per length), run
+// concurrently.  An autotuner times the candidate schedules on the members'
+// own fields and keeps the fastest.  Checks, CFL-controlled dt and the
+// device error word stay per member, as in plc_step.
 
 #include <algorithm>
 #include <cmath>
@@ -38,6 +43,18 @@ struct plc_ensemble {
   int ngroups = 1;
   int scheme = PLC_ENS_CONCURRENT;
   std::vector<double> cost;  // measured ms per step of each member alone (0 = not measured)
+  // PLC_ENS_BATCHED: streams (and their join events) of the concurrent
+  // launches of a batched transform stage, one per line length
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> aux_join;
+  // PLC_ENS_BATCHED with two chains: the second chain's stream, its fork from
+  // the ensemble stream and its join, and the fork events of both chains'
+  // batched transform stages
+  cudaStream_t chain_stream = nullptr;
+  cudaEvent_t chain_join = nullptr;
+  cudaEvent_t stage_fork[2] = {nullptr, nullptr};
+  int chains = 1;        // batched chains of mixed-form members, run concurrently (1 or 2)
+  plc::BatchPlan bplan;  // families, tiles and z chunk of the batched launches
   std::string err;
 };
 
@@ -77,9 +94,101 @@ void drop(plc_ensemble *e) {
   }
 }
 
+constexpr int kAuxStreams = 8;
+
+// One batched transform stage of a chain: its launches (one per line
+// length) on the chain's auxiliary streams aux[a0 .. a0+na), forked from and
+// joined to the chain's stream st.
+template <class F>
+cudaError_t batched_stage(plc_ensemble *e, cudaStream_t st, cudaEvent_t fork, int a0, int na,
+                          int groups, F &&launch) {
+  if (groups <= 1 || na <= 1) return launch(&st, 1);
+  na = std::min(groups, na);
+  cudaError_t r = cudaEventRecord(fork, st);
+  for (int a = a0; a < a0 + na && r == cudaSuccess; ++a) r = cudaStreamWaitEvent(e->aux[a], fork, 0);
+  if (r == cudaSuccess) r = launch(e->aux.data() + a0, na);
+  for (int a = a0; a < a0 + na && r == cudaSuccess; ++a) {
+    if ((r = cudaEventRecord(e->aux_join[a], e->aux[a])) == cudaSuccess)
+      r = cudaStreamWaitEvent(st, e->aux_join[a], 0);
+  }
+  return r;
+}
+
+// `steps` steps of the mixed-form channels cs[0..n) stage by stage on stream
+// st, each stage one launch over all of them (the transforms: one per line
+// length, concurrently on aux[a0 .. a0+na)).
+int enqueue_chain(plc_ensemble *e, plc_ctx *const *cs, int n, int steps, cudaStream_t st,
+                  cudaEvent_t fork, int a0, int na) {
+  const int gx = plc::fft_batch_groups(cs, n, false), gy = plc::fft_batch_groups(cs, n, true);
+  const int kc = e->bplan.rk_kchunk, mb = e->bplan.rk_minb;
+  const plc::BatchPlan *bp = &e->bplan;
+  for (int q = 0; q < steps; ++q) {
+    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 1, kc, mb, st));  // RK1 + bound(u1)
+    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 2, kc, mb, st));  // RK2 + bound(u) + forcing
+    ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gx, [&](const cudaStream_t *ss, int ns) {
+               return plc::launch_fft_x_fwd_batch(cs, n, bp, ss, ns);  // calcRHS + x-FFT
+             }));
+    ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
+               return plc::launch_fft_y_batch(cs, n, false, bp, ss, ns);  // y-FFT
+             }));
+    ENS_CUDA(e, plc::launch_trid_batch(cs, n, st));  // z solve
+    ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
+               return plc::launch_fft_y_batch(cs, n, true, bp, ss, ns);  // y-iFFT
+             }));
+    ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gx, [&](const cudaStream_t *ss, int ns) {
+               return plc::launch_fft_x_bwd_batch(cs, n, bp, ss, ns);  // x-iFFT + bound(p)
+             }));
+    ENS_CUDA(e, plc::launch_correct_batch(cs, n, st));  // correct + force + bound(u)
+  }
+  return PLC_OK;
+}
+
+// The PLC_ENS_BATCHED form of `steps` ensemble steps (inside a capture on the
+// ensemble stream): the FP64 members' fused steps as branches; the
+// mixed-form members in e->chains chains (cost-balanced, longest first),
+// each chain's steps stage by stage, the chains concurrently.
+int enqueue_batched(plc_ensemble *e, int steps) {
+  std::vector<int> mixed, fp64;
+  for (size_t m = 0; m < e->members.size(); ++m) (e->members[m]->mixed ? mixed : fp64).push_back((int)m);
+  ENS_CUDA(e, cudaEventRecord(e->fork, e->stream));
+  for (int m : fp64) {
+    plc_ctx *c = e->members[m];
+    ENS_CUDA(e, cudaStreamWaitEvent(c->stream, e->fork, 0));
+    for (int q = 0; q < steps; ++q)
+      if (int rc = plc::capture_step(c, c->stream)) return member_error(e, m, rc);
+    ENS_CUDA(e, cudaEventRecord(e->join[m], c->stream));
+  }
+  const int nch = (int)mixed.size() >= 2 ? e->chains : 1;
+  std::vector<plc_ctx *> chain[2];
+  {
+    std::vector<int> order = mixed;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return e->cost[a] > e->cost[b]; });
+    double load[2] = {0.0, 0.0};
+    for (int m : order) {
+      const int k = (nch == 2 && load[1] < load[0]) ? 1 : 0;
+      chain[k].push_back(e->members[m]);
+      load[k] += e->cost[m];
+    }
+  }
+  if (nch == 2) {
+    ENS_CUDA(e, cudaStreamWaitEvent(e->chain_stream, e->fork, 0));
+    if (int rc = enqueue_chain(e, chain[1].data(), (int)chain[1].size(), steps, e->chain_stream,
+                               e->stage_fork[1], kAuxStreams / 2, kAuxStreams / 2))
+      return rc;
+    ENS_CUDA(e, cudaEventRecord(e->chain_join, e->chain_stream));
+  }
+  if (!chain[0].empty())
+    if (int rc = enqueue_chain(e, chain[0].data(), (int)chain[0].size(), steps, e->stream,
+                               e->stage_fork[0], 0, nch == 2 ? kAuxStreams / 2 : kAuxStreams))
+      return rc;
+  if (nch == 2) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->chain_join, 0));
+  for (int m : fp64) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
+  return PLC_OK;
+}
+
 // Captures `steps` ensemble steps into *out: per group, a fork from the
 // ensemble stream to the members' streams, each member's fused steps in a
-// row, a join back.
+// row, a join back (PLC_ENS_BATCHED: enqueue_batched).
 int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsigned> &epochs) {
   const int n = (int)e->members.size();
   bool stale = *out == nullptr;
@@ -96,7 +205,10 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
   ENS_CUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   int rc = PLC_OK;
   cudaError_t r = cudaSuccess;
-  for (int grp = 0; grp < e->ngroups && rc == PLC_OK && r == cudaSuccess; ++grp) {
+  if (e->scheme == PLC_ENS_BATCHED) rc = enqueue_batched(e, steps);
+  for (int grp = 0; grp < e->ngroups && rc == PLC_OK && r == cudaSuccess &&
+                    e->scheme != PLC_ENS_BATCHED;
+       ++grp) {
     if ((r = cudaEventRecord(e->fork, e->stream)) != cudaSuccess) break;
     for (int m = 0; m < n && rc == PLC_OK && r == cudaSuccess; ++m) {
       if (e->group[m] != grp) continue;
@@ -198,11 +310,17 @@ int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
     ENS_CUDA(e, cudaGraphLaunch(block ? e->graph_k : e->graph, e->stream));
     if (host)
       if (int rc = members_after_ens(e)) return rc;
-    for (int r = 0; r < q; ++r)
+    for (int r = 0; r < q; ++r) {
+      // the members' checks queued first, then one wait for all of them
       for (int m = 0; m < n; ++m)
-        if (int rc = plc::post_step(e->members[m])) return member_error(e, m, rc);
-    // a member's host work (checks, a new dt) finished on its stream before
-    // post_step returned; the next launch is queued after it
+        if (int rc = plc::post_step_begin(e->members[m])) return member_error(e, m, rc);
+      for (int m = 0; m < n; ++m)
+        if (int rc = plc::post_step_end(e->members[m])) return member_error(e, m, rc);
+    }
+    // a member's host work ends with a new dt copied on its stream: the next
+    // launch is queued after it
+    if (host)
+      if (int rc = ens_after_members(e)) return rc;
     s += q;
   }
   if (ms) {
@@ -319,6 +437,12 @@ int apply_scheme(plc_ensemble *e, int scheme) {
       for (int q = 0; q < n; ++q) e->group[order[q]] = q;
       e->ngroups = n;
       break;
+    case PLC_ENS_BATCHED: {  // stage by stage over the mixed-form members, full budgets
+      bool any = false;
+      for (const plc_ctx *c : e->members) any = any || c->mixed;
+      if (!any) return ens_error(e, PLC_ERR_ARG, "the batched schedule needs mixed-form members");
+      break;
+    }
     default:
       return ens_error(e, PLC_ERR_ARG, "unknown ensemble schedule");
   }
@@ -372,6 +496,21 @@ int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_
       ens_cuda(e, r, "ensemble events");
       return fail(PLC_ERR_CUDA);
     }
+  if ((r = cudaStreamCreateWithFlags(&e->chain_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (r = cudaEventCreateWithFlags(&e->chain_join, cudaEventDisableTiming)) != cudaSuccess ||
+      (r = cudaEventCreateWithFlags(&e->stage_fork[0], cudaEventDisableTiming)) != cudaSuccess ||
+      (r = cudaEventCreateWithFlags(&e->stage_fork[1], cudaEventDisableTiming)) != cudaSuccess) {
+    ens_cuda(e, r, "ensemble chain stream/events");
+    return fail(PLC_ERR_CUDA);
+  }
+  e->aux.assign(kAuxStreams, nullptr);
+  e->aux_join.assign(kAuxStreams, nullptr);
+  for (int a = 0; a < kAuxStreams; ++a)
+    if ((r = cudaStreamCreateWithFlags(&e->aux[a], cudaStreamNonBlocking)) != cudaSuccess ||
+        (r = cudaEventCreateWithFlags(&e->aux_join[a], cudaEventDisableTiming)) != cudaSuccess) {
+      ens_cuda(e, r, "ensemble auxiliary streams");
+      return fail(PLC_ERR_CUDA);
+    }
   e->epochs.assign(n, ~0u);
   e->epochs_k.assign(n, ~0u);
   e->group.assign(n, 0);
@@ -394,6 +533,13 @@ int plc_ensemble_destroy(plc_ensemble *e) {
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : {e->fork, e->done, e->t0, e->t1})
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : e->aux_join)
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {e->chain_join, e->stage_fork[0], e->stage_fork[1]})
+    if (ev) cudaEventDestroy(ev);
+  if (e->chain_stream) cudaStreamDestroy(e->chain_stream);
+  for (cudaStream_t st : e->aux)
+    if (st) cudaStreamDestroy(st);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return PLC_OK;
@@ -450,6 +596,8 @@ int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
   Snapshot snap;
   if (int rc = snapshot(e, snap, true)) return rc;
   int rc = PLC_OK;
+  bool any_mixed = false;
+  for (const plc_ctx *c : e->members) any_mixed = any_mixed || c->mixed;
   // 1. cost model: each member's step time alone, full budget
   for (int m = 0; m < n && rc == PLC_OK; ++m) {
     if ((rc = plc_set_sm_budget(e->members[m], e->members[m]->device_sms)) != PLC_OK) {
@@ -459,16 +607,44 @@ int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
     float t = 0.f;
     if ((rc = time_member(e, m, steps, &t)) == PLC_OK) e->cost[m] = t;
   }
-  // 2. every schedule on the ensemble graph; the fastest is kept
+  // 2. the batched launches' families, tiles and z chunk on the members' fields
+  if (rc == PLC_OK && any_mixed) {
+    std::vector<plc_ctx *> mixed;
+    for (plc_ctx *c : e->members)
+      if (c->mixed) mixed.push_back(c);
+    for (plc_ctx *c : mixed) {
+      const cudaError_t r = cudaStreamSynchronize(c->stream);
+      if (r != cudaSuccess) rc = ens_cuda(e, r, "cudaStreamSynchronize");
+    }
+    if (rc == PLC_OK) {
+      const cudaError_t r = plc::batch_autotune(mixed.data(), (int)mixed.size(), e->stream, &e->bplan);
+      if (r != cudaSuccess) rc = ens_cuda(e, r, "batch_autotune");
+      drop(e);
+    }
+  }
+  // 3. every schedule on the ensemble graph; the fastest is kept
   int best = PLC_ENS_CONCURRENT;
   float best_t = -1.f;
+  int best_chains = e->chains;
   for (int s = 0; s < PLC_ENS_NUM_SCHEDULES && rc == PLC_OK; ++s) {
-    if (s == PLC_ENS_TWO_GROUPS && n < 2) {
+    if ((s == PLC_ENS_TWO_GROUPS && n < 2) || (s == PLC_ENS_BATCHED && !any_mixed)) {
       if (ms_per_scheme) ms_per_scheme[s] = -1.f;
       continue;
     }
-    float t = 0.f;
-    if ((rc = apply_scheme(e, s)) != PLC_OK || (rc = time_launches(e, steps, &t)) != PLC_OK) break;
+    // the batched schedule: one chain of all the mixed-form members, or two
+    // cost-balanced chains run concurrently
+    float t = -1.f;
+    const int max_chains = s == PLC_ENS_BATCHED ? 2 : 1;
+    for (int ch = 1; ch <= max_chains && rc == PLC_OK; ++ch) {
+      float tc = 0.f;
+      if (s == PLC_ENS_BATCHED) e->chains = ch;
+      if ((rc = apply_scheme(e, s)) != PLC_OK || (rc = time_launches(e, steps, &tc)) != PLC_OK) break;
+      if (t < 0.f || tc < t) {
+        t = tc;
+        if (s == PLC_ENS_BATCHED) best_chains = ch;
+      }
+    }
+    if (rc != PLC_OK) break;
     t /= steps;
     if (ms_per_scheme) ms_per_scheme[s] = t;
     if (best_t < 0.f || t < best_t) {
@@ -476,9 +652,31 @@ int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
       best = s;
     }
   }
+  e->chains = best_chains;
   if (rc == PLC_OK) rc = apply_scheme(e, best);
   const int rc2 = snapshot(e, snap, false);
   return rc != PLC_OK ? rc : rc2;
+}
+
+int plc_ensemble_set_batch_chains(plc_ensemble *e, int chains) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  if (chains < 1 || chains > 2) return ens_error(e, PLC_ERR_ARG, "chains must be 1 or 2");
+  if (chains != e->chains) {
+    e->chains = chains;
+    drop(e);
+  }
+  return PLC_OK;
+}
+
+int plc_ensemble_batch_choice(const plc_ensemble *e, int *chains, int *rk_kchunk,
+                              int *rk_blocks_per_sm, int *fft_groups) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  if (chains) *chains = e->chains;
+  if (rk_kchunk) *rk_kchunk = e->bplan.rk_kchunk;
+  if (rk_blocks_per_sm) *rk_blocks_per_sm = e->bplan.rk_minb;
+  if (fft_groups)
+    for (int d = 0; d < 3; ++d) fft_groups[d] = (int)e->bplan.dir[d].size();
+  return PLC_OK;
 }
 
 int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of) {

@@ -36,7 +36,10 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <type_traits>
+#include <vector>
 
 #include "plc_device.cuh"
 #include "plc_internal.h"
@@ -656,6 +659,59 @@ __global__ void __launch_bounds__(256) k_fft_x_fwd_div(Geo g, FftDev<typename Cx
   }
 }
 
+// The same for one block of a batched launch over several channels (the
+// block's coordinates from the work list).  The single-channel kernel keeps
+// its own copy of these lines: a body shared between the two changed the
+// single-channel kernel's code generation and made it slower.
+template <class T, int N, bool FUSED, int PL>
+__device__ __forceinline__ void fft_x_fwd_div_body(Geo g, FftDev<typename Cx<T>::V> P,
+                                                   int nl, const StepConst *__restrict__ sc,
+                                                   const T *__restrict__ p,
+                                                   const T *__restrict__ u,
+                                                   const T *__restrict__ v,
+                                                   const T *__restrict__ w,
+                                                   T *__restrict__ var, VBlk vb) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : g.nx, LS = line_stride<V>(n);
+  V *A = smem, *B = smem + nl * LS;
+  const int j0 = vb.x() * 2 * nl;  // 0-based row in the plane
+  const int k = vb.y();            // 0-based plane
+  T dti = 0, dtidxi = 0, dtidyi = 0, dzfi = 0;
+  if (FUSED) {
+    dti = T(sc->dti);
+    dtidxi = T(sc->dtidxi);
+    dtidyi = T(sc->dtidyi);
+    dzfi = T(__ldg(g.dzf_inv + k + 1));
+  }
+  for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+    const int l = e / n, t = e - l * n;
+    const long long ca = g.at(t + 1, j0 + 2 * l + 1, k + 1);
+    const long long cb = ca + g.X;
+    T a, b;
+    if (FUSED) {
+      a = div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
+      b = div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
+    } else {
+      a = p[ca];
+      b = p[cb];
+    }
+    A[l * LS + padi<V>(t)] = mk<V>(a, b);
+  }
+  __syncthreads();
+  const V *Z = fft_run_n<N, false, PL>(A, B, nl, LS, P);
+  const int half = n >> 1;
+  for (int e = threadIdx.x; e < nl * half; e += blockDim.x) {
+    const int l = e / half, m = e - l * half;
+    V a, b;
+    unpack_four(Z + l * LS, n, m, a, b);
+    const long long row = (long long)k * g.ny + j0 + 2 * l;
+    reinterpret_cast<V *>(var + row * n)[m] = a;
+    reinterpret_cast<V *>(var + (row + 1) * n)[m] = b;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Persistent transform kernels.  Each block takes tiles t = blockIdx.x,
 // blockIdx.x + gridDim.x, ...; the raw rows of the next tile are copied into
@@ -861,6 +917,135 @@ __global__ void __launch_bounds__(128) k_fft_x_bwd(Geo g, FftDev<typename Cx<T>:
   }
 }
 
+// The same for one block of a batched launch over several channels (the
+// block's coordinates from the work list).  The single-channel kernel keeps
+// its own copy of these lines: a body shared between the two changed the
+// single-channel kernel's code generation and made it slower.
+template <class T, int N, bool FUSE_BC, int PL>
+__device__ __forceinline__ void fft_x_bwd_body(Geo g, FftDev<typename Cx<T>::V> P,
+                                               int nl, double nf, const T *__restrict__ var, T *p,
+                                               int rev, VBlk vb) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : g.nx, LS = line_stride<V>(n), R = 2 * nl;
+  V *A = smem, *B = smem + nl * LS;
+  T *S = reinterpret_cast<T *>(B + nl * LS);  // R rows of n elements
+  const int tiles_y = g.ny / R;
+  const int ntiles = tiles_y * g.nz;
+  const T scale = T(nf);
+  const FastDiv fcpr(n / (16 / sizeof(T)));
+  auto issue = [&](int tile) {
+    const int tt = rev ? ntiles - 1 - tile : tile;  // plane order
+    const int j0 = (tt % tiles_y) * R, k = tt / tiles_y;
+    stage_rows(S, var + ((long long)k * g.ny + j0) * n, R, n, n, fcpr);
+    cp_async_commit();
+  };
+  int tile = vb.x();
+  if (tile < ntiles) issue(tile);
+  const int half = n >> 1;
+  for (; tile < ntiles; tile += vb.gx()) {
+    const int tt = rev ? ntiles - 1 - tile : tile;
+    const int j0 = (tt % tiles_y) * R, k = tt / tiles_y;
+    cp_async_wait_all();
+    __syncthreads();
+    for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
+      const int l = e / (half + 1), m = e - l * (half + 1);
+      pack_pair_rows(A + l * LS, n, m, S + (2 * l) * n, S + (2 * l + 1) * n);
+    }
+    __syncthreads();
+    if (tile + vb.gx() < ntiles) issue(tile + vb.gx());
+    V *Z = fft_run_n<N, true, PL>(A, B, nl, LS, P);
+    // rows j = j0 + 2l + 1 (a) and j + 1 (b) of plane k + 1
+    const int kk = k + 1;
+    // FP32 with the pressure halos (updateBoundP) and rows shorter than a
+    // line of the FFT buffer the last pass left free (n >= 64): the scaled
+    // rows are laid out whole there -- x images and row padding included --
+    // then stored as float4, each row once more to its y image row and z
+    // ghost plane where it has one.  Rows start on 16-byte boundaries (the
+    // pitch is a multiple of 4); the free buffer's start is rounded up to 16
+    // bytes (it is 8-byte aligned), which the slack of at least 2*nl elements
+    // covers.  (The FP64 kernel measured slower this way, 0.58 against 0.46 ms
+    // at 768 x 384 x 256: it keeps the element loop below.)
+    if (FUSE_BC && sizeof(T) == 4 && g.X < LS &&
+        (reinterpret_cast<unsigned long long>(p) & 15ull) == 0) {
+      using T16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+      constexpr int VW = 16 / sizeof(T);
+      const int X = g.X, nq = X / VW;
+      const FastDiv fnq(nq);
+      // line l: rows a, b at 2*l*X
+      T *O = reinterpret_cast<T *>(
+          (reinterpret_cast<unsigned long long>(Z == A ? B : A) + 15ull) & ~15ull);
+      for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+        const int l = e / n, t = e - l * n;
+        const V z = Z[l * LS + padi<V>(t)];
+        T *oa = O + 2 * l * X, *ob = oa + X;
+        const T a = scale * z.x, b = scale * z.y;
+        oa[t + 1] = a;
+        ob[t + 1] = b;
+        if (t == 0) {  // x image of i = 1
+          oa[n + 1] = a;
+          ob[n + 1] = b;
+        }
+        if (t == n - 1) {  // x image of i = n
+          oa[0] = a;
+          ob[0] = b;
+        }
+      }
+      for (int e = threadIdx.x; e < nl * 2 * (X - n - 2); e += blockDim.x) {
+        const int r = e / (X - n - 2);  // row padding
+        O[r * X + n + 2 + (e - r * (X - n - 2))] = T(0);
+      }
+      __syncthreads();
+      const int kimg = kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1);
+      for (int e = threadIdx.x; e < 2 * nl * nq; e += blockDim.x) {
+        const int r = fnq.div(e), q = e - r * nq;  // r = 2l + h
+        const T16 val = reinterpret_cast<const T16 *>(O + r * X)[q];
+        const int j = j0 + r + 1;
+        const int jimg = j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1);
+        auto row = [&](int jj, int kq) {
+          reinterpret_cast<T16 *>(p + (long long)jj * X + (long long)kq * g.XY)[q] = val;
+        };
+        row(j, kk);
+        if (jimg >= 0) row(jimg, kk);
+        if (kimg >= 0) {
+          row(j, kimg);
+          if (jimg >= 0) row(jimg, kimg);
+        }
+      }
+    } else {
+      // element by element; with FUSE_BC also the periodic images (x ends of
+      // each row, the y image row) and the zero-gradient ghost plane, decided
+      // per row
+      const int kimg = !FUSE_BC ? -1 : (kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1));
+      for (int e = threadIdx.x; e < nl * n; e += blockDim.x) {
+        const int l = e / n, t = e - l * n;
+        const V z = Z[l * LS + padi<V>(t)];
+        const T ab[2] = {scale * z.x, scale * z.y};
+        const int i = t + 1;
+        const int iimg = !FUSE_BC ? -1 : (i == g.nx ? 0 : (i == 1 ? g.nx + 1 : -1));
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = j0 + 2 * l + 1 + h;
+          const int jimg = !FUSE_BC ? -1 : (j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1));
+          const T v = ab[h];
+          auto row = [&](int jj, int kq) {
+            T *r = p + (long long)jj * g.X + (long long)kq * g.XY;
+            r[i] = v;
+            if (iimg >= 0) r[iimg] = v;
+          };
+          row(j, kk);
+          if (jimg >= 0) row(jimg, kk);
+          if (kimg >= 0) {
+            row(j, kimg);
+            if (jimg >= 0) row(jimg, kimg);
+          }
+        }
+      }
+    }
+  }
+}
+
 // y transform in place on the spectral array: tile = columns i0..i0+2nl-1 of
 // plane k (TX = 2nl x-contiguous elements per row, row stride nx).
 template <class T, int N, bool INV, int PL>
@@ -912,6 +1097,79 @@ __global__ void __launch_bounds__(256) k_fft_y(int nx, int ny, int nz,
     }
     __syncthreads();
     if (tile + (int)gridDim.x < ntiles) issue(tile + gridDim.x);
+    const V *Z = fft_run_n<N, INV, PL>(A, B, nl, LS, P);
+    if (!INV) {
+      for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
+        const int m = fnl.div(e), l = e - m * nl;
+        V a, b;
+        unpack_four(Z + l * LS, n, m, a, b);
+        const int q0 = (m == 0) ? 0 : 2 * m;
+        // row q0: (A, B) of columns 2l, 2l+1; row q0+1 likewise
+        reinterpret_cast<V *>(plane + (long long)q0 * nx)[l] = mk<V>(a.x, b.x);
+        reinterpret_cast<V *>(plane + (long long)(q0 + 1) * nx)[l] = mk<V>(a.y, b.y);
+      }
+    } else {
+      for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const int t = fnl.div(e), l = e - t * nl;
+        reinterpret_cast<V *>(plane + (long long)t * nx)[l] = Z[l * LS + padi<V>(t)];
+      }
+    }
+  }
+}
+
+// The same for one block of a batched launch over several channels (the
+// block's coordinates from the work list).  The single-channel kernel keeps
+// its own copy of these lines: a body shared between the two changed the
+// single-channel kernel's code generation and made it slower.
+template <class T, int N, bool INV, int PL>
+__device__ __forceinline__ void fft_y_body(int nx, int ny, int nz,
+                                           FftDev<typename Cx<T>::V> P, int nl,
+                                           T *__restrict__ var, int rev, VBlk vb) {
+  using V = typename Cx<T>::V;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *smem = reinterpret_cast<V *>(fft_smem);
+  const int n = N > 0 ? N : ny, LS = line_stride<V>(n), TX = 2 * nl;
+  V *A = smem, *B = smem + nl * LS;
+  T *S = reinterpret_cast<T *>(B + nl * LS);  // n rows of TX elements
+  const int tiles_x = nx / TX;
+  const int ntiles = tiles_x * nz;
+  const FastDiv fcpr(TX / (16 / sizeof(T))), fnl(nl);
+  auto issue = [&](int tile) {
+    const int tt = rev ? ntiles - 1 - tile : tile;  // plane order
+    const int i0 = (tt % tiles_x) * TX, k = tt / tiles_x;
+    stage_rows(S, var + (long long)k * nx * ny + i0, n, TX, nx, fcpr);
+    cp_async_commit();
+  };
+  int tile = vb.x();
+  if (tile < ntiles) issue(tile);
+  const int half = n >> 1;
+  for (; tile < ntiles; tile += vb.gx()) {
+    const int tt = rev ? ntiles - 1 - tile : tile;
+    const int i0 = (tt % tiles_x) * TX, k = tt / tiles_x;
+    T *plane = var + (long long)k * nx * ny + i0;
+    cp_async_wait_all();
+    __syncthreads();
+    if (!INV) {
+      // columns 2l, 2l+1 of row t form element t of line l: one vector
+      // load and store per pair
+      for (int e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const int t = fnl.div(e), l = e - t * nl;
+        A[l * LS + padi<V>(t)] = reinterpret_cast<const V *>(S + t * TX)[l];
+      }
+    } else {
+      // consecutive threads take consecutive column pairs l: their reads of
+      // the staged rows are adjacent (a stride of 2*TX elements between
+      // threads would put every lane in one bank)
+      for (int e = threadIdx.x; e < nl * (half + 1); e += blockDim.x) {
+        const int m = fnl.div(e), l = e - m * nl;
+        if constexpr (sizeof(T) == 4)
+          pack_pair_cols(A + l * LS, n, m, reinterpret_cast<const V *>(S) + l, nl);
+        else  // FP64: scalar loads (16-byte ones measured 3% slower)
+          pack_pair_cols_scalar(A + l * LS, n, m, S + 2 * l, TX);
+      }
+    }
+    __syncthreads();
+    if (tile + vb.gx() < ntiles) issue(tile + vb.gx());
     const V *Z = fft_run_n<N, INV, PL>(A, B, nl, LS, P);
     if (!INV) {
       for (int e = threadIdx.x; e < half * nl; e += blockDim.x) {
@@ -1604,6 +1862,122 @@ __global__ void __launch_bounds__(128) k_trid_mixed(
   }
 }
 
+// The same for one block of a batched launch over several channels (the
+// block's coordinates from the work list).  The single-channel kernel keeps
+// its own copy of these lines: a body shared between the two changed the
+// single-channel kernel's code generation and made it slower.
+__device__ __forceinline__ void trid_mixed_body(
+    int nx, int ny, int nz, const float *__restrict__ rpiv32, const float *__restrict__ a32,
+    const float *__restrict__ c32, const double *__restrict__ rpiv,
+    const double *__restrict__ a, const double *__restrict__ c, float *__restrict__ var,
+    double *__restrict__ low, int bx) {
+  const int t = bx * blockDim.x + threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  if (t >= plane) return;
+  int i, j;
+  long long pv;
+  trid_index(t, nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  if (i < kLowModes && j < kLowModes) {
+    constexpr long long LP = (long long)kLowModes * kLowModes;
+    thomas_sweep<double, 8>(
+        nz, LowSys{var + t, plane, low + j * kLowModes + i, LP, rpiv + pv, PS, a, c});
+  } else {
+    // 24 planes of loads in flight (0.238 ms against 0.252 for 16 and 0.259
+    // for 8 at 768 x 384 x 256)
+    thomas_inplace<float, 24>(nz, var + t, plane, rpiv32 + pv, PS, a32, c32);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched launches over the mixed-form channels of an ensemble: one launch
+// per stage (and line length) carries each channel's arguments in its
+// parameters; block b works for channel m, start[m] <= b < start[m + 1], as
+// block b - start[m] of that channel's own grid (for the persistent kernels:
+// of the channel's share of the launch's blocks, vblocks).
+// ---------------------------------------------------------------------------
+struct XfMember {
+  Geo g;
+  FftDev<float2> P;
+  int nl, gx, gy;
+  const StepConst *sc;
+  const float *u, *v, *w;
+  float *var;
+};
+struct XfBatch {
+  int n;
+  int start[kBatchMax + 1];
+  XfMember m[kBatchMax];
+};
+template <int N, int PL>
+__global__ void __launch_bounds__(256) k_fft_x_fwd_div_batch(const __grid_constant__ XfBatch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const XfMember &a = b.m[q];
+  fft_x_fwd_div_body<float, N, true, PL>(a.g, a.P, a.nl, a.sc, nullptr, a.u, a.v, a.w, a.var,
+                                         VBlk::of((int)blockIdx.x - b.start[q], a.gx, a.gy, 1));
+}
+
+struct YMember {
+  int nx, ny, nz, nl, rev, vblocks;
+  FftDev<float2> P;
+  float *var;
+};
+struct YBatch {
+  int n;
+  int start[kBatchMax + 1];
+  YMember m[kBatchMax];
+};
+template <int N, bool INV, int PL>
+__global__ void __launch_bounds__(256) k_fft_y_batch(const __grid_constant__ YBatch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const YMember &a = b.m[q];
+  fft_y_body<float, N, INV, PL>(a.nx, a.ny, a.nz, a.P, a.nl, a.var, a.rev,
+                                VBlk::of((int)blockIdx.x - b.start[q], a.vblocks, 1, 1));
+}
+
+struct XbMember {
+  Geo g;
+  FftDev<float2> P;
+  int nl, rev, vblocks;
+  double nf;
+  const float *var;
+  float *p;
+};
+struct XbBatch {
+  int n;
+  int start[kBatchMax + 1];
+  XbMember m[kBatchMax];
+};
+template <int N, int PL>
+__global__ void __launch_bounds__(128) k_fft_x_bwd_batch(const __grid_constant__ XbBatch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const XbMember &a = b.m[q];
+  fft_x_bwd_body<float, N, true, PL>(a.g, a.P, a.nl, a.nf, a.var, a.p, a.rev,
+                                     VBlk::of((int)blockIdx.x - b.start[q], a.vblocks, 1, 1));
+}
+
+struct TrMember {
+  int nx, ny, nz;
+  const float *rpiv32, *a32, *c32;
+  const double *rpiv, *a, *c;
+  float *var;
+  double *low;
+};
+struct TrBatch {
+  int n;
+  int start[kBatchMax + 1];
+  TrMember m[kBatchMax];
+};
+__global__ void __launch_bounds__(128) k_trid_mixed_batch(const __grid_constant__ TrBatch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const TrMember &a = b.m[q];
+  trid_mixed_body(a.nx, a.ny, a.nz, a.rpiv32, a.a32, a.c32, a.rpiv, a.a, a.c, a.var, a.low,
+                  (int)blockIdx.x - b.start[q]);
+}
+static_assert(sizeof(XfBatch) <= 32000 && sizeof(YBatch) <= 32000 && sizeof(XbBatch) <= 32000 &&
+                  sizeof(TrBatch) <= 32000,
+              "kernel parameters are limited to 32764 bytes");
+
 // ---------------------------------------------------------------------------
 // Thomas sweep with the right-hand side held on chip.  A block of 32 threads
 // owns 32 consecutive systems (packed x indices i0 .. i0+31 of one packed y
@@ -1987,6 +2361,10 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_fft_x_bwd<float, N, false, PL>));
         PLC_SMEM((k_fft_y<float, N, true, PL>));
         PLC_SMEM((k_fft_y<float, N, false, PL>));
+        PLC_SMEM((k_fft_x_fwd_div_batch<N, PL>));
+        PLC_SMEM((k_fft_x_bwd_batch<N, PL>));
+        PLC_SMEM((k_fft_y_batch<N, true, PL>));
+        PLC_SMEM((k_fft_y_batch<N, false, PL>));
         return cudaSuccess;
       };
       if constexpr (N > 0 && wp_base_lines(N) > 0) {
@@ -2395,6 +2773,365 @@ cudaError_t launch_trid(const plc_ctx *c, float *var, cudaStream_t s) {
       c->nx, c->ny, c->nz, c->d_rpiv32, c->d_ac32, c->d_ac32 + c->nz, c->d_rpiv, c->d_ac,
       c->d_ac + c->nz, var, c->d_low);
   return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Launchers of the batched stages (mixed-form channels of an ensemble).
+// ---------------------------------------------------------------------------
+namespace {
+// Channels of one batched transform launch: those whose line length has the
+// same compiled plan (every length without one shares the runtime plan,
+// N = 0), with the family and the tile of the batch plan, else of the
+// group's largest channel and the largest tile all its channels admit (the
+// warp-line family runs as family 0 in a batch; tiles only change the speed).
+struct BatchGroup {
+  int N = 0, PL = 0, nl = 1;
+  size_t smem = 0;
+  std::vector<plc_ctx *> ms;
+};
+
+int compiled_len(int n) {
+  int key = 0;
+  with_size(n, [&](auto NC) -> cudaError_t {
+    key = decltype(NC)::value;
+    return cudaSuccess;
+  });
+  return key;
+}
+
+// line pairs of a channel's tiles (the lines of the other axis) and the step
+// of the tile sizes (FP32 y tiles span a multiple of 4 columns)
+int batch_pairs(const plc_ctx *c, int dir) { return (dir == BATCH_Y ? c->nx : c->ny) / 2; }
+int batch_step(int dir) { return dir == BATCH_Y ? 2 : 1; }
+size_t batch_bytes(const plc_ctx *c, int dir, int d) {
+  return dir == BATCH_Y ? smem_y<float>(c->ny, d)
+                        : (dir == BATCH_XF ? fft_bytes<float>(c->nx, d) : smem_x_bwd<float>(c->nx, d));
+}
+// whether every channel of the group admits tiles of d line pairs
+bool batch_tile_ok(const BatchGroup &g, int dir, int d) {
+  if (d < batch_step(dir) || d % batch_step(dir)) return false;
+  for (const plc_ctx *c : g.ms)
+    if (batch_pairs(c, dir) % d || batch_bytes(c, dir, d) > c->trid_smem_max) return false;
+  return true;
+}
+bool batch_family_ok(int N, int pl) { return pl == 0 || (pl == 1 && N > 0 && plan_has24(N)); }
+void batch_set_tile(BatchGroup &g, int dir, int nl) {
+  g.nl = nl;
+  g.smem = 0;
+  for (const plc_ctx *c : g.ms) g.smem = std::max(g.smem, batch_bytes(c, dir, nl));
+}
+
+std::vector<BatchGroup> batch_groups(plc_ctx *const *cs, int n, int dir, const BatchPlan *bp) {
+  std::vector<BatchGroup> out;
+  for (int m = 0; m < n; ++m) {
+    plc_ctx *c = cs[m];
+    const int key = compiled_len(dir == BATCH_Y ? c->ny : c->nx);
+    BatchGroup *g = nullptr;
+    for (BatchGroup &x : out)
+      if (x.N == key) g = &x;
+    if (!g) {
+      out.emplace_back();
+      g = &out.back();
+      g->N = key;
+    }
+    g->ms.push_back(c);
+  }
+  for (BatchGroup &g : out) {
+    const plc_ctx *lead = g.ms[0];
+    for (const plc_ctx *c : g.ms)
+      if ((double)c->nx * c->ny * c->nz > (double)lead->nx * lead->ny * lead->nz) lead = c;
+    int pl = dir == BATCH_Y ? lead->fft_plan_y
+                            : (dir == BATCH_XF && lead->fft_plan_xf >= 0 ? lead->fft_plan_xf
+                                                                         : lead->fft_plan_x);
+    if (!batch_family_ok(g.N, pl)) pl = 0;
+    g.PL = pl;
+    // default tile: the largest admitted by all the channels, up to 16 pairs
+    // and 64 KB of shared memory
+    int nl = 0;
+    for (int d = 16; d >= batch_step(dir) && nl == 0; --d) {
+      bool ok = batch_tile_ok(g, dir, d);
+      for (const plc_ctx *c : g.ms) ok = ok && batch_bytes(c, dir, d) <= 64 * 1024;
+      if (ok) nl = d;
+    }
+    if (nl == 0) nl = batch_step(dir);
+    if (bp)
+      for (const BatchPlan::Group &q : bp->dir[dir])
+        if (q.len_key == g.N) {
+          if (batch_family_ok(g.N, q.pl)) g.PL = q.pl;
+          if (batch_tile_ok(g, dir, q.nl)) nl = q.nl;
+        }
+    batch_set_tile(g, dir, nl);
+  }
+  return out;
+}
+
+// resident blocks of a kernel on the whole device
+template <class K>
+long long device_blocks(K kernel, int threads, size_t smem, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return (long long)per_sm * sms;
+}
+
+// the persistent blocks of each channel: its tiles spread over its share of
+// the launch's resident blocks (tiles per block alike for all the channels)
+template <class B>
+int share_blocks(B &b, const long long *tiles, long long resident) {
+  long long tot = 0;
+  for (int q = 0; q < b.n; ++q) tot += tiles[q];
+  const long long per = std::max(1ll, (tot + resident - 1) / resident);
+  int start = 0;
+  for (int q = 0; q < b.n; ++q) {
+    b.start[q] = start;
+    b.m[q].vblocks = (int)std::max(1ll, (tiles[q] + per - 1) / per);
+    start += b.m[q].vblocks;
+  }
+  b.start[b.n] = start;
+  return start;
+}
+
+cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s) {
+  for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
+    XfBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = (int)std::min<size_t>(kBatchMax, G.ms.size() - q0);
+    int tot = 0;
+    for (int q = 0; q < b.n; ++q) {
+      const plc_ctx *c = G.ms[q0 + q];
+      XfMember &a = b.m[q];
+      a.g = c->geo();
+      a.P = dev_plan<float>(c->plan_x);
+      a.nl = G.nl;
+      a.gx = c->ny / (2 * G.nl);
+      a.gy = c->nz;
+      a.sc = c->d_sc;
+      a.u = c->f_field[PLC_U];
+      a.v = c->f_field[PLC_V];
+      a.w = c->f_field[PLC_W];
+      a.var = c->f_field[PLC_SPEC];
+      b.start[q] = tot;
+      tot += a.gx * a.gy;
+    }
+    b.start[b.n] = tot;
+    const cudaError_t e = with_size(G.N, [&](auto NC) -> cudaError_t {
+      constexpr int N = decltype(NC)::value;
+      return with_plan<N>(G.PL, [&](auto PC) -> cudaError_t {
+        constexpr int PL = decltype(PC)::value;
+        k_fft_x_fwd_div_batch<N, PL><<<tot, 256, G.smem, s>>>(b);
+        return cudaGetLastError();
+      });
+    });
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
+  for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
+    YBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = (int)std::min<size_t>(kBatchMax, G.ms.size() - q0);
+    long long tiles[kBatchMax];
+    for (int q = 0; q < b.n; ++q) {
+      const plc_ctx *c = G.ms[q0 + q];
+      YMember &a = b.m[q];
+      a.nx = c->nx;
+      a.ny = c->ny;
+      a.nz = c->nz;
+      a.nl = G.nl;
+      a.rev = c->order[inverse ? SK_YB : SK_YF];
+      a.P = dev_plan<float>(c->plan_y);
+      a.var = c->f_field[PLC_SPEC];
+      tiles[q] = (long long)(c->nx / (2 * G.nl)) * c->nz;
+    }
+    const int sms = G.ms[0]->device_sms;
+    const cudaError_t e = with_size(G.N, [&](auto NC) -> cudaError_t {
+      constexpr int N = decltype(NC)::value;
+      return with_plan<N>(G.PL, [&](auto PC) -> cudaError_t {
+        constexpr int PL = decltype(PC)::value;
+        if (inverse) {
+          const int tot =
+              share_blocks(b, tiles, device_blocks(k_fft_y_batch<N, true, PL>, 256, G.smem, sms));
+          k_fft_y_batch<N, true, PL><<<tot, 256, G.smem, s>>>(b);
+        } else {
+          const int tot =
+              share_blocks(b, tiles, device_blocks(k_fft_y_batch<N, false, PL>, 256, G.smem, sms));
+          k_fft_y_batch<N, false, PL><<<tot, 256, G.smem, s>>>(b);
+        }
+        return cudaGetLastError();
+      });
+    });
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_group_xb(const BatchGroup &G, cudaStream_t s) {
+  for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
+    XbBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = (int)std::min<size_t>(kBatchMax, G.ms.size() - q0);
+    long long tiles[kBatchMax];
+    for (int q = 0; q < b.n; ++q) {
+      const plc_ctx *c = G.ms[q0 + q];
+      XbMember &a = b.m[q];
+      a.g = c->geo();
+      a.P = dev_plan<float>(c->plan_x);
+      a.nl = G.nl;
+      a.rev = c->order[SK_XB];
+      a.nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
+      a.var = c->f_field[PLC_SPEC];
+      a.p = c->f_field[PLC_P];
+      tiles[q] = (long long)(c->ny / (2 * G.nl)) * c->nz;
+    }
+    const int sms = G.ms[0]->device_sms;
+    const cudaError_t e = with_size(G.N, [&](auto NC) -> cudaError_t {
+      constexpr int N = decltype(NC)::value;
+      return with_plan<N>(G.PL, [&](auto PC) -> cudaError_t {
+        constexpr int PL = decltype(PC)::value;
+        const int tot =
+            share_blocks(b, tiles, device_blocks(k_fft_x_bwd_batch<N, PL>, 128, G.smem, sms));
+        k_fft_x_bwd_batch<N, PL><<<tot, 128, G.smem, s>>>(b);
+        return cudaGetLastError();
+      });
+    });
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+}  // namespace
+
+int fft_batch_groups(plc_ctx *const *cs, int n, bool ydir) {
+  return (int)batch_groups(cs, n, ydir ? BATCH_Y : BATCH_XF, nullptr).size();
+}
+
+cudaError_t launch_fft_x_fwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
+                                   const cudaStream_t *ss, int ns) {
+  const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_XF, bp);
+  for (size_t gi = 0; gi < gs.size(); ++gi)
+    if (cudaError_t e = launch_group_xf(gs[gi], ss[gi % ns])) return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_fft_y_batch(plc_ctx *const *cs, int n, bool inverse, const BatchPlan *bp,
+                               const cudaStream_t *ss, int ns) {
+  const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_Y, bp);
+  for (size_t gi = 0; gi < gs.size(); ++gi)
+    if (cudaError_t e = launch_group_y(gs[gi], inverse, ss[gi % ns])) return e;
+  return cudaSuccess;
+}
+
+cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
+                                   const cudaStream_t *ss, int ns) {
+  const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_XB, bp);
+  for (size_t gi = 0; gi < gs.size(); ++gi)
+    if (cudaError_t e = launch_group_xb(gs[gi], ss[gi % ns])) return e;
+  return cudaSuccess;
+}
+
+// The batch autotuner: for every group of every batched transform, the
+// feasible families (only the channels' own where they are pinned) and
+// tiles, one untimed launch and the best of three timed ones each; then the
+// RK stages' z chunk (unless a channel pins its own) and resident blocks per
+// SM, both stages timed.
+cudaError_t batch_autotune(plc_ctx *const *cs, int n, cudaStream_t s, BatchPlan *bp) {
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  auto time_of = [&](auto launch) -> float {
+    if (launch() != cudaSuccess) return -1.f;
+    float best = -1.f;
+    for (int r = 0; r < 3; ++r) {
+      if (cudaEventRecord(e0, s) != cudaSuccess || launch() != cudaSuccess ||
+          cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+        return -1.f;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (best < 0.f || ms < best) best = ms;
+    }
+    return best;
+  };
+  bool fam_pinned = false, rk_pinned = false;
+  for (int m = 0; m < n; ++m) {
+    fam_pinned = fam_pinned || cs[m]->fft_plans_pinned;
+    rk_pinned = rk_pinned || cs[m]->rk_pinned;
+  }
+  *bp = BatchPlan();
+  for (int dir = 0; dir < 3; ++dir) {
+    std::vector<BatchGroup> gs = batch_groups(cs, n, dir, nullptr);
+    for (BatchGroup &G : gs) {
+      BatchPlan::Group best{G.N, G.PL, G.nl};
+      float best_t = -1.f;
+      for (int pl = 0; pl <= 1; ++pl) {
+        if (!batch_family_ok(G.N, pl) || (fam_pinned && pl != G.PL)) continue;
+        G.PL = pl;
+        for (int d = batch_step(dir); d <= 16; d += batch_step(dir)) {
+          if (!batch_tile_ok(G, dir, d)) continue;
+          batch_set_tile(G, dir, d);
+          const float t = time_of([&]() -> cudaError_t {
+            if (dir == BATCH_XF) return launch_group_xf(G, s);
+            if (dir == BATCH_XB) return launch_group_xb(G, s);
+            const cudaError_t r = launch_group_y(G, false, s);
+            return r == cudaSuccess ? launch_group_y(G, true, s) : r;
+          });
+          if (t >= 0.f && (best_t < 0.f || t < best_t)) {
+            best_t = t;
+            best = BatchPlan::Group{G.N, pl, d};
+          }
+        }
+      }
+      bp->dir[dir].push_back(best);
+    }
+  }
+  {
+    float best_t = -1.f;
+    for (int minb = 3; minb <= 4; ++minb)
+      for (int kc : kRkChunks) {
+        if (rk_pinned && kc != kRkChunks[0]) continue;  // the channels' own chunks
+        const int k = rk_pinned ? 0 : kc;
+        const float t = time_of([&]() -> cudaError_t {
+          const cudaError_t r = launch_rk_batch(cs, n, 1, k, minb, s);
+          return r == cudaSuccess ? launch_rk_batch(cs, n, 2, k, minb, s) : r;
+        });
+        if (t >= 0.f && (best_t < 0.f || t < best_t)) {
+          best_t = t;
+          bp->rk_kchunk = k;
+          bp->rk_minb = minb;
+        }
+      }
+  }
+  cudaGetLastError();  // a candidate that failed to launch leaves no error behind
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cudaSuccess;
+}
+
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+  for (int q0 = 0; q0 < n; q0 += kBatchMax) {
+    TrBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = std::min(kBatchMax, n - q0);
+    int tot = 0;
+    for (int q = 0; q < b.n; ++q) {
+      const plc_ctx *c = cs[q0 + q];
+      b.m[q] = TrMember{c->nx,     c->ny,         c->nz,  c->d_rpiv32, c->d_ac32,
+                        c->d_ac32 + c->nz, c->d_rpiv, c->d_ac, c->d_ac + c->nz,
+                        c->f_field[PLC_SPEC], c->d_low};
+      b.start[q] = tot;
+      tot += (int)(((long long)c->nx * c->ny + 127) / 128);
+    }
+    b.start[b.n] = tot;
+    k_trid_mixed_batch<<<tot, 128, 0, s>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace plc

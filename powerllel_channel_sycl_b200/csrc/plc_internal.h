@@ -115,6 +115,8 @@ struct plc_ctx {
   // z planes per block of the RK stages (0: the kernels' maximum), chosen by
   // the autotuner among kRkChunks; PLC_RK_KCHUNK pins it
   int rk_kchunk = 0;
+  bool rk_pinned = false;  // PLC_RK_KCHUNK(_F32) set
+  int pending_check = 0;   // checks queued by post_step_begin (0: none)
   size_t trid_smem_max = 0;
   bool fft_plans_pinned = false;
   // Plane order of the step kernels (0: low planes first, 1: high planes
@@ -275,6 +277,47 @@ bool fft_has_two_plans(int n);
 bool fft_has_warp_plan(int n, int lines_axis);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
+// Batched launches over the mixed-form channels of an ensemble: one launch
+// per step stage covers all the channels (the stages whose code depends on a
+// line length: one launch per length, on the streams ss[0..ns) in turn, which
+// the caller forks from and joins to its own), each block working on a tile
+// of one channel.  The arguments of up to kBatchMax channels travel in the
+// kernel parameters; more channels take more launches.  Each channel's
+// results are those of its own step with the same transform families.
+constexpr int kBatchMax = 32;
+// Choices of the batched launches, made by the ensemble's batch autotuner:
+// per transform (forward x, backward x, y) and line-length group (len_key:
+// the compiled length, 0 for the runtime plan) the plan family and the line
+// pairs per tile; the RK stages' z planes per block (0: each channel's own).
+// Without a choice for a group, the family of the group's largest channel
+// and the largest tile all its channels admit are used.
+struct BatchPlan {
+  struct Group {
+    int len_key, pl, nl;
+  };
+  std::vector<Group> dir[3];  // BATCH_XF, BATCH_XB, BATCH_Y
+  int rk_kchunk = 0;
+  int rk_minb = 4;  // resident blocks per SM the RK kernels are compiled for (3 or 4)
+};
+enum BatchDir { BATCH_XF = 0, BATCH_XB = 1, BATCH_Y = 2 };
+cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, int minb,
+                            cudaStream_t s);
+cudaError_t launch_fft_x_fwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
+                                   const cudaStream_t *ss, int ns);
+cudaError_t launch_fft_y_batch(plc_ctx *const *cs, int n, bool inverse, const BatchPlan *bp,
+                               const cudaStream_t *ss, int ns);
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
+                                   const cudaStream_t *ss, int ns);
+cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+// the number of launches (line-length groups) of the batched x and y stages
+int fft_batch_groups(plc_ctx *const *cs, int n, bool ydir);
+// times the candidate families and tiles of every group of the batched
+// transforms on stream s (overwrites the channels' spectral arrays and p)
+// and the RK stages' z chunks (overwrites u1, v1, w1, u, v, w), keeping the
+// fastest in *bp
+cudaError_t batch_autotune(plc_ctx *const *cs, int n, cudaStream_t s, BatchPlan *bp);
+
 // var -= delta on the interior of the context's field (either form), synchronous
 int shift_field(plc_ctx *c, int field, double delta);
 // the launches of one fused step on stream s (for capture into a caller's graph)
@@ -289,6 +332,10 @@ void drop_graph(plc_ctx *c);
 // before the context's stream
 int pre_steps(plc_ctx *c);
 int post_step(plc_ctx *c);
+// post_step in two halves (queue the checks; wait and act on them), so that
+// several contexts share one wait
+int post_step_begin(plc_ctx *c);
+int post_step_end(plc_ctx *c);
 // true when post_step will do host work after the next step
 bool step_needs_host(const plc_ctx *c);
 // closes the monitor files and releases the I/O state (plc_io.cc)

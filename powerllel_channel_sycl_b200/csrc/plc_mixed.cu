@@ -22,6 +22,9 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "plc_device.cuh"
@@ -506,12 +509,279 @@ __global__ void __launch_bounds__(RX *TY, 4)
   }
 }
 
+// The same stage for one block of a batched launch over several channels
+// (k_rk32_batch, below): the block's coordinates come from the work list and
+// the tensor maps by address.  The single-channel kernel above keeps its own
+// copy of these lines: at its limit of 64 registers a shared body changed
+// its register allocation (it spilled in RK2, which the copy does not).
+template <int STAGE, bool FUSE, bool CRF>
+__device__ __forceinline__ void rk32_body(const CUtensorMap *mu, const CUtensorMap *mv,
+                                          const CUtensorMap *mw, Geo g, RkConst K,
+                                          const Coef *__restrict__ coef,
+                                          const StepConst *__restrict__ sc, float bc_u, float *ou,
+                                          float *ov, float *ow, int kchunk, int *err,
+                                          BulkMean bm, VBlk vb) {
+  extern __shared__ unsigned char smem_raw[];
+  float *slot = reinterpret_cast<float *>(
+      (reinterpret_cast<unsigned long long>(smem_raw) + 127ull) & ~127ull);
+  Coef *zc = reinterpret_cast<Coef *>(slot + 3 * NSLOT * SLOT);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(zc + KCHUNK + 2);
+  unsigned long long *empty = bar + NSLOT;
+  constexpr unsigned kWarps = RX * TY / 32;
+
+  constexpr bool kMean = (STAGE == 2 && FUSE);
+  // the first stage carries its z-face terms from plane to plane (about a
+  // tenth fewer instructions: RK1 0.554 -> 0.506 ms at 768 x 384 x 256); in the
+  // second stage the carried values no longer fit the 64 registers of four
+  // blocks per SM (it spilled and took 0.91 against 0.73 ms)
+  constexpr bool kCarry = (STAGE == 1);
+  float msum[3] = {0.f, 0.f, 0.f};  // kMean: the thread's dz-weighted sums
+  const int tid = threadIdx.x;
+  const int tx = tid & (RX - 1), ty = tid / RX;
+  const int x0 = vb.x() * RX, y0 = vb.y() * RY;  // halo'd coords of the tile corner
+  const int i = x0 + tx + 1, ja = y0 + 2 * ty + 1, jb = ja + 1;
+  const bool act_a = (i <= g.nx) && (ja <= g.ny);
+  const bool act_b = act_a && (jb <= g.ny);
+  const int kb = vb.z() * kchunk + 1;
+  const int ke = min(kb + kchunk - 1, g.nz);
+  const int plast = ke + 1;  // last plane to bring in
+
+  auto issue = [&](int p) {  // thread 0 only
+    const int s = (p - (kb - 1)) % NSLOT;
+    mbar_expect_tx(&bar[s], PLANE_TX_BYTES);
+    tma_load_plane(slot + s * SLOT, mu, x0, y0, p, &bar[s]);
+    tma_load_plane(slot + NSLOT * SLOT + s * SLOT, mv, x0, y0, p, &bar[s]);
+    tma_load_plane(slot + 2 * NSLOT * SLOT + s * SLOT, mw, x0, y0, p, &bar[s]);
+  };
+  // bounded waits for plane p's copy to land (full) or to be read by every
+  // warp for the last time (empty)
+  auto wait_on = [&](unsigned long long *b, int p, long long limit) -> bool {
+    const int rel = p - (kb - 1);
+    const unsigned parity = (unsigned)((rel / NSLOT) & 1);
+    for (long long it = 0; it < limit; ++it)
+      if (mbar_try_wait(&b[rel % NSLOT], parity)) return true;
+    return false;
+  };
+
+  int issued = min(kb + 2, plast);  // thread 0: the last plane copied
+  if (tid == 0) {
+    for (int s = 0; s < NSLOT; ++s) {
+      mbar_init(&bar[s], 1);
+      mbar_init(&empty[s], kWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int p = kb - 1; p <= issued; ++p) issue(p);
+  }
+  // coefficient rows of the block's planes (and, for the bulk mean, dzf/lz)
+  __shared__ float zl[KCHUNK];
+  for (int e = tid; e < (ke - kb + 1) * NCOEF; e += blockDim.x)
+    reinterpret_cast<float *>(zc)[e] = __ldg(reinterpret_cast<const float *>(coef + kb) + e);
+  if (kMean && tid < ke - kb + 1) zl[tid] = float(__ldg(g.dzflzi + kb + tid));
+  __syncthreads();
+
+  const float dt = float(sc->dt);
+  const long long X = g.X, XY = g.XY;
+  long long c = g.at(act_a ? i : 1, act_a ? ja : 1, kb);  // point a; point b is c + X
+  // RK2 base values (u, v, w) of plane k at rows a and b, read a plane ahead
+  float ba[3] = {0.f, 0.f, 0.f}, bb[3] = {0.f, 0.f, 0.f};
+  if (STAGE == 2 && act_a) {
+    ba[0] = ou[c];
+    ba[1] = ov[c];
+    ba[2] = ow[c];
+    if (act_b) {
+      bb[0] = ou[c + X];
+      bb[1] = ov[c + X];
+      bb[2] = ow[c + X];
+    }
+  }
+  ZFace fa_c{}, fb_c{};  // z-face terms carried from plane k-1 (rows a, b)
+  const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
+  const bool xy_edge = (ha.dx | ha.dy | hb.dx | hb.dy) != 0;  // images in x or y
+  const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
+  int sm = 0, s0 = 1, sp = 2;                  // slots of planes k-1, k, k+1
+  for (int k = kb; k <= ke; ++k) {
+    bool ok = true;
+    if (tid == 0 && k + 3 <= plast) {
+      // the slot of plane k+3 last held plane k+3-NSLOT
+      if (k + 3 - NSLOT >= kb - 1) ok = wait_on(empty, k + 3 - NSLOT, kWaitLimit);
+      if (ok) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(k + 3);
+        issued = k + 3;
+      }
+    }
+    if (ok && k == kb) ok = wait_on(bar, kb - 1, kWaitLimit) && wait_on(bar, kb, kWaitLimit);
+    ok = ok && wait_on(bar, k + 1, kWaitLimit);
+    if (!ok) {
+      atomicExch(err, 1);
+      break;  // the other threads' waits run out as well
+    }
+    float na[3] = {0.f, 0.f, 0.f}, nb[3] = {0.f, 0.f, 0.f};  // base values of plane k+1
+    if (STAGE == 2 && act_a && k < ke) {
+      na[0] = ou[c + XY];
+      na[1] = ov[c + XY];
+      na[2] = ow[c + XY];
+      if (act_b) {
+        nb[0] = ou[c + X + XY];
+        nb[1] = ov[c + X + XY];
+        nb[2] = ow[c + X + XY];
+      }
+    }
+    if (act_a) {
+      const Coef z = zc[k - kb];
+      float va[3], vb[3];
+      {
+        // two rows in scalar FP32
+        SmemAcc32 a;
+        a.base = slot;
+        a.off[0] = sm * SLOT + o;
+        a.off[1] = s0 * SLOT + o;
+        a.off[2] = sp * SLOT + o;
+        SmemAcc32 b = a;
+        b.off[0] += HX;
+        b.off[1] += HX;
+        b.off[2] += HX;
+        Rhs3f ra, rb;
+        if constexpr (kCarry) {
+          if (k == kb) {
+            ra = momentum_rhs32c<CRF, true>(K, z, a, fa_c, fa_c);
+            rb = momentum_rhs32c<CRF, true>(K, z, b, fb_c, fb_c);
+          } else {
+            ra = momentum_rhs32c<CRF, false>(K, z, a, fa_c, fa_c);
+            rb = momentum_rhs32c<CRF, false>(K, z, b, fb_c, fb_c);
+          }
+        } else {
+          ra = momentum_rhs32<CRF>(K, z, a);
+          rb = momentum_rhs32<CRF>(K, z, b);
+        }
+        const float fa[3] = {ra.u, ra.v, ra.w}, fb[3] = {rb.u, rb.v, rb.w};
+        const float qa[3] = {a(0, 0, 0, 0), a(1, 0, 0, 0), a(2, 0, 0, 0)};
+        const float qb[3] = {b(0, 0, 0, 0), b(1, 0, 0, 0), b(2, 0, 0, 0)};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          va[d] = fmaf(dt, fa[d], qa[d]);
+          vb[d] = fmaf(dt, fb[d], qb[d]);
+          if (STAGE == 2) {
+            va[d] = (va[d] + ba[d]) * 0.5f;
+            vb[d] = (vb[d] + bb[d]) * 0.5f;
+          }
+        }
+      }
+      if (kMean) {
+        const float dzl = zl[k - kb];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (bm.forced[d]) {  // uniform
+            // the stored value: w(nz) is the wall value 0
+            const bool wall = (d == 2 && k == g.nz);
+            const float x = wall ? 0.f : va[d] + (act_b ? vb[d] : 0.f);
+            msum[d] = fmaf(x, dzl, msum[d]);
+          }
+      }
+      if (FUSE && (xy_edge || k == 1 || k == g.nz)) {
+        store_point(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
+        store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
+        store_point(ow, g, ha, c, k, va[2], BC_FACE, 0.f);
+        if (act_b) {
+          store_point(ou, g, hb, c + X, k, vb[0], BC_CENTRED, bc_u);
+          store_point(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.f);
+          store_point(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.f);
+        }
+      } else {  // no image or ghost to write
+        ou[c] = va[0];
+        ov[c] = va[1];
+        ow[c] = va[2];
+        if (act_b) {
+          ou[c + X] = vb[0];
+          ov[c + X] = vb[1];
+          ow[c + X] = vb[2];
+        }
+      }
+    }
+
+    // this warp is done with plane k-1 (slot sm)
+    __syncwarp();
+    if ((tid & 31) == 0) mbar_arrive(&empty[sm]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ba[d] = na[d];
+      bb[d] = nb[d];
+    }
+    sm = s0;
+    s0 = sp;
+    sp = (sp + 1 == NSLOT) ? 0 : sp + 1;
+    c += XY;
+  }
+  if (tid == 0) {
+    // no copy may still be writing into shared memory when the block leaves
+    // (after an error; on the normal path every copy has been waited for)
+    for (int p = max(kb - 1, issued - NSLOT + 1); p <= issued; ++p) wait_on(bar, p, 1 << 20);
+  }
+  if constexpr (kMean) {
+    __shared__ float red[RX * TY / 32][3];
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (bm.forced[d]) {  // uniform: only the forced components are reduced
+        float x = msum[d];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) x += __shfl_down_sync(0xffffffffu, x, o2);
+        if (lane == 0) red[wid][d] = x;
+      }
+    __syncthreads();
+    if (tid < 3) {
+      // (a parameter array indexed at run time would be copied to local memory)
+      const int forced = tid == 0 ? bm.forced[0] : (tid == 1 ? bm.forced[1] : bm.forced[2]);
+      double x = 0.0;
+      if (forced)
+        for (int w2 = 0; w2 < RX * TY / 32; ++w2) x += double(red[w2][tid]);
+      const unsigned nblocks = vb.gx() * vb.gy() * vb.gz();
+      bm.partials[tid * nblocks + vb.x() + vb.gx() * (vb.y() + vb.gy() * vb.z())] = x;
+    }
+  }
+}
+
+// One RK stage over the channels of an ensemble in one launch: the
+// arguments of each channel's k_rk32 launch, tensor maps included, travel in
+// the kernel parameters (a TMA copy may name a tensor map there), and block
+// b works on tile b - start[m] of channel m.
+struct Rk32Member {
+  CUtensorMap map[3];
+  Geo g;
+  RkConst K;
+  const Coef *coef;
+  const StepConst *sc;
+  float bc_u;
+  float *ou, *ov, *ow;
+  int kchunk;
+  int *err;
+  BulkMean bm;
+  int gx, gy, gz;
+};
+struct Rk32Batch {
+  int n;
+  int start[kBatchMax + 1];
+  Rk32Member m[kBatchMax];
+};
+static_assert(sizeof(Rk32Batch) <= 32000, "kernel parameters are limited to 32764 bytes");
+
+// MINB resident blocks per SM: 4 as the single-channel kernel (64 registers:
+// the work-list arguments then spill a little in RK2) or 3 (80 registers, no
+// spills); the batch autotuner times both.
+template <int STAGE, bool FUSE, bool CRF, int MINB>
+__global__ void __launch_bounds__(RX *TY, MINB) k_rk32_batch(const __grid_constant__ Rk32Batch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const Rk32Member &a = b.m[q];
+  const VBlk vb = VBlk::of((int)blockIdx.x - b.start[q], a.gx, a.gy, a.gz);
+  rk32_body<STAGE, FUSE, CRF>(&a.map[0], &a.map[1], &a.map[2], a.g, a.K, a.coef, a.sc, a.bc_u,
+                              a.ou, a.ov, a.ow, a.kchunk, a.err, a.bm, vb);
+}
+
 // The forcing of the mixed form from the fused RK2's partial sums:
 // sc->mean[d] = sum / (nx*ny), sc->force[d] = vel_force[d] - mean
 // (forceVel, mod_calcVel.cc:280-301).  One block; the partials are added in a
 // fixed order.
-__global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkMean bm,
-                                                     int nblocks) {
+__device__ __forceinline__ void bulk_force_body(int nx, int ny, StepConst *sc, BulkMean bm,
+                                                int nblocks) {
   __shared__ double red[32][3];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double part[3] = {0.0, 0.0, 0.0};
@@ -529,10 +799,28 @@ __global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkM
     const int d = threadIdx.x;
     double tot = 0.0;
     for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot += red[w2][d];
-    const double mean = tot / g.nx / g.ny;
+    const double mean = tot / nx / ny;
     sc->mean[d] = bm.forced[d] ? mean : 0.0;
     sc->force[d] = bm.forced[d] ? bm.vel_force[d] - mean : 0.0;
   }
+}
+__global__ void __launch_bounds__(1024) k_bulk_force(Geo g, StepConst *sc, BulkMean bm,
+                                                     int nblocks) {
+  bulk_force_body(g.nx, g.ny, sc, bm, nblocks);
+}
+// the same for the channels of an ensemble: block m reduces channel m's partials
+struct BulkMember {
+  int nx, ny, nblocks;
+  StepConst *sc;
+  BulkMean bm;
+};
+struct BulkBatch {
+  int n;
+  BulkMember m[kBatchMax];
+};
+__global__ void __launch_bounds__(1024) k_bulk_force_batch(const __grid_constant__ BulkBatch b) {
+  const BulkMember &a = b.m[blockIdx.x];
+  bulk_force_body(a.nx, a.ny, a.sc, a.bm, a.nblocks);
 }
 
 // Tensor map of one FP32 halo'd field: dims (pitch, Y, Z), box = one 36 x 18
@@ -633,8 +921,33 @@ cudaError_t rk32_configure() {
   PLC_RK32_ATTR(2, false, true)
   PLC_RK32_ATTR(2, false, false)
 #undef PLC_RK32_ATTR
+#define PLC_RK32B_ATTR(S, C, M)                                                            \
+  if (e == cudaSuccess)                                                                   \
+    e = cudaFuncSetAttribute(k_rk32_batch<S, true, C, M>,                                 \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  PLC_RK32B_ATTR(1, true, 3)
+  PLC_RK32B_ATTR(1, false, 3)
+  PLC_RK32B_ATTR(2, true, 3)
+  PLC_RK32B_ATTR(2, false, 3)
+  PLC_RK32B_ATTR(1, true, 4)
+  PLC_RK32B_ATTR(1, false, 4)
+  PLC_RK32B_ATTR(2, true, 4)
+  PLC_RK32B_ATTR(2, false, 4)
+#undef PLC_RK32B_ATTR
   return e;
 }
+
+namespace {
+RkConst rk32_const(const plc_ctx *c, double u_crf) {
+  RkConst K;
+  K.qx = float(0.25 * c->dx_inv);
+  K.qy = float(0.25 * c->dy_inv);
+  K.rx = float(c->re_inv * c->dx_inv * c->dx_inv);
+  K.ry = float(c->re_inv * c->dy_inv * c->dy_inv);
+  K.crf = float(0.5 * u_crf * c->dx_inv);
+  return K;
+}
+}  // namespace
 
 cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, const float *qu,
                       const float *qv, const float *qw, float *ou, float *ov, float *ow,
@@ -645,12 +958,7 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
   if (!field_tensor_map32(&m[0], qu, g) || !field_tensor_map32(&m[1], qv, g) ||
       !field_tensor_map32(&m[2], qw, g))
     return cudaErrorInvalidValue;  // FP32 fields are allocated 16-byte aligned and padded
-  RkConst K;
-  K.qx = float(0.25 * c->dx_inv);
-  K.qy = float(0.25 * c->dy_inv);
-  K.rx = float(c->re_inv * c->dx_inv * c->dx_inv);
-  K.ry = float(c->re_inv * c->dy_inv * c->dy_inv);
-  K.crf = float(0.5 * u_crf * c->dx_inv);
+  const RkConst K = rk32_const(c, u_crf);
   const float bc_u = float(0.0 - u_crf);
   const bool crf = (u_crf != 0.0);
 #define PLC_RK32(S, F, C) return launch_rk32_t<S, F, C>(c, m, K, bc_u, ou, ov, ow, s)
@@ -669,6 +977,87 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
   if (crf) PLC_RK32(2, false, true);
   PLC_RK32(2, false, false);
 #undef PLC_RK32
+}
+
+// One fused RK stage (halos written; the second stage also reduces each
+// channel's bulk forcing) of n mixed-form channels: one launch for the
+// channels at rest in their frame and one for those in a convecting frame,
+// each of up to kBatchMax channels.  kchunk > 0: z planes per block of every
+// channel whose own choice is not pinned (the bulk-mean partials then round
+// differently in FP32 from the channel's own step); 0: each channel's own.
+cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, int minb,
+                            cudaStream_t s) {
+  const size_t smem = rk32_smem_bytes();
+  for (int crf = 0; crf < 2; ++crf) {
+    std::vector<int> idx;
+    for (int m = 0; m < n; ++m)
+      if ((cs[m]->prm.u_crf != 0.0) == (crf == 1)) idx.push_back(m);
+    for (size_t q0 = 0; q0 < idx.size(); q0 += kBatchMax) {
+      const int cnt = (int)std::min<size_t>(kBatchMax, idx.size() - q0);
+      Rk32Batch b;
+      BulkBatch bb;
+      std::memset(&b, 0, sizeof b);
+      std::memset(&bb, 0, sizeof bb);
+      b.n = bb.n = cnt;
+      int tot = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const plc_ctx *c = cs[idx[q0 + q]];
+        if (!c->mixed) return cudaErrorInvalidValue;
+        float *const *f = c->f_field;
+        const int iq = stage == 1 ? PLC_U : PLC_U1, io = stage == 1 ? PLC_U1 : PLC_U;
+        Rk32Member &a = b.m[q];
+        a.g = c->geo();
+        for (int d = 0; d < 3; ++d)
+          if (!field_tensor_map32(&a.map[d], f[iq + d], a.g)) return cudaErrorInvalidValue;
+        a.K = rk32_const(c, c->prm.u_crf);
+        a.coef = reinterpret_cast<const Coef *>(c->d_coef32);
+        a.sc = c->d_sc;
+        a.bc_u = float(0.0 - c->prm.u_crf);
+        a.ou = f[io];
+        a.ov = f[io + 1];
+        a.ow = f[io + 2];
+        a.kchunk = (kchunk > 0 && !c->rk_pinned) ? std::min(std::min(kchunk, KCHUNK), c->nz)
+                                                 : rk_chunk(c, KCHUNK);
+        a.err = c->d_err;
+        for (int d = 0; d < 3; ++d) {
+          a.bm.forced[d] = c->prm.is_forced[d] ? 1 : 0;
+          a.bm.vel_force[d] = c->prm.vel_force[d];
+        }
+        a.bm.partials = c->d_mean_partials;
+        a.gx = (c->nx + RX - 1) / RX;
+        a.gy = (c->ny + RY - 1) / RY;
+        a.gz = (c->nz + a.kchunk - 1) / a.kchunk;
+        b.start[q] = tot;
+        tot += a.gx * a.gy * a.gz;
+        bb.m[q] = BulkMember{c->nx, c->ny, a.gx * a.gy * a.gz, c->d_sc, a.bm};
+      }
+      b.start[cnt] = tot;
+      auto go = [&](auto SC, auto CC, auto MC) {
+        k_rk32_batch<decltype(SC)::value, true, decltype(CC)::value, decltype(MC)::value>
+            <<<tot, RX * TY, smem, s>>>(b);
+      };
+      using I1 = std::integral_constant<int, 1>;
+      using I2 = std::integral_constant<int, 2>;
+      using B0 = std::integral_constant<bool, false>;
+      using B1 = std::integral_constant<bool, true>;
+      using M3 = std::integral_constant<int, 3>;
+      using M4 = std::integral_constant<int, 4>;
+      const bool m4 = minb != 3;
+      if (stage == 1) {
+        if (crf) m4 ? go(I1{}, B1{}, M4{}) : go(I1{}, B1{}, M3{});
+        else m4 ? go(I1{}, B0{}, M4{}) : go(I1{}, B0{}, M3{});
+      } else {
+        if (crf) m4 ? go(I2{}, B1{}, M4{}) : go(I2{}, B1{}, M3{});
+        else m4 ? go(I2{}, B0{}, M4{}) : go(I2{}, B0{}, M3{});
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        k_bulk_force_batch<<<cnt, 1024, 0, s>>>(bb);
+      }
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_to_f32(const plc_ctx *c, const double *src, float *dst, long long rows, int len,

@@ -18,6 +18,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstring>
 #include <type_traits>
 
 #include "plc_device.cuh"
@@ -914,6 +916,77 @@ __global__ void __launch_bounds__(BX *BY) k_correct_forced(Geo g, const StepCons
     }
 }
 
+// The same for one block of a batched launch over several channels (the
+// block's coordinates from the work list).  The single-channel kernel keeps
+// its own copy of these lines: a body shared between the two changed the
+// single-channel kernel's code generation and made it slower.
+template <class T, int KZ>
+__device__ __forceinline__ void correct_forced_body(Geo g, const StepConst *__restrict__ sc,
+                                                    double u_crf, const T *__restrict__ p, T *u,
+                                                    T *v, T *w, VBlk vb) {
+  const int i = vb.x() * BX + threadIdx.x + 1;
+  const int j = vb.y() * BY + threadIdx.y + 1;
+  const int k0 = vb.z() * KZ + 1;
+  if (i > g.nx || j > g.ny) return;
+  const int nk = min(KZ, g.nz - k0 + 1);
+  const T dtdxi = T(sc->dtdxi), dtdyi = T(sc->dtdyi), dt = T(sc->dt);
+  const T fu = T(sc->force[0]), fv = T(sc->force[1]), fw = T(sc->force[2]);
+  const long long c0 = g.at(i, j, k0), X = g.X, XY = g.XY;
+  const HaloCol h = halo_col(g, i, j);
+  T pc[KZ + 1], px[KZ], py[KZ], uu[KZ], vv[KZ], ww[KZ];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q)
+    if (q < nk) {
+      const long long c = c0 + q * XY;
+      pc[q] = p[c];
+      px[q] = p[c + 1];
+      py[q] = p[c + X];
+      uu[q] = u[c];
+      vv[q] = v[c];
+      ww[q] = w[c];
+    }
+#pragma unroll
+  for (int q = 1; q <= KZ; ++q)
+    if (q == nk) pc[q] = p[c0 + q * XY];
+#pragma unroll
+  for (int q = 0; q < KZ; ++q)
+    if (q < nk) {
+      const int k = k0 + q;
+      const long long c = c0 + q * XY;
+      const T nu = uu[q] - (px[q] - pc[q]) * dtdxi + fu;
+      const T nv = vv[q] - (py[q] - pc[q]) * dtdyi + fv;
+      const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k)) + fw;
+      store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - u_crf));
+      store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
+      store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+    }
+}
+
+// The same over the mixed-form channels of an ensemble in one launch (the
+// arguments of each channel in the parameters; block b works for channel m,
+// start[m] <= b < start[m + 1], as block b - start[m] of its own grid).
+struct CorrMember {
+  Geo g;
+  const StepConst *sc;
+  double u_crf;
+  const float *p;
+  float *u, *v, *w;
+  int gx, gy, gz;
+};
+struct CorrBatch {
+  int n;
+  int start[kBatchMax + 1];
+  CorrMember m[kBatchMax];
+};
+static_assert(sizeof(CorrBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
+template <int KZ>
+__global__ void __launch_bounds__(BX *BY) k_correct_forced_batch(const __grid_constant__ CorrBatch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const CorrMember &a = b.m[q];
+  correct_forced_body<float, KZ>(a.g, a.sc, a.u_crf, a.p, a.u, a.v, a.w,
+                                 VBlk::of((int)blockIdx.x - b.start[q], a.gx, a.gy, a.gz));
+}
+
 // Adds sc->force[d] to the interior of each forced component
 // (mod_calcVel.cc:296-316); with FUSE the halos of those components are
 // refreshed from the new interior values (the final updateBoundVel of
@@ -1321,6 +1394,10 @@ cudaError_t launch_calc_rhs(const plc_ctx *c, const double *u, const double *v, 
 }
 
 namespace {
+// planes a thread of the mixed form's correction takes: 8 (0.418 ms against
+// 0.437 for 4, FP32, 768x384x256)
+constexpr int kCorrKzMixed = 8;
+
 template <class T>
 cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cudaStream_t s) {
   // KZ planes per work item (the loads of one item live in registers): 6 in
@@ -1335,7 +1412,7 @@ cudaError_t correct_fused_t(const plc_ctx *c, const T *p, T *u, T *v, T *w, cuda
   if (nb > kMaxBlocksReduce) nb = kMaxBlocksReduce;
   if (c->mixed) {
     // the mixed form's fused RK2 stage has reduced the forcing already
-    constexpr int KZF = 8;  // 8 planes a thread: 0.418 ms against 0.437 for 4 (FP32, 768x384x256)
+    constexpr int KZF = kCorrKzMixed;
     dim3 grid((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, (c->nz + KZF - 1) / KZF);
     k_correct_forced<T, KZF><<<grid, dim3(BX, BY), 0, s>>>(c->geo(), c->d_sc, c->prm.u_crf, p, u,
                                                           v, w);
@@ -1484,6 +1561,40 @@ cudaError_t launch_add_vortices(const plc_ctx *c, double *v, double *w, const do
 cudaError_t launch_add_vortices(const plc_ctx *c, float *v, float *w, const double *d_zf,
                                 cudaStream_t s) {
   return vortices_t(c, v, w, d_zf, s);
+}
+
+// The mixed form's correction (with the forcing and halos) of n channels in
+// launches of up to kBatchMax channels.
+cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+  constexpr int KZ = kCorrKzMixed;
+  for (int q0 = 0; q0 < n; q0 += kBatchMax) {
+    CorrBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = std::min(kBatchMax, n - q0);
+    int tot = 0;
+    for (int q = 0; q < b.n; ++q) {
+      const plc_ctx *c = cs[q0 + q];
+      if (!c->mixed) return cudaErrorInvalidValue;
+      CorrMember &a = b.m[q];
+      a.g = c->geo();
+      a.sc = c->d_sc;
+      a.u_crf = c->prm.u_crf;
+      a.p = c->f_field[PLC_P];
+      a.u = c->f_field[PLC_U];
+      a.v = c->f_field[PLC_V];
+      a.w = c->f_field[PLC_W];
+      a.gx = (c->nx + BX - 1) / BX;
+      a.gy = (c->ny + BY - 1) / BY;
+      a.gz = (c->nz + KZ - 1) / KZ;
+      b.start[q] = tot;
+      tot += a.gx * a.gy * a.gz;
+    }
+    b.start[b.n] = tot;
+    k_correct_forced_batch<KZ><<<tot, dim3(BX, BY), 0, s>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace plc

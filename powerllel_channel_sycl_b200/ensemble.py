@@ -14,7 +14,7 @@ import numpy as np
 from ._lib import PlcError, PlcParams, lib
 from .channel import Channel
 
-SCHEDULES = ("concurrent", "proportional", "two_groups", "sequential")
+SCHEDULES = ("concurrent", "proportional", "two_groups", "sequential", "batched")
 
 
 def _check(rc: int, ens=None) -> None:
@@ -84,6 +84,22 @@ class Ensemble:
         budgets = (C.c_int * n)()
         self._check(lib().plc_ensemble_schedule(self._ens, C.byref(s), groups, budgets))
         return SCHEDULES[s.value], list(groups), list(budgets)
+
+    def set_batch_chains(self, chains: int):
+        """The batched schedule's concurrent chains of mixed-form members (1 or 2)."""
+        self._check(lib().plc_ensemble_set_batch_chains(self._ens, int(chains)))
+
+    def batch_choice(self):
+        """The batched schedule's tuned choices: the concurrent chains of
+        mixed-form members, the RK z planes per block (0: each member's own),
+        resident blocks per SM of the RK kernels, and the number of tuned
+        line-length groups of the forward x, backward x and y transforms."""
+        ch, kc, mb = C.c_int(), C.c_int(), C.c_int()
+        groups = (C.c_int * 3)()
+        self._check(lib().plc_ensemble_batch_choice(self._ens, C.byref(ch), C.byref(kc),
+                                                    C.byref(mb), groups))
+        return {"chains": ch.value, "rk_kchunk": kc.value, "rk_blocks_per_sm": mb.value,
+                "fft_groups": list(groups)}
 
     def autotune(self, steps: int = 5) -> dict:
         """Times every schedule (ms per ensemble step) and keeps the fastest."""

@@ -1,13 +1,16 @@
-"""Batched ensembles on one GPU: every schedule, and the launches of several
-steps per member branch between host events, give each member exactly the
-fields it gets stepping alone; the autotuner restores the state it
-advances; checks stay per member."""
+"""Batched ensembles on one GPU: every schedule -- the members as graph
+branches, or (batched) each stage of the mixed-form members' step as one
+launch over all of them -- and the launches of several steps between host
+events, give each member exactly the fields it gets stepping alone; a member
+stepped in an ensemble matches the oracle; the autotuner restores the state
+it advances; checks stay per member."""
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
-from helpers import case_kwargs, channel_params
+import oracle
+from helpers import case_kwargs, channel_params, demean, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -37,12 +40,16 @@ def standalone(spec, nsteps, **extra):
 
 @pytest.fixture(scope="module", autouse=True)
 def pinned_fft_families():
-    """The transform families pinned for the whole module: the autotuner of
-    each context may pick different families (whose results differ by
-    rounding) for a member and for the same channel alone."""
+    """The transform families and the RK stages' z chunk pinned for the whole
+    module: the autotuner of each context may pick different families (whose
+    results differ by rounding) or, in the mixed form, chunks (which change
+    the FP32 rounding of the bulk-mean partials) for a member and for the
+    same channel alone."""
     with pytest.MonkeyPatch.context() as mp:
         mp.setenv("PLC_FFT_PLANS", "0,0")
         mp.setenv("PLC_FFT_PLANS_F32", "0,0")
+        mp.setenv("PLC_RK_KCHUNK", "8")
+        mp.setenv("PLC_RK_KCHUNK_F32", "8")
         yield
 
 
@@ -51,7 +58,8 @@ def alone(pinned_fft_families):
     return [standalone(s, 6, nt_check=3, cfl_limit=10.0, div_limit=1e-8) for s in MEMBERS]
 
 
-@pytest.mark.parametrize("schedule", ["concurrent", "proportional", "two_groups", "sequential"])
+@pytest.mark.parametrize("schedule", ["concurrent", "proportional", "two_groups", "sequential",
+                                      "batched"])
 def test_members_match_standalone(alone, schedule):
     from powerllel_channel_sycl_b200 import Ensemble
     ens = Ensemble([member_params(*s, nt_check=3, cfl_limit=10.0, div_limit=1e-8)
@@ -81,7 +89,7 @@ def test_autotune_restores_state(alone):
     ens.step(3)
     before = [{q: m.download(q) for q in "uvwp"} for m in ens.members]
     times = ens.autotune(steps=3)
-    assert set(times) == {"concurrent", "proportional", "two_groups", "sequential"}
+    assert set(times) == {"concurrent", "proportional", "two_groups", "sequential", "batched"}
     assert all(t is not None and t > 0 for t in times.values())
     best = min(times, key=times.get)
     assert ens.schedule()[0] == best
@@ -93,6 +101,61 @@ def test_autotune_restores_state(alone):
     for m, ref in zip(ens.members, alone):
         for q in "uvw":
             assert np.array_equal(m.download(q), ref[q]), q
+
+
+# mixed-form members for the batched launches: lengths shared by several
+# members (one launch each), lengths without a compiled plan (36, 24: the
+# runtime plan), and x lengths that are not multiples of the 32-column RK tile
+MIXED = [(64, 48, 48), (64, 64, 32), (96, 48, 32), (32, 24, 16), (36, 24, 16), (48, 32, 24)]
+
+
+@pytest.fixture(scope="module")
+def mixed_alone(pinned_fft_families):
+    specs = [(nx, ny, nz, 1, 1000.0 + 400.0 * q) for q, (nx, ny, nz) in enumerate(MIXED)]
+    kw = dict(nt_check=3, cfl_limit=10.0, div_limit=1e-8)
+    return specs, kw, [standalone(s, 7, **kw) for s in specs]
+
+
+@pytest.mark.parametrize("chains", [1, 2])
+def test_batched_mixed_members_match_standalone(mixed_alone, chains):
+    from powerllel_channel_sycl_b200 import Ensemble
+    specs, kw, ref = mixed_alone
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    ens.set_schedule("batched")
+    ens.set_batch_chains(chains)
+    assert ens.batch_choice()["chains"] == chains
+    ens.initFlow()
+    ens.step(5)
+    ens.step(2)
+    for q, (m, r) in enumerate(zip(ens.members, ref)):
+        assert m.step_count == 7
+        for f in "uvwp":
+            assert np.array_equal(m.download(f), r[f]), (specs[q], f)
+    ens.close()
+
+
+@pytest.mark.parametrize("schedule", ["concurrent", "batched"])
+def test_member_matches_oracle(schedule):
+    """The smallest FP64 member, stepped 5 times inside an ensemble (beside a
+    mixed-form member), against the oracle: the FP64 parity bar (1e-12 in
+    u, v, w; p - mean(p) within its round-off floor at this size)."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    spec = (32, 24, 16, 0, 2800.0)
+    case = oracle.Case(**case_kwargs(32, 24, 16, re=2800.0))
+    u, v, w = case.init_flow("poi", noise_intensity=0.1)
+    p = case.zeros()
+    ens = Ensemble([member_params(*spec), member_params(64, 48, 48, 1, 2000.0)])
+    ens.set_schedule(schedule)
+    ens.initFlow()
+    m = ens.members[0]
+    for name, a in zip("uvwp", (u, v, w, p)):
+        m.upload(name, a)
+    ens.step(5)
+    case.step(u, v, w, case.zeros(), case.zeros(), case.zeros(), p, nsteps=5)
+    for name, a in zip("uvw", (u, v, w)):
+        assert rel_l2(m.download(name), a) <= 1e-12, name
+    assert rel_l2(demean(m.download("p")), demean(p)) <= 4e-12
+    ens.close()
 
 
 def test_member_check_failure_names_the_member():
