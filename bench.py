@@ -229,7 +229,7 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
     ms_max = max_over_ranks(ms, pg, local)
     value = world * npts * args.steps / (ms_max / 1e3)
     ok, cfl, div = ch.check()
-    tiles = dict(ch.fft_tiles, rk_kchunk=ch.rk_kchunk)
+    tiles = dict(ch.fft_tiles, rk_kchunk=ch.rk_kchunk, rk2_carry=ch.rk2_carry)
     prof_steps = max(2, min(5, args.steps))
     prof = ch.profile_step(prof_steps)
     total = sum(prof.values())
@@ -250,18 +250,12 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
     b.initFlow()
     a.step(nerr)
     b.step(nerr)
-    err = {}
-    for name in "uvw":
-        x = a.download(name)[1:-1, 1:-1, 1:-1]
-        y = b.download(name)[1:-1, 1:-1, 1:-1]
-        err[name] = float(np.linalg.norm((y - x).ravel()) / np.linalg.norm(x.ravel()))
-        if name == "u":
-            mx, my = x.mean(axis=(1, 2)), y.mean(axis=(1, 2))
-            err["u_mean_profile_max_rel"] = float(np.max(np.abs(my - mx)) / np.max(np.abs(mx)))
-        del x, y
+    err = rel_errors(a, b)
     _, _, div_b = b.check()
     a.close()
     b.close()
+    developed = (mixed_error_developed(wl, local, nerr, args.developed_steps)
+                 if args.developed_steps > 0 else None)
     return {
         "value": value, "unit": "grid-pt*step/s", "ms_per_step": ms_max / args.steps,
         "speedup_vs_fp64": fp64_ms / ms_max, "dtype": "f32 fields, f64 scalars/reductions/trid",
@@ -277,7 +271,58 @@ def run_mixed(args, wl, world, local, pg, fp64_ms):
         "fft_tiles": tiles,
         "error_vs_fp64": {"steps": nerr, "dt": wl["dt"], "vel_rel_l2": err,
                           "div_max_mixed": div_b[0]},
+        "error_vs_fp64_developed": developed,
     }
+
+
+def rel_errors(a, b):
+    """Relative L2 errors of b's u, v, w against a's (interiors), and of the
+    plane-mean u profile (max over planes, relative to the profile's max)."""
+    err = {}
+    for name in "uvw":
+        x = a.download(name)[1:-1, 1:-1, 1:-1]
+        y = b.download(name)[1:-1, 1:-1, 1:-1]
+        err[name] = float(np.linalg.norm((y - x).ravel()) / np.linalg.norm(x.ravel()))
+        if name == "u":
+            mx, my = x.mean(axis=(1, 2)), y.mean(axis=(1, 2))
+            err["u_mean_profile_max_rel"] = float(np.max(np.abs(my - mx)) / np.max(np.abs(mx)))
+        del x, y
+    return err
+
+
+def mixed_error_developed(wl, local, nerr, spin):
+    """The mixed form's 10-step error against FP64 from a developed turbulent
+    state of the same workload: laminar + noise + streamwise vortices
+    (amplitude 0.15) spun up in the mixed form under CFL control until the
+    flow is turbulent (Re_tau well above its laminar value), then the state
+    copied into an FP64 and a fresh mixed context and both stepped nerr times
+    with the last dt fixed."""
+    from powerllel_channel_sycl_b200 import Channel
+    prm = channel_params(wl, 50, precision="mixed")
+    prm.init_vortex_amp = 0.15
+    ch = Channel(prm, device=local)
+    ch.initFlow()
+    t0 = time.perf_counter()
+    ch.step(spin)
+    wall = time.perf_counter() - t0
+    re_tau, dt = ch.re_tau(), ch.dt
+    state = {name: ch.download(name) for name in "uvwp"}
+    ch.close()
+    out = {"spin_steps": spin, "spin_wall_s": wall, "re_tau": re_tau, "dt": dt, "steps": nerr}
+    a = Channel(channel_params(wl, 0, precision="fp64", cfl_target=0.0), device=local)
+    b = Channel(channel_params(wl, 0, precision="mixed", cfl_target=0.0), device=local)
+    for c in (a, b):
+        for name in "uvwp":
+            c.upload(name, state[name])
+        c.dt = dt
+    del state
+    a.step(nerr)
+    b.step(nerr)
+    out["vel_rel_l2"] = rel_errors(a, b)
+    out["div_max_mixed"] = b.check()[2][0]
+    a.close()
+    b.close()
+    return out
 
 
 def cpu_reference_rate(wl, budget_s: float, max_steps: int, warmup: int):
@@ -655,6 +700,9 @@ def main():
                     help="skip the 16-channel ensemble measurement")
     ap.add_argument("--no-spinup", action="store_true",
                     help="skip the learned-initialiser spin-up comparison")
+    ap.add_argument("--developed-steps", type=int, default=4000,
+                    help="spin-up steps of the developed state the mixed form's error is "
+                         "measured from (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

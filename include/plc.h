@@ -183,6 +183,11 @@ int plc_fft_plan_x_fwd(const plc_ctx *ctx, int *plan);
  * RK2 sums the bulk mean per block in FP32 (by FP32 rounding).  No
  * counterpart in the reference. */
 int plc_rk_kchunk(const plc_ctx *ctx, int *kchunk);
+/* Whether the mixed form's second RK stage carries its z-face terms from
+ * plane to plane (at 3 resident blocks per SM instead of 4), as the
+ * autotuner chose (PLC_RK2_CARRY = 0 or 1 pins it).  Changes the mixed
+ * results by FP32 rounding only; always 0 in the FP64 form. */
+int plc_rk2_carry(const plc_ctx *ctx, int *carry);
 /* Copy a whole halo'd field (or the spectral array) between host and device. */
 int plc_upload(plc_ctx *ctx, int field, const double *h_src);
 int plc_download(plc_ctx *ctx, int field, double *h_dst);

@@ -94,6 +94,7 @@ _SIGS = {
     "plc_fft_plans": [_vp, C.POINTER(_int), C.POINTER(_int)],
     "plc_fft_plan_x_fwd": [_vp, C.POINTER(_int)],
     "plc_rk_kchunk": [_vp, C.POINTER(_int)],
+    "plc_rk2_carry": [_vp, C.POINTER(_int)],
     "plc_upload": [_vp, _int, _hp],
     "plc_download": [_vp, _int, _hp],
     "plc_get_dt": [_vp, C.POINTER(_dbl)],

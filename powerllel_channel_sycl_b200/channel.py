@@ -177,6 +177,14 @@ class Channel:
         self._check(lib().plc_rk_kchunk(self._ctx, C.byref(k)))
         return k.value
 
+    @property
+    def rk2_carry(self) -> bool:
+        """Whether the mixed form's second RK stage carries its z-face terms
+        (the autotuner's choice)."""
+        k = C.c_int()
+        self._check(lib().plc_rk2_carry(self._ctx, C.byref(k)))
+        return bool(k.value)
+
     def ptr_f32(self, f):
         """(device pointer, element count, row pitch) of an FP32 field of a mixed context."""
         fid = FIELDS[f] if isinstance(f, str) else int(f)

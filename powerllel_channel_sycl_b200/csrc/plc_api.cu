@@ -268,30 +268,41 @@ cudaError_t rk_autotune(plc_ctx *c) {
     }
     return r;
   };
-  int best_k = 0, last = -1;
+  int best_k = 0;
+  bool best_carry = c->rk2_carry;
   float best_t = -1.f;
-  for (int k : kRkChunks) {
-    c->rk_kchunk = k;
-    const int eff = rk_chunk(c, 32);
-    if (eff == last) continue;  // the same chunk once clamped to nz
-    last = eff;
-    if ((e = launch()) != cudaSuccess) break;
-    float best = -1.f;
-    for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
-      if ((e = cudaEventRecord(e0, s)) != cudaSuccess || (e = launch()) != cudaSuccess ||
-          (e = cudaEventRecord(e1, s)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess)
-        break;
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (best < 0.f || ms < best) best = ms;
-    }
-    if (e != cudaSuccess) break;
-    if (best_t < 0.f || best < best_t) {
-      best_t = best;
-      best_k = k;
+  // the mixed form's second stage with or without the z-face carry (unless
+  // PLC_RK2_CARRY pins it), with every chunk
+  const bool tune_carry = c->mixed && !c->rk2_carry_pinned;
+  for (int v = 0; v < (tune_carry ? 2 : 1) && e == cudaSuccess; ++v) {
+    if (tune_carry) c->rk2_carry = v == 1;
+    int last = -1;
+    for (int k : kRkChunks) {
+      c->rk_kchunk = k;
+      const int eff = rk_chunk(c, 32);
+      if (eff == last) continue;  // the same chunk once clamped to nz
+      last = eff;
+      if ((e = launch()) != cudaSuccess) break;
+      float best = -1.f;
+      for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+        if ((e = cudaEventRecord(e0, s)) != cudaSuccess || (e = launch()) != cudaSuccess ||
+            (e = cudaEventRecord(e1, s)) != cudaSuccess ||
+            (e = cudaEventSynchronize(e1)) != cudaSuccess)
+          break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best < 0.f || ms < best) best = ms;
+      }
+      if (e != cudaSuccess) break;
+      if (best_t < 0.f || best < best_t) {
+        best_t = best;
+        best_k = k;
+        best_carry = c->rk2_carry;
+      }
     }
   }
   c->rk_kchunk = best_k;
+  c->rk2_carry = best_carry;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -679,6 +690,14 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     pinned = true;
   }
   if (!pinned && (e = fft_autotune(c)) != cudaSuccess) return fail(cuda_status(c, e, "fft_autotune"));
+  // PLC_RK2_CARRY = 0 / 1 pins the mixed form's second RK stage without or
+  // with the z-face carry instead of timing both
+  if (const char *env = getenv("PLC_RK2_CARRY")) {
+    if (strcmp(env, "0") != 0 && strcmp(env, "1") != 0)
+      return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_RK2_CARRY: ") + env));
+    c->rk2_carry = c->mixed && strcmp(env, "1") == 0;
+    c->rk2_carry_pinned = true;
+  }
   // PLC_RK_KCHUNK pins the RK stages' z planes per block instead of timing
   // the candidates
   if (const char *env = getenv(c->mixed ? "PLC_RK_KCHUNK_F32" : "PLC_RK_KCHUNK")) {
@@ -782,6 +801,12 @@ int plc_fft_plans(const plc_ctx *c, int *plan_x, int *plan_y) {
 int plc_rk_kchunk(const plc_ctx *c, int *kchunk) {
   if (!c || !kchunk) return set_error(nullptr, PLC_ERR_ARG, "null argument");
   *kchunk = rk_chunk(c, 32);
+  return PLC_OK;
+}
+
+int plc_rk2_carry(const plc_ctx *c, int *carry) {
+  if (!c || !carry) return set_error(nullptr, PLC_ERR_ARG, "null argument");
+  *carry = c->rk2_carry ? 1 : 0;
   return PLC_OK;
 }
 

@@ -116,6 +116,10 @@ struct plc_ctx {
   // the autotuner among kRkChunks; PLC_RK_KCHUNK pins it
   int rk_kchunk = 0;
   bool rk_pinned = false;  // PLC_RK_KCHUNK(_F32) set
+  // mixed form: the second RK stage carries its z-face terms (at 3 blocks
+  // per SM), chosen by the autotuner; PLC_RK2_CARRY pins it
+  bool rk2_carry = false;
+  bool rk2_carry_pinned = false;
   int pending_check = 0;   // checks queued by post_step_begin (0: none)
   size_t trid_smem_max = 0;
   bool fft_plans_pinned = false;

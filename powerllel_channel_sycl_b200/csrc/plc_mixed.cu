@@ -283,8 +283,11 @@ struct BulkMean {
 // base values o of its two points one plane ahead from global memory.  Both
 // stages run at 4 blocks per SM (64 registers, 50 KB of shared memory; RK1
 // measured 0.56 ms at 4 blocks against 0.59 ms at 3, 768 x 384 x 256).
-template <int STAGE, bool FUSE, bool CRF>
-__global__ void __launch_bounds__(RX *TY, 4)
+// C2: the second stage carries its z-face terms as well, at 3 blocks per SM
+// (the carried values need the registers of a smaller block count); the
+// autotuner times it against the plain second stage.
+template <int STAGE, bool FUSE, bool CRF, bool C2 = false>
+__global__ void __launch_bounds__(RX *TY, (STAGE == 2 && C2) ? 3 : 4)
     k_rk32(const __grid_constant__ CUtensorMap mu, const __grid_constant__ CUtensorMap mv,
            const __grid_constant__ CUtensorMap mw, Geo g, RkConst K,
            const Coef *__restrict__ coef, const StepConst *__restrict__ sc, float bc_u,
@@ -301,8 +304,8 @@ __global__ void __launch_bounds__(RX *TY, 4)
   // the first stage carries its z-face terms from plane to plane (about a
   // tenth fewer instructions: RK1 0.554 -> 0.506 ms at 768 x 384 x 256); in the
   // second stage the carried values no longer fit the 64 registers of four
-  // blocks per SM (it spilled and took 0.91 against 0.73 ms)
-  constexpr bool kCarry = (STAGE == 1);
+  // blocks per SM (it spilled and took 0.91 against 0.73 ms): there only with C2
+  constexpr bool kCarry = (STAGE == 1) || C2;
   float msum[3] = {0.f, 0.f, 0.f};  // kMean: the thread's dz-weighted sums
   const int tid = threadIdx.x;
   const int tx = tid & (RX - 1), ty = tid / RX;
@@ -852,10 +855,20 @@ cudaError_t launch_rk32_t(const plc_ctx *c, const CUtensorMap (&m)[3], const RkC
     bm.vel_force[d] = c->prm.vel_force[d];
   }
   bm.partials = c->d_mean_partials;
-  k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
-      m[0], m[1], m[2], c->geo(), K,
-      reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err,
-      bm);
+  bool carried = false;
+  if constexpr (STAGE == 2 && FUSE) {
+    if (c->rk2_carry) {
+      k_rk32<STAGE, FUSE, CRF, true><<<grid, RX * TY, smem, s>>>(
+          m[0], m[1], m[2], c->geo(), K, reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc,
+          bc_u, ou, ov, ow, kchunk, c->d_err, bm);
+      carried = true;
+    }
+  }
+  if (!carried)
+    k_rk32<STAGE, FUSE, CRF><<<grid, RX * TY, smem, s>>>(
+        m[0], m[1], m[2], c->geo(), K,
+        reinterpret_cast<const Coef *>(c->d_coef32), c->d_sc, bc_u, ou, ov, ow, kchunk, c->d_err,
+        bm);
   if constexpr (STAGE == 2 && FUSE) {
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -921,6 +934,12 @@ cudaError_t rk32_configure() {
   PLC_RK32_ATTR(2, false, true)
   PLC_RK32_ATTR(2, false, false)
 #undef PLC_RK32_ATTR
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rk32<2, true, true, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_rk32<2, true, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 #define PLC_RK32B_ATTR(S, C, M)                                                            \
   if (e == cudaSuccess)                                                                   \
     e = cudaFuncSetAttribute(k_rk32_batch<S, true, C, M>,                                 \
