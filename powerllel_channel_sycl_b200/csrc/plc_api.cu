@@ -1322,17 +1322,12 @@ int post_step_begin(plc_ctx *c) {
   return PLC_OK;
 }
 
-int post_step_end(plc_ctx *c) {
+// Acts on a full check's result in c->h_check (main.cc:156-178): the NaN,
+// CFL and divergence limits, then the new dt under CFL control -- copied to
+// the device here, or (device_dt) already set there by the check's own
+// k_cfl_dt, of which the host keeps the same value.
+int check_result(plc_ctx *c, bool device_dt) {
   const plc_params &P = c->prm;
-  const int what = c->pending_check;
-  c->pending_check = 0;
-  if (!what) return PLC_OK;
-  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
-  if (what == 2) {
-    if (c->h_check->cfl > 0.0)
-      if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl)) return rc;
-    return PLC_OK;
-  }
   c->last_nan_passed = c->h_check->nan_found ? 0 : 1;
   to_ijk(c, c->h_check->cfl_idx, &c->last_cfl, c->h_check->cfl * c->dt_host);
   to_ijk(c, c->h_check->div_idx, &c->last_div, c->h_check->div);
@@ -1359,14 +1354,74 @@ int post_step_end(plc_ctx *c) {
              c->nstep, cm.value, cm.ig, cm.jg, cm.kg, dm.value, dm.ig, dm.jg, dm.kg);
     return set_error(c, PLC_ERR_CHECK, msg + buf);
   }
-  if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0)
-    if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl)) return rc;
+  if (P.cfl_target > 0.0 && c->h_check->cfl > 0.0) {
+    if (device_dt)
+      c->dt_host = P.cfl_target / c->h_check->cfl;
+    else if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl))
+      return rc;
+  }
   return PLC_OK;
+}
+
+int post_step_end(plc_ctx *c) {
+  const plc_params &P = c->prm;
+  const int what = c->pending_check;
+  c->pending_check = 0;
+  if (!what) return PLC_OK;
+  PLC_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (what == 2) {
+    if (c->h_check->cfl > 0.0)
+      if (int rc = upload_step_consts_async(c, P.cfl_target / c->h_check->cfl)) return rc;
+    return PLC_OK;
+  }
+  return check_result(c, false);
 }
 
 int post_step(plc_ctx *c) {
   if (int rc = post_step_begin(c)) return rc;
   return post_step_end(c);
+}
+
+namespace {
+// CFL control on the device after a full check (the host's arithmetic of
+// upload_step_consts: one division for dt, the derived factors from it).
+__global__ void k_cfl_dt(const CheckResult *__restrict__ res, StepConst *sc, double cfl_target,
+                         double dx_inv, double dy_inv) {
+  const double rate = res->cfl;
+  if (rate > 0.0) {
+    const double dt = cfl_target / rate;
+    const double dti = 1.0 / dt;
+    sc->dt = dt;
+    sc->dti = dti;
+    sc->dtidxi = dti * dx_inv;
+    sc->dtidyi = dti * dy_inv;
+    sc->dtdxi = dt * dx_inv;
+    sc->dtdyi = dt * dy_inv;
+  }
+}
+}  // namespace
+
+int enqueue_check_tail(plc_ctx *c, cudaStream_t s) {
+  if (c->mixed)
+    PLC_CUDA(c, launch_check(c, c->f_field[PLC_U], c->f_field[PLC_V], c->f_field[PLC_W], 7, s));
+  else
+    PLC_CUDA(c, launch_check(c, c->d_field[PLC_U], c->d_field[PLC_V], c->d_field[PLC_W], 7, s));
+  if (c->prm.cfl_target > 0.0) {
+    k_cfl_dt<<<1, 1, 0, s>>>(c->d_check, c->d_sc, c->prm.cfl_target, c->dx_inv, c->dy_inv);
+    PLC_CUDA(c, cudaGetLastError());
+  }
+  PLC_CUDA(c, cudaMemcpyAsync(c->h_check, c->d_check, sizeof(CheckResult), cudaMemcpyDeviceToHost, s));
+  return PLC_OK;
+}
+
+bool device_check_due(const plc_ctx *c, int steps) {
+  const plc_params &P = c->prm;
+  return P.nt_check == steps && c->nstep % steps == 0;
+}
+
+int post_steps_device_check(plc_ctx *c, int steps) {
+  c->nstep += steps;
+  return check_result(c, true);
 }
 
 }  // namespace plc

@@ -35,10 +35,12 @@ struct plc_ensemble {
   cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t graph = nullptr;
-  cudaGraphExec_t graph_k = nullptr;  // K steps per branch
+  cudaGraphExec_t graph_k = nullptr;   // K steps per branch
+  cudaGraphExec_t graph_kc = nullptr;  // K steps ending on a check step, with the checks
   int k_steps = 0;
-  std::vector<unsigned> epochs;    // member graph epochs the graph was captured at
-  std::vector<unsigned> epochs_k;  // ... and the K-step graph
+  std::vector<unsigned> epochs;     // member graph epochs the graph was captured at
+  std::vector<unsigned> epochs_k;   // ... and the K-step graphs
+  std::vector<unsigned> epochs_kc;
   std::vector<int> group;        // group of each member
   int ngroups = 1;
   int scheme = PLC_ENS_CONCURRENT;
@@ -91,6 +93,10 @@ void drop(plc_ensemble *e) {
   if (e->graph_k) {
     cudaGraphExecDestroy(e->graph_k);
     e->graph_k = nullptr;
+  }
+  if (e->graph_kc) {
+    cudaGraphExecDestroy(e->graph_kc);
+    e->graph_kc = nullptr;
   }
 }
 
@@ -147,7 +153,7 @@ int enqueue_chain(plc_ensemble *e, plc_ctx *const *cs, int n, int steps, cudaStr
 // ensemble stream): the FP64 members' fused steps as branches; the
 // mixed-form members in e->chains chains (cost-balanced, longest first),
 // each chain's steps stage by stage, the chains concurrently.
-int enqueue_batched(plc_ensemble *e, int steps) {
+int enqueue_batched(plc_ensemble *e, int steps, bool checks) {
   std::vector<int> mixed, fp64;
   for (size_t m = 0; m < e->members.size(); ++m) (e->members[m]->mixed ? mixed : fp64).push_back((int)m);
   ENS_CUDA(e, cudaEventRecord(e->fork, e->stream));
@@ -156,6 +162,8 @@ int enqueue_batched(plc_ensemble *e, int steps) {
     ENS_CUDA(e, cudaStreamWaitEvent(c->stream, e->fork, 0));
     for (int q = 0; q < steps; ++q)
       if (int rc = plc::capture_step(c, c->stream)) return member_error(e, m, rc);
+    if (checks)
+      if (int rc = plc::enqueue_check_tail(c, c->stream)) return member_error(e, m, rc);
     ENS_CUDA(e, cudaEventRecord(e->join[m], c->stream));
   }
   const int nch = (int)mixed.size() >= 2 ? e->chains : 1;
@@ -182,14 +190,27 @@ int enqueue_batched(plc_ensemble *e, int steps) {
                                e->stage_fork[0], 0, nch == 2 ? kAuxStreams / 2 : kAuxStreams))
       return rc;
   if (nch == 2) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->chain_join, 0));
+  if (checks) {
+    // the mixed-form members' checks side by side on their own streams
+    ENS_CUDA(e, cudaEventRecord(e->done, e->stream));
+    for (int m : mixed) {
+      plc_ctx *c = e->members[m];
+      ENS_CUDA(e, cudaStreamWaitEvent(c->stream, e->done, 0));
+      if (int rc = plc::enqueue_check_tail(c, c->stream)) return member_error(e, m, rc);
+      ENS_CUDA(e, cudaEventRecord(e->join[m], c->stream));
+      ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
+    }
+  }
   for (int m : fp64) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
   return PLC_OK;
 }
 
 // Captures `steps` ensemble steps into *out: per group, a fork from the
 // ensemble stream to the members' streams, each member's fused steps in a
-// row, a join back (PLC_ENS_BATCHED: enqueue_batched).
-int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsigned> &epochs) {
+// row (with `checks`, then its full check and CFL-controlled dt), a join
+// back (PLC_ENS_BATCHED: enqueue_batched).
+int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsigned> &epochs,
+            bool checks = false) {
   const int n = (int)e->members.size();
   bool stale = *out == nullptr;
   for (int m = 0; m < n && !stale; ++m) stale = epochs[m] != e->members[m]->graph_epoch;
@@ -205,7 +226,7 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
   ENS_CUDA(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
   int rc = PLC_OK;
   cudaError_t r = cudaSuccess;
-  if (e->scheme == PLC_ENS_BATCHED) rc = enqueue_batched(e, steps);
+  if (e->scheme == PLC_ENS_BATCHED) rc = enqueue_batched(e, steps, checks);
   for (int grp = 0; grp < e->ngroups && rc == PLC_OK && r == cudaSuccess &&
                     e->scheme != PLC_ENS_BATCHED;
        ++grp) {
@@ -216,6 +237,8 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
       if ((r = cudaStreamWaitEvent(c->stream, e->fork, 0)) != cudaSuccess) break;
       for (int q = 0; q < steps && rc == PLC_OK; ++q)
         if ((rc = plc::capture_step(c, c->stream)) != PLC_OK) rc = member_error(e, m, rc);
+      if (rc == PLC_OK && checks && (rc = plc::enqueue_check_tail(c, c->stream)) != PLC_OK)
+        rc = member_error(e, m, rc);
       if (rc != PLC_OK) break;
       r = cudaEventRecord(e->join[m], c->stream);
     }
@@ -285,14 +308,17 @@ int members_after_ens(plc_ensemble *e) {
 int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
   if (nsteps < 0) return ens_error(e, PLC_ERR_ARG, "nsteps < 0");
   const int n = (int)e->members.size();
-  if (int rc = build(e)) return rc;
   const int K = k_of(e);
-  if (K != e->k_steps && e->graph_k) {
-    cudaGraphExecDestroy(e->graph_k);
-    e->graph_k = nullptr;
-  }
+  if (K != e->k_steps) drop(e);
   e->k_steps = K;
+  if (int rc = build(e)) return rc;
   if (int rc = capture(e, K, &e->graph_k, e->epochs_k)) return rc;
+  // the block that ends on every member's check step carries the checks
+  // (and the CFL-controlled dt) in the graph itself
+  bool kc_possible = true;
+  for (const plc_ctx *c : e->members) kc_possible = kc_possible && c->prm.nt_check == K;
+  if (kc_possible)
+    if (int rc = capture(e, K, &e->graph_kc, e->epochs_kc, true)) return rc;
   for (int m = 0; m < n; ++m)
     if (int rc = plc::pre_steps(e->members[m])) return member_error(e, m, rc);
   if (int rc = ens_after_members(e)) return rc;
@@ -306,6 +332,17 @@ int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
       c->nstep += q - 1;  // the last step of the launch decides
       host = host || plc::step_needs_host(c);
       c->nstep -= q - 1;
+    }
+    bool dev_checks = block && kc_possible;
+    for (const plc_ctx *c : e->members) dev_checks = dev_checks && plc::device_check_due(c, K);
+    if (dev_checks) {
+      // one launch and one wait for the K steps and every member's check
+      ENS_CUDA(e, cudaGraphLaunch(e->graph_kc, e->stream));
+      ENS_CUDA(e, cudaStreamSynchronize(e->stream));
+      for (int m = 0; m < n; ++m)
+        if (int rc = plc::post_steps_device_check(e->members[m], K)) return member_error(e, m, rc);
+      s += q;
+      continue;
     }
     ENS_CUDA(e, cudaGraphLaunch(block ? e->graph_k : e->graph, e->stream));
     if (host)
@@ -513,6 +550,7 @@ int plc_ensemble_create(int n, const plc_params *prms, const double *const *dzf_
     }
   e->epochs.assign(n, ~0u);
   e->epochs_k.assign(n, ~0u);
+  e->epochs_kc.assign(n, ~0u);
   e->group.assign(n, 0);
   // cost model before measurement: grid points (FP32 fields move half the bytes)
   e->cost.resize(n);

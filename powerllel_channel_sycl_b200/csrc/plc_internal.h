@@ -340,6 +340,16 @@ int post_step(plc_ctx *c);
 // several contexts share one wait
 int post_step_begin(plc_ctx *c);
 int post_step_end(plc_ctx *c);
+// Checks inside a captured graph: after the last of `steps` steps that ends
+// on a check step, enqueue_check_tail queues the full check (main.cc:156-178)
+// on stream s, the new dt under CFL control set on the device, and the
+// result's copy to the host; device_check_due says whether the next `steps`
+// steps end on a check step (every nt_check == steps steps from a multiple
+// of it) and post_steps_device_check advances the step counter and acts on
+// the copied result once the graph has finished.
+int enqueue_check_tail(plc_ctx *c, cudaStream_t s);
+bool device_check_due(const plc_ctx *c, int steps);
+int post_steps_device_check(plc_ctx *c, int steps);
 // true when post_step will do host work after the next step
 bool step_needs_host(const plc_ctx *c);
 // closes the monitor files and releases the I/O state (plc_io.cc)

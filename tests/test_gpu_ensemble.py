@@ -181,6 +181,26 @@ def test_ensemble_cfl_controlled_dt():
         assert ok and 0.2 < cfl[0] < 0.5
 
 
+@pytest.mark.parametrize("schedule", ["concurrent", "batched"])
+def test_cfl_controlled_members_match_standalone(schedule):
+    """Under CFL control the checks every nt_check steps run inside the
+    ensemble's graph, which sets each member's new dt on the device: the same
+    division as the host's, so each member still steps exactly as alone."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    kw = dict(nt_check=4, cfl_limit=1.0, div_limit=1e-3, cfl_target=0.4)
+    specs = [MEMBERS[0], MIXED[1] + (1, 1500.0), MEMBERS[2]]
+    ref = [standalone(s, 14, **kw) for s in specs]
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    ens.set_schedule(schedule)
+    ens.initFlow()
+    ens.step(14)
+    for m, r, spec in zip(ens.members, ref, specs):
+        assert m.step_count == 14
+        for f in "uvwp":
+            assert np.array_equal(m.download(f), r[f]), (schedule, spec, f)
+    ens.close()
+
+
 def test_ensemble_timed_and_throughput():
     """16 uneven channels: one graph launch per ensemble step beats stepping
     the members one after another."""
