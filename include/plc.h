@@ -169,7 +169,10 @@ int plc_fft_tiles(const plc_ctx *ctx, int *lines_xf, int *lines_x, int *lines_y)
  * 8/4/2, then 3s; 1: for lengths 3 * 2^a with 3 <= a <= 7, two passes
  * ending in a radix-24 butterfly; 2: warp-line kernels, groups of four
  * warps transforming their own lines with no block barrier, for lengths
- * 32, 48, 64, 96, 128, 192, 256, 384, 512, 768).  PLC_FFT_PLANS (FP64) and
+ * 32, 48, 64, 96, 128, 192, 256, 384, 512, 768; 3, y lines only: two passes
+ * held in registers with one shared-memory exchange, for lengths 32, 48,
+ * 64, 96, 128, 192, 256, 384 over whole blocks of 32 (FP32) or 16 (FP64)
+ * columns).  PLC_FFT_PLANS (FP64) and
  * PLC_FFT_PLANS_F32 (mixed), "x,y" or "x,y,xf", pin them (x for both x
  * transforms unless xf gives the forward one's).  No counterpart in the
  * reference. */

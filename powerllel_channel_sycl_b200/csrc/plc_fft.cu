@@ -1585,6 +1585,120 @@ __global__ void __launch_bounds__(256) k_wfft_x_bwd(Geo g, const typename Cx<T>:
 }
 
 // ---------------------------------------------------------------------------
+// Two-pass y transforms (plan family 3).  A line of length N = R1 * R2 is
+// transformed as X[k1 + R1 k2] = sum_n2 W_N^(n2 k1) W_R2^(n2 k2)
+// sum_n1 x[R2 n1 + n2] W_R1^(n1 k1): the first pass loads the R1 elements
+// x[R2 n1 + n2] of one (line, n2) straight from global memory into
+// registers, transforms them, applies the twiddles W_N^(n2 k1) and writes the
+// result to shared memory; after one barrier the second pass reads the R2
+// values of one (line, k1) into registers and transforms them.  The inverse
+// stores its outputs from there; the forward transform writes them back to
+// shared memory (every thread holds at most one second-pass task: the
+// block has L R1 threads) and, after one more barrier, separates the two
+// real spectra of each complex line while storing them.  A block holds
+// L complex lines (2L adjacent columns of one plane): with the line index
+// fastest in shared memory ([row][line]), every global access of a warp is
+// two whole 128-byte row segments and every shared-memory access runs at
+// full width.  Two or three barriers per tile instead of one per Stockham
+// pass, and no staging buffer.
+// ---------------------------------------------------------------------------
+// first-pass radix R1 of the plans (0: no plan)
+__host__ __device__ constexpr int y2_r1(int n) {
+  return n == 384 ? 16 : n == 256 ? 16 : n == 192 ? 8 : n == 128 ? 8 : n == 96 ? 4
+       : n == 64 ? 8 : n == 48 ? 4 : n == 32 ? 4 : 0;
+}
+// complex lines per block: two 128-byte row segments per warp access
+template <class T>
+__host__ __device__ constexpr int y2_lines() {
+  return sizeof(T) == 4 ? 16 : 8;
+}
+
+template <class T, int N, bool INV>
+__global__ void __launch_bounds__(y2_lines<T>() * y2_r1(N)) k_fft_y2(int nx, int ny, int nz,
+                                                                   const typename Cx<T>::V *__restrict__ tw,
+                                                                   T *__restrict__ var, int rev) {
+  using V = typename Cx<T>::V;
+  using S = T;
+  constexpr int R1 = y2_r1(N), R2 = N / R1, L = y2_lines<T>(), H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *Y = reinterpret_cast<V *>(fft_smem);  // [row][line]
+  const int tiles_x = nx / (2 * L);
+  const int tile = (int)blockIdx.x;
+  const int k = rev ? nz - 1 - tile / tiles_x : tile / tiles_x;
+  const int i0 = (tile % tiles_x) * 2 * L;
+  T *plane = var + (long long)k * nx * ny + i0;
+  auto row = [&](int t) { return reinterpret_cast<V *>(plane + (long long)t * nx); };
+  // pass 1: (line l, n2) tasks, R1 elements each
+  for (int task = threadIdx.x; task < L * R2; task += blockDim.x) {
+    const int l = task % L, n2 = task / L;
+    V v[R1];
+    if (!INV) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = row(R2 * n1 + n2)[l];
+    } else {
+      // element e of line l from the packed spectra of columns 2l, 2l+1
+      // (rows 2m, 2m+1 of mode m; rows 0 and 1 the real modes 0 and N/2)
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const int e = R2 * n1 + n2;
+        if (e == 0 || e == H) {
+          v[n1] = row(e == 0 ? 0 : 1)[l];
+        } else {
+          const int m = e < H ? e : N - e;
+          const V re = row(2 * m)[l], im = row(2 * m + 1)[l];
+          v[n1] = e < H ? mk<V>(re.x - im.y, im.x + re.y) : mk<V>(re.x + im.y, re.y - im.x);
+        }
+      }
+    }
+    Dft<R1, INV>::run(v);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      V x = v[k1];
+      if (k1 > 0 && n2 > 0) {
+        const V w = __ldg(tw + n2 * k1);
+        x = INV ? cmulc(x, w) : cmul(x, w);
+      }
+      Y[(k1 * R2 + n2) * L + l] = x;
+    }
+  }
+  __syncthreads();
+  // pass 2: (line l, k1) tasks, R2 elements each; at most one per thread
+  const int l = threadIdx.x % L, k1 = threadIdx.x / L;
+  V v[R2];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) v[n2] = Y[(k1 * R2 + n2) * L + l];
+  Dft<R2, INV>::run(v);
+  if (INV) {
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) row(k1 + R1 * k2)[l] = v[k2];
+    return;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k2 = 0; k2 < R2; ++k2) Y[(k1 + R1 * k2) * L + l] = v[k2];
+  __syncthreads();
+  // the two real spectra A (column 2l) and B (column 2l+1) of each line:
+  // rows 2m, 2m+1 hold (Re, Im) of mode m, rows 0 and 1 the real modes 0, N/2
+  const S half = S(0.5);
+  for (int task = threadIdx.x; task < L * H; task += blockDim.x) {
+    const int ll = task % L, m = task / L;
+    V a, b;
+    if (m == 0) {
+      const V z0 = Y[ll], zh = Y[H * L + ll];
+      a = mk<V>((z0.x + z0.x) * half, (zh.x + zh.x) * half);
+      b = mk<V>((z0.y + z0.y) * half, (zh.y + zh.y) * half);
+    } else {
+      const V zm = Y[m * L + ll], zc = Y[(N - m) * L + ll];
+      a = mk<V>((zm.x + zc.x) * half, (zm.y - zc.y) * half);
+      b = mk<V>((zm.y + zc.y) * half, (zc.x - zm.x) * half);
+    }
+    const int q0 = m == 0 ? 0 : 2 * m;
+    row(q0)[ll] = mk<V>(a.x, b.x);
+    row(q0 + 1)[ll] = mk<V>(a.y, b.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Thomas sweep per (i,j) system with the reciprocal pivot table
 // rpiv[(k*(ny/2+1) + my)*(nx/2+1) + mx]; the reference's divisions by b
 // become multiplications by 1/b (mod_poisson_solver.cc:334-354).
@@ -2321,6 +2435,12 @@ bool fft_has_warp_plan(int n, int lines_axis) {
   const int L = wp_lines(n, true);
   return L > 0 && lines_axis % (2 * L) == 0;
 }
+// A two-pass y plan (family 3) for line length ny over nx columns (whole
+// blocks of 2 y2_lines columns) in the form whose elements have elem bytes.
+bool fft_has_y2_plan(int ny, int nx, int elem) {
+  const int L = elem == 4 ? y2_lines<float>() : y2_lines<double>();
+  return y2_r1(ny) > 0 && nx % (2 * L) == 0;
+}
 bool fft_has_two_plans(int n) {
   bool two = false;
   with_size(n, [&](auto NC) -> cudaError_t {
@@ -2367,6 +2487,12 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_fft_y_batch<N, false, PL>));
         return cudaSuccess;
       };
+      if constexpr (N > 0 && y2_r1(N) > 0) {
+        PLC_SMEM((k_fft_y2<double, N, false>));
+        PLC_SMEM((k_fft_y2<double, N, true>));
+        PLC_SMEM((k_fft_y2<float, N, false>));
+        PLC_SMEM((k_fft_y2<float, N, true>));
+      }
       if constexpr (N > 0 && wp_base_lines(N) > 0) {
         PLC_SMEM((k_wfft_y<double, N, false>));
         PLC_SMEM((k_wfft_y<double, N, true>));
@@ -2551,6 +2677,22 @@ cudaError_t fft_y_t(const plc_ctx *c, T *var, bool inverse, cudaStream_t s) {
   const size_t sm = smem_y<T>(c->ny, nl);
   return with_size(c->ny, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0 && y2_r1(N) > 0) {
+      if (c->fft_plan_y == 3) {
+        using V = typename Cx<T>::V;
+        constexpr int L = y2_lines<T>(), threads = L * y2_r1(N);
+        const unsigned grid = (unsigned)(c->nx / (2 * L) * c->nz);
+        const size_t smem = (size_t)L * N * sizeof(V);
+        const auto tw = dev_plan<T>(c->plan_y).tw;
+        if (inverse)
+          k_fft_y2<T, N, true><<<grid, threads, smem, s>>>(c->nx, c->ny, c->nz, tw, var,
+                                                           c->order[SK_YB]);
+        else
+          k_fft_y2<T, N, false><<<grid, threads, smem, s>>>(c->nx, c->ny, c->nz, tw, var,
+                                                            c->order[SK_YF]);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (N > 0 && wp_base_lines(N) > 0) {
       if (c->fft_plan_y == 2) {
         const WpLaunch<T, N, true> lc(c->nx, c->nz);
@@ -2642,18 +2784,18 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
   // `step`) and, when `plan` is given and the length has two plan families
   // (`two`), the family *plan with it; `fits` says whether a value fits the
   // device
-  auto tune = [&](int *field, int *plan, bool two, bool warp, int pairs, int step, auto fits,
-                  auto launch) {
+  auto tune = [&](int *field, int *plan, bool two, bool warp, bool y2, int pairs, int step,
+                  auto fits, auto launch) {
     int best_d = *field, best_p = plan ? *plan : 0;
     float best_t = -1.f;
     const bool free_plan = plan && !c->fft_plans_pinned;
     const int p0 = free_plan ? 0 : (plan ? *plan : 0);
-    const int p1 = free_plan ? (warp ? 2 : (two ? 1 : 0)) : p0;
+    const int p1 = free_plan ? (y2 ? 3 : (warp ? 2 : (two ? 1 : 0))) : p0;
     for (int pl = p0; pl <= p1; ++pl) {
-      if (pl == 1 && !two) continue;
+      if ((pl == 1 && !two) || (pl == 2 && !warp) || (pl == 3 && !y2)) continue;
       if (plan) *plan = pl;
-      if (pl == 2) {
-        // the warp-line kernels have no tile size of their own
+      if (pl >= 2) {
+        // the warp-line and two-pass kernels have no tile size of their own
         const float t = time_of(launch);
         if (t >= 0.f && (best_t < 0.f || t < best_t)) {
           best_t = t;
@@ -2679,8 +2821,8 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
   };
   T *u = f[PLC_U], *v = f[PLC_V], *w = f[PLC_W], *p = f[PLC_P], *spec = f[PLC_SPEC];
   // y: tile and plan family timed on a forward and an inverse transform
-  tune(&c->fft_lines_y, &c->fft_plan_y, fft_has_two_plans(ny), fft_has_warp_plan(ny, nx), nx / 2,
-       sizeof(T) == 4 ? 2 : 1,
+  tune(&c->fft_lines_y, &c->fft_plan_y, fft_has_two_plans(ny), fft_has_warp_plan(ny, nx),
+       fft_has_y2_plan(ny, nx, sizeof(T)), nx / 2, sizeof(T) == 4 ? 2 : 1,
        [&](int d) { return smem_y<T>(ny, d) <= dev_max; },
        [&]() -> cudaError_t {
          cudaError_t r = launch_fft_y(c, spec, false, s);
@@ -2688,11 +2830,11 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
        });
   // x: the plan family (shared by both x transforms) with the backward tile,
   // then the forward tile under that family
-  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), ny / 2,
-       1,
+  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), false,
+       ny / 2, 1,
        [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
-  tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny),
+  tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), false,
        ny / 2, 1,
        [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t {

@@ -279,6 +279,8 @@ cudaError_t fft_autotune(plc_ctx *c);
 bool fft_has_two_plans(int n);
 // a warp-line plan (family 2) for length n with `lines_axis` real lines
 bool fft_has_warp_plan(int n, int lines_axis);
+// a two-pass y plan (family 3) for y lines of length ny over nx columns
+bool fft_has_y2_plan(int ny, int nx, int elem);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 // Batched launches over the mixed-form channels of an ensemble: one launch

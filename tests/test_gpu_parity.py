@@ -250,9 +250,12 @@ def test_step_parity(nx, ny, nz, nsteps, p_tol):
     assert abs(ch.Mean(var="u") - 1.0) < 1e-12
 
 
-def test_step_matches_module_sequence():
-    """The fused graph step equals the reference's call sequence of entry points."""
+def test_step_matches_module_sequence(monkeypatch):
+    """The fused graph step equals the reference's call sequence of entry
+    points (the transform families pinned: the two contexts' autotuners could
+    pick families whose results differ by rounding)."""
     from powerllel_channel_sycl_b200 import Channel
+    monkeypatch.setenv("PLC_FFT_PLANS", "0,0")
     kwargs = case_kwargs(48, 32, 16)
     a = Channel(channel_params(**kwargs))
     b = Channel(channel_params(**kwargs))
