@@ -649,8 +649,8 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   }
   // PLC_FFT_PLANS / PLC_FFT_PLANS_F32 = "x,y" pin the plan families of the x
   // and y transforms (0: radix 16/8/4/2/3 passes, 1: two passes ending in
-  // radix 24, 2: warp-line kernels, 3 (y only): two passes in registers; 1,
-  // 2 and 3 only for lengths that have them)
+  // radix 24, 2: warp-line kernels, 3: two passes in registers; 1, 2 and 3
+  // only for lengths that have them)
   // the same way; the tiles are then timed under the pinned families.
   // A third value pins the forward x transform's family apart from the
   // backward one's ("x,y,xf").
@@ -659,8 +659,8 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
     const int nread = sscanf(env, "%d,%d,%d", &px, &py, &pxf);
     if (nread == 2) pxf = px;
     auto valid_x = [&](int q) {
-      return q >= 0 && q <= 2 && (q != 1 || fft_has_two_plans(c->nx)) &&
-             (q != 2 || fft_has_warp_plan(c->nx, c->ny));
+      return q >= 0 && q <= 3 && (q != 1 || fft_has_two_plans(c->nx)) &&
+             (q != 2 || fft_has_warp_plan(c->nx, c->ny)) && (q != 3 || fft_has_x2_plan(c->nx, c->ny));
     };
     if (nread < 2 || !valid_x(px) || !valid_x(pxf) || py < 0 || py > 3 ||
         (py == 1 && !fft_has_two_plans(c->ny)) ||

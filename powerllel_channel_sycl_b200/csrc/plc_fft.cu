@@ -211,6 +211,42 @@ struct Dft<16, INV> {
   }
 };
 
+// 32 points: a radix-2 step over two 16-point transforms, X_k = E_k + W32^k O_k,
+// X_{k+16} = E_k - W32^k O_k, W32 = exp(-+ 2 pi i / 32)
+template <bool INV>
+struct Dft<32, INV> {
+  template <class V>
+  __device__ __forceinline__ static void run(V (&v)[32]) {
+    using S = ScalarOf<V>;
+    // cos and sin of j pi / 16, j = 0 .. 7
+    const S c[8] = {S(1),
+                    S(0.98078528040323044913),
+                    S(0.92387953251128675613),
+                    S(0.83146961230254523708),
+                    S(0.70710678118654752440),
+                    S(0.55557023301960222474),
+                    S(0.38268343236508977173),
+                    S(0.19509032201612826785)};
+    V e[16], o[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      e[m] = v[2 * m];
+      o[m] = v[2 * m + 1];
+    }
+    Dft<16, INV>::run(e);
+    Dft<16, INV>::run(o);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      // W32^k = cos(k pi/16) - i sin(k pi/16); for k >= 8, -i W32^(k-8)
+      const V w = k < 8 ? mk<V>(c[k], k == 0 ? S(0) : -c[8 - k])
+                        : mk<V>(k == 8 ? S(0) : -c[16 - k], -c[k - 8]);
+      const V t = k == 0 ? o[0] : (INV ? cmulc(o[k], w) : cmul(o[k], w));
+      v[k] = cadd(e[k], t);
+      v[k + 16] = csub(e[k], t);
+    }
+  }
+};
+
 template <bool INV>
 struct Dft<3, INV> {
   template <class V>
@@ -1698,6 +1734,193 @@ __global__ void __launch_bounds__(y2_lines<T>() * y2_r1(N)) k_fft_y2(int nx, int
   }
 }
 
+// Two-pass x transforms (plan family 3 of the x lines).  The same two passes
+// as k_fft_y2, along contiguous rows: a complex line is a pair of rows
+// (j, j+1) of one plane, and a warp's tasks run along a line, so that its
+// global accesses are consecutive elements of a row.  Shared memory holds
+// each line's first-pass results as R1 rows of R2 + 1 elements and the
+// second pass's as R2 rows of R1 + 1 (odd row lengths: the strided accesses
+// of the other pass hit distinct banks).  The block has L R1 threads, one
+// second-pass task each.  Lengths with R1, R2 <= 32.
+__host__ __device__ constexpr int x2_r1(int n) {
+  return n == 768 ? 32 : n == 512 ? 32 : n == 384 ? 16 : n == 256 ? 16 : n == 192 ? 8
+       : n == 128 ? 8 : n == 96 ? 4 : n == 64 ? 8 : n == 48 ? 4 : n == 32 ? 4 : 0;
+}
+// line pairs (complex lines) per block: 256 threads, at most 16 lines
+__host__ __device__ constexpr int x2_lines(int n) {
+  return x2_r1(n) > 0 ? (256 / x2_r1(n) < 16 ? 256 / x2_r1(n) : 16) : 0;
+}
+__host__ __device__ constexpr int x2_line_elems(int n) {
+  return x2_r1(n) > 0 ? ((x2_r1(n) * (n / x2_r1(n) + 1) > (n / x2_r1(n)) * (x2_r1(n) + 1))
+                             ? x2_r1(n) * (n / x2_r1(n) + 1)
+                             : (n / x2_r1(n)) * (x2_r1(n) + 1))
+                      : 0;
+}
+
+// Forward: rows (j0 + 2l, j0 + 2l + 1) of plane k (div(u)/dt with FUSED, p
+// otherwise) -> packed spectra.  Grid (ny / (2 L), nz).
+template <class T, int N, bool FUSED>
+__global__ void __launch_bounds__(x2_lines(N) * x2_r1(N))
+    k_fft_x2_fwd(Geo g, const typename Cx<T>::V *__restrict__ tw, const StepConst *__restrict__ sc,
+                 const T *__restrict__ p, const T *__restrict__ u, const T *__restrict__ v,
+                 const T *__restrict__ w, T *__restrict__ var) {
+  using V = typename Cx<T>::V;
+  using S = T;
+  constexpr int R1 = x2_r1(N), R2 = N / R1, L = x2_lines(N), E = x2_line_elems(N), H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *buf = reinterpret_cast<V *>(fft_smem);
+  const int j0 = blockIdx.x * 2 * L;  // 0-based row in the plane
+  const int k = blockIdx.y;           // 0-based plane
+  T dti = 0, dtidxi = 0, dtidyi = 0, dzfi = 0;
+  if (FUSED) {
+    dti = T(sc->dti);
+    dtidxi = T(sc->dtidxi);
+    dtidyi = T(sc->dtidyi);
+    dzfi = T(__ldg(g.dzf_inv + k + 1));
+  }
+  // pass 1: (n2, line) tasks, n2 fastest
+  for (int task = threadIdx.x; task < L * R2; task += blockDim.x) {
+    const int n2 = task % R2, l = task / R2;
+    const long long ca0 = g.at(1, j0 + 2 * l + 1, k + 1);
+    V x[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const long long ca = ca0 + R2 * n1 + n2, cb = ca + g.X;
+      T a, b;
+      if (FUSED) {
+        a = div_dt(u, v, w, ca, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
+        b = div_dt(u, v, w, cb, g.X, g.XY, dtidxi, dtidyi, dti, dzfi);
+      } else {
+        a = p[ca];
+        b = p[cb];
+      }
+      x[n1] = mk<V>(a, b);
+    }
+    Dft<R1, false>::run(x);
+    V *Y = buf + l * E;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      V y = x[k1];
+      if (k1 > 0 && n2 > 0) y = cmul(y, __ldg(tw + n2 * k1));
+      Y[k1 * (R2 + 1) + n2] = y;
+    }
+  }
+  __syncthreads();
+  // pass 2: (k1, line) tasks, one per thread
+  const int k1 = threadIdx.x % R1, l = threadIdx.x / R1;
+  V *Yl = buf + l * E;
+  V x[R2];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) x[n2] = Yl[k1 * (R2 + 1) + n2];
+  Dft<R2, false>::run(x);
+  __syncthreads();
+  // X[k1 + R1 k2] at row k2, column k1 (rows of R1 + 1)
+#pragma unroll
+  for (int k2 = 0; k2 < R2; ++k2) Yl[k2 * (R1 + 1) + k1] = x[k2];
+  __syncthreads();
+  auto X = [&](const V *Z, int kk) { return Z[(kk / R1) * (R1 + 1) + kk % R1]; };
+  const S half = S(0.5);
+  for (int task = threadIdx.x; task < L * H; task += blockDim.x) {
+    const int m = task % H, ll = task / H;
+    const V *Z = buf + ll * E;
+    V a, b;
+    if (m == 0) {
+      const V z0 = X(Z, 0), zh = X(Z, H);
+      a = mk<V>((z0.x + z0.x) * half, (zh.x + zh.x) * half);
+      b = mk<V>((z0.y + z0.y) * half, (zh.y + zh.y) * half);
+    } else {
+      const V zm = X(Z, m), zc = X(Z, N - m);
+      a = mk<V>((zm.x + zc.x) * half, (zm.y - zc.y) * half);
+      b = mk<V>((zm.y + zc.y) * half, (zc.x - zm.x) * half);
+    }
+    const long long row = (long long)k * g.ny + j0 + 2 * ll;
+    reinterpret_cast<V *>(var + row * N)[m] = a;
+    reinterpret_cast<V *>(var + (row + 1) * N)[m] = b;
+  }
+}
+
+// Backward: packed spectra -> p interior scaled by nf; with FUSE_BC the
+// pressure halos as well (updateBoundP).  Grid (ny / (2 L), nz).
+template <class T, int N, bool FUSE_BC>
+__global__ void __launch_bounds__(x2_lines(N) * x2_r1(N))
+    k_fft_x2_bwd(Geo g, const typename Cx<T>::V *__restrict__ tw, double nf,
+                 const T *__restrict__ var, T *p, int rev) {
+  using V = typename Cx<T>::V;
+  using S = T;
+  constexpr int R1 = x2_r1(N), R2 = N / R1, L = x2_lines(N), E = x2_line_elems(N), H = N / 2;
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V *buf = reinterpret_cast<V *>(fft_smem);
+  const int j0 = blockIdx.x * 2 * L;
+  const int k = rev ? g.nz - 1 - (int)blockIdx.y : (int)blockIdx.y;
+  const T scale = T(nf);
+  // pass 1: element e of line l from the packed spectra of rows a and b
+  for (int task = threadIdx.x; task < L * R2; task += blockDim.x) {
+    const int n2 = task % R2, l = task / R2;
+    const T *ra = var + ((long long)k * g.ny + j0 + 2 * l) * N, *rb = ra + N;
+    V x[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const int e = R2 * n1 + n2;
+      const int m = e <= H ? e : N - e;
+      S reA, reB, imA = S(0), imB = S(0);
+      if (m == 0 || m == H) {
+        reA = ra[m == 0 ? 0 : 1];
+        reB = rb[m == 0 ? 0 : 1];
+      } else {
+        const V a = reinterpret_cast<const V *>(ra)[m], b = reinterpret_cast<const V *>(rb)[m];
+        reA = a.x;
+        imA = a.y;
+        reB = b.x;
+        imB = b.y;
+      }
+      x[n1] = e <= H ? mk<V>(reA - imB, imA + reB) : mk<V>(reA + imB, reB - imA);
+    }
+    Dft<R1, true>::run(x);
+    V *Y = buf + l * E;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      V y = x[k1];
+      if (k1 > 0 && n2 > 0) y = cmulc(y, __ldg(tw + n2 * k1));
+      Y[k1 * (R2 + 1) + n2] = y;
+    }
+  }
+  __syncthreads();
+  const int k1 = threadIdx.x % R1, l = threadIdx.x / R1;
+  const V *Yl = buf + l * E;
+  V x[R2];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) x[n2] = Yl[k1 * (R2 + 1) + n2];
+  Dft<R2, true>::run(x);
+  // element t = k1 + R1 k2 of rows j = j0 + 2l + 1 (a) and j + 1 (b) of
+  // plane k + 1, with the periodic images and the zero-gradient ghost plane
+  const int kk = k + 1;
+  const int kimg = !FUSE_BC ? -1 : (kk == 1 ? 0 : (kk == g.nz ? g.nz + 1 : -1));
+#pragma unroll
+  for (int k2 = 0; k2 < R2; ++k2) {
+    const V z = x[k2];
+    const T ab[2] = {scale * z.x, scale * z.y};
+    const int i = k1 + R1 * k2 + 1;
+    const int iimg = !FUSE_BC ? -1 : (i == g.nx ? 0 : (i == 1 ? g.nx + 1 : -1));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int j = j0 + 2 * l + 1 + h;
+      const int jimg = !FUSE_BC ? -1 : (j == g.ny ? 0 : (j == 1 ? g.ny + 1 : -1));
+      const T val = ab[h];
+      auto put = [&](int jj, int kq) {
+        T *r = p + (long long)jj * g.X + (long long)kq * g.XY;
+        r[i] = val;
+        if (iimg >= 0) r[iimg] = val;
+      };
+      put(j, kk);
+      if (jimg >= 0) put(jimg, kk);
+      if (kimg >= 0) {
+        put(j, kimg);
+        if (jimg >= 0) put(jimg, kimg);
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Thomas sweep per (i,j) system with the reciprocal pivot table
 // rpiv[(k*(ny/2+1) + my)*(nx/2+1) + mx]; the reference's divisions by b
@@ -2441,6 +2664,11 @@ bool fft_has_y2_plan(int ny, int nx, int elem) {
   const int L = elem == 4 ? y2_lines<float>() : y2_lines<double>();
   return y2_r1(ny) > 0 && nx % (2 * L) == 0;
 }
+// A two-pass x plan (family 3) for line length nx over ny rows (whole
+// blocks of 2 x2_lines rows).
+bool fft_has_x2_plan(int nx, int ny) {
+  return x2_r1(nx) > 0 && ny % (2 * x2_lines(nx)) == 0;
+}
 bool fft_has_two_plans(int n) {
   bool two = false;
   with_size(n, [&](auto NC) -> cudaError_t {
@@ -2487,6 +2715,16 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_fft_y_batch<N, false, PL>));
         return cudaSuccess;
       };
+      if constexpr (N > 0 && x2_r1(N) > 0) {
+        PLC_SMEM((k_fft_x2_fwd<double, N, false>));
+        PLC_SMEM((k_fft_x2_fwd<double, N, true>));
+        PLC_SMEM((k_fft_x2_bwd<double, N, false>));
+        PLC_SMEM((k_fft_x2_bwd<double, N, true>));
+        PLC_SMEM((k_fft_x2_fwd<float, N, false>));
+        PLC_SMEM((k_fft_x2_fwd<float, N, true>));
+        PLC_SMEM((k_fft_x2_bwd<float, N, false>));
+        PLC_SMEM((k_fft_x2_bwd<float, N, true>));
+      }
       if constexpr (N > 0 && y2_r1(N) > 0) {
         PLC_SMEM((k_fft_y2<double, N, false>));
         PLC_SMEM((k_fft_y2<double, N, true>));
@@ -2605,9 +2843,25 @@ cudaError_t fft_x_fwd_t(const plc_ctx *c, const T *p, const T *u, const T *v, co
   // the forward transform's own family (the backward one's when not set);
   // the shared-memory families take the backward one's radix family
   const int pf = c->fft_plan_xf >= 0 ? c->fft_plan_xf : c->fft_plan_x;
-  const int pfam = pf == 2 ? (c->fft_plan_x == 2 ? 0 : c->fft_plan_x) : pf;
+  const int pfam = pf >= 2 ? (c->fft_plan_x >= 2 ? 0 : c->fft_plan_x) : pf;
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0 && x2_r1(N) > 0) {
+      if (pf == 3) {
+        using V = typename Cx<T>::V;
+        constexpr int L = x2_lines(N);
+        const dim3 grid(c->ny / (2 * L), c->nz);
+        const size_t smem = (size_t)L * x2_line_elems(N) * sizeof(V);
+        const auto tw = dev_plan<T>(c->plan_x).tw;
+        if (p)
+          k_fft_x2_fwd<T, N, false><<<grid, L * x2_r1(N), smem, s>>>(
+              c->geo(), tw, c->d_sc, p, nullptr, nullptr, nullptr, var);
+        else
+          k_fft_x2_fwd<T, N, true><<<grid, L * x2_r1(N), smem, s>>>(c->geo(), tw, c->d_sc,
+                                                                    nullptr, u, v, w, var);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (N > 0 && wp_base_lines(N) > 0) {
       if (pf == 2) {
         const WpLaunch<T, N, false> lc(c->ny, c->nz);
@@ -2645,6 +2899,22 @@ cudaError_t fft_x_bwd_t(const plc_ctx *c, const T *var, T *p, bool fuse_bc, cuda
   const double nf = 1.0 / (c->nx * c->ny);  // mod_fft.cc:57
   return with_size(c->nx, [&](auto NC) -> cudaError_t {
     constexpr int N = decltype(NC)::value;
+    if constexpr (N > 0 && x2_r1(N) > 0) {
+      if (c->fft_plan_x == 3) {
+        using V = typename Cx<T>::V;
+        constexpr int L = x2_lines(N);
+        const dim3 grid(c->ny / (2 * L), c->nz);
+        const size_t smem = (size_t)L * x2_line_elems(N) * sizeof(V);
+        const auto tw = dev_plan<T>(c->plan_x).tw;
+        if (fuse_bc)
+          k_fft_x2_bwd<T, N, true><<<grid, L * x2_r1(N), smem, s>>>(c->geo(), tw, nf, var, p,
+                                                                   c->order[SK_XB]);
+        else
+          k_fft_x2_bwd<T, N, false><<<grid, L * x2_r1(N), smem, s>>>(c->geo(), tw, nf, var, p,
+                                                                    c->order[SK_XB]);
+        return cudaGetLastError();
+      }
+    }
     if constexpr (N > 0 && wp_base_lines(N) > 0) {
       if (c->fft_plan_x == 2) {
         const WpLaunch<T, N, false> lc(c->ny, c->nz);
@@ -2784,15 +3054,15 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
   // `step`) and, when `plan` is given and the length has two plan families
   // (`two`), the family *plan with it; `fits` says whether a value fits the
   // device
-  auto tune = [&](int *field, int *plan, bool two, bool warp, bool y2, int pairs, int step,
+  auto tune = [&](int *field, int *plan, bool two, bool warp, bool f3, int pairs, int step,
                   auto fits, auto launch) {
     int best_d = *field, best_p = plan ? *plan : 0;
     float best_t = -1.f;
     const bool free_plan = plan && !c->fft_plans_pinned;
     const int p0 = free_plan ? 0 : (plan ? *plan : 0);
-    const int p1 = free_plan ? (y2 ? 3 : (warp ? 2 : (two ? 1 : 0))) : p0;
+    const int p1 = free_plan ? (f3 ? 3 : (warp ? 2 : (two ? 1 : 0))) : p0;
     for (int pl = p0; pl <= p1; ++pl) {
-      if ((pl == 1 && !two) || (pl == 2 && !warp) || (pl == 3 && !y2)) continue;
+      if ((pl == 1 && !two) || (pl == 2 && !warp) || (pl == 3 && !f3)) continue;
       if (plan) *plan = pl;
       if (pl >= 2) {
         // the warp-line and two-pass kernels have no tile size of their own
@@ -2830,12 +3100,12 @@ cudaError_t fft_autotune_t(plc_ctx *c, T *const *f, size_t dev_max, int sms) {
        });
   // x: the plan family (shared by both x transforms) with the backward tile,
   // then the forward tile under that family
-  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), false,
-       ny / 2, 1,
+  tune(&c->fft_lines_x, &c->fft_plan_x, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny),
+       fft_has_x2_plan(nx, ny), ny / 2, 1,
        [&](int d) { return smem_x_bwd<T>(nx, d) <= dev_max && smem_x_fwd<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t { return launch_fft_x_bwd(c, spec, p, true, s); });
-  tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny), false,
-       ny / 2, 1,
+  tune(&c->fft_lines_xf, &c->fft_plan_xf, fft_has_two_plans(nx), fft_has_warp_plan(nx, ny),
+       fft_has_x2_plan(nx, ny), ny / 2, 1,
        [&](int d) { return fft_bytes<T>(nx, d) <= dev_max; },
        [&]() -> cudaError_t {
          if constexpr (sizeof(T) == 8)

@@ -281,6 +281,8 @@ bool fft_has_two_plans(int n);
 bool fft_has_warp_plan(int n, int lines_axis);
 // a two-pass y plan (family 3) for y lines of length ny over nx columns
 bool fft_has_y2_plan(int ny, int nx, int elem);
+// a two-pass x plan (family 3) for x lines of length nx over ny rows
+bool fft_has_x2_plan(int nx, int ny);
 cudaError_t fft_set_lines(plc_ctx *c, int lines_xf, int lines_x, int lines_y);
 
 // Batched launches over the mixed-form channels of an ensemble: one launch
