@@ -1650,16 +1650,15 @@ __host__ __device__ constexpr int y2_lines() {
 }
 
 template <class T, int N, bool INV>
-__global__ void __launch_bounds__(y2_lines<T>() * y2_r1(N)) k_fft_y2(int nx, int ny, int nz,
-                                                                   const typename Cx<T>::V *__restrict__ tw,
-                                                                   T *__restrict__ var, int rev) {
+__device__ __forceinline__ void fft_y2_body(int nx, int ny, int nz,
+                                            const typename Cx<T>::V *__restrict__ tw,
+                                            T *__restrict__ var, int rev, int tile) {
   using V = typename Cx<T>::V;
   using S = T;
   constexpr int R1 = y2_r1(N), R2 = N / R1, L = y2_lines<T>(), H = N / 2;
   extern __shared__ __align__(16) unsigned char fft_smem[];
   V *Y = reinterpret_cast<V *>(fft_smem);  // [row][line]
   const int tiles_x = nx / (2 * L);
-  const int tile = (int)blockIdx.x;
   const int k = rev ? nz - 1 - tile / tiles_x : tile / tiles_x;
   const int i0 = (tile % tiles_x) * 2 * L;
   T *plane = var + (long long)k * nx * ny + i0;
@@ -1732,6 +1731,33 @@ __global__ void __launch_bounds__(y2_lines<T>() * y2_r1(N)) k_fft_y2(int nx, int
     row(q0)[ll] = mk<V>(a.x, b.x);
     row(q0 + 1)[ll] = mk<V>(a.y, b.y);
   }
+}
+
+template <class T, int N, bool INV>
+__global__ void __launch_bounds__(y2_lines<T>() * y2_r1(N))
+    k_fft_y2(int nx, int ny, int nz, const typename Cx<T>::V *__restrict__ tw,
+             T *__restrict__ var, int rev) {
+  fft_y2_body<T, N, INV>(nx, ny, nz, tw, var, rev, (int)blockIdx.x);
+}
+
+// The same over the mixed-form channels of an ensemble: block b works on
+// tile b - start[m] of channel m (start[m] <= b < start[m + 1]).
+struct Y2Member {
+  int nx, ny, nz, rev;
+  const float2 *tw;
+  float *var;
+};
+struct Y2Batch {
+  int n;
+  int start[kBatchMax + 1];
+  Y2Member m[kBatchMax];
+};
+template <int N, bool INV>
+__global__ void __launch_bounds__(y2_lines<float>() * y2_r1(N))
+    k_fft_y2_batch(const __grid_constant__ Y2Batch b) {
+  const int q = batch_member(b.start, b.n, (int)blockIdx.x);
+  const Y2Member &a = b.m[q];
+  fft_y2_body<float, N, INV>(a.nx, a.ny, a.nz, a.tw, a.var, a.rev, (int)blockIdx.x - b.start[q]);
 }
 
 // Two-pass x transforms (plan family 3 of the x lines).  The same two passes
@@ -2730,6 +2756,8 @@ cudaError_t fft_configure(size_t max_bytes) {
         PLC_SMEM((k_fft_y2<double, N, true>));
         PLC_SMEM((k_fft_y2<float, N, false>));
         PLC_SMEM((k_fft_y2<float, N, true>));
+        PLC_SMEM((k_fft_y2_batch<N, false>));
+        PLC_SMEM((k_fft_y2_batch<N, true>));
       }
       if constexpr (N > 0 && wp_base_lines(N) > 0) {
         PLC_SMEM((k_wfft_y<double, N, false>));
@@ -3226,7 +3254,14 @@ bool batch_tile_ok(const BatchGroup &g, int dir, int d) {
     if (batch_pairs(c, dir) % d || batch_bytes(c, dir, d) > c->trid_smem_max) return false;
   return true;
 }
-bool batch_family_ok(int N, int pl) { return pl == 0 || (pl == 1 && N > 0 && plan_has24(N)); }
+bool batch_family_ok(const BatchGroup &g, int dir, int pl) {
+  if (pl == 0) return true;
+  if (pl == 1) return g.N > 0 && plan_has24(g.N);
+  if (pl != 3 || dir != BATCH_Y || g.N <= 0 || y2_r1(g.N) == 0) return false;
+  for (const plc_ctx *c : g.ms)  // the two-pass y kernels take whole blocks of columns
+    if (c->nx % (2 * y2_lines<float>())) return false;
+  return true;
+}
 void batch_set_tile(BatchGroup &g, int dir, int nl) {
   g.nl = nl;
   g.smem = 0;
@@ -3255,7 +3290,7 @@ std::vector<BatchGroup> batch_groups(plc_ctx *const *cs, int n, int dir, const B
     int pl = dir == BATCH_Y ? lead->fft_plan_y
                             : (dir == BATCH_XF && lead->fft_plan_xf >= 0 ? lead->fft_plan_xf
                                                                          : lead->fft_plan_x);
-    if (!batch_family_ok(g.N, pl)) pl = 0;
+    if (!batch_family_ok(g, dir, pl)) pl = 0;
     g.PL = pl;
     // default tile: the largest admitted by all the channels, up to 16 pairs
     // and 64 KB of shared memory
@@ -3269,7 +3304,7 @@ std::vector<BatchGroup> batch_groups(plc_ctx *const *cs, int n, int dir, const B
     if (bp)
       for (const BatchPlan::Group &q : bp->dir[dir])
         if (q.len_key == g.N) {
-          if (batch_family_ok(g.N, q.pl)) g.PL = q.pl;
+          if (batch_family_ok(g, dir, q.pl)) g.PL = q.pl;
           if (batch_tile_ok(g, dir, q.nl)) nl = q.nl;
         }
     batch_set_tile(g, dir, nl);
@@ -3341,6 +3376,38 @@ cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s) {
 }
 
 cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
+  if (G.PL == 3) {
+    return with_size(G.N, [&](auto NC) -> cudaError_t {
+      constexpr int N = decltype(NC)::value;
+      if constexpr (N > 0 && y2_r1(N) > 0) {
+        constexpr int L = y2_lines<float>(), threads = L * y2_r1(N);
+        const size_t smem = (size_t)L * N * sizeof(float2);
+        for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
+          Y2Batch b;
+          std::memset(&b, 0, sizeof b);
+          b.n = (int)std::min<size_t>(kBatchMax, G.ms.size() - q0);
+          int tot = 0;
+          for (int q = 0; q < b.n; ++q) {
+            const plc_ctx *c = G.ms[q0 + q];
+            b.m[q] = Y2Member{c->nx, c->ny, c->nz, c->order[inverse ? SK_YB : SK_YF],
+                              dev_plan<float>(c->plan_y).tw, c->f_field[PLC_SPEC]};
+            b.start[q] = tot;
+            tot += c->nx / (2 * L) * c->nz;
+          }
+          b.start[b.n] = tot;
+          if (inverse)
+            k_fft_y2_batch<N, true><<<tot, threads, smem, s>>>(b);
+          else
+            k_fft_y2_batch<N, false><<<tot, threads, smem, s>>>(b);
+          const cudaError_t e = cudaGetLastError();
+          if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+      } else {
+        return cudaErrorInvalidValue;
+      }
+    });
+  }
   for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
     YBatch b;
     std::memset(&b, 0, sizeof b);
@@ -3480,11 +3547,11 @@ cudaError_t batch_autotune(plc_ctx *const *cs, int n, cudaStream_t s, BatchPlan 
     for (BatchGroup &G : gs) {
       BatchPlan::Group best{G.N, G.PL, G.nl};
       float best_t = -1.f;
-      for (int pl = 0; pl <= 1; ++pl) {
-        if (!batch_family_ok(G.N, pl) || (fam_pinned && pl != G.PL)) continue;
+      for (int pl = 0; pl <= 3; ++pl) {
+        if (!batch_family_ok(G, dir, pl) || (fam_pinned && pl != G.PL)) continue;
         G.PL = pl;
         for (int d = batch_step(dir); d <= 16; d += batch_step(dir)) {
-          if (!batch_tile_ok(G, dir, d)) continue;
+          if (!batch_tile_ok(G, dir, d) || (pl == 3 && d != G.nl)) continue;  // no tile in family 3
           batch_set_tile(G, dir, d);
           const float t = time_of([&]() -> cudaError_t {
             if (dir == BATCH_XF) return launch_group_xf(G, s);
