@@ -119,6 +119,28 @@ static __device__ __forceinline__ void store_point(T *q, const Geo &g, const Hal
   if ((h.dx | h.dy) != 0 || k == 1 || k == g.nz) store_images(q, g, h, c, k, v, kind, bc);
 }
 
+// The same writes inline: for kernels where boundary columns are common (the
+// small channels of an ensemble), whose warps take this path together -- the
+// image stores are predicated per lane, the ghost writes uniform per plane.
+template <class T>
+static __device__ __forceinline__ void store_point_inline(T *q, const Geo &g, const HaloCol &h,
+                                                          long long c, int k, T val, int kind,
+                                                          T bc) {
+  T v = val;
+  if (kind == BC_FACE && k == g.nz) v = bc;  // w(nz) = bcvalue
+  store_col(q, c, h, v);
+  if (k == 1 || k == g.nz) {
+    T gv;
+    if (kind == BC_CENTRED)
+      gv = T(2) * bc - v;
+    else if (kind == BC_FACE)
+      gv = bc;
+    else
+      gv = v;
+    store_col(q, k == 1 ? c - g.XY : c + g.XY, h, gv);
+  }
+}
+
 // Block coordinates of a kernel body that runs as one block of a batched
 // launch over several channels of an ensemble: the block's place in its
 // channel's share of the grid.

@@ -137,7 +137,7 @@ int enqueue_chain(plc_ensemble *e, plc_ctx *const *cs, int n, int steps, cudaStr
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_y_batch(cs, n, false, bp, ss, ns);  // y-FFT
              }));
-    ENS_CUDA(e, plc::launch_trid_batch(cs, n, st));  // z solve
+    ENS_CUDA(e, plc::launch_trid_batch(cs, n, bp->trid_tile, st));  // z solve
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_y_batch(cs, n, true, bp, ss, ns);  // y-iFFT
              }));

@@ -2584,6 +2584,58 @@ __global__ void __launch_bounds__(32) k_trid_mixed_tile(
   if (lane == 0) trid_drain(bar, err);
 }
 
+// The same over the mixed-form channels of an ensemble: block b works on the
+// 32 systems of block b - start[m] of channel m (start[m] <= b < start[m+1]);
+// the shared memory holds the longest column of the launch.
+struct TrtMember {
+  int nx, ny, nz;
+  const float *rpiv32, *a32, *c32;
+  const double *rpiv, *a, *c;
+  float *var;
+  double *low;
+  int *err;
+};
+struct TrtBatch {
+  int n;
+  int start[kBatchMax + 1];
+  TrtMember m[kBatchMax];
+};
+static_assert(sizeof(TrtBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
+__global__ void __launch_bounds__(32) k_trid_mixed_tile_batch(const __grid_constant__ TrtBatch bt) {
+  const int q = batch_member(bt.start, bt.n, (int)blockIdx.x);
+  const TrtMember &M = bt.m[q];
+  const int nx = M.nx, ny = M.ny, nz = M.nz;
+  float *var = M.var;
+  extern __shared__ __align__(128) unsigned char trid_smem[];
+  float *xs = reinterpret_cast<float *>(trid_smem);
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(
+      trid_smem + ((size_t)nz * 32 * sizeof(float) + 15) / 16 * 16);
+  const int lane = threadIdx.x;
+  const long long plane = (long long)nx * ny;
+  const long long t0 = (long long)((int)blockIdx.x - bt.start[q]) * 32;
+  const int cp = (nz + kTridChunks - 1) / kTridChunks;
+  trid_tile_load(xs, bar, var + t0, plane, nz, cp);
+  int i, j;
+  long long pv;
+  trid_index((int)(t0 + lane), nx, ny, i, j, pv);
+  const long long PS = (long long)((nx >> 1) + 1) * ((ny >> 1) + 1);
+  bool ok = true;
+  if (i < kLowModes && j < kLowModes) {
+    for (int ch = 0; ch < kTridChunks && ok; ++ch) ok = trid_wait_chunk(bar, ch, M.err);
+    if (ok) {
+      constexpr long long LP = (long long)kLowModes * kLowModes;
+      thomas_sweep<double, 8>(nz, LowSysSmem{xs + lane, var + t0 + lane, plane,
+                                             M.low + j * kLowModes + i, LP, M.rpiv + pv, PS, M.a,
+                                             M.c});
+    }
+  } else {
+    trid_tile_sweep<float>(xs, nz, cp, bar, M.rpiv32 + pv, PS, M.a32, M.c32, var + t0 + lane,
+                           plane, M.err, ok);
+  }
+  __syncwarp();
+  if (lane == 0) trid_drain(bar, M.err);
+}
+
 template <class T>
 FftDev<typename Cx<T>::V> dev_plan(const FftPlan &p) {
   FftDev<typename Cx<T>::V> d;
@@ -2776,6 +2828,7 @@ cudaError_t fft_configure(size_t max_bytes) {
       if constexpr (N == 0) {
         PLC_SMEM(k_trid_tile);
         PLC_SMEM(k_trid_mixed_tile);
+        PLC_SMEM(k_trid_mixed_tile_batch);
       }
       r = conf(std::integral_constant<int, 0>{});
       if (r != cudaSuccess) return r;
@@ -3568,6 +3621,21 @@ cudaError_t batch_autotune(plc_ctx *const *cs, int n, cudaStream_t s, BatchPlan 
       bp->dir[dir].push_back(best);
     }
   }
+  // the Thomas sweep: streamed, or with the columns on chip (as the channels
+  // have it where PLC_TRID pins it)
+  bp->trid_tile = false;
+  bool trid_pinned = false, trid_tiles = true;
+  for (int m = 0; m < n; ++m) {
+    trid_pinned = trid_pinned || cs[m]->trid_pinned;
+    trid_tiles = trid_tiles && cs[m]->trid_tile;
+  }
+  if (trid_pinned) {
+    bp->trid_tile = trid_tiles && trid_tile_batch_ok(cs, n);
+  } else if (trid_tile_batch_ok(cs, n)) {
+    const float ts = time_of([&]() { return launch_trid_batch(cs, n, false, s); });
+    const float tt = time_of([&]() { return launch_trid_batch(cs, n, true, s); });
+    bp->trid_tile = tt >= 0.f && (ts < 0.f || tt < ts);
+  }
   {
     float best_t = -1.f;
     for (int minb = 3; minb <= 4; ++minb)
@@ -3591,7 +3659,38 @@ cudaError_t batch_autotune(plc_ctx *const *cs, int n, cudaStream_t s, BatchPlan 
   return cudaSuccess;
 }
 
-cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+// whether every channel admits the on-chip sweep (whole blocks of 32 systems,
+// its column in shared memory)
+bool trid_tile_batch_ok(plc_ctx *const *cs, int n) {
+  for (int m = 0; m < n; ++m)
+    if (cs[m]->nx % 32 || trid_tile_smem(cs[m]->nz, sizeof(float)) > cs[m]->trid_smem_max)
+      return false;
+  return n > 0;
+}
+
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s) {
+  if (tile && trid_tile_batch_ok(cs, n)) {
+    for (int q0 = 0; q0 < n; q0 += kBatchMax) {
+      TrtBatch b;
+      std::memset(&b, 0, sizeof b);
+      b.n = std::min(kBatchMax, n - q0);
+      int tot = 0, nzmax = 0;
+      for (int q = 0; q < b.n; ++q) {
+        const plc_ctx *c = cs[q0 + q];
+        b.m[q] = TrtMember{c->nx,     c->ny,     c->nz,           c->d_rpiv32, c->d_ac32,
+                           c->d_ac32 + c->nz, c->d_rpiv, c->d_ac, c->d_ac + c->nz,
+                           c->f_field[PLC_SPEC], c->d_low, c->d_err};
+        b.start[q] = tot;
+        tot += (int)((long long)c->nx * c->ny / 32);
+        nzmax = std::max(nzmax, c->nz);
+      }
+      b.start[b.n] = tot;
+      k_trid_mixed_tile_batch<<<tot, 32, trid_tile_smem(nzmax, sizeof(float)), s>>>(b);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
   for (int q0 = 0; q0 < n; q0 += kBatchMax) {
     TrBatch b;
     std::memset(&b, 0, sizeof b);

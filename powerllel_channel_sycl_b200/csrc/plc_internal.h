@@ -306,6 +306,7 @@ struct BatchPlan {
   std::vector<Group> dir[3];  // BATCH_XF, BATCH_XB, BATCH_Y
   int rk_kchunk = 0;
   int rk_minb = 4;  // resident blocks per SM the RK kernels are compiled for (3 or 4)
+  bool trid_tile = false;  // the Thomas sweep with its columns on chip
 };
 enum BatchDir { BATCH_XF = 0, BATCH_XB = 1, BATCH_Y = 2 };
 cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, int minb,
@@ -314,7 +315,9 @@ cudaError_t launch_fft_x_fwd_batch(plc_ctx *const *cs, int n, const BatchPlan *b
                                    const cudaStream_t *ss, int ns);
 cudaError_t launch_fft_y_batch(plc_ctx *const *cs, int n, bool inverse, const BatchPlan *bp,
                                const cudaStream_t *ss, int ns);
-cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s);
+// whether every channel admits the batched on-chip Thomas sweep
+bool trid_tile_batch_ok(plc_ctx *const *cs, int n);
 cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
                                    const cudaStream_t *ss, int ns);
 cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s);

@@ -600,6 +600,9 @@ __device__ __forceinline__ void rk32_body(const CUtensorMap *mu, const CUtensorM
   ZFace fa_c{}, fb_c{};  // z-face terms carried from plane k-1 (rows a, b)
   const HaloCol ha = halo_col(g, i, ja), hb = halo_col(g, i, jb);
   const bool xy_edge = (ha.dx | ha.dy | hb.dx | hb.dy) != 0;  // images in x or y
+  // the whole warp takes the image path when one of its lanes has images (in
+  // small channels most warps do): no divergence between the two paths
+  const bool edge_w = __any_sync(0xffffffffu, xy_edge);
   const int o = (2 * ty + 1) * HX + (tx + 1);  // point a in a slot
   int sm = 0, s0 = 1, sp = 2;                  // slots of planes k-1, k, k+1
   for (int k = kb; k <= ke; ++k) {
@@ -681,14 +684,14 @@ __device__ __forceinline__ void rk32_body(const CUtensorMap *mu, const CUtensorM
             msum[d] = fmaf(x, dzl, msum[d]);
           }
       }
-      if (FUSE && (xy_edge || k == 1 || k == g.nz)) {
-        store_point(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
-        store_point(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
-        store_point(ow, g, ha, c, k, va[2], BC_FACE, 0.f);
+      if (FUSE && (edge_w || k == 1 || k == g.nz)) {
+        store_point_inline(ou, g, ha, c, k, va[0], BC_CENTRED, bc_u);
+        store_point_inline(ov, g, ha, c, k, va[1], BC_CENTRED, 0.f);
+        store_point_inline(ow, g, ha, c, k, va[2], BC_FACE, 0.f);
         if (act_b) {
-          store_point(ou, g, hb, c + X, k, vb[0], BC_CENTRED, bc_u);
-          store_point(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.f);
-          store_point(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.f);
+          store_point_inline(ou, g, hb, c + X, k, vb[0], BC_CENTRED, bc_u);
+          store_point_inline(ov, g, hb, c + X, k, vb[1], BC_CENTRED, 0.f);
+          store_point_inline(ow, g, hb, c + X, k, vb[2], BC_FACE, 0.f);
         }
       } else {  // no image or ghost to write
         ou[c] = va[0];

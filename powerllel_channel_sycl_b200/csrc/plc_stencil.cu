@@ -956,9 +956,10 @@ __device__ __forceinline__ void correct_forced_body(Geo g, const StepConst *__re
       const T nu = uu[q] - (px[q] - pc[q]) * dtdxi + fu;
       const T nv = vv[q] - (py[q] - pc[q]) * dtdyi + fv;
       const T nw = ww[q] - (pc[q + 1] - pc[q]) * dt * T(__ldg(g.dzc_inv + k)) + fw;
-      store_point(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - u_crf));
-      store_point(v, g, h, c, k, nv, BC_CENTRED, T(0));
-      store_point(w, g, h, c, k, nw, BC_FACE, T(0));
+      // inline image stores: in small channels most warps have boundary lanes
+      store_point_inline(u, g, h, c, k, nu, BC_CENTRED, T(0.0 - u_crf));
+      store_point_inline(v, g, h, c, k, nv, BC_CENTRED, T(0));
+      store_point_inline(w, g, h, c, k, nw, BC_FACE, T(0));
     }
 }
 

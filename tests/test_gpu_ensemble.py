@@ -134,6 +134,27 @@ def test_batched_mixed_members_match_standalone(mixed_alone, chains):
     ens.close()
 
 
+@pytest.mark.parametrize("trid", ["tile", "stream"])
+def test_batched_thomas_sweeps(monkeypatch, trid):
+    """The batched schedule's Thomas sweep, on chip or streamed (pinned by
+    PLC_TRID as the channels' own), after the batch autotuner: each member as
+    alone with the same sweep."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    monkeypatch.setenv("PLC_TRID", trid)
+    specs = [(64, 48, 48, 1, 1500.0), (96, 64, 32, 1, 2500.0), (32, 24, 16, 1, 1800.0)]
+    kw = dict(nt_check=3, cfl_limit=10.0, div_limit=1e-8)
+    ref = [standalone(s, 5, **kw) for s in specs]
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    ens.initFlow()
+    ens.autotune(steps=2)
+    ens.set_schedule("batched")
+    ens.step(5)
+    for m, r, spec in zip(ens.members, ref, specs):
+        for f in "uvwp":
+            assert np.array_equal(m.download(f), r[f]), (trid, spec, f)
+    ens.close()
+
+
 @pytest.mark.parametrize("schedule", ["concurrent", "batched"])
 def test_member_matches_oracle(schedule):
     """The smallest FP64 member, stepped 5 times inside an ensemble (beside a
