@@ -190,16 +190,11 @@ int enqueue_batched(plc_ensemble *e, int steps, bool checks) {
                                e->stage_fork[0], 0, nch == 2 ? kAuxStreams / 2 : kAuxStreams))
       return rc;
   if (nch == 2) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->chain_join, 0));
-  if (checks) {
-    // the mixed-form members' checks side by side on their own streams
-    ENS_CUDA(e, cudaEventRecord(e->done, e->stream));
-    for (int m : mixed) {
-      plc_ctx *c = e->members[m];
-      ENS_CUDA(e, cudaStreamWaitEvent(c->stream, e->done, 0));
-      if (int rc = plc::enqueue_check_tail(c, c->stream)) return member_error(e, m, rc);
-      ENS_CUDA(e, cudaEventRecord(e->join[m], c->stream));
-      ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
-    }
+  if (checks && !mixed.empty()) {
+    // the mixed-form members' checks and new dt in one launch
+    std::vector<plc_ctx *> ms;
+    for (int m : mixed) ms.push_back(e->members[m]);
+    ENS_CUDA(e, plc::launch_check_batch(ms.data(), (int)ms.size(), e->stream));
   }
   for (int m : fp64) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
   return PLC_OK;

@@ -321,6 +321,10 @@ bool trid_tile_batch_ok(plc_ctx *const *cs, int n);
 cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
                                    const cudaStream_t *ss, int ns);
 cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+// the full checks of the mixed-form channels at a graph's check step: results
+// on the device and in each channel's pinned host copy, the new dt under CFL
+// control set on the device
+cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s);
 // the number of launches (line-length groups) of the batched x and y stages
 int fft_batch_groups(plc_ctx *const *cs, int n, bool ydir);
 // times the candidate families and tiles of every group of the batched

@@ -1261,6 +1261,117 @@ __global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restr
   }
 }
 
+// The full check (what = 7) of the mixed-form channels of an ensemble in one
+// launch, with what each channel's check step does after it: block b works
+// as block b - start[m] of nb blocks of channel m (start[m] <= b <
+// start[m + 1]); the last block of a channel writes its result to the
+// device and to the channel's pinned host copy, and, under CFL control, the
+// new dt and its derived factors (the host's arithmetic: one division, then
+// the products).  The same maxima and indices as k_check (ties to the
+// lowest index); the NaN flag travels in the partials, so nothing has to be
+// cleared first.
+struct ChkMember {
+  Geo g;
+  const float *u, *v, *w;
+  double *partials;
+  unsigned int *counter;
+  CheckResult *out, *out_host;
+  StepConst *sc;
+  double cfl_target;
+  int nb;
+};
+struct ChkBatch {
+  int n;
+  int start[kBatchMax + 1];
+  ChkMember m[kBatchMax];
+};
+static_assert(sizeof(ChkBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
+__global__ void __launch_bounds__(256) k_check_batch(const __grid_constant__ ChkBatch bt) {
+  __shared__ MaxIdx smem[32];
+  __shared__ int nan_s;
+  __shared__ bool am_last;
+  const int q = batch_member(bt.start, bt.n, (int)blockIdx.x);
+  const ChkMember &M = bt.m[q];
+  const Geo g = M.g;
+  const int lb = (int)blockIdx.x - bt.start[q], nb = M.nb;
+  if (threadIdx.x == 0) nan_s = 0;
+  __syncthreads();
+  const long long first = g.at(1, 1, 1);
+  MaxIdx cfl{0.0, first}, div{0.0, first};
+  int nan_found = 0;
+  const long long nall = (long long)g.XY * (g.nz + 2);
+  for (long long t = (long long)lb * blockDim.x + threadIdx.x; t < nall;
+       t += (long long)nb * blockDim.x)
+    if (isnan(M.u[t])) nan_found = 1;
+  const int nrows = g.ny * g.nz;
+  for (int row = lb; row < nrows; row += nb) {
+    const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
+    const double dzfi = __ldg(g.dzf_inv + k);
+    for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+      const long long c = g.at(i, j, k);
+      const double uc = M.u[c], um = M.u[c - 1], vc = M.v[c], vm = M.v[c - g.X], wc = M.w[c],
+                   wm = M.w[c - g.XY];
+      const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
+                       fabs((wc + wm) * 0.5) * dzfi;
+      max_combine(cfl, r, c);
+      const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
+      max_combine(div, d, c);
+    }
+  }
+  if (nan_found) atomicOr(&nan_s, 1);
+  block_max(cfl, smem);
+  block_max(div, smem);
+  double *partials = M.partials;
+  if (threadIdx.x == 0) {
+    partials[0 * kMaxBlocksReduce + lb] = cfl.v;
+    partials[1 * kMaxBlocksReduce + lb] = __longlong_as_double(cfl.i);
+    partials[2 * kMaxBlocksReduce + lb] = div.v;
+    partials[3 * kMaxBlocksReduce + lb] = __longlong_as_double(div.i);
+    partials[4 * kMaxBlocksReduce + lb] = nan_s ? 1.0 : 0.0;
+    __threadfence();
+    const unsigned int t = atomicAdd(M.counter, 1u);
+    am_last = (t == (unsigned)nb - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  MaxIdx c2{0.0, first}, d2{0.0, first};
+  int nan_any = 0;
+  for (int b2 = threadIdx.x; b2 < nb; b2 += blockDim.x) {
+    max_combine(c2, __ldcg(partials + b2), __double_as_longlong(__ldcg(partials + kMaxBlocksReduce + b2)));
+    max_combine(d2, __ldcg(partials + 2 * kMaxBlocksReduce + b2),
+                __double_as_longlong(__ldcg(partials + 3 * kMaxBlocksReduce + b2)));
+    if (__ldcg(partials + 4 * kMaxBlocksReduce + b2) != 0.0) nan_any = 1;
+  }
+  if (threadIdx.x == 0) nan_s = 0;
+  __syncthreads();
+  if (nan_any) atomicOr(&nan_s, 1);
+  block_max(c2, smem);
+  block_max(d2, smem);
+  if (threadIdx.x == 0) {
+    CheckResult res;
+    res.nan_found = nan_s;
+    res.pad = 0;
+    res.cfl = c2.v;
+    res.cfl_idx = c2.i;
+    res.div = d2.v;
+    res.div_idx = d2.i;
+    *M.out = res;
+    *M.out_host = res;
+    if (M.cfl_target > 0.0 && c2.v > 0.0) {
+      const double dt = M.cfl_target / c2.v;
+      const double dti = 1.0 / dt;
+      M.sc->dt = dt;
+      M.sc->dti = dti;
+      M.sc->dtidxi = dti * g.dx_inv;
+      M.sc->dtidyi = dti * g.dy_inv;
+      M.sc->dtdxi = dt * g.dx_inv;
+      M.sc->dtdyi = dt * g.dy_inv;
+    }
+    *M.counter = 0u;
+  }
+}
+
 inline dim3 interior_grid(const plc_ctx *c) {
   return dim3((c->nx + BX - 1) / BX, (c->ny + BY - 1) / BY, c->nz);
 }
@@ -1592,6 +1703,44 @@ cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
     }
     b.start[b.n] = tot;
     k_correct_forced_batch<KZ><<<tot, dim3(BX, BY), 0, s>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// The full checks of n mixed-form channels, their CFL-controlled dt and the
+// results in their pinned host copies, in launches of up to kBatchMax
+// channels (the check step of a graph that carries its checks).
+cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+  for (int q0 = 0; q0 < n; q0 += kBatchMax) {
+    ChkBatch b;
+    std::memset(&b, 0, sizeof b);
+    b.n = std::min(kBatchMax, n - q0);
+    int tot = 0;
+    for (int q = 0; q < b.n; ++q) {
+      plc_ctx *c = cs[q0 + q];
+      if (!c->mixed) return cudaErrorInvalidValue;
+      ChkMember &a = b.m[q];
+      a.g = c->geo();
+      a.u = c->f_field[PLC_U];
+      a.v = c->f_field[PLC_V];
+      a.w = c->f_field[PLC_W];
+      a.partials = c->d_partials;
+      a.counter = c->d_counter + 2;
+      a.out = c->d_check;
+      void *hp = nullptr;
+      const cudaError_t e = cudaHostGetDevicePointer(&hp, c->h_check, 0);
+      if (e != cudaSuccess) return e;
+      a.out_host = static_cast<CheckResult *>(hp);
+      a.sc = c->d_sc;
+      a.cfl_target = c->prm.cfl_target;
+      a.nb = reduce_blocks(c);
+      b.start[q] = tot;
+      tot += a.nb;
+    }
+    b.start[b.n] = tot;
+    k_check_batch<<<tot, 256, 0, s>>>(b);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

@@ -190,6 +190,20 @@ def test_member_check_failure_names_the_member():
     assert e.value.code == -5 and "member 1" in str(e.value) and "checkDiv" in str(e.value)
 
 
+def test_batched_check_failure_names_the_member():
+    """The batched schedule's checks (one launch for the mixed-form members,
+    inside the graph) report a failing member by its index."""
+    from powerllel_channel_sycl_b200 import Ensemble, PlcError
+    prms = [member_params(64, 48, 48, 1, 1500.0, nt_check=2, cfl_limit=10.0, div_limit=1e-8),
+            member_params(96, 64, 32, 1, 2500.0, nt_check=2, cfl_limit=10.0, div_limit=1e-300)]
+    ens = Ensemble(prms)
+    ens.set_schedule("batched")
+    ens.initFlow()
+    with pytest.raises(PlcError) as e:
+        ens.step(4)
+    assert e.value.code == -5 and "member 1" in str(e.value) and "checkDiv" in str(e.value)
+
+
 def test_ensemble_cfl_controlled_dt():
     from powerllel_channel_sycl_b200 import Ensemble
     prms = [member_params(*s, nt_check=4, cfl_limit=1.0, div_limit=1e-3, cfl_target=0.4)
