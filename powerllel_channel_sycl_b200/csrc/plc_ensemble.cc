@@ -257,12 +257,14 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
 int build(plc_ensemble *e) { return capture(e, 1, &e->graph, e->epochs); }
 
 // K of the multi-step graph: the members' common check period when they
-// share one (a block then ends on a check step), else 8.
+// share one of at most kMaxBlockSteps steps (a block then ends on a check
+// step), else 8.  The cap bounds the captured graph: its nodes grow with K.
+constexpr int kMaxBlockSteps = 32;
 int k_of(const plc_ensemble *e) {
   int k = e->members[0]->prm.nt_check;
   for (const plc_ctx *c : e->members)
     if (c->prm.nt_check != k) k = 0;
-  return k > 1 ? k : 8;
+  return (k > 1 && k <= kMaxBlockSteps) ? k : 8;
 }
 
 // Steps, at most `limit`, until (and including) the next step that needs the

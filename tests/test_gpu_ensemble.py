@@ -236,6 +236,20 @@ def test_cfl_controlled_members_match_standalone(schedule):
     ens.close()
 
 
+def test_long_check_period_keeps_blocks_short():
+    """A check period far above the multi-step block's cap (nt_check 100000)
+    steps in blocks of the default length: the captured graphs stay small."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    import time
+    ens = Ensemble([member_params(*s, nt_check=100000) for s in MEMBERS[:2]])
+    ens.initFlow()
+    t0 = time.perf_counter()
+    ens.step(20)
+    assert time.perf_counter() - t0 < 30.0
+    assert all(m.step_count == 20 for m in ens.members)
+    ens.close()
+
+
 def test_ensemble_timed_and_throughput():
     """16 uneven channels: one graph launch per ensemble step beats stepping
     the members one after another."""
