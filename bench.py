@@ -496,7 +496,10 @@ def run_ensemble(args, world, rank, local, pg):
     ens = Ensemble(prms, device=local)
     ens.initFlow()
     tune = ens.autotune(steps=5)
-    ens.step(args.warmup)
+    # warm-up up to a check step, so that the timed steps run in whole check
+    # blocks (one graph launch per nt_check steps, the checks inside it)
+    ntc = args.nt_check if args.nt_check > 0 else 1
+    ens.step(-(-max(args.warmup, ntc) // ntc) * ntc)
     torch.cuda.synchronize(local)
     barrier(pg, local)
     ms = ens.step_timed(args.steps)
