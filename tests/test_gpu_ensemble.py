@@ -134,6 +134,26 @@ def test_batched_mixed_members_match_standalone(mixed_alone, chains):
     ens.close()
 
 
+def test_batched_two_pass_y_transforms(monkeypatch):
+    """The batched schedule's y transforms in the two-pass family (pinned as
+    the members' own): each member as alone."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    monkeypatch.setenv("PLC_FFT_PLANS_F32", "0,3")
+    specs = [(64, 48, 48, 1, 1500.0), (64, 64, 32, 1, 2000.0), (96, 48, 32, 1, 2500.0),
+             (32, 96, 16, 1, 1800.0)]
+    kw = dict(nt_check=3, cfl_limit=10.0, div_limit=1e-8)
+    ref = [standalone(s, 5, **kw) for s in specs]
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    assert all(m.fft_tiles["plan_y"] == 3 for m in ens.members)
+    ens.set_schedule("batched")
+    ens.initFlow()
+    ens.step(5)
+    for m, r, spec in zip(ens.members, ref, specs):
+        for f in "uvwp":
+            assert np.array_equal(m.download(f), r[f]), (spec, f)
+    ens.close()
+
+
 @pytest.mark.parametrize("trid", ["tile", "stream"])
 def test_batched_thomas_sweeps(monkeypatch, trid):
     """The batched schedule's Thomas sweep, on chip or streamed (pinned by
