@@ -154,6 +154,23 @@ def test_batched_two_pass_y_transforms(monkeypatch):
     ens.close()
 
 
+def test_batched_more_members_than_one_launch_holds():
+    """40 mixed-form members: the batched stages take two launches each (32
+    members' arguments per launch); every member still steps as alone."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    kw = dict(nt_check=3, cfl_limit=10.0, div_limit=1e-8)
+    specs = [(32, 24, 16, 1, 1000.0 + 50.0 * q) for q in range(40)]
+    ref = {q: standalone(specs[q], 4, **kw) for q in (0, 31, 32, 39)}
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    ens.set_schedule("batched")
+    ens.initFlow()
+    ens.step(4)
+    for q, r in ref.items():
+        for f in "uvwp":
+            assert np.array_equal(ens.members[q].download(f), r[f]), (q, f)
+    ens.close()
+
+
 @pytest.mark.parametrize("trid", ["tile", "stream"])
 def test_batched_thomas_sweeps(monkeypatch, trid):
     """The batched schedule's Thomas sweep, on chip or streamed (pinned by
