@@ -703,8 +703,10 @@ int plc_create(const plc_params *prm, const double *h_dzf_global, int device, pl
   // PLC_RK_KCHUNK pins the RK stages' z planes per block instead of timing
   // the candidates
   if (const char *env = getenv(c->mixed ? "PLC_RK_KCHUNK_F32" : "PLC_RK_KCHUNK")) {
+    // at least the smallest candidate: the mixed form's bulk-mean partials
+    // hold the blocks of a grid of that chunk (rk32_blocks)
     const int k = atoi(env);
-    if (k < 1 || k > 32)
+    if (k < kRkChunks[0] || k > 32)
       return fail(set_error(c, PLC_ERR_ARG, std::string("invalid PLC_RK_KCHUNK: ") + env));
     c->rk_kchunk = k;
     c->rk_pinned = true;

@@ -49,8 +49,13 @@ def test_rk_chunk_changes_no_result(monkeypatch, precision):
                 assert rel_l2(demean(a), demean(b)) <= 5e-3, (k, q)
 
 
-def test_rk_chunk_pin_rejected(monkeypatch):
+@pytest.mark.parametrize("value", ["0", "4", "33"])
+def test_rk_chunk_pin_rejected(monkeypatch, value):
+    """Pins outside 8..32 are refused (below 8 the mixed form's bulk-mean
+    partials would not hold the blocks)."""
     from powerllel_channel_sycl_b200 import Channel, PlcError
-    monkeypatch.setenv("PLC_RK_KCHUNK", "0")
+    monkeypatch.setenv("PLC_RK_KCHUNK_F32", value)
+    prm = channel_params(**case_kwargs(32, 24, 16))
+    prm.precision = 1
     with pytest.raises(PlcError):
-        Channel(channel_params(**case_kwargs(32, 24, 16)))
+        Channel(prm)
