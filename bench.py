@@ -497,9 +497,10 @@ def run_ensemble(args, world, rank, local, pg):
     ens.initFlow()
     tune = ens.autotune(steps=5)
     # warm-up up to a check step, so that the timed steps run in whole check
-    # blocks (one graph launch per nt_check steps, the checks inside it)
+    # blocks (one graph launch per nt_check steps, the checks inside it), and
+    # through one such block at least
     ntc = args.nt_check if args.nt_check > 0 else 1
-    ens.step(-(-max(args.warmup, ntc) // ntc) * ntc)
+    ens.step(-(-max(args.warmup, 2 * ntc) // ntc) * ntc)
     torch.cuda.synchronize(local)
     barrier(pg, local)
     ms = ens.step_timed(args.steps)

@@ -382,6 +382,8 @@ int build_graph(plc_ctx *c) {
   e = cudaGraphInstantiate(&c->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_status(c, e, "cudaGraphInstantiate");
+  // the graph's first launch would otherwise carry its upload to the device
+  PLC_CUDA(c, cudaGraphUpload(c->graph, c->stream));
   c->graph_kernels = (int)nodes;
   return PLC_OK;
 }

@@ -250,6 +250,8 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
   r = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
   if (r != cudaSuccess) return ens_cuda(e, r, "cudaGraphInstantiate");
+  // the graph's first launch would otherwise carry its upload to the device
+  ENS_CUDA(e, cudaGraphUpload(*out, e->stream));
   for (int m = 0; m < n; ++m) epochs[m] = e->members[m]->graph_epoch;
   return PLC_OK;
 }
