@@ -503,7 +503,8 @@ def run_ensemble(args, world, rank, local, pg):
     ens.step(-(-max(args.warmup, 2 * ntc) // ntc) * ntc)
     torch.cuda.synchronize(local)
     barrier(pg, local)
-    ms = ens.step_timed(args.steps)
+    with nvtx_range("ensemble_step"):
+        ms = ens.step_timed(args.steps)
     torch.cuda.synchronize(local)
     barrier(pg, local)
     ms_max = max_over_ranks(ms, pg, local)
