@@ -520,6 +520,7 @@ def run_ensemble(args, world, rank, local, pg):
         "dtype": "f32 fields (mixed form)", "scaling": "strong",
         "schedule": sched, "sm_budgets": budgets, "groups": groups,
         "autotune_ms_per_step": tune,
+        "batch_choice": ens.batch_choice() if sched == "batched" else None,
         "speedup_vs_sequential": (seq / (ms / args.steps)) if seq else None,
         "sequential_value_this_rank": (mine_pts / (seq / 1e3)) if seq else None,
     }

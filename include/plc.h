@@ -528,6 +528,14 @@ int plc_ensemble_batch_choice(const plc_ensemble *ens, int *chains, int *rk_kchu
                               int *rk_blocks_per_sm, int *fft_groups);
 /* Sets the batched schedule's chains (1 or 2) instead of the autotuner. */
 int plc_ensemble_set_batch_chains(plc_ensemble *ens, int chains);
+/* Programmatic dependent launch in the batched schedule: on != 0 launches
+ * each batched kernel with programmatic stream serialisation, so that its
+ * blocks become resident while the stage before it drains (they wait for
+ * its completion before reading anything).  The autotuner times both and
+ * keeps the faster unless PLC_ENS_PDL=0|1 pins it.  Results are the same
+ * either way.  *on may be read with plc_ensemble_batch_pdl. */
+int plc_ensemble_set_batch_pdl(plc_ensemble *ens, int on);
+int plc_ensemble_batch_pdl(const plc_ensemble *ens, int *on);
 /* Multi-GPU placement of members: longest-processing-time-first over the
  * given costs; gpu_of[i] in [0, n_gpus).  Host only. */
 int plc_ensemble_partition(int n, const double *cost, int n_gpus, int *gpu_of);

@@ -178,6 +178,8 @@ _SIGS = {
     "plc_ensemble_batch_choice": [_vp, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int),
                                   C.POINTER(_int)],
     "plc_ensemble_set_batch_chains": [_vp, _int],
+    "plc_ensemble_set_batch_pdl": [_vp, _int],
+    "plc_ensemble_batch_pdl": [_vp, C.POINTER(_int)],
     "plc_ensemble_partition": [_int, C.POINTER(_dbl), _int, C.POINTER(_int)],
     "plc_set_output_dir": [_vp, C.c_char_p],
     "plc_write_field_h5": [_vp, C.c_char_p, _int, _int],

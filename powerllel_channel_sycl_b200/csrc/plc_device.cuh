@@ -167,4 +167,16 @@ static __device__ __forceinline__ int batch_member(const int *start, int n, int 
   return m;
 }
 
+// First statement of a batched kernel, which may be launched with
+// programmatic stream serialisation (its blocks then become resident while
+// the kernels it depends on drain): wait until those kernels have completed
+// and their writes are visible, then allow the next kernel's launch to
+// begin.  Both instructions are no-ops in a plain launch.  Every block runs
+// it before anything else, so that this grid's completion implies its
+// predecessors' completion for the kernels that in turn wait on it.
+static __device__ __forceinline__ void batch_grid_sync() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace plc

@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -128,23 +129,24 @@ int enqueue_chain(plc_ensemble *e, plc_ctx *const *cs, int n, int steps, cudaStr
   const int gx = plc::fft_batch_groups(cs, n, false), gy = plc::fft_batch_groups(cs, n, true);
   const int kc = e->bplan.rk_kchunk, mb = e->bplan.rk_minb;
   const plc::BatchPlan *bp = &e->bplan;
+  const bool pdl = bp->pdl;
   for (int q = 0; q < steps; ++q) {
-    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 1, kc, mb, st));  // RK1 + bound(u1)
-    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 2, kc, mb, st));  // RK2 + bound(u) + forcing
+    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 1, kc, mb, st, pdl));  // RK1 + bound(u1)
+    ENS_CUDA(e, plc::launch_rk_batch(cs, n, 2, kc, mb, st, pdl));  // RK2 + bound(u) + forcing
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gx, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_x_fwd_batch(cs, n, bp, ss, ns);  // calcRHS + x-FFT
              }));
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_y_batch(cs, n, false, bp, ss, ns);  // y-FFT
              }));
-    ENS_CUDA(e, plc::launch_trid_batch(cs, n, bp->trid_tile, st));  // z solve
+    ENS_CUDA(e, plc::launch_trid_batch(cs, n, bp->trid_tile, st, pdl));  // z solve
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gy, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_y_batch(cs, n, true, bp, ss, ns);  // y-iFFT
              }));
     ENS_CUDA(e, batched_stage(e, st, fork, a0, na, gx, [&](const cudaStream_t *ss, int ns) {
                return plc::launch_fft_x_bwd_batch(cs, n, bp, ss, ns);  // x-iFFT + bound(p)
              }));
-    ENS_CUDA(e, plc::launch_correct_batch(cs, n, st));  // correct + force + bound(u)
+    ENS_CUDA(e, plc::launch_correct_batch(cs, n, st, pdl));  // correct + force + bound(u)
   }
   return PLC_OK;
 }
@@ -194,7 +196,7 @@ int enqueue_batched(plc_ensemble *e, int steps, bool checks) {
     // the mixed-form members' checks and new dt in one launch
     std::vector<plc_ctx *> ms;
     for (int m : mixed) ms.push_back(e->members[m]);
-    ENS_CUDA(e, plc::launch_check_batch(ms.data(), (int)ms.size(), e->stream));
+    ENS_CUDA(e, plc::launch_check_batch(ms.data(), (int)ms.size(), e->stream, e->bplan.pdl));
   }
   for (int m : fp64) ENS_CUDA(e, cudaStreamWaitEvent(e->stream, e->join[m], 0));
   return PLC_OK;
@@ -663,23 +665,40 @@ int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
   int best = PLC_ENS_CONCURRENT;
   float best_t = -1.f;
   int best_chains = e->chains;
+  bool best_pdl = e->bplan.pdl;
+  const char *pdl_env = std::getenv("PLC_ENS_PDL");
+  const int pdl_pin = pdl_env && pdl_env[0] == '1' ? 1 : pdl_env && pdl_env[0] == '0' ? 0 : -1;
   for (int s = 0; s < PLC_ENS_NUM_SCHEDULES && rc == PLC_OK; ++s) {
     if ((s == PLC_ENS_TWO_GROUPS && n < 2) || (s == PLC_ENS_BATCHED && !any_mixed)) {
       if (ms_per_scheme) ms_per_scheme[s] = -1.f;
       continue;
     }
     // the batched schedule: one chain of all the mixed-form members, or two
-    // cost-balanced chains run concurrently
+    // cost-balanced chains run concurrently; each with and without
+    // programmatic dependent launch (unless PLC_ENS_PDL pins it)
     float t = -1.f;
     const int max_chains = s == PLC_ENS_BATCHED ? 2 : 1;
+    const int pdl_lo = s == PLC_ENS_BATCHED && pdl_pin != 1 ? 0 : 1;
+    const int pdl_hi = s == PLC_ENS_BATCHED && pdl_pin != 0 ? 1 : 0;
     for (int ch = 1; ch <= max_chains && rc == PLC_OK; ++ch) {
-      float tc = 0.f;
-      if (s == PLC_ENS_BATCHED) e->chains = ch;
-      if ((rc = apply_scheme(e, s)) != PLC_OK || (rc = time_launches(e, steps, &tc)) != PLC_OK) break;
-      if (t < 0.f || tc < t) {
-        t = tc;
-        if (s == PLC_ENS_BATCHED) best_chains = ch;
+      for (int pd = s == PLC_ENS_BATCHED ? pdl_lo : 0; pd <= (s == PLC_ENS_BATCHED ? pdl_hi : 0);
+           ++pd) {
+        float tc = 0.f;
+        if (s == PLC_ENS_BATCHED) {
+          e->chains = ch;
+          e->bplan.pdl = pd == 1;
+        }
+        if ((rc = apply_scheme(e, s)) != PLC_OK || (rc = time_launches(e, steps, &tc)) != PLC_OK)
+          break;
+        if (t < 0.f || tc < t) {
+          t = tc;
+          if (s == PLC_ENS_BATCHED) {
+            best_chains = ch;
+            best_pdl = pd == 1;
+          }
+        }
       }
+      if (rc != PLC_OK) break;
     }
     if (rc != PLC_OK) break;
     t /= steps;
@@ -690,6 +709,8 @@ int plc_ensemble_autotune(plc_ensemble *e, int steps, float *ms_per_scheme) {
     }
   }
   e->chains = best_chains;
+  e->bplan.pdl = best_pdl;
+  drop(e);
   if (rc == PLC_OK) rc = apply_scheme(e, best);
   const int rc2 = snapshot(e, snap, false);
   return rc != PLC_OK ? rc : rc2;
@@ -702,6 +723,21 @@ int plc_ensemble_set_batch_chains(plc_ensemble *e, int chains) {
     e->chains = chains;
     drop(e);
   }
+  return PLC_OK;
+}
+
+int plc_ensemble_set_batch_pdl(plc_ensemble *e, int on) {
+  if (!e) return ens_error(nullptr, PLC_ERR_ARG, "null ensemble");
+  if ((on != 0) != e->bplan.pdl) {
+    e->bplan.pdl = on != 0;
+    drop(e);
+  }
+  return PLC_OK;
+}
+
+int plc_ensemble_batch_pdl(const plc_ensemble *e, int *on) {
+  if (!e || !on) return ens_error(nullptr, PLC_ERR_ARG, "null argument");
+  *on = e->bplan.pdl ? 1 : 0;
   return PLC_OK;
 }
 

@@ -1755,6 +1755,7 @@ struct Y2Batch {
 template <int N, bool INV>
 __global__ void __launch_bounds__(y2_lines<float>() * y2_r1(N))
     k_fft_y2_batch(const __grid_constant__ Y2Batch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const Y2Member &a = b.m[q];
   fft_y2_body<float, N, INV>(a.nx, a.ny, a.nz, a.tw, a.var, a.rev, (int)blockIdx.x - b.start[q]);
@@ -2274,6 +2275,7 @@ struct XfBatch {
 };
 template <int N, int PL>
 __global__ void __launch_bounds__(256) k_fft_x_fwd_div_batch(const __grid_constant__ XfBatch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const XfMember &a = b.m[q];
   fft_x_fwd_div_body<float, N, true, PL>(a.g, a.P, a.nl, a.sc, nullptr, a.u, a.v, a.w, a.var,
@@ -2292,6 +2294,7 @@ struct YBatch {
 };
 template <int N, bool INV, int PL>
 __global__ void __launch_bounds__(256) k_fft_y_batch(const __grid_constant__ YBatch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const YMember &a = b.m[q];
   fft_y_body<float, N, INV, PL>(a.nx, a.ny, a.nz, a.P, a.nl, a.var, a.rev,
@@ -2313,6 +2316,7 @@ struct XbBatch {
 };
 template <int N, int PL>
 __global__ void __launch_bounds__(128) k_fft_x_bwd_batch(const __grid_constant__ XbBatch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const XbMember &a = b.m[q];
   fft_x_bwd_body<float, N, true, PL>(a.g, a.P, a.nl, a.nf, a.var, a.p, a.rev,
@@ -2332,6 +2336,7 @@ struct TrBatch {
   TrMember m[kBatchMax];
 };
 __global__ void __launch_bounds__(128) k_trid_mixed_batch(const __grid_constant__ TrBatch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const TrMember &a = b.m[q];
   trid_mixed_body(a.nx, a.ny, a.nz, a.rpiv32, a.a32, a.c32, a.rpiv, a.a, a.c, a.var, a.low,
@@ -2602,6 +2607,7 @@ struct TrtBatch {
 };
 static_assert(sizeof(TrtBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
 __global__ void __launch_bounds__(32) k_trid_mixed_tile_batch(const __grid_constant__ TrtBatch bt) {
+  batch_grid_sync();
   const int q = batch_member(bt.start, bt.n, (int)blockIdx.x);
   const TrtMember &M = bt.m[q];
   const int nx = M.nx, ny = M.ny, nz = M.nz;
@@ -3392,7 +3398,7 @@ int share_blocks(B &b, const long long *tiles, long long resident) {
   return start;
 }
 
-cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s) {
+cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s, bool pdl = false) {
   for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
     XfBatch b;
     std::memset(&b, 0, sizeof b);
@@ -3419,8 +3425,8 @@ cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s) {
       constexpr int N = decltype(NC)::value;
       return with_plan<N>(G.PL, [&](auto PC) -> cudaError_t {
         constexpr int PL = decltype(PC)::value;
-        k_fft_x_fwd_div_batch<N, PL><<<tot, 256, G.smem, s>>>(b);
-        return cudaGetLastError();
+        return launch_batched(k_fft_x_fwd_div_batch<N, PL>, (unsigned)tot, dim3(256), G.smem, s, b,
+                              pdl);
       });
     });
     if (e != cudaSuccess) return e;
@@ -3428,7 +3434,7 @@ cudaError_t launch_group_xf(const BatchGroup &G, cudaStream_t s) {
   return cudaSuccess;
 }
 
-cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
+cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s, bool pdl = false) {
   if (G.PL == 3) {
     return with_size(G.N, [&](auto NC) -> cudaError_t {
       constexpr int N = decltype(NC)::value;
@@ -3448,11 +3454,11 @@ cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
             tot += c->nx / (2 * L) * c->nz;
           }
           b.start[b.n] = tot;
-          if (inverse)
-            k_fft_y2_batch<N, true><<<tot, threads, smem, s>>>(b);
-          else
-            k_fft_y2_batch<N, false><<<tot, threads, smem, s>>>(b);
-          const cudaError_t e = cudaGetLastError();
+          const cudaError_t e =
+              inverse ? launch_batched(k_fft_y2_batch<N, true>, (unsigned)tot, dim3(threads), smem,
+                                       s, b, pdl)
+                      : launch_batched(k_fft_y2_batch<N, false>, (unsigned)tot, dim3(threads), smem,
+                                       s, b, pdl);
           if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -3486,13 +3492,14 @@ cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
         if (inverse) {
           const int tot =
               share_blocks(b, tiles, device_blocks(k_fft_y_batch<N, true, PL>, 256, G.smem, sms));
-          k_fft_y_batch<N, true, PL><<<tot, 256, G.smem, s>>>(b);
+          return launch_batched(k_fft_y_batch<N, true, PL>, (unsigned)tot, dim3(256), G.smem, s, b,
+                                pdl);
         } else {
           const int tot =
               share_blocks(b, tiles, device_blocks(k_fft_y_batch<N, false, PL>, 256, G.smem, sms));
-          k_fft_y_batch<N, false, PL><<<tot, 256, G.smem, s>>>(b);
+          return launch_batched(k_fft_y_batch<N, false, PL>, (unsigned)tot, dim3(256), G.smem, s,
+                                b, pdl);
         }
-        return cudaGetLastError();
       });
     });
     if (e != cudaSuccess) return e;
@@ -3500,7 +3507,7 @@ cudaError_t launch_group_y(const BatchGroup &G, bool inverse, cudaStream_t s) {
   return cudaSuccess;
 }
 
-cudaError_t launch_group_xb(const BatchGroup &G, cudaStream_t s) {
+cudaError_t launch_group_xb(const BatchGroup &G, cudaStream_t s, bool pdl = false) {
   for (size_t q0 = 0; q0 < G.ms.size(); q0 += kBatchMax) {
     XbBatch b;
     std::memset(&b, 0, sizeof b);
@@ -3525,8 +3532,7 @@ cudaError_t launch_group_xb(const BatchGroup &G, cudaStream_t s) {
         constexpr int PL = decltype(PC)::value;
         const int tot =
             share_blocks(b, tiles, device_blocks(k_fft_x_bwd_batch<N, PL>, 128, G.smem, sms));
-        k_fft_x_bwd_batch<N, PL><<<tot, 128, G.smem, s>>>(b);
-        return cudaGetLastError();
+        return launch_batched(k_fft_x_bwd_batch<N, PL>, (unsigned)tot, dim3(128), G.smem, s, b, pdl);
       });
     });
     if (e != cudaSuccess) return e;
@@ -3543,7 +3549,7 @@ cudaError_t launch_fft_x_fwd_batch(plc_ctx *const *cs, int n, const BatchPlan *b
                                    const cudaStream_t *ss, int ns) {
   const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_XF, bp);
   for (size_t gi = 0; gi < gs.size(); ++gi)
-    if (cudaError_t e = launch_group_xf(gs[gi], ss[gi % ns])) return e;
+    if (cudaError_t e = launch_group_xf(gs[gi], ss[gi % ns], bp && bp->pdl)) return e;
   return cudaSuccess;
 }
 
@@ -3551,7 +3557,7 @@ cudaError_t launch_fft_y_batch(plc_ctx *const *cs, int n, bool inverse, const Ba
                                const cudaStream_t *ss, int ns) {
   const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_Y, bp);
   for (size_t gi = 0; gi < gs.size(); ++gi)
-    if (cudaError_t e = launch_group_y(gs[gi], inverse, ss[gi % ns])) return e;
+    if (cudaError_t e = launch_group_y(gs[gi], inverse, ss[gi % ns], bp && bp->pdl)) return e;
   return cudaSuccess;
 }
 
@@ -3559,7 +3565,7 @@ cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *b
                                    const cudaStream_t *ss, int ns) {
   const std::vector<BatchGroup> gs = batch_groups(cs, n, BATCH_XB, bp);
   for (size_t gi = 0; gi < gs.size(); ++gi)
-    if (cudaError_t e = launch_group_xb(gs[gi], ss[gi % ns])) return e;
+    if (cudaError_t e = launch_group_xb(gs[gi], ss[gi % ns], bp && bp->pdl)) return e;
   return cudaSuccess;
 }
 
@@ -3668,7 +3674,7 @@ bool trid_tile_batch_ok(plc_ctx *const *cs, int n) {
   return n > 0;
 }
 
-cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s) {
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s, bool pdl) {
   if (tile && trid_tile_batch_ok(cs, n)) {
     for (int q0 = 0; q0 < n; q0 += kBatchMax) {
       TrtBatch b;
@@ -3685,8 +3691,8 @@ cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t
         nzmax = std::max(nzmax, c->nz);
       }
       b.start[b.n] = tot;
-      k_trid_mixed_tile_batch<<<tot, 32, trid_tile_smem(nzmax, sizeof(float)), s>>>(b);
-      const cudaError_t e = cudaGetLastError();
+      const cudaError_t e = launch_batched(k_trid_mixed_tile_batch, (unsigned)tot, dim3(32),
+                                           trid_tile_smem(nzmax, sizeof(float)), s, b, pdl);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -3705,8 +3711,7 @@ cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t
       tot += (int)(((long long)c->nx * c->ny + 127) / 128);
     }
     b.start[b.n] = tot;
-    k_trid_mixed_batch<<<tot, 128, 0, s>>>(b);
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e = launch_batched(k_trid_mixed_batch, (unsigned)tot, dim3(128), 0, s, b, pdl);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

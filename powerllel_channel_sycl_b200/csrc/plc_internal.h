@@ -307,24 +307,48 @@ struct BatchPlan {
   int rk_kchunk = 0;
   int rk_minb = 4;  // resident blocks per SM the RK kernels are compiled for (3 or 4)
   bool trid_tile = false;  // the Thomas sweep with its columns on chip
+  // programmatic dependent launch: each batched kernel launched with
+  // programmatic stream serialisation, so that its blocks become resident
+  // while the kernels it depends on drain
+  bool pdl = false;
 };
 enum BatchDir { BATCH_XF = 0, BATCH_XB = 1, BATCH_Y = 2 };
+// Launches a batched kernel k(p) (one parameter struct) on stream s; with
+// pdl, with programmatic stream serialisation: allowed only for kernels
+// whose every block calls batch_grid_sync() first.  In a stream capture the
+// edges from the kernels it depends on become programmatic edges.
+template <class P>
+cudaError_t launch_batched(void (*k)(P), unsigned grid, dim3 block, size_t smem, cudaStream_t s,
+                           const P &p, bool pdl) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, p);
+}
 cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, int minb,
-                            cudaStream_t s);
+                            cudaStream_t s, bool pdl = false);
 cudaError_t launch_fft_x_fwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
                                    const cudaStream_t *ss, int ns);
 cudaError_t launch_fft_y_batch(plc_ctx *const *cs, int n, bool inverse, const BatchPlan *bp,
                                const cudaStream_t *ss, int ns);
-cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s);
+cudaError_t launch_trid_batch(plc_ctx *const *cs, int n, bool tile, cudaStream_t s,
+                              bool pdl = false);
 // whether every channel admits the batched on-chip Thomas sweep
 bool trid_tile_batch_ok(plc_ctx *const *cs, int n);
 cudaError_t launch_fft_x_bwd_batch(plc_ctx *const *cs, int n, const BatchPlan *bp,
                                    const cudaStream_t *ss, int ns);
-cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s, bool pdl = false);
 // the full checks of the mixed-form channels at a graph's check step: results
 // on the device and in each channel's pinned host copy, the new dt under CFL
 // control set on the device
-cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s);
+cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s, bool pdl = false);
 // the number of launches (line-length groups) of the batched x and y stages
 int fft_batch_groups(plc_ctx *const *cs, int n, bool ydir);
 // times the candidate families and tiles of every group of the batched

@@ -775,6 +775,7 @@ static_assert(sizeof(Rk32Batch) <= 32000, "kernel parameters are limited to 3276
 // spills); the batch autotuner times both.
 template <int STAGE, bool FUSE, bool CRF, int MINB>
 __global__ void __launch_bounds__(RX *TY, MINB) k_rk32_batch(const __grid_constant__ Rk32Batch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const Rk32Member &a = b.m[q];
   const VBlk vb = VBlk::of((int)blockIdx.x - b.start[q], a.gx, a.gy, a.gz);
@@ -825,6 +826,7 @@ struct BulkBatch {
   BulkMember m[kBatchMax];
 };
 __global__ void __launch_bounds__(1024) k_bulk_force_batch(const __grid_constant__ BulkBatch b) {
+  batch_grid_sync();
   const BulkMember &a = b.m[blockIdx.x];
   bulk_force_body(a.nx, a.ny, a.sc, a.bm, a.nblocks);
 }
@@ -1008,7 +1010,7 @@ cudaError_t launch_rk(const plc_ctx *c, int stage, bool fuse_bc, double u_crf, c
 // channel whose own choice is not pinned (the bulk-mean partials then round
 // differently in FP32 from the channel's own step); 0: each channel's own.
 cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, int minb,
-                            cudaStream_t s) {
+                            cudaStream_t s, bool pdl) {
   const size_t smem = rk32_smem_bytes();
   for (int crf = 0; crf < 2; ++crf) {
     std::vector<int> idx;
@@ -1055,8 +1057,9 @@ cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, in
       }
       b.start[cnt] = tot;
       auto go = [&](auto SC, auto CC, auto MC) {
-        k_rk32_batch<decltype(SC)::value, true, decltype(CC)::value, decltype(MC)::value>
-            <<<tot, RX * TY, smem, s>>>(b);
+        return launch_batched(
+            k_rk32_batch<decltype(SC)::value, true, decltype(CC)::value, decltype(MC)::value>,
+            (unsigned)tot, dim3(RX * TY), smem, s, b, pdl);
       };
       using I1 = std::integral_constant<int, 1>;
       using I2 = std::integral_constant<int, 2>;
@@ -1065,17 +1068,16 @@ cudaError_t launch_rk_batch(plc_ctx *const *cs, int n, int stage, int kchunk, in
       using M3 = std::integral_constant<int, 3>;
       using M4 = std::integral_constant<int, 4>;
       const bool m4 = minb != 3;
+      cudaError_t e;
       if (stage == 1) {
-        if (crf) m4 ? go(I1{}, B1{}, M4{}) : go(I1{}, B1{}, M3{});
-        else m4 ? go(I1{}, B0{}, M4{}) : go(I1{}, B0{}, M3{});
+        if (crf) e = m4 ? go(I1{}, B1{}, M4{}) : go(I1{}, B1{}, M3{});
+        else e = m4 ? go(I1{}, B0{}, M4{}) : go(I1{}, B0{}, M3{});
       } else {
-        if (crf) m4 ? go(I2{}, B1{}, M4{}) : go(I2{}, B1{}, M3{});
-        else m4 ? go(I2{}, B0{}, M4{}) : go(I2{}, B0{}, M3{});
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        k_bulk_force_batch<<<cnt, 1024, 0, s>>>(bb);
+        if (crf) e = m4 ? go(I2{}, B1{}, M4{}) : go(I2{}, B1{}, M3{});
+        else e = m4 ? go(I2{}, B0{}, M4{}) : go(I2{}, B0{}, M3{});
+        if (e == cudaSuccess)
+          e = launch_batched(k_bulk_force_batch, (unsigned)cnt, dim3(1024), 0, s, bb, pdl);
       }
-      const cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
   }

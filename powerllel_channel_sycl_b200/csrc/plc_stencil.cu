@@ -982,6 +982,7 @@ struct CorrBatch {
 static_assert(sizeof(CorrBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
 template <int KZ>
 __global__ void __launch_bounds__(BX *BY) k_correct_forced_batch(const __grid_constant__ CorrBatch b) {
+  batch_grid_sync();
   const int q = batch_member(b.start, b.n, (int)blockIdx.x);
   const CorrMember &a = b.m[q];
   correct_forced_body<float, KZ>(a.g, a.sc, a.u_crf, a.p, a.u, a.v, a.w,
@@ -1184,9 +1185,76 @@ __device__ void block_max(MaxIdx &a, MaxIdx *smem) {
   __syncthreads();
 }
 
+// The scan of the checks of main.cc:156-178 over one channel by block lb of
+// nb: NaN anywhere in u (what & 1), the CFL rate (what & 2) and the
+// divergence (what & 4) at every interior point, FP32 fields in FP64
+// arithmetic.  The interior rows (j, k) are cut into 64-point segments, one
+// segment per warp at a time (two points per lane, all loads issued first),
+// so that short rows keep every lane busy.  The maxima keep the lowest index
+// among equal values: the result does not depend on the partition.
+template <class T>
+__device__ __forceinline__ void check_scan(const Geo &g, int what, const T *__restrict__ u,
+                                           const T *__restrict__ v, const T *__restrict__ w,
+                                           int lb, int nb, MaxIdx &cfl, MaxIdx &div,
+                                           int &nan_found) {
+  if (what & 1) {
+    const long long nall = g.XY * (g.nz + 2);
+    const long long stride = (long long)nb * blockDim.x;
+    long long t = (long long)lb * blockDim.x + threadIdx.x;
+    for (; t + 3 * stride < nall; t += 4 * stride) {
+      const T a0 = u[t], a1 = u[t + stride], a2 = u[t + 2 * stride], a3 = u[t + 3 * stride];
+      if (isnan(a0) || isnan(a1) || isnan(a2) || isnan(a3)) nan_found = 1;
+    }
+    for (; t < nall; t += stride)
+      if (isnan(u[t])) nan_found = 1;
+  }
+  if (what & 6) {
+    constexpr int SEG = 64;
+    const int segs = (g.nx + SEG - 1) / SEG;
+    // ny * nz * segs stays far below 2^31 for any channel whose fields fit in memory
+    const int ntask = g.ny * g.nz * segs;
+    const int wpb = (int)(blockDim.x >> 5), lane = (int)(threadIdx.x & 31);
+    for (int task = lb * wpb + (int)(threadIdx.x >> 5); task < ntask; task += nb * wpb) {
+      const int row = task / segs, sg = task - row * segs;
+      const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
+      const double dzfi = __ldg(g.dzf_inv + k);
+      double uc[2], um[2], vc[2], vm[2], wc[2], wm[2];
+      long long cc[2];
+      bool in[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int i = sg * SEG + 32 * r + lane + 1;
+        in[r] = i <= g.nx;
+        const long long c = g.at(in[r] ? i : 1, j, k);
+        cc[r] = c;
+        uc[r] = u[c];
+        um[r] = u[c - 1];
+        vc[r] = v[c];
+        vm[r] = v[c - g.X];
+        wc[r] = w[c];
+        wm[r] = w[c - g.XY];
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        if (!in[r]) continue;
+        if (what & 2) {
+          const double q = fabs((uc[r] + um[r]) * 0.5) * g.dx_inv +
+                           fabs((vc[r] + vm[r]) * 0.5) * g.dy_inv + fabs((wc[r] + wm[r]) * 0.5) * dzfi;
+          max_combine(cfl, q, cc[r]);
+        }
+        if (what & 4) {
+          const double d =
+              fabs((uc[r] - um[r]) * g.dx_inv + (vc[r] - vm[r]) * g.dy_inv + (wc[r] - wm[r]) * dzfi);
+          max_combine(div, d, cc[r]);
+        }
+      }
+    }
+  }
+}
+
 // (an FP32 field is checked in FP64 arithmetic)
 template <class T>
-__global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restrict__ u,
+__global__ void __launch_bounds__(256, 4) k_check(Geo g, int what, const T *__restrict__ u,
                                                const T *__restrict__ v, const T *__restrict__ w,
                                                double *partials, unsigned int *counter,
                                                CheckResult *out) {
@@ -1198,35 +1266,7 @@ __global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restr
   const long long first = g.at(1, 1, 1);
   MaxIdx cfl{0.0, first}, div{0.0, first};
   int nan_found = 0;
-  if (what & 1) {
-    const long long nall = (long long)g.XY * (g.nz + 2);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nall;
-         t += (long long)gridDim.x * blockDim.x)
-      if (isnan(u[t])) nan_found = 1;
-  }
-  if (what & 6) {
-    // interior rows (j, k) over the blocks, the x points of a row over the
-    // threads: one division per row instead of two per point
-    const int nrows = g.ny * g.nz;
-    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
-      const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
-      const double dzfi = __ldg(g.dzf_inv + k);
-      for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
-        const long long c = g.at(i, j, k);
-        const double uc = u[c], um = u[c - 1], vc = v[c], vm = v[c - g.X], wc = w[c],
-                     wm = w[c - g.XY];
-        if (what & 2) {
-          const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
-                           fabs((wc + wm) * 0.5) * dzfi;
-          max_combine(cfl, r, c);
-        }
-        if (what & 4) {
-          const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
-          max_combine(div, d, c);
-        }
-      }
-    }
-  }
+  check_scan<T>(g, what, u, v, w, (int)blockIdx.x, (int)gridDim.x, cfl, div, nan_found);
   if (nan_found) atomicOr(&nan_s, 1);
   block_max(cfl, smem);
   block_max(div, smem);
@@ -1287,6 +1327,7 @@ struct ChkBatch {
 };
 static_assert(sizeof(ChkBatch) <= 32000, "kernel parameters are limited to 32764 bytes");
 __global__ void __launch_bounds__(256) k_check_batch(const __grid_constant__ ChkBatch bt) {
+  batch_grid_sync();
   __shared__ MaxIdx smem[32];
   __shared__ int nan_s;
   __shared__ bool am_last;
@@ -1299,25 +1340,7 @@ __global__ void __launch_bounds__(256) k_check_batch(const __grid_constant__ Chk
   const long long first = g.at(1, 1, 1);
   MaxIdx cfl{0.0, first}, div{0.0, first};
   int nan_found = 0;
-  const long long nall = (long long)g.XY * (g.nz + 2);
-  for (long long t = (long long)lb * blockDim.x + threadIdx.x; t < nall;
-       t += (long long)nb * blockDim.x)
-    if (isnan(M.u[t])) nan_found = 1;
-  const int nrows = g.ny * g.nz;
-  for (int row = lb; row < nrows; row += nb) {
-    const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
-    const double dzfi = __ldg(g.dzf_inv + k);
-    for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
-      const long long c = g.at(i, j, k);
-      const double uc = M.u[c], um = M.u[c - 1], vc = M.v[c], vm = M.v[c - g.X], wc = M.w[c],
-                   wm = M.w[c - g.XY];
-      const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
-                       fabs((wc + wm) * 0.5) * dzfi;
-      max_combine(cfl, r, c);
-      const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
-      max_combine(div, d, c);
-    }
-  }
+  check_scan<float>(g, 7, M.u, M.v, M.w, lb, nb, cfl, div, nan_found);
   if (nan_found) atomicOr(&nan_s, 1);
   block_max(cfl, smem);
   block_max(div, smem);
@@ -1677,7 +1700,7 @@ cudaError_t launch_add_vortices(const plc_ctx *c, float *v, float *w, const doub
 
 // The mixed form's correction (with the forcing and halos) of n channels in
 // launches of up to kBatchMax channels.
-cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s, bool pdl) {
   constexpr int KZ = kCorrKzMixed;
   for (int q0 = 0; q0 < n; q0 += kBatchMax) {
     CorrBatch b;
@@ -1702,8 +1725,8 @@ cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
       tot += a.gx * a.gy * a.gz;
     }
     b.start[b.n] = tot;
-    k_correct_forced_batch<KZ><<<tot, dim3(BX, BY), 0, s>>>(b);
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e =
+        launch_batched(k_correct_forced_batch<KZ>, (unsigned)tot, dim3(BX, BY), 0, s, b, pdl);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1712,7 +1735,7 @@ cudaError_t launch_correct_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
 // The full checks of n mixed-form channels, their CFL-controlled dt and the
 // results in their pinned host copies, in launches of up to kBatchMax
 // channels (the check step of a graph that carries its checks).
-cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
+cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s, bool pdl) {
   for (int q0 = 0; q0 < n; q0 += kBatchMax) {
     ChkBatch b;
     std::memset(&b, 0, sizeof b);
@@ -1740,8 +1763,7 @@ cudaError_t launch_check_batch(plc_ctx *const *cs, int n, cudaStream_t s) {
       tot += a.nb;
     }
     b.start[b.n] = tot;
-    k_check_batch<<<tot, 256, 0, s>>>(b);
-    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e = launch_batched(k_check_batch, (unsigned)tot, dim3(256), 0, s, b, pdl);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

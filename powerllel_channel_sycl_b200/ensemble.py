@@ -89,17 +89,25 @@ class Ensemble:
         """The batched schedule's concurrent chains of mixed-form members (1 or 2)."""
         self._check(lib().plc_ensemble_set_batch_chains(self._ens, int(chains)))
 
+    def set_batch_pdl(self, on: bool):
+        """Programmatic dependent launch of the batched schedule's kernels
+        (each stage's blocks become resident while the previous stage drains;
+        results are the same either way)."""
+        self._check(lib().plc_ensemble_set_batch_pdl(self._ens, 1 if on else 0))
+
     def batch_choice(self):
         """The batched schedule's tuned choices: the concurrent chains of
         mixed-form members, the RK z planes per block (0: each member's own),
-        resident blocks per SM of the RK kernels, and the number of tuned
-        line-length groups of the forward x, backward x and y transforms."""
-        ch, kc, mb = C.c_int(), C.c_int(), C.c_int()
+        resident blocks per SM of the RK kernels, the number of tuned
+        line-length groups of the forward x, backward x and y transforms, and
+        whether the kernels use programmatic dependent launch."""
+        ch, kc, mb, pdl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         groups = (C.c_int * 3)()
         self._check(lib().plc_ensemble_batch_choice(self._ens, C.byref(ch), C.byref(kc),
                                                     C.byref(mb), groups))
+        self._check(lib().plc_ensemble_batch_pdl(self._ens, C.byref(pdl)))
         return {"chains": ch.value, "rk_kchunk": kc.value, "rk_blocks_per_sm": mb.value,
-                "fft_groups": list(groups)}
+                "fft_groups": list(groups), "pdl": bool(pdl.value)}
 
     def autotune(self, steps: int = 5) -> dict:
         """Times every schedule (ms per ensemble step) and keeps the fastest."""

@@ -117,13 +117,18 @@ def mixed_alone(pinned_fft_families):
 
 
 @pytest.mark.parametrize("chains", [1, 2])
-def test_batched_mixed_members_match_standalone(mixed_alone, chains):
+@pytest.mark.parametrize("pdl", [False, True])
+def test_batched_mixed_members_match_standalone(mixed_alone, chains, pdl):
+    """With one or two chains, with or without programmatic dependent
+    launch of the batched kernels: each member as alone."""
     from powerllel_channel_sycl_b200 import Ensemble
     specs, kw, ref = mixed_alone
     ens = Ensemble([member_params(*s, **kw) for s in specs])
     ens.set_schedule("batched")
     ens.set_batch_chains(chains)
+    ens.set_batch_pdl(pdl)
     assert ens.batch_choice()["chains"] == chains
+    assert ens.batch_choice()["pdl"] == pdl
     ens.initFlow()
     ens.step(5)
     ens.step(2)
@@ -227,7 +232,8 @@ def test_member_check_failure_names_the_member():
     assert e.value.code == -5 and "member 1" in str(e.value) and "checkDiv" in str(e.value)
 
 
-def test_batched_check_failure_names_the_member():
+@pytest.mark.parametrize("pdl", [False, True])
+def test_batched_check_failure_names_the_member(pdl):
     """The batched schedule's checks (one launch for the mixed-form members,
     inside the graph) report a failing member by its index."""
     from powerllel_channel_sycl_b200 import Ensemble, PlcError
@@ -235,6 +241,7 @@ def test_batched_check_failure_names_the_member():
             member_params(96, 64, 32, 1, 2500.0, nt_check=2, cfl_limit=10.0, div_limit=1e-300)]
     ens = Ensemble(prms)
     ens.set_schedule("batched")
+    ens.set_batch_pdl(pdl)
     ens.initFlow()
     with pytest.raises(PlcError) as e:
         ens.step(4)
@@ -253,7 +260,7 @@ def test_ensemble_cfl_controlled_dt():
         assert ok and 0.2 < cfl[0] < 0.5
 
 
-@pytest.mark.parametrize("schedule", ["concurrent", "batched"])
+@pytest.mark.parametrize("schedule", ["concurrent", "batched", "batched_pdl"])
 def test_cfl_controlled_members_match_standalone(schedule):
     """Under CFL control the checks every nt_check steps run inside the
     ensemble's graph, which sets each member's new dt on the device: the same
@@ -263,7 +270,8 @@ def test_cfl_controlled_members_match_standalone(schedule):
     specs = [MEMBERS[0], MIXED[1] + (1, 1500.0), MEMBERS[2]]
     ref = [standalone(s, 14, **kw) for s in specs]
     ens = Ensemble([member_params(*s, **kw) for s in specs])
-    ens.set_schedule(schedule)
+    ens.set_schedule(schedule.replace("_pdl", ""))
+    ens.set_batch_pdl(schedule.endswith("_pdl"))
     ens.initFlow()
     ens.step(14)
     for m, r, spec in zip(ens.members, ref, specs):
