@@ -1422,7 +1422,7 @@ int enqueue_check_tail(plc_ctx *c, cudaStream_t s) {
 
 bool device_check_due(const plc_ctx *c, int steps) {
   const plc_params &P = c->prm;
-  return P.nt_check == steps && c->nstep % steps == 0;
+  return P.nt_check > 0 && P.nt_check % steps == 0 && (c->nstep + steps) % P.nt_check == 0;
 }
 
 int post_steps_device_check(plc_ctx *c, int steps) {

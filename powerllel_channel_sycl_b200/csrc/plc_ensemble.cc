@@ -260,15 +260,21 @@ int capture(plc_ensemble *e, int steps, cudaGraphExec_t *out, std::vector<unsign
 
 int build(plc_ensemble *e) { return capture(e, 1, &e->graph, e->epochs); }
 
-// K of the multi-step graph: the members' common check period when they
-// share one of at most kMaxBlockSteps steps (a block then ends on a check
-// step), else 8.  The cap bounds the captured graph: its nodes grow with K.
+// K of the multi-step graph: when the members share one check period, that
+// period if it is at most kMaxBlockSteps steps, else its largest divisor
+// between 8 and kMaxBlockSteps (25 for the reference's nt_check = 100), so
+// that every check step ends a block; otherwise 8.  The cap bounds the
+// captured graph: its nodes grow with K.
 constexpr int kMaxBlockSteps = 32;
 int k_of(const plc_ensemble *e) {
   int k = e->members[0]->prm.nt_check;
   for (const plc_ctx *c : e->members)
     if (c->prm.nt_check != k) k = 0;
-  return (k > 1 && k <= kMaxBlockSteps) ? k : 8;
+  if (k > 1 && k <= kMaxBlockSteps) return k;
+  if (k > kMaxBlockSteps)
+    for (int d = kMaxBlockSteps; d >= 8; --d)
+      if (k % d == 0) return d;
+  return 8;
 }
 
 // Steps, at most `limit`, until (and including) the next step that needs the
@@ -317,7 +323,8 @@ int ens_steps(plc_ensemble *e, int nsteps, double *ms) {
   // the block that ends on every member's check step carries the checks
   // (and the CFL-controlled dt) in the graph itself
   bool kc_possible = true;
-  for (const plc_ctx *c : e->members) kc_possible = kc_possible && c->prm.nt_check == K;
+  for (const plc_ctx *c : e->members)
+    kc_possible = kc_possible && c->prm.nt_check > 0 && c->prm.nt_check % K == 0;
   if (kc_possible)
     if (int rc = capture(e, K, &e->graph_kc, e->epochs_kc, true)) return rc;
   for (int m = 0; m < n; ++m)

@@ -379,9 +379,9 @@ int post_step_end(plc_ctx *c);
 // on a check step, enqueue_check_tail queues the full check (main.cc:156-178)
 // on stream s, the new dt under CFL control set on the device, and the
 // result's copy to the host; device_check_due says whether the next `steps`
-// steps end on a check step (every nt_check == steps steps from a multiple
-// of it) and post_steps_device_check advances the step counter and acts on
-// the copied result once the graph has finished.
+// steps end on a check step (steps a divisor of nt_check) and
+// post_steps_device_check advances the step counter and acts on the copied
+// result once the graph has finished.
 int enqueue_check_tail(plc_ctx *c, cudaStream_t s);
 bool device_check_due(const plc_ctx *c, int steps);
 int post_steps_device_check(plc_ctx *c, int steps);

@@ -281,9 +281,29 @@ def test_cfl_controlled_members_match_standalone(schedule):
     ens.close()
 
 
+@pytest.mark.parametrize("schedule", ["concurrent", "batched"])
+def test_check_period_above_block_cap_matches_standalone(schedule):
+    """A check period above the multi-step block's cap (nt_check 40: blocks
+    of 20 steps, every second one carrying the checks and the new dt in the
+    graph) under CFL control: each member steps exactly as alone."""
+    from powerllel_channel_sycl_b200 import Ensemble
+    kw = dict(nt_check=40, cfl_limit=1.0, div_limit=1e-3, cfl_target=0.4)
+    specs = [MEMBERS[0], MIXED[1] + (1, 1500.0), MEMBERS[2]]
+    ref = [standalone(s, 85, **kw) for s in specs]
+    ens = Ensemble([member_params(*s, **kw) for s in specs])
+    ens.set_schedule(schedule)
+    ens.initFlow()
+    ens.step(85)
+    for m, r, spec in zip(ens.members, ref, specs):
+        assert m.step_count == 85
+        for f in "uvwp":
+            assert np.array_equal(m.download(f), r[f]), (schedule, spec, f)
+    ens.close()
+
+
 def test_long_check_period_keeps_blocks_short():
     """A check period far above the multi-step block's cap (nt_check 100000)
-    steps in blocks of the default length: the captured graphs stay small."""
+    steps in blocks of at most 32 steps: the captured graphs stay small."""
     from powerllel_channel_sycl_b200 import Ensemble
     import time
     ens = Ensemble([member_params(*s, nt_check=100000) for s in MEMBERS[:2]])
