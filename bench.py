@@ -492,36 +492,39 @@ def run_ensemble(args, world, rank, local, pg):
     specs = ensemble_members()
     costs = [float(s["nx"] * s["ny"] * s["nz"]) for s in specs]
     mine = members_of_rank(costs, rank, world)
-    prms = [channel_params(specs[i], args.nt_check, precision="mixed") for i in mine]
+    ens_ntc = args.nt_check if args.ens_nt_check is None else args.ens_nt_check
+    prms = [channel_params(specs[i], ens_ntc, precision="mixed") for i in mine]
     ens = Ensemble(prms, device=local)
     ens.initFlow()
     tune = ens.autotune(steps=5)
     # warm-up up to a check step, so that the timed steps run in whole check
     # blocks (one graph launch per nt_check steps, the checks inside it), and
     # through one such block at least
-    ntc = args.nt_check if args.nt_check > 0 else 1
+    ntc = ens_ntc if ens_ntc > 0 else 1
     ens.step(-(-max(args.warmup, 2 * ntc) // ntc) * ntc)
+    # whole check periods, so that the timed steps carry their share of checks
+    steps = -(-args.steps // ntc) * ntc
     torch.cuda.synchronize(local)
     barrier(pg, local)
     with nvtx_range("ensemble_step"):
-        ms = ens.step_timed(args.steps)
+        ms = ens.step_timed(steps)
     torch.cuda.synchronize(local)
     barrier(pg, local)
     ms_max = max_over_ranks(ms, pg, local)
     total_pts = sum(costs)
-    value = total_pts * args.steps / (ms_max / 1e3)
+    value = total_pts * steps / (ms_max / 1e3)
     sched, groups, budgets = ens.schedule()
     seq = tune.get("sequential")
     mine_pts = sum(costs[i] for i in mine)
     out = {
-        "value": value, "unit": "grid-pt*step/s", "ms_per_step": ms_max / args.steps,
-        "members": len(specs), "members_this_rank": len(mine), "points": int(total_pts),
+        "value": value, "unit": "grid-pt*step/s", "ms_per_step": ms_max / steps,
+        "steps": steps, "nt_check": ens_ntc, "members": len(specs), "members_this_rank": len(mine), "points": int(total_pts),
         "grids": [f"{s['nx']}x{s['ny']}x{s['nz']}" for s in specs],
         "dtype": "f32 fields (mixed form)", "scaling": "strong",
         "schedule": sched, "sm_budgets": budgets, "groups": groups,
         "autotune_ms_per_step": tune,
         "batch_choice": ens.batch_choice() if sched == "batched" else None,
-        "speedup_vs_sequential": (seq / (ms / args.steps)) if seq else None,
+        "speedup_vs_sequential": (seq / (ms / steps)) if seq else None,
         "sequential_value_this_rank": (mine_pts / (seq / 1e3)) if seq else None,
     }
     ens.close()
@@ -678,7 +681,17 @@ def run_ours(args, wl, rank, world, local, pg):
     if not args.no_ensemble:
         ens = run_ensemble(args, world, rank, local, pg)
         line["ensemble"] = ens
-        line["gpu_launches"] += args.steps * ens["members_this_rank"] * len(MIXED_BYTES_PER_POINT)
+        if ens["schedule"] == "batched":
+            # per chain and step: RK1, RK2, forcing, Thomas sweep and correction,
+            # plus one launch per line-length group of each transform (at most);
+            # one check launch per check period
+            g = ens["batch_choice"]["fft_groups"]
+            per_step = ens["batch_choice"]["chains"] * (5 + g[0] + g[1] + 2 * g[2])
+            line["gpu_launches"] += (ens["steps"] * per_step
+                                     + ens["steps"] // max(ens["nt_check"], 1))
+        else:
+            line["gpu_launches"] += (ens["steps"] * ens["members_this_rank"]
+                                     * len(MIXED_BYTES_PER_POINT))
     if rank == 0 and not args.no_spinup:
         line["spinup"] = run_spinup(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -703,6 +716,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="re550")
     ap.add_argument("--nt-check", type=int, default=10)
+    ap.add_argument("--ens-nt-check", type=int, default=None,
+                    help="check period of the ensemble's channels (default: --nt-check; the "
+                         "reference's template param.json uses 100)")
     ap.add_argument("--cpu-budget", type=float, default=60.0)
     ap.add_argument("--ref-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
