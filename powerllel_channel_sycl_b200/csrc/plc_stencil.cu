@@ -1254,7 +1254,7 @@ __device__ __forceinline__ void check_scan(const Geo &g, int what, const T *__re
 
 // (an FP32 field is checked in FP64 arithmetic)
 template <class T>
-__global__ void __launch_bounds__(256, 4) k_check(Geo g, int what, const T *__restrict__ u,
+__global__ void __launch_bounds__(256) k_check(Geo g, int what, const T *__restrict__ u,
                                                const T *__restrict__ v, const T *__restrict__ w,
                                                double *partials, unsigned int *counter,
                                                CheckResult *out) {
@@ -1266,7 +1266,35 @@ __global__ void __launch_bounds__(256, 4) k_check(Geo g, int what, const T *__re
   const long long first = g.at(1, 1, 1);
   MaxIdx cfl{0.0, first}, div{0.0, first};
   int nan_found = 0;
-  check_scan<T>(g, what, u, v, w, (int)blockIdx.x, (int)gridDim.x, cfl, div, nan_found);
+  if (what & 1) {
+    const long long nall = (long long)g.XY * (g.nz + 2);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nall;
+         t += (long long)gridDim.x * blockDim.x)
+      if (isnan(u[t])) nan_found = 1;
+  }
+  if (what & 6) {
+    // interior rows (j, k) over the blocks, the x points of a row over the
+    // threads: one division per row instead of two per point
+    const int nrows = g.ny * g.nz;
+    for (int row = blockIdx.x; row < nrows; row += gridDim.x) {
+      const int k = row / g.ny + 1, j = row - (k - 1) * g.ny + 1;
+      const double dzfi = __ldg(g.dzf_inv + k);
+      for (int i = threadIdx.x + 1; i <= g.nx; i += blockDim.x) {
+        const long long c = g.at(i, j, k);
+        const double uc = u[c], um = u[c - 1], vc = v[c], vm = v[c - g.X], wc = w[c],
+                     wm = w[c - g.XY];
+        if (what & 2) {
+          const double r = fabs((uc + um) * 0.5) * g.dx_inv + fabs((vc + vm) * 0.5) * g.dy_inv +
+                           fabs((wc + wm) * 0.5) * dzfi;
+          max_combine(cfl, r, c);
+        }
+        if (what & 4) {
+          const double d = fabs((uc - um) * g.dx_inv + (vc - vm) * g.dy_inv + (wc - wm) * dzfi);
+          max_combine(div, d, c);
+        }
+      }
+    }
+  }
   if (nan_found) atomicOr(&nan_s, 1);
   block_max(cfl, smem);
   block_max(div, smem);
