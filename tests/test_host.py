@@ -157,3 +157,18 @@ def test_no_device_fails_loudly():
         plc.Channel(nx=16, ny=8, nz=8, lx=1.0, ly=1.0, lz=2.0, dt=1e-3, re=100.0, u_ref=1.0,
                     l_ref=1.0)
     assert e.value.code == -4
+
+
+def test_ensemble_entry_points_reject_null():
+    """The ensemble's schedule setters and getters check their arguments on
+    the host (no device needed): a null ensemble is an argument error."""
+    import ctypes as C
+    from powerllel_channel_sycl_b200._lib import lib
+    L = lib()
+    on = C.c_int(-1)
+    assert L.plc_ensemble_set_batch_pdl(None, 1) == -1
+    assert L.plc_ensemble_batch_pdl(None, C.byref(on)) == -1
+    assert on.value == -1
+    assert L.plc_ensemble_set_batch_chains(None, 2) == -1
+    assert L.plc_ensemble_batch_choice(None, None, None, None, None) == -1
+    assert L.plc_ensemble_step(None, 1) == -1
